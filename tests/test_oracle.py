@@ -1,0 +1,119 @@
+"""The CPU restatement (oracle/) against the reference's golden vectors and,
+where the reference build is present, against the reference itself."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import oracle as O
+
+
+@pytest.fixture(scope="module")
+def hpx_golden():
+    z = np.load(os.path.join(GOLDEN, "healpix.npz"))
+    return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("nside", [1, 2, 4, 64, 1024, 8192, 32768])
+def test_healpix_functions_match_reference(hpx_golden, nside):
+    g = hpx_golden
+    h = O.healpix(nside)
+    u = g["n%d_state_u" % nside]
+    d = g["n%d_state_d" % nside]
+    assert [h.nside, h.order, h.nrings, h.npface, h.ncap, h.npix] == [int(x) for x in u[:6]]
+    assert [h.fact1, h.fact2, h.resolution, h.omega] == list(d)
+    keys = O.ang2pix(h, g["n%d_theta" % nside], g["n%d_phi" % nside])
+    np.testing.assert_array_equal(keys, g["n%d_keys" % nside])
+    pix = g["n%d_pix" % nside]
+    np.testing.assert_array_equal(O.pix2ring(h, pix), g["n%d_pix2ring" % nside])
+    th, ph = O.pix2ang(h, pix)
+    np.testing.assert_array_equal(th, g["n%d_pix2ang_theta" % nside])
+    np.testing.assert_array_equal(ph, g["n%d_pix2ang_phi" % nside])
+
+
+def test_optimal_nside_matches_reference(hpx_golden):
+    for k, v in hpx_golden.items():
+        if k.startswith("nside_for_"):
+            res = float(k[len("nside_for_"):])
+            assert O.lib().orc_set_optimal_nside(np.deg2rad(res)) == int(v)
+
+
+def test_prepare_grid_kernel(golden_case):
+    c = golden_case
+    g = O.prepare_grid_kernel(float(c["sigma"]), float(c["sphere_radius"]), float(c["hpx_max_res"]))
+    assert g.params[0] == float(c["kparam"])
+    assert g.disc_size == float(c["disc_size"])
+    assert g.hpx.nside == int(c["nside"])
+
+
+def test_presort_and_lut_match_reference(golden_case):
+    c = golden_case
+    h = O.healpix(int(c["nside"]))
+    ps = O.presort(h, c["lon"], c["lat"])
+    np.testing.assert_array_equal(ps.keys, c["keys"])
+    np.testing.assert_array_equal(ps.perm, c["perm"])
+    assert ps.firstring == int(c["firstring"]) and ps.usedrings == int(c["usedrings"])
+    np.testing.assert_array_equal(ps.lut, c["lut"])
+
+
+def test_grid_matches_reference_bitexact(golden_case):
+    """FP64 cube and weights identical to the reference kernel body."""
+    c = golden_case
+    g = O.prepare_grid_kernel(float(c["sigma"]), float(c["sphere_radius"]), float(c["hpx_max_res"]))
+    ps = O.presort(g.hpx, c["lon"], c["lat"])
+    perm = ps.perm
+    cube, wts, st = O.grid(g, ps, c["lon"][perm], c["lat"][perm], c["values"][perm], c["xwcs"], c["ywcs"])
+    assert st.a3_events == 0
+    np.testing.assert_array_equal(wts, c["wts"])
+    np.testing.assert_array_equal(cube, c["cube"])
+
+
+def test_exact_disc_contains_compat(golden_case):
+    """Exact-disc selection is a superset of the reference's ring windows."""
+    c = golden_case
+    g = O.prepare_grid_kernel(float(c["sigma"]), float(c["sphere_radius"]), float(c["hpx_max_res"]))
+    ps = O.presort(g.hpx, c["lon"], c["lat"])
+    perm = ps.perm
+    args = (g, ps, c["lon"][perm], c["lat"][perm], c["values"][perm, 0], c["xwcs"], c["ywcs"])
+    _, w0, s0 = O.grid(*args, mode=0)
+    _, w1, s1 = O.grid(*args, mode=1)
+    assert s1.pairs_within >= s0.pairs_within
+    assert np.all(w1 >= w0 * (1 - 1e-12))
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference host build (oracle/_ref) not present")
+@pytest.mark.parametrize("nside", [8192, 32768])
+def test_ang2pix_random_vs_reference(nside):
+    rng = np.random.default_rng(nside)
+    n = 200_000
+    th = rng.uniform(0, np.pi, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    O.ref().ref_healpix_init(nside)
+    rk = np.empty(n, np.uint64)
+    O.ref().ref_ang2pix(n, th, ph, rk)
+    np.testing.assert_array_equal(O.ang2pix(O.healpix(nside), th, ph), rk)
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference host build (oracle/_ref) not present")
+def test_config1_reduced_vs_reference():
+    """A reduced config-1 raster through the live reference build."""
+    from hcgrid_b200 import synth
+    job = synth.config1(n=40_000, nx=64)
+    import fitsutil
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "t.fits")
+        fitsutil.write_header_only(p, job.header)
+        nx, ny, nz, xw, yw = O.ref_target_wcs(p)
+    params, disc, st = O.ref_prepare(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    vals = job.values.astype(np.float64)
+    keys, slon, slat, sdat, fr, ur, lut = O.ref_presort(job.lon, job.lat, vals, 2)
+    cube_r, wts_r = O.ref_grid(keys, slon, slat, sdat, lut, fr, ur, nx, ny, xw, yw)
+    g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    ps = O.presort(g.hpx, job.lon, job.lat)
+    np.testing.assert_array_equal(ps.keys, keys)
+    np.testing.assert_array_equal(ps.lut, lut)
+    cube, wts, s = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm], xw, yw)
+    np.testing.assert_array_equal(wts, wts_r)
+    np.testing.assert_array_equal(cube, cube_r)
