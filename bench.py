@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 gridder on the reference's headline workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload config2|config1]
+
+A step is one gridding pass (hcg_grid: pixel setup, candidate selection,
+FP64 weights, channel sums, normalisation) over the resident field of the
+workload: config 2 = 4,000,000 raster-scan samples x 1,024 float32 channels
+onto a 1200x1200 SIN grid, GAUSS1D FWHM 180" (seeded synthetic data, see
+hcgrid_b200/synth.py). `value` is gridded sample-channels/s with inputs
+resident in HBM; `e2e` repeats the metric through the C ABI from host
+buffers (field creation with the on-device sort, spectra upload, gridding,
+cube download). Inputs are larger than L2 (16 GB of spectra), so no flush.
+
+Multi-GPU (torchrun): every rank grids its own copy of the job (weak
+scaling, no collective on the data path); timings are the max over ranks.
+
+--impl reference times the reference's own CPU path (oracle/_ref: HCGrid's
+host pre-sort plus its kernel body built for the host cores) on a bounded
+sample of the same workload and extrapolates to the whole job.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
+METRIC = "gridded sample-channels/s"
+UNIT = "sample-channels/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config1"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        d = json.load(open(MEASURED))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# workload
+
+def job_for(name):
+    from hcgrid_b200 import synth
+    if name == "config1":
+        return synth.config1()
+    return synth.config2()
+
+
+def algorithmic_bytes(n, c, p):
+    """Per sample FP64 lon/lat + FP32 spectrum read once; per pixel FP32 cube
+    row + FP32 weight written once."""
+    return n * (16 + 4 * c) + p * (4 * c + 4)
+
+
+def device_spectra(job, torch, dev):
+    """[N][C] float32 spectra on the device: G @ L + N(0, noise), seeded."""
+    if job.values is not None:
+        v = torch.from_numpy(np.ascontiguousarray(job.values.reshape(job.n, -1))).to(dev)
+        return v
+    G, L, noise = job.factors
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(job.seed)
+    Ld = torch.from_numpy(L).to(dev)
+    S = torch.empty((job.n, job.nchan), dtype=torch.float32, device=dev)
+    step = 1 << 18
+    for i in range(0, job.n, step):
+        Gd = torch.from_numpy(G[i:i + step]).to(dev)
+        torch.matmul(Gd, Ld, out=S[i:i + step])
+        S[i:i + step].add_(torch.randn((Gd.shape[0], job.nchan), generator=gen, device=dev), alpha=noise)
+    return S
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.uuid, "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 8:
+                    continue
+                try:
+                    sm.append(float(f[0]))
+                    mx.append(float(f[1]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[4:8]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the reference's own host build, else the oracle port)
+
+def cpu_baseline(job, budget_s=20.0):
+    """Reference CPU path on a bounded sample: full pre-sort of all samples
+    plus the kernel body for one channel on a central square of the target;
+    extrapolated to the whole job as HCGrid+ runs it (geometry repeated per
+    channel): T = T_sort + C * T_kernel(1 channel, all pixels)."""
+    from hcgrid_b200 import api
+    from oracle import oracle as O
+    nx, ny, xw, yw = api.header_coords(job.header)
+    P = nx * ny
+    vals = job.values if job.values is not None else (job.factors[0] @ job.factors[1][:, :1])[:, 0]
+    vals = np.asarray(vals, np.float64).reshape(job.n, -1)[:, 0].copy()
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    side = min(nx, 400 if job.n > 1_000_000 else nx)
+    x0 = (nx - side) // 2
+    sel = (np.arange(side)[:, None] + x0) * nx + (np.arange(side)[None, :] + x0)
+    sx, sy = np.ascontiguousarray(xw[sel.ravel()]), np.ascontiguousarray(yw[sel.ravel()])
+    if O.have_ref():
+        kind = "reference"
+        O.ref_prepare(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+        t0 = time.perf_counter()
+        keys, slon, slat, sdat, fr, ur, lut = O.ref_presort(job.lon, job.lat, vals, 2)
+        t_sort = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.ref_grid(keys, slon, slat, sdat, lut, fr, ur, side, side, sx, sy)
+        t_sub = time.perf_counter() - t0
+    else:
+        kind = "port"
+        g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+        t0 = time.perf_counter()
+        ps = O.presort(g.hpx, job.lon, job.lat)
+        t_sort = time.perf_counter() - t0
+        sl, sb, sd = job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm]
+        t0 = time.perf_counter()
+        O.grid(g, ps, sl, sb, sd, sx, sy)
+        t_sub = time.perf_counter() - t0
+    t_kernel = t_sub * P / (side * side)
+    t_job = t_sort + job.nchan * t_kernel
+    value = job.n * job.nchan / t_job
+    sample = ("pre-sort of all %d samples (%.2f s) + kernel body for 1 channel on the central %dx%d pixels "
+              "(%.2f s), extrapolated to %d pixels x %d channels (T = %.1f s)"
+              % (job.n, t_sort, side, side, t_sub, P, job.nchan, t_job))
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+            "seconds_measured": t_sort + t_sub}
+
+
+# ---------------------------------------------------------------------------
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reduce_max(torch, dist, v):
+    if dist is None:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    job = job_for(args.workload)
+    P = job.nx * job.ny
+    if args.impl == "reference":
+        if rank == 0:
+            vals = []
+            info = None
+            for i in range(args.warmup + args.steps):
+                info = cpu_baseline(job)
+                if i >= args.warmup:
+                    vals.append(info["value"])
+            v = statistics.median(vals)
+            info["value"] = v
+            out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+                   "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                   "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, %s generator)" % job.name,
+                   "config": {"workload": "%s: %d samples x %d channels -> %dx%d SIN, GAUSS1D FWHM %g\""
+                              % (job.name, job.n, job.nchan, job.nx, job.ny, job.fwhm_arcsec)},
+                   "cpu_baseline": info, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                                 "d2h_bytes_per_step": 0}}
+            print(json.dumps(out))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from hcgrid_b200 import api
+    api.load(build_if_missing=True)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = api.Context(local, stream=stream.cuda_stream)
+    kp = np.array([job.sigma_deg, 0.0, 0.0])
+    ctx.prepare_grid_kernel(api.GAUSS1D, kp, job.sphere_radius, job.hpx_max_res)
+    with torch.cuda.stream(stream):
+        lon_d = torch.from_numpy(job.lon).to(dev)
+        lat_d = torch.from_numpy(job.lat).to(dev)
+        S = device_spectra(job, torch, dev)
+    stream.synchronize()
+    field = ctx.field(lon_d, lat_d)
+    field.set_spectra(S)
+    target = ctx.target_from_header(job.header)
+    ctx.synchronize()
+    S_host = None
+    if args.e2e_steps > 0:
+        S_host = torch.empty((job.n, job.nchan), dtype=torch.float32, pin_memory=True)
+        S_host.copy_(S)
+    del S
+    torch.cuda.empty_cache()
+    cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
+    wts = torch.empty(P, dtype=torch.float32, device=dev)
+    launches_per_step = 2 if job.nchan == 1 else 5
+
+    for _ in range(args.warmup):
+        ctx.grid(field, target, cube, wts)
+    ctx.synchronize()
+    stats = ctx.stats()
+
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    phase_ms = [[] for _ in range(4)]
+    step_ms = []
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(uuid) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.grid(field, target, cube, wts)
+            st = ctx.stats()  # phase times of this step (device events on the launching stream)
+            for i in range(4):
+                phase_ms[i].append(st.ms_phase[i])
+            step_ms.append(st.ms_total)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    total_ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        dist.barrier()
+    ms_per_step = reduce_max(torch, dist, total_ms / args.steps)
+    clocks = clk.summary()
+    work = job.n * job.nchan
+    value = work * world / (ms_per_step * 1e-3)
+    st = ctx.stats()
+
+    # dominant kernel and its roofline
+    phase_names = ["pixel setup", "candidate count+scan", "FP64 weights (k_group)", "channel sums (k_group_accum)"]
+    kernels = ["k_pixel_prep", "k_group<true>+k_scan_offsets", "k_group<false>", "k_group_accum"]
+    if job.nchan == 1:
+        phase_names[3] = "single-channel gridding (k_grid_1chan)"
+        kernels[3] = "k_grid_1chan"
+    avg = [statistics.mean(x) for x in phase_ms]
+    dom = int(np.argmax(avg))
+    if dom == 3:
+        alg = job.n * 4 * job.nchan + P * (4 * job.nchan + 4)
+        if job.nchan == 1:
+            alg = algorithmic_bytes(job.n, 1, P)
+    else:
+        alg = algorithmic_bytes(job.n, 0, 0) if dom == 2 else P * 16
+    peak, peak_kind = peaks()
+    achieved = alg / (avg[dom] * 1e-3) / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(TRAFFIC))
+        t = tr.get(job.name, {}).get(kernels[dom])
+        traffic = t if t is None else float(t)
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "kernel": kernels[dom], "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s", "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg, "kernel_ms": round(avg[dom], 3),
+                "phase_ms": {n: round(a, 3) for n, a in zip(phase_names, avg)},
+                "whole_step_hbm_frac": round(algorithmic_bytes(job.n, job.nchan, P) / (ms_per_step * 1e-3) / 1e9 / peak, 4),
+                "pairs_within": int(st.pairs_within), "pairs_candidate": int(st.pairs_candidate)}
+
+    # end to end through the C ABI from host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        lon_h, lat_h = np.ascontiguousarray(job.lon), np.ascontiguousarray(job.lat)
+        cube_h = torch.empty((P, job.nchan), dtype=torch.float32, pin_memory=True)
+        w_h = torch.empty(P, dtype=torch.float32, pin_memory=True)
+        times = []
+        for i in range(args.e2e_steps + 1):
+            if dist is not None:
+                dist.barrier()
+            t0 = time.perf_counter()
+            f2 = ctx.field(lon_h, lat_h)
+            f2.set_spectra(S_host)
+            t2 = ctx.target_from_header(job.header)
+            ctx.grid(f2, t2, cube_h, w_h)
+            dt = time.perf_counter() - t0
+            f2.close()
+            t2.close()
+            if i > 0:
+                times.append(dt)
+        t_e2e = reduce_max(torch, dist, statistics.mean(times))
+        h2d = 16 * job.n + 4 * job.n * job.nchan
+        d2h = 4 * P * job.nchan + 4 * P
+        e2e = {"value": work * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "s_per_step": round(t_e2e, 4),
+               "path": "hcg_field_create + hcg_field_set_spectra + hcg_target_from_header + hcg_grid, host pinned"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(job)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "error": repr(ex)}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 geometry)",
+               "data": "synthetic (seeded %s generator, hcgrid_b200/synth.py)" % job.name,
+               "config": {"workload": "%s: %d samples x %d channels -> %dx%d RA---SIN/DEC--SIN, GAUSS1D FWHM %g\", "
+                                      "sphere_radius 3 sigma" % (job.name, job.n, job.nchan, job.nx, job.ny,
+                                                                  job.fwhm_arcsec),
+                          "samples": job.n, "channels": job.nchan, "pixels": P, "nside": ctx.info(field).nside,
+                          "parallelism": "replica per GPU" if world > 1 else "single GPU",
+                          "l2": "inputs larger than L2 (spectra %.1f GB), no flush" % (4 * job.n * job.nchan / 1e9),
+                          "engine": "FP32 CUDA-core channel sums, FP64 geometry"},
+               "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,
+               "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(out))
+    field.close()
+    target.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

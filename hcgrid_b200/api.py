@@ -1,0 +1,270 @@
+"""Python binding of the C ABI (include/hcgrid_c.h) through ctypes.
+
+Host arrays are numpy; device arrays are any object exposing
+``data_ptr()`` (torch CUDA tensors) and are passed as device pointers.
+The library must have been built (``python -m hcgrid_b200.build``); there is
+no fallback: loading fails loudly without it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+GAUSS1D, GAUSS2D, TAPERED_SINC = 1, 2, 3
+MEM_HOST, MEM_DEVICE = 0, 1
+SAMPLE_MAJOR, CHANNEL_MAJOR = 0, 1
+ENGINE_AUTO, ENGINE_FP32 = 0, 1
+
+STATUS = {0: "HCG_OK", 1: "HCG_EINVAL", 2: "HCG_ENOMEM", 3: "HCG_ETIMEOUT", 4: "HCG_EDEVICE", 5: "HCG_EIO",
+          6: "HCG_EUNSUPPORTED", 7: "HCG_ESTATE"}
+
+
+class HcgError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+class Info(C.Structure):
+    _fields_ = [("nside", C.c_uint64), ("npix", C.c_uint64), ("firstring", C.c_uint64), ("usedrings", C.c_uint64),
+                ("resolution", C.c_double), ("disc_size", C.c_double), ("kernel_param0", C.c_double),
+                ("sphere_radius", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("pairs_candidate", C.c_uint64), ("pairs_within", C.c_uint64), ("ring_skips", C.c_uint64),
+                ("hard_roundings", C.c_uint64), ("ms_total", C.c_double), ("ms_phase", C.c_double * 4)]
+
+
+EXPORTS = {
+    "hcg_status_string": ([C.c_int], C.c_char_p),
+    "hcg_context_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "hcg_context_destroy": ([C.c_void_p], C.c_int),
+    "hcg_last_error": ([C.c_void_p], C.c_char_p),
+    "hcg_prepare_grid_kernel": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_double, C.c_double], C.c_int),
+    "hcg_get_info": ([C.c_void_p, C.c_void_p, C.POINTER(Info)], C.c_int),
+    "hcg_field_create": ([C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                          C.POINTER(C.c_void_p)], C.c_int),
+    "hcg_field_set_spectra": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_field_sorted": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "hcg_field_destroy": ([C.c_void_p], C.c_int),
+    "hcg_target_create": ([C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int,
+                           C.POINTER(C.c_void_p)], C.c_int),
+    "hcg_target_from_header": ([C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
+    "hcg_target_coords": ([C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p],
+                          C.c_int),
+    "hcg_target_destroy": ([C.c_void_p], C.c_int),
+    "hcg_header_coords": ([C.c_char_p, C.c_size_t, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p,
+                           C.c_void_p], C.c_int),
+    "hcg_grid": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
+    "hcg_synchronize": ([C.c_void_p], C.c_int),
+}
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = False):
+    """Load libhcgrid_b200.so (optionally compiling it first)."""
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            if not build_if_missing:
+                raise RuntimeError("hcgrid_b200 native library not built: %s (run python -m hcgrid_b200.build)" % path)
+            _build.build()
+        L = C.CDLL(path)
+        for name, (args, res) in EXPORTS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    """(pointer, mem) of a numpy array or a CUDA tensor."""
+    if a is None:
+        return None, MEM_HOST
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return C.c_void_p(a.data_ptr()), (MEM_DEVICE if a.is_cuda else MEM_HOST)
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return C.c_void_p(a.ctypes.data), MEM_HOST
+
+
+def header_coords(header: str):
+    """SIN target pixel centres (degrees) of a FITS header, on the host."""
+    L = load()
+    hb = header.encode("ascii")
+    nx, ny = C.c_uint32(), C.c_uint32()
+    st = L.hcg_header_coords(hb, len(hb), C.byref(nx), C.byref(ny), None, None)
+    if st != 0:
+        raise HcgError(st, "header")
+    x = np.empty(nx.value * ny.value)
+    y = np.empty(nx.value * ny.value)
+    st = L.hcg_header_coords(hb, len(hb), C.byref(nx), C.byref(ny), x.ctypes.data, y.ctypes.data)
+    if st != 0:
+        raise HcgError(st, "header")
+    return nx.value, ny.value, x, y
+
+
+class Context:
+    """hcg_context: one CUDA device and stream plus the kernel setup."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.L = load()
+        h = C.c_void_p()
+        self._check(self.L.hcg_context_create(device, C.c_void_p(stream) if stream else None, C.byref(h)), None)
+        self.h = h
+
+    def _check(self, st, h=None):
+        if st != 0:
+            msg = self.L.hcg_last_error(h if h is not None else getattr(self, "h", None))
+            raise HcgError(st, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hcg_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def prepare_grid_kernel(self, kernel_type: int, kernel_params, sphere_radius: float, hpx_max_res: float):
+        """_prepare_grid_kernel; kernel_params (float64, len 3) is updated in place."""
+        kp = kernel_params if isinstance(kernel_params, np.ndarray) else np.array(kernel_params, np.float64)
+        assert kp.dtype == np.float64 and kp.size >= 3
+        self._check(self.L.hcg_prepare_grid_kernel(self.h, kernel_type, kp.ctypes.data, sphere_radius, hpx_max_res))
+        return kp
+
+    def info(self, field=None) -> Info:
+        inf = Info()
+        self._check(self.L.hcg_get_info(self.h, field.h if field else None, C.byref(inf)))
+        return inf
+
+    def field(self, lon, lat, weights=None) -> "Field":
+        return Field(self, lon, lat, weights)
+
+    def target(self, nx, ny, xwcs, ywcs) -> "Target":
+        return Target(self, nx, ny, xwcs, ywcs)
+
+    def target_from_header(self, header: str) -> "Target":
+        t = Target.__new__(Target)
+        t.ctx = self
+        h = C.c_void_p()
+        hb = header.encode("ascii")
+        self._check(self.L.hcg_target_from_header(self.h, hb, len(hb), C.byref(h)))
+        t.h = h
+        nx, ny = C.c_uint32(), C.c_uint32()
+        self._check(self.L.hcg_target_coords(h, C.byref(nx), C.byref(ny), None, None))
+        t.nx, t.ny = nx.value, ny.value
+        return t
+
+    def grid(self, field: "Field", target: "Target", cube=None, weights=None, layout: int = SAMPLE_MAJOR,
+             engine: int = ENGINE_AUTO):
+        """Grid and normalise. Without `cube`, returns host numpy arrays
+        (cube [npix, nchan] or [nchan, npix], weights [npix])."""
+        npix = target.nx * target.ny
+        shape = (npix, field.nchan) if layout == SAMPLE_MAJOR else (field.nchan, npix)
+        if cube is None:
+            cube = np.empty(shape, np.float32)
+            weights = np.empty(npix, np.float32)
+        cp, mem = _ptr(cube)
+        wp, _ = _ptr(weights)
+        self._check(self.L.hcg_grid(self.h, field.h, target.h, cp, layout, wp, mem, engine))
+        return cube, weights
+
+    def stats(self) -> Stats:
+        s = Stats()
+        self._check(self.L.hcg_get_stats(self.h, C.byref(s)))
+        return s
+
+    def synchronize(self):
+        self._check(self.L.hcg_synchronize(self.h))
+
+
+class Field:
+    """hcg_field: sorted samples, ring LUT and resident spectra."""
+
+    def __init__(self, ctx: Context, lon, lat, weights=None):
+        self.ctx = ctx
+        self.n = len(lon)
+        lp, mem = _ptr(lon)
+        bp, _ = _ptr(lat)
+        wp, _ = _ptr(weights)
+        h = C.c_void_p()
+        ctx._check(ctx.L.hcg_field_create(ctx.h, self.n, lp, bp, wp, mem, C.byref(h)))
+        self.h = h
+        self.nchan = 0
+
+    def set_spectra(self, values, layout: int = SAMPLE_MAJOR):
+        vp, mem = _ptr(values)
+        if layout == SAMPLE_MAJOR:
+            nchan = 1 if len(values.shape) == 1 else values.shape[1]
+        else:
+            nchan = values.shape[0]
+        self.ctx._check(self.ctx.L.hcg_field_set_spectra(self.h, nchan, vp, layout, mem))
+        self.nchan = nchan
+
+    def sorted(self):
+        inf = self.ctx.info(self)
+        keys = np.empty(self.n + 1, np.uint64)
+        perm = np.empty(self.n, np.uint32)
+        lut = np.empty(inf.usedrings + 1, np.uint32)
+        self.ctx._check(self.ctx.L.hcg_field_sorted(self.h, keys.ctypes.data, perm.ctypes.data, lut.ctypes.data))
+        return keys, perm, lut, inf.firstring, inf.usedrings
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.hcg_field_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Target:
+    """hcg_target: target pixel centres (degrees), yy*nx + xx order."""
+
+    def __init__(self, ctx: Context, nx: int, ny: int, xwcs, ywcs):
+        self.ctx = ctx
+        self.nx, self.ny = nx, ny
+        xp, mem = _ptr(xwcs)
+        yp, _ = _ptr(ywcs)
+        h = C.c_void_p()
+        ctx._check(ctx.L.hcg_target_create(ctx.h, nx, ny, xp, yp, mem, C.byref(h)))
+        self.h = h
+
+    def coords(self):
+        x = np.empty(self.nx * self.ny)
+        y = np.empty(self.nx * self.ny)
+        self.ctx._check(self.ctx.L.hcg_target_coords(self.h, None, None, x.ctypes.data, y.ctypes.data))
+        return x, y
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.hcg_target_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,464 @@
+// C ABI of the gridder (declared in include/hcgrid_c.h).
+//
+// Host-side setup mirrors the reference's _prepare_grid_kernel
+// (HCGrid/gmap.cpp:64-99) and HEALPix initialisation (HCGrid/healpix.cu:42-65,
+// HCGrid/helpers.cu:98-114) with the same expressions, so nside,
+// disc_size and the transformed kernel parameter are bit-identical; all
+// sample and pixel work runs on the device.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+#include <vector>
+
+#include "hcg_internal.h"
+
+using namespace hcg;
+
+namespace {
+
+struct Guard {
+    hcg_context *c;
+    std::lock_guard<std::mutex> lk;
+    explicit Guard(hcg_context *ctx) : c(ctx), lk(ctx->mu) { cudaSetDevice(ctx->device); }
+};
+
+hcg_status fail(hcg_context *ctx, hcg_status s, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return s;
+}
+
+hcg_status cuda_fail(hcg_context *ctx, cudaError_t e, const char *where, const std::string &why = "") {
+    cudaGetLastError();
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    if (!why.empty()) m += " (" + why + ")";
+    if (e == cudaErrorMemoryAllocation) return fail(ctx, HCG_ENOMEM, m);
+    if (e == cudaErrorInvalidValue && !why.empty()) return fail(ctx, HCG_EINVAL, m);
+    return fail(ctx, HCG_EDEVICE, m);
+}
+
+#define CK(ctx, x, where)                                        \
+    do {                                                         \
+        cudaError_t e_ = (x);                                    \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+    } while (0)
+
+// helpers.cu:40-64
+uint64_t ilog2_u64(uint64_t arg) {
+    uint64_t r = 0;
+    while (arg > 1) { arg >>= 1; ++r; }
+    return r;
+}
+
+// helpers.cu:98-102 and healpix.cu:52-65, same expressions as the reference.
+void healpix_params(double hpx_max_res, HpxParams &h) {
+    const double PI = 3.1415926535897932384626433832;
+    double target_res = (PI / 180.) * hpx_max_res;
+    uint64_t nside = (uint64_t)(sqrt(PI / 3.) / target_res + 0.5);
+    nside = 1ULL << (ilog2_u64(nside) + 1);
+    h.nside = nside;
+    h.order = ilog2_u64(nside);
+    uint64_t npface = nside * nside;
+    h.ncap = (npface - nside) << 1;
+    h.npix = 12 * npface;
+    h.fact2 = 4. / h.npix;
+    h.fact1 = (nside << 1) * h.fact2;
+    double omega = 4. * PI / h.npix;
+    h.resolution = sqrt(omega);
+}
+
+}  // namespace
+
+void *hcg::Scratch::get(int slot, size_t bytes, cudaStream_t s, cudaError_t &err) {
+    if (slot >= (int)ptr.size()) {
+        ptr.resize(slot + 1, nullptr);
+        size.resize(slot + 1, 0);
+    }
+    if (bytes == 0) bytes = 16;
+    if (size[slot] < bytes) {
+        if (ptr[slot]) cudaFreeAsync(ptr[slot], s);
+        size_t want = bytes + bytes / 4;
+        void *p = nullptr;
+        cudaError_t e = cudaMallocAsync(&p, want, s);
+        if (e != cudaSuccess) {
+            ptr[slot] = nullptr;
+            size[slot] = 0;
+            err = e;
+            return nullptr;
+        }
+        ptr[slot] = p;
+        size[slot] = want;
+    }
+    return ptr[slot];
+}
+
+void hcg::Scratch::release(cudaStream_t s) {
+    for (auto &p : ptr)
+        if (p) cudaFreeAsync(p, s);
+    ptr.clear();
+    size.clear();
+}
+
+extern "C" {
+
+const char *hcg_status_string(hcg_status s) {
+    switch (s) {
+        case HCG_OK: return "ok";
+        case HCG_EINVAL: return "invalid argument";
+        case HCG_ENOMEM: return "out of memory";
+        case HCG_ETIMEOUT: return "device wait timed out";
+        case HCG_EDEVICE: return "CUDA error";
+        case HCG_EIO: return "I/O error";
+        case HCG_EUNSUPPORTED: return "unsupported";
+        case HCG_ESTATE: return "call out of order";
+    }
+    return "unknown status";
+}
+
+hcg_status hcg_context_create(int device, void *stream, hcg_context **out) {
+    if (!out) return HCG_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return HCG_EDEVICE;
+    }
+    hcg_context *c = new (std::nothrow) hcg_context();
+    if (!c) return HCG_ENOMEM;
+    c->device = device;
+    cudaSetDevice(device);
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return HCG_EDEVICE;
+        }
+        c->own_stream = true;
+    }
+    if (cudaMalloc(&c->d_stats, sizeof(DevStats)) != cudaSuccess || cudaMemset(c->d_stats, 0, sizeof(DevStats)) ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->evp[0]) != cudaSuccess || cudaEventCreate(&c->evp[1]) != cudaSuccess ||
+        cudaEventCreate(&c->evp[2]) != cudaSuccess || cudaEventCreate(&c->evp[3]) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return HCG_EDEVICE;
+    }
+    *out = c;
+    return HCG_OK;
+}
+
+hcg_status hcg_context_destroy(hcg_context *ctx) {
+    if (!ctx) return HCG_EINVAL;
+    {
+        Guard g(ctx);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->scratch.release(ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->d_stats);
+        cudaEventDestroy(ctx->ev0);
+        cudaEventDestroy(ctx->ev1);
+        for (auto &ev : ctx->evp) cudaEventDestroy(ev);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return HCG_OK;
+}
+
+const char *hcg_last_error(const hcg_context *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+hcg_status hcg_prepare_grid_kernel(hcg_context *ctx, uint32_t kernel_type, double *kernel_params,
+                                   double sphere_radius, double hpx_max_res) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    if (!kernel_params) return fail(ctx, HCG_EINVAL, "kernel_params is NULL");
+    if (!(sphere_radius > 0) || !(hpx_max_res > 0)) return fail(ctx, HCG_EINVAL, "sphere_radius and hpx_max_res must be > 0");
+    // gmap.cpp:69-80
+    if (kernel_type == HCG_GAUSS1D) {
+        kernel_params[0] = 0.5 / pow(kernel_params[0], 2.);
+        ctx->bearing = false;
+    } else if (kernel_type == HCG_GAUSS2D) {
+        ctx->bearing = true;
+    } else if (kernel_type == HCG_TAPERED_SINC) {
+        ctx->bearing = false;
+    } else {
+        return fail(ctx, HCG_EINVAL, "unknown kernel type");
+    }
+    ctx->kernel_type = kernel_type;
+    memcpy(ctx->kparams, kernel_params, 3 * sizeof(double));
+    // gmap.cpp:89-95: rebuild HEALPix only when the sphere moved by > 3e-5
+    if (!ctx->prepared || fabs(ctx->last_r - sphere_radius) > 3e-5 || fabs(ctx->last_res - hpx_max_res) > 3e-5) {
+        healpix_params(hpx_max_res, ctx->hpx);
+        ctx->last_r = sphere_radius;
+        ctx->last_res = hpx_max_res;
+    }
+    ctx->sphere_radius = sphere_radius;
+    const double PI = 3.1415926535897932384626433832;
+    ctx->disc_size = ((PI / 180.) * sphere_radius + ctx->hpx.resolution);
+    ctx->prepared = true;
+    return HCG_OK;
+}
+
+hcg_status hcg_get_info(const hcg_context *ctx, const hcg_field *field, hcg_info *out) {
+    if (!ctx || !out) return HCG_EINVAL;
+    const HpxParams &h = field ? field->hpx : ctx->hpx;
+    out->nside = h.nside;
+    out->npix = h.npix;
+    out->firstring = field ? field->firstring : 0;
+    out->usedrings = field ? field->usedrings : 0;
+    out->resolution = h.resolution;
+    out->disc_size = ctx->disc_size;
+    out->kernel_param0 = ctx->kparams[0];
+    out->sphere_radius = ctx->sphere_radius;
+    return HCG_OK;
+}
+
+hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, const double *lat,
+                            const double *weights, int mem, hcg_field **out) {
+    if (!ctx || !out) return HCG_EINVAL;
+    Guard g(ctx);
+    *out = nullptr;
+    if (!ctx->prepared) return fail(ctx, HCG_ESTATE, "hcg_prepare_grid_kernel must come first");
+    if (n == 0 || n >= 0xffffffffULL) return fail(ctx, HCG_EINVAL, "sample count must be in [1, 2^32-2]");
+    if (!lon || !lat) return fail(ctx, HCG_EINVAL, "lon/lat are NULL");
+    cudaStream_t s = ctx->stream;
+    hcg_field *f = new (std::nothrow) hcg_field();
+    if (!f) return fail(ctx, HCG_ENOMEM, "host allocation");
+    f->ctx = ctx;
+    f->n = n;
+    f->hpx = ctx->hpx;
+    const double *dl = lon, *db = lat, *dw = weights;
+    double *tmp = nullptr;
+    if (mem == HCG_MEM_HOST) {
+        size_t nb = n * sizeof(double);
+        cudaError_t e = cudaMallocAsync(&tmp, 3 * nb, s);
+        if (e != cudaSuccess) { delete f; return cuda_fail(ctx, e, "field upload"); }
+        cudaMemcpyAsync(tmp, lon, nb, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(tmp + n, lat, nb, cudaMemcpyHostToDevice, s);
+        if (weights) cudaMemcpyAsync(tmp + 2 * n, weights, nb, cudaMemcpyHostToDevice, s);
+        dl = tmp;
+        db = tmp + n;
+        dw = weights ? tmp + 2 * n : nullptr;
+    }
+    std::string why;
+    cudaError_t e = build_field(ctx, f, dl, db, dw, why);
+    if (tmp) cudaFreeAsync(tmp, s);
+    if (e != cudaSuccess) {
+        hcg_status st = cuda_fail(ctx, e, "field build", why);
+        cudaStreamSynchronize(s);
+        hcg_field_destroy(f);
+        return st;
+    }
+    *out = f;
+    return HCG_OK;
+}
+
+hcg_status hcg_field_set_spectra(hcg_field *field, uint32_t nchan, const float *values, int layout, int mem) {
+    if (!field) return HCG_EINVAL;
+    hcg_context *ctx = field->ctx;
+    Guard g(ctx);
+    if (nchan == 0 || !values) return fail(ctx, HCG_EINVAL, "need nchan >= 1 and values");
+    if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
+        return fail(ctx, HCG_EINVAL, "unknown layout");
+    cudaStream_t s = ctx->stream;
+    const float *dv = values;
+    float *tmp = nullptr;
+    if (mem == HCG_MEM_HOST) {
+        size_t nb = field->n * (size_t)nchan * sizeof(float);
+        cudaError_t e = cudaMallocAsync(&tmp, nb, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "spectra upload");
+        CK(ctx, cudaMemcpyAsync(tmp, values, nb, cudaMemcpyHostToDevice, s), "spectra upload");
+        dv = tmp;
+    }
+    cudaError_t e = permute_spectra(ctx, field, dv, nchan, layout);
+    if (tmp) cudaFreeAsync(tmp, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "spectra permute");
+    return HCG_OK;
+}
+
+hcg_status hcg_field_sorted(const hcg_field *field, uint64_t *keys, uint32_t *perm, uint32_t *lut) {
+    if (!field) return HCG_EINVAL;
+    hcg_context *ctx = field->ctx;
+    Guard g(ctx);
+    cudaStream_t s = ctx->stream;
+    if (keys) CK(ctx, cudaMemcpyAsync(keys, field->d_keys, (field->n + 1) * 8, cudaMemcpyDeviceToHost, s), "keys");
+    if (perm) CK(ctx, cudaMemcpyAsync(perm, field->d_perm, field->n * 4, cudaMemcpyDeviceToHost, s), "perm");
+    if (lut) CK(ctx, cudaMemcpyAsync(lut, field->d_lut, (field->usedrings + 1) * 4, cudaMemcpyDeviceToHost, s), "lut");
+    CK(ctx, cudaStreamSynchronize(s), "sorted readback");
+    return HCG_OK;
+}
+
+hcg_status hcg_field_destroy(hcg_field *f) {
+    if (!f) return HCG_EINVAL;
+    hcg_context *ctx = f->ctx;
+    {
+        Guard g(ctx);
+        cudaStream_t s = ctx->stream;
+        void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_lut, f->d_rings, f->d_spec};
+        for (void *p : ps)
+            if (p) cudaFreeAsync(p, s);
+    }
+    delete f;
+    return HCG_OK;
+}
+
+static hcg_status make_target(hcg_context *ctx, uint32_t nx, uint32_t ny, const double *x, const double *y,
+                              cudaMemcpyKind kind, hcg_target **out) {
+    cudaStream_t s = ctx->stream;
+    hcg_target *t = new (std::nothrow) hcg_target();
+    if (!t) return fail(ctx, HCG_ENOMEM, "host allocation");
+    t->ctx = ctx;
+    t->nx = nx;
+    t->ny = ny;
+    size_t nb = (size_t)nx * ny * sizeof(double);
+    cudaError_t e = cudaMallocAsync(&t->d_x, nb, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&t->d_y, nb, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t->d_x, x, nb, kind, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t->d_y, y, nb, kind, s);
+    if (e == cudaSuccess && kind == cudaMemcpyHostToDevice) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        if (t->d_x) cudaFreeAsync(t->d_x, s);
+        if (t->d_y) cudaFreeAsync(t->d_y, s);
+        delete t;
+        return cuda_fail(ctx, e, "target upload");
+    }
+    *out = t;
+    return HCG_OK;
+}
+
+hcg_status hcg_target_create(hcg_context *ctx, uint32_t nx, uint32_t ny, const double *xwcs, const double *ywcs,
+                             int mem, hcg_target **out) {
+    if (!ctx || !out) return HCG_EINVAL;
+    Guard g(ctx);
+    *out = nullptr;
+    if (nx == 0 || ny == 0 || !xwcs || !ywcs) return fail(ctx, HCG_EINVAL, "empty target");
+    return make_target(ctx, nx, ny, xwcs, ywcs,
+                       mem == HCG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, out);
+}
+
+hcg_status hcg_target_from_header(hcg_context *ctx, const char *header, size_t len, hcg_target **out) {
+    if (!ctx || !out || !header) return HCG_EINVAL;
+    Guard g(ctx);
+    *out = nullptr;
+    uint32_t nx, ny;
+    std::vector<double> x, y;
+    std::string why;
+    int st = sin_target_coords(header, len, nx, ny, x, y, why);
+    if (st != HCG_OK) return fail(ctx, (hcg_status)st, why);
+    return make_target(ctx, nx, ny, x.data(), y.data(), cudaMemcpyHostToDevice, out);
+}
+
+hcg_status hcg_target_coords(const hcg_target *t, uint32_t *nx, uint32_t *ny, double *xwcs, double *ywcs) {
+    if (!t) return HCG_EINVAL;
+    hcg_context *ctx = t->ctx;
+    Guard g(ctx);
+    if (nx) *nx = t->nx;
+    if (ny) *ny = t->ny;
+    size_t nb = (size_t)t->nx * t->ny * sizeof(double);
+    if (xwcs) CK(ctx, cudaMemcpyAsync(xwcs, t->d_x, nb, cudaMemcpyDeviceToHost, ctx->stream), "coords");
+    if (ywcs) CK(ctx, cudaMemcpyAsync(ywcs, t->d_y, nb, cudaMemcpyDeviceToHost, ctx->stream), "coords");
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "coords");
+    return HCG_OK;
+}
+
+hcg_status hcg_header_coords(const char *header, size_t len, uint32_t *nx, uint32_t *ny, double *xwcs,
+                             double *ywcs) {
+    if (!header || !nx || !ny) return HCG_EINVAL;
+    uint32_t w, h;
+    std::vector<double> x, y;
+    std::string why;
+    int st = sin_target_coords(header, len, w, h, x, y, why);
+    if (st != HCG_OK) return (hcg_status)st;
+    *nx = w;
+    *ny = h;
+    if (xwcs) memcpy(xwcs, x.data(), x.size() * sizeof(double));
+    if (ywcs) memcpy(ywcs, y.data(), y.size() * sizeof(double));
+    return HCG_OK;
+}
+
+hcg_status hcg_target_destroy(hcg_target *t) {
+    if (!t) return HCG_EINVAL;
+    hcg_context *ctx = t->ctx;
+    {
+        Guard g(ctx);
+        if (t->d_x) cudaFreeAsync(t->d_x, ctx->stream);
+        if (t->d_y) cudaFreeAsync(t->d_y, ctx->stream);
+    }
+    delete t;
+    return HCG_OK;
+}
+
+hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube, int layout,
+                    float *weights_out, int mem, int engine) {
+    if (!ctx || !field || !target || !cube) return HCG_EINVAL;
+    Guard g(ctx);
+    if (!ctx->prepared) return fail(ctx, HCG_ESTATE, "hcg_prepare_grid_kernel must come first");
+    if (ctx->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
+    if (field->hpx.nside != ctx->hpx.nside)
+        return fail(ctx, HCG_ESTATE, "field was built for another HEALPix resolution; rebuild it");
+    if (!field->d_spec) return fail(ctx, HCG_ESTATE, "field has no spectra (hcg_field_set_spectra)");
+    if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
+        return fail(ctx, HCG_EINVAL, "unknown layout");
+    if (engine != HCG_ENGINE_AUTO && engine != HCG_ENGINE_FP32) return fail(ctx, HCG_EINVAL, "unknown engine");
+    cudaStream_t s = ctx->stream;
+    const size_t P = (size_t)target->nx * target->ny;
+    const size_t cube_bytes = P * field->nchan * sizeof(float);
+    float *dc = cube, *dw = weights_out;
+    if (mem == HCG_MEM_HOST) {
+        cudaError_t e = cudaSuccess;
+        dc = (float *)ctx->scratch.get(16, cube_bytes, s, e);
+        if (weights_out) dw = (float *)ctx->scratch.get(17, P * sizeof(float), s, e);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "output buffers");
+    }
+    CK(ctx, cudaMemsetAsync(ctx->d_stats, 0, offsetof(DevStats, invalid_input), s), "stats reset");
+    std::string why;
+    cudaError_t e = grid_field(ctx, field, target, dc, layout, dw, engine, why);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "grid", why);
+    if (mem == HCG_MEM_HOST) {
+        CK(ctx, cudaMemcpyAsync(cube, dc, cube_bytes, cudaMemcpyDeviceToHost, s), "cube download");
+        if (weights_out)
+            CK(ctx, cudaMemcpyAsync(weights_out, dw, P * sizeof(float), cudaMemcpyDeviceToHost, s), "weights download");
+        CK(ctx, cudaStreamSynchronize(s), "grid");
+    }
+    return HCG_OK;
+}
+
+hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out) {
+    if (!ctx || !out) return HCG_EINVAL;
+    Guard g(ctx);
+    DevStats d;
+    CK(ctx, cudaMemcpyAsync(&d, ctx->d_stats, sizeof d, cudaMemcpyDeviceToHost, ctx->stream), "stats");
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "stats");
+    out->pairs_candidate = d.pairs_candidate;
+    out->pairs_within = d.pairs_within;
+    out->ring_skips = d.ring_skips;
+    out->hard_roundings = d.hard_roundings;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        ms = 0.f;
+    }
+    out->ms_total = ms;
+    // phases: ev0 | prep | evp0 | count+scan | evp1 | weights | evp2 | channel sums | ev1
+    cudaEvent_t marks[5] = {ctx->ev0, ctx->evp[0], ctx->evp[1], ctx->evp[2], ctx->ev1};
+    for (int i = 0; i < 4; ++i) {
+        float m = 0.f;
+        if (cudaEventElapsedTime(&m, marks[i], marks[i + 1]) != cudaSuccess) {
+            cudaGetLastError();
+            m = 0.f;
+        }
+        out->ms_phase[i] = m;
+    }
+    return HCG_OK;
+}
+
+hcg_status hcg_synchronize(hcg_context *ctx) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+    return HCG_OK;
+}
+
+}  // extern "C"

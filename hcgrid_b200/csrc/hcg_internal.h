@@ -1,0 +1,114 @@
+// Internal types of the B200 gridder (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "hcg_math.cuh"
+#include "hcgrid_c.h"
+
+namespace hcg {
+
+// Counters the kernels bump (read back by hcg_get_stats).
+struct DevStats {
+    unsigned long long pairs_candidate;
+    unsigned long long pairs_within;
+    unsigned long long ring_skips;
+    unsigned long long hard_roundings;
+    unsigned long long invalid_input;
+    unsigned long long overflow;
+};
+
+// One HEALPix ring that holds samples, with the ring half of loc2pix
+// precomputed (healpix.cu:126-165 splits into a ring part and a phi part).
+struct RingRec {
+    uint64_t startpix;
+    uint64_t npr;
+    double t2;       // equatorial: nside*z*0.75; polar: the `tmp` factor
+    uint32_t lut_lo; // first sorted sample of the ring (start_int)
+    uint32_t lut_hi; // first sample of the next ring (end_int)
+    int eq;          // |z| <= 2/3
+    int zpos;        // z > 0
+};
+
+// One target pixel: its coordinates and the phi half of loc2pix for the two
+// window edges phi -/+ disc_size (gridding.cu:306-351).
+struct PixPrep {
+    double l1, b1, cb1;    // radians, cos(b1)
+    double tt[2];          // fmodulo((phi -/+ disc) / (pi/2), 4)
+    double t1[2];          // nside * (0.5 + tt)
+    double tp[2];          // tt - trunc(tt)
+    int ur;                // first ring, relative to firstring
+    int nr;                // number of rings (0: pixel sees no samples)
+    int polar;             // whole-ring windows (theta <= 20 or >= 160 deg)
+    int pad;
+};
+
+// Grow-only device scratch buffers, stream-ordered.
+struct Scratch {
+    std::vector<void *> ptr;
+    std::vector<size_t> size;
+    void *get(int slot, size_t bytes, cudaStream_t s, cudaError_t &err);
+    void release(cudaStream_t s);
+};
+
+}  // namespace hcg
+
+struct hcg_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::mutex mu;
+    std::string err;
+    // _prepare_grid_kernel state (gmap.cpp:64-99)
+    bool prepared = false;
+    uint32_t kernel_type = 0;
+    double kparams[3] = {0, 0, 0};
+    double sphere_radius = 0, disc_size = 0;
+    bool bearing = false;
+    double last_r = -1, last_res = -1;
+    hcg::HpxParams hpx = {};
+    hcg::DevStats *d_stats = nullptr;
+    hcg::Scratch scratch;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evp[4] = {nullptr, nullptr, nullptr, nullptr};  // phase boundaries inside hcg_grid
+    float last_ms = 0.f;
+};
+
+struct hcg_field {
+    hcg_context *ctx = nullptr;
+    uint64_t n = 0;
+    hcg::HpxParams hpx = {};
+    uint64_t firstring = 0, usedrings = 0;
+    uint64_t *d_keys = nullptr;   // n + 1, sorted, sentinel npix
+    uint32_t *d_perm = nullptr;   // sorted position -> input index
+    double *d_l2 = nullptr;       // radians, sorted
+    double *d_b2 = nullptr;
+    double *d_cb2 = nullptr;      // cos(b2)
+    double *d_w = nullptr;        // per-sample input weight, sorted
+    uint32_t *d_lut = nullptr;    // usedrings + 1
+    hcg::RingRec *d_rings = nullptr;
+    float *d_spec = nullptr;      // [n][cstride], sorted
+    uint32_t nchan = 0, cstride = 0;
+};
+
+struct hcg_target {
+    hcg_context *ctx = nullptr;
+    uint32_t nx = 0, ny = 0;
+    double *d_x = nullptr, *d_y = nullptr;  // degrees
+};
+
+// Launchers (hcg_field.cu, hcg_grid.cu). All return cudaGetLastError().
+namespace hcg {
+cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, const double *d_lat,
+                        const double *d_w, std::string &why);
+cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, uint32_t nchan, int layout);
+cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t, float *d_cube, int layout,
+                       float *d_wts, int engine, std::string &why);
+int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny, std::vector<double> &x,
+                      std::vector<double> &y, std::string &why);
+}  // namespace hcg

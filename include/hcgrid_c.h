@@ -1,0 +1,142 @@
+/*
+ * hcgrid_b200 -- C ABI of the B200 convolution gridder.
+ *
+ * A drop-in for the gridding path of HCGrid / HCGrid+: HEALPix pre-sort,
+ * two-level ring lookup table, GAUSS1D gather gridding and weight
+ * normalisation. Plain pointers and sizes only; every call returns an
+ * hcg_status (no exit()), and a context is safe to use from one host thread
+ * at a time (calls on one context are serialised by an internal lock).
+ *
+ * Reference interfaces each entry point replaces (paths inside the HCGrid
+ * project):
+ *   hcg_prepare_grid_kernel  _prepare_grid_kernel       HCGrid/gmap.h:121, gmap.cpp:64-99
+ *   hcg_field_create         init_input_with_cpu/thrust  HCGrid/gridding.h:53-60, gridding.cu:70-216
+ *                            (+ data_alloc/data_h2d of the sample arrays, gridding.cu:406-445)
+ *   hcg_field_set_spectra    read_input_map data / HCGrid+ pre_order_data
+ *                                                        HCGrid/gmap.cpp:102-148, HCGrid+/gridding-omp.cu:146-157
+ *   hcg_target_create        set_WCS output (h_xwcs/h_ywcs) HCGrid/gmap.cpp:183-250
+ *   hcg_target_from_header   read_output_map + set_WCS   HCGrid/gmap.cpp:151-250
+ *   hcg_grid                 hcgrid<<<>>> + data_d2h + normalisation
+ *                                                        HCGrid/gridding.cu:277-403, 448-452; gmap.cpp:306-312
+ *   hcg_field_sorted         h_hpx_idx / h_start_ring (for parity checks)
+ *                                                        HCGrid/gmap.h:78-81
+ */
+#ifndef HCGRID_C_H
+#define HCGRID_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    HCG_OK = 0,
+    HCG_EINVAL = 1,       /* bad argument (sizes, NaN or |lat| > 90 coordinates, unknown kernel) */
+    HCG_ENOMEM = 2,       /* device or host allocation failed */
+    HCG_ETIMEOUT = 3,     /* a bounded device wait ran out */
+    HCG_EDEVICE = 4,      /* CUDA error */
+    HCG_EIO = 5,          /* file read/write failed */
+    HCG_EUNSUPPORTED = 6, /* feature not available in this build (e.g. HDF5 without libhdf5) */
+    HCG_ESTATE = 7        /* call out of order (e.g. grid before prepare) */
+} hcg_status;
+
+/* Kernel types (HCGrid/constants.h:66-69). Only GAUSS1D is gridded. */
+#define HCG_GAUSS1D 1
+#define HCG_GAUSS2D 2
+#define HCG_TAPERED_SINC 3
+
+/* Where a buffer lives. */
+#define HCG_MEM_HOST 0
+#define HCG_MEM_DEVICE 1
+
+/* Spectra / cube layouts. SAMPLE_MAJOR: values[sample][channel] (cube
+ * [pixel][channel]); CHANNEL_MAJOR: values[channel][sample] (cube
+ * [channel][pixel], the FITS NAXIS3-slowest order and HCGrid+'s per-channel
+ * planes). */
+#define HCG_LAYOUT_SAMPLE_MAJOR 0
+#define HCG_LAYOUT_CHANNEL_MAJOR 1
+
+/* Gridding engines. */
+#define HCG_ENGINE_AUTO 0
+#define HCG_ENGINE_FP32 1 /* FP64 geometry, FP32 CUDA-core channel accumulation */
+
+typedef struct hcg_context hcg_context;
+typedef struct hcg_field hcg_field;
+typedef struct hcg_target hcg_target;
+
+typedef struct {
+    uint64_t nside, npix, firstring, usedrings;
+    double resolution; /* radians */
+    double disc_size;  /* radians: sphere_radius + resolution */
+    double kernel_param0; /* GAUSS1D: 0.5 / sigma^2 (sigma in degrees) */
+    double sphere_radius; /* degrees */
+} hcg_info;
+
+typedef struct {
+    uint64_t pairs_candidate; /* (pixel, sample) pairs inside the ring windows */
+    uint64_t pairs_within;    /* of those, distance < sphere_radius */
+    uint64_t ring_skips;      /* rings the reference would loop on forever (lpix/rpix outside ring) */
+    uint64_t hard_roundings;  /* cos/sin roundings the double-double test could not decide */
+    double ms_total;          /* device time of the last hcg_grid call */
+    double ms_phase[4];       /* of which: pixel setup, candidate count + scan, FP64 weights, channel sums */
+} hcg_stats;
+
+const char *hcg_status_string(hcg_status s);
+
+/* Context on CUDA device `device`; `stream` (cudaStream_t, may be NULL for a
+ * private stream) orders all work of the context. */
+hcg_status hcg_context_create(int device, void *stream, hcg_context **out);
+hcg_status hcg_context_destroy(hcg_context *ctx);
+const char *hcg_last_error(const hcg_context *ctx);
+
+/* _prepare_grid_kernel: GAUSS1D params[0] = sigma (deg) is replaced in place
+ * by 0.5/sigma^2, as the reference does; nside follows from hpx_max_res
+ * (deg); HEALPix is rebuilt only if sphere_radius or hpx_max_res moved by
+ * more than 3e-5 since the previous call on this context. */
+hcg_status hcg_prepare_grid_kernel(hcg_context *ctx, uint32_t kernel_type, double *kernel_params,
+                                   double sphere_radius, double hpx_max_res);
+hcg_status hcg_get_info(const hcg_context *ctx, const hcg_field *field, hcg_info *out);
+
+/* Samples: lon/lat in degrees (float64), optional per-sample weights
+ * (float64, NULL = 1 as in the reference). Computes HEALPix keys, the stable
+ * on-device radix sort, the permuted geometry and the ring lookup table. */
+hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, const double *lat,
+                            const double *weights, int mem, hcg_field **out);
+/* Attach spectra (float32) in either layout; permuted into sorted order on
+ * the device and kept resident. */
+hcg_status hcg_field_set_spectra(hcg_field *field, uint32_t nchan, const float *values, int layout, int mem);
+/* Sorted keys (n+1 with the npix sentinel), permutation (n) and ring LUT
+ * (usedrings+1); any pointer may be NULL. Host memory. */
+hcg_status hcg_field_sorted(const hcg_field *field, uint64_t *keys, uint32_t *perm, uint32_t *lut);
+hcg_status hcg_field_destroy(hcg_field *field);
+
+/* Target pixel centres in degrees, indexed yy*nx + xx. */
+hcg_status hcg_target_create(hcg_context *ctx, uint32_t nx, uint32_t ny, const double *xwcs, const double *ywcs,
+                             int mem, hcg_target **out);
+/* Target from a FITS header (80-char cards): RA---SIN / DEC--SIN with
+ * CRPIX/CDELT/CRVAL (and LONPOLE); pixel (xx+1, yy+1) as set_WCS does. */
+hcg_status hcg_target_from_header(hcg_context *ctx, const char *header, size_t len, hcg_target **out);
+hcg_status hcg_target_coords(const hcg_target *t, uint32_t *nx, uint32_t *ny, double *xwcs, double *ywcs);
+/* The same SIN pixel centres on the host, without a device: first call with
+ * xwcs = ywcs = NULL for nx, ny; then with arrays of nx*ny doubles. */
+hcg_status hcg_header_coords(const char *header, size_t len, uint32_t *nx, uint32_t *ny, double *xwcs,
+                             double *ywcs);
+hcg_status hcg_target_destroy(hcg_target *t);
+
+/* Grid the field's spectra onto the target and normalise: cube = sum(w x) /
+ * sum(w) (NaN where no sample contributes, as the reference's 0/0), float32;
+ * weights_out (optional, float32 [npix]) = sum(w). mem says where cube and
+ * weights_out live. */
+hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube, int layout,
+                    float *weights_out, int mem, int engine);
+hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out);
+
+/* Wait for all work queued on the context's stream. */
+hcg_status hcg_synchronize(hcg_context *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
