@@ -63,6 +63,12 @@ EXPORTS = {
     "hcg_grid": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "hcg_synchronize": ([C.c_void_p], C.c_int),
+    "hcg_fits_read_samples": ([C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
+                               C.c_void_p], C.c_int),
+    "hcg_fits_read_header": ([C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+    "hcg_fits_write_cube": ([C.c_char_p, C.c_char_p, C.c_size_t, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                             C.c_void_p, C.c_int], C.c_int),
+    "hcg_fits_write_samples": ([C.c_char_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
 }
 
 _lib = None
@@ -117,6 +123,48 @@ def header_coords(header: str):
     if st != 0:
         raise HcgError(st, "header")
     return nx.value, ny.value, x, y
+
+
+def fits_read_samples(path: str):
+    """(lon, lat, values[nchan, n]) of an input map in the reference's layout."""
+    L = load()
+    n, c = C.c_uint64(), C.c_uint32()
+    st = L.hcg_fits_read_samples(path.encode(), C.byref(n), C.byref(c), None, None, None)
+    if st != 0:
+        raise HcgError(st, path)
+    lon, lat = np.empty(n.value), np.empty(n.value)
+    vals = np.empty((c.value, n.value), np.float32)
+    st = L.hcg_fits_read_samples(path.encode(), C.byref(n), C.byref(c), lon.ctypes.data, lat.ctypes.data,
+                                 vals.ctypes.data)
+    if st != 0:
+        raise HcgError(st, path)
+    return lon, lat, vals
+
+
+def fits_read_header(path: str) -> str:
+    L = load()
+    ln = C.c_size_t()
+    st = L.hcg_fits_read_header(path.encode(), None, 0, C.byref(ln))
+    if st != 0:
+        raise HcgError(st, path)
+    buf = C.create_string_buffer(ln.value + 1)
+    st = L.hcg_fits_read_header(path.encode(), buf, ln.value + 1, C.byref(ln))
+    if st != 0:
+        raise HcgError(st, path)
+    return buf.value.decode("ascii")
+
+
+def fits_write_cube(path: str, header: str, nx: int, ny: int, cube, weights=None, bitpix: int = -32):
+    """cube: float32 [nchan, ny*nx] (channel-major)."""
+    L = load()
+    cube = np.ascontiguousarray(cube, np.float32)
+    nchan = cube.shape[0] if cube.ndim == 2 else 1
+    hb = header.encode("ascii")
+    w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+    st = L.hcg_fits_write_cube(path.encode(), hb, len(hb), nx, ny, nchan, cube.ctypes.data,
+                               None if w is None else w.ctypes.data, bitpix)
+    if st != 0:
+        raise HcgError(st, path)
 
 
 class Context:

@@ -22,7 +22,8 @@ LIB = os.path.join(LIBDIR, "libhcgrid_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["hcg_field.cu", "hcg_grid.cu", "hcg_capi.cu"]
-CXX_SOURCES = ["hcg_wcs.cpp"]
+CXX_SOURCES = ["hcg_wcs.cpp", "hcg_fits.cpp", "hcg_compat.cpp"]
+CLI = os.path.join(PKG, "bin", "HCGrid")
 
 
 def nvcc() -> str:
@@ -66,6 +67,12 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         log += _run(cmd)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         log += _run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"])
+    # flag-compatible command line (HCGrid/HCGrid.cpp) linked against the library
+    cli_src = os.path.join(CSRC, "hcg_cli.cpp")
+    if not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB), os.path.getmtime(cli_src)):
+        os.makedirs(os.path.dirname(CLI), exist_ok=True)
+        log += _run(["g++", "-O2", "-std=c++17", *inc, cli_src, "-o", CLI, "-L", LIBDIR, "-lhcgrid_b200",
+                     "-Wl,-rpath,$ORIGIN/../lib"])
     if verbose and log:
         print(log)
     return LIB

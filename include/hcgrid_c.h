@@ -136,6 +136,27 @@ hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out);
 /* Wait for all work queued on the context's stream. */
 hcg_status hcg_synchronize(hcg_context *ctx);
 
+/* FITS boundary, host only, in the reference's formats (HCGrid/gmap.cpp):
+ *   hcg_fits_read_samples   read_input_map (gmap.cpp:102-148): values from the
+ *                           primary image (N = NAXIS1*NAXIS2 samples, NAXIS3
+ *                           channels, written [nchan][n]), lon/lat (deg) from
+ *                           the second HDU. Call with NULL arrays for n, nchan.
+ *   hcg_fits_read_header    read_output_map (gmap.cpp:151-180): the primary
+ *                           header as 80-char cards ending with END.
+ *   hcg_fits_write_cube     write_output_map (gmap.cpp:253-323): the cube
+ *                           [nchan][ny][nx] (BITPIX -32 or -64) with the
+ *                           target's cards, plus a WEIGHTS image extension when
+ *                           weights is not NULL.
+ *   hcg_fits_write_samples  write_ordered_map (gmap.cpp:326-379): samples in
+ *                           the given (sorted) order, same layout as the input. */
+hcg_status hcg_fits_read_samples(const char *path, uint64_t *n, uint32_t *nchan, double *lon, double *lat,
+                                 float *values);
+hcg_status hcg_fits_read_header(const char *path, char *header, size_t cap, size_t *len);
+hcg_status hcg_fits_write_cube(const char *path, const char *target_header, size_t len, uint32_t nx, uint32_t ny,
+                               uint32_t nchan, const float *cube, const float *weights, int bitpix);
+hcg_status hcg_fits_write_samples(const char *path, uint64_t n, uint32_t nchan, const double *lon,
+                                  const double *lat, const float *values);
+
 #ifdef __cplusplus
 }
 #endif

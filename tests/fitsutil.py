@@ -56,3 +56,32 @@ def write_header_only(path: str, header: str) -> None:
     with open(path, "wb") as f:
         f.write(h)
         f.write(b"\0" * (nb + (-nb) % 2880))
+
+
+def write_input_map(path: str, values: np.ndarray, lon: np.ndarray, lat: np.ndarray) -> None:
+    """Input map in the reference's layout (HCGrid/gmap.cpp:102-148):
+    primary image NAXIS1=1, NAXIS2=N[, NAXIS3=C] of float32 values, then an
+    IMAGE extension NAXIS1=N, NAXIS2=2 holding lon then lat (float64)."""
+    values = np.asarray(values, np.float32).reshape(-1, len(lon))
+    nchan, n = values.shape
+
+    def card(k, v):
+        return ("%-8s= %20s" % (k, v)).ljust(80)
+
+    h = [card("SIMPLE", "T"), card("BITPIX", -32), card("NAXIS", 3 if nchan > 1 else 2), card("NAXIS1", 1),
+         card("NAXIS2", n)] + ([card("NAXIS3", nchan)] if nchan > 1 else []) + [card("EXTEND", "T"), "END".ljust(80)]
+    e = [("%-8s= %-20s" % ("XTENSION", "'IMAGE   '")).ljust(80), card("BITPIX", -64), card("NAXIS", 2),
+         card("NAXIS1", n), card("NAXIS2", 2), card("PCOUNT", 0), card("GCOUNT", 1), "END".ljust(80)]
+
+    def block(b):
+        return b + b"\0" * ((-len(b)) % 2880)
+
+    def hblock(cards):
+        s = "".join(cards).encode("ascii")
+        return s + b" " * ((-len(s)) % 2880)
+
+    with open(path, "wb") as f:
+        f.write(hblock(h))
+        f.write(block(values.astype(">f4").tobytes()))
+        f.write(hblock(e))
+        f.write(block(np.concatenate([lon, lat]).astype(">f8").tobytes()))
