@@ -63,6 +63,7 @@ EXPORTS = {
     "hcg_grid": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "hcg_synchronize": ([C.c_void_p], C.c_int),
+    "hcg_set_entry_budget": ([C.c_void_p, C.c_uint64], C.c_int),
     "hcg_fits_read_samples": ([C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
                                C.c_void_p], C.c_int),
     "hcg_fits_read_header": ([C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
@@ -243,6 +244,9 @@ class Context:
 
     def synchronize(self):
         self._check(self.L.hcg_synchronize(self.h))
+
+    def set_entry_budget(self, nbytes: int):
+        self._check(self.L.hcg_set_entry_budget(self.h, nbytes))
 
 
 class Field:

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "hcg_internal.h"
+#include "hcg_wcs.cuh"
 
 using namespace hcg;
 
@@ -343,11 +344,29 @@ hcg_status hcg_target_from_header(hcg_context *ctx, const char *header, size_t l
     Guard g(ctx);
     *out = nullptr;
     uint32_t nx, ny;
-    std::vector<double> x, y;
+    SinWcs w;
     std::string why;
-    int st = sin_target_coords(header, len, nx, ny, x, y, why);
+    int st = parse_sin_header(header, len, nx, ny, w, why);
     if (st != HCG_OK) return fail(ctx, (hcg_status)st, why);
-    return make_target(ctx, nx, ny, x.data(), y.data(), cudaMemcpyHostToDevice, out);
+    if (nx == 0 || ny == 0) return fail(ctx, HCG_EINVAL, "empty target");
+    cudaStream_t s = ctx->stream;
+    hcg_target *t = new (std::nothrow) hcg_target();
+    if (!t) return fail(ctx, HCG_ENOMEM, "host allocation");
+    t->ctx = ctx;
+    t->nx = nx;
+    t->ny = ny;
+    size_t nb = (size_t)nx * ny * sizeof(double);
+    cudaError_t e = cudaMallocAsync(&t->d_x, nb, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&t->d_y, nb, s);
+    if (e == cudaSuccess) e = sin_coords_device(w, nx, ny, t->d_x, t->d_y, s);  // pixel centres on the device
+    if (e != cudaSuccess) {
+        if (t->d_x) cudaFreeAsync(t->d_x, s);
+        if (t->d_y) cudaFreeAsync(t->d_y, s);
+        delete t;
+        return cuda_fail(ctx, e, "target");
+    }
+    *out = t;
+    return HCG_OK;
 }
 
 hcg_status hcg_target_coords(const hcg_target *t, uint32_t *nx, uint32_t *ny, double *xwcs, double *ywcs) {
@@ -451,6 +470,13 @@ hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out) {
         }
         out->ms_phase[i] = m;
     }
+    return HCG_OK;
+}
+
+hcg_status hcg_set_entry_budget(hcg_context *ctx, uint64_t bytes) {
+    if (!ctx || bytes < 4096) return HCG_EINVAL;
+    Guard g(ctx);
+    ctx->entry_budget = bytes;
     return HCG_OK;
 }
 

@@ -77,6 +77,7 @@ struct hcg_context {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evp[4] = {nullptr, nullptr, nullptr, nullptr};  // phase boundaries inside hcg_grid
     float last_ms = 0.f;
+    unsigned long long entry_budget = 4ULL << 30;  // bytes of (sample, weights) entries per launch run
 };
 
 struct hcg_field {
@@ -111,4 +112,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
                        float *d_wts, int engine, std::string &why);
 int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny, std::vector<double> &x,
                       std::vector<double> &y, std::string &why);
+struct SinWcs;
+int parse_sin_header(const char *header, size_t len, uint32_t &nx, uint32_t &ny, SinWcs &w, std::string &why);
+cudaError_t sin_coords_device(const SinWcs &w, uint32_t nx, uint32_t ny, double *d_x, double *d_y, cudaStream_t s);
 }  // namespace hcg

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "hcg_internal.h"
+#include "hcg_wcs.cuh"
 
 namespace hcg {
 namespace {
@@ -52,13 +53,9 @@ double num(const std::map<std::string, std::string> &kv, const char *k, double d
     return strtod(it->second.c_str(), nullptr);
 }
 
-constexpr double D2R = 0x1.1df46a2529d39p-6;
-constexpr double R2D = 0x1.ca5dc1a63c1f8p+5;
-
 }  // namespace
 
-int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny, std::vector<double> &X,
-                      std::vector<double> &Y, std::string &why) {
+int parse_sin_header(const char *header, size_t len, uint32_t &nx, uint32_t &ny, SinWcs &w, std::string &why) {
     auto kv = parse_cards(header, len);
     bool h;
     nx = (uint32_t)num(kv, "NAXIS1", 0, h);
@@ -70,19 +67,21 @@ int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny
         why = "only SIN projections are supported (CTYPE1='" + t1 + "', CTYPE2='" + t2 + "')";
         return HCG_EUNSUPPORTED;
     }
-    double crpix1 = num(kv, "CRPIX1", 0, h), crpix2 = num(kv, "CRPIX2", 0, h);
+    w.crpix1 = num(kv, "CRPIX1", 0, h);
+    w.crpix2 = num(kv, "CRPIX2", 0, h);
     double crval1 = num(kv, "CRVAL1", 0, h), crval2 = num(kv, "CRVAL2", 0, h);
-    double pc[2][2] = {{1, 0}, {0, 1}}, cdelt[2] = {1, 1};
+    w.pc[0][0] = 1; w.pc[0][1] = 0; w.pc[1][0] = 0; w.pc[1][1] = 1;
+    w.cdelt[0] = w.cdelt[1] = 1;
     bool hc;
     num(kv, "CD1_1", 0, hc);
     if (hc) {
-        pc[0][0] = num(kv, "CD1_1", 0, h); pc[0][1] = num(kv, "CD1_2", 0, h);
-        pc[1][0] = num(kv, "CD2_1", 0, h); pc[1][1] = num(kv, "CD2_2", 0, h);
+        w.pc[0][0] = num(kv, "CD1_1", 0, h); w.pc[0][1] = num(kv, "CD1_2", 0, h);
+        w.pc[1][0] = num(kv, "CD2_1", 0, h); w.pc[1][1] = num(kv, "CD2_2", 0, h);
     } else {
-        cdelt[0] = num(kv, "CDELT1", 1, h);
-        cdelt[1] = num(kv, "CDELT2", 1, h);
-        pc[0][0] = num(kv, "PC1_1", 1, h); pc[0][1] = num(kv, "PC1_2", 0, h);
-        pc[1][0] = num(kv, "PC2_1", 0, h); pc[1][1] = num(kv, "PC2_2", 1, h);
+        w.cdelt[0] = num(kv, "CDELT1", 1, h);
+        w.cdelt[1] = num(kv, "CDELT2", 1, h);
+        w.pc[0][0] = num(kv, "PC1_1", 1, h); w.pc[0][1] = num(kv, "PC1_2", 0, h);
+        w.pc[1][0] = num(kv, "PC2_1", 0, h); w.pc[1][1] = num(kv, "PC2_2", 1, h);
     }
     bool hxi, heta;
     double xi = num(kv, "PV2_1", 0, hxi), eta = num(kv, "PV2_2", 0, heta);
@@ -91,33 +90,25 @@ int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny
     // the native frame is the reference point; LONPOLE defaults to 180 deg
     // when CRVAL2 < 90 (Paper II, sec. 2.5).
     double lonpole = num(kv, "LONPOLE", crval2 < 90.0 ? 180.0 : 0.0, h);
-    double ap = crval1 * D2R, dp = crval2 * D2R, pp = lonpole * D2R;
-    double sdp = sin(dp), cdp = cos(dp);
+    w.ap = crval1 * kWcsD2R;
+    w.sdp = sin(crval2 * kWcsD2R);
+    w.cdp = cos(crval2 * kWcsD2R);
+    w.pp = lonpole * kWcsD2R;
+    return HCG_OK;
+}
+
+int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny, std::vector<double> &X,
+                      std::vector<double> &Y, std::string &why) {
+    SinWcs w;
+    int st = parse_sin_header(header, len, nx, ny, w, why);
+    if (st != HCG_OK) return st;
     X.resize((size_t)nx * ny);
     Y.resize((size_t)nx * ny);
-    for (uint32_t yy = 0; yy < ny; ++yy) {
+    for (uint32_t yy = 0; yy < ny; ++yy)
         for (uint32_t xx = 0; xx < nx; ++xx) {
-            double q1 = (xx + 1) - crpix1, q2 = (yy + 1) - crpix2;
-            double x = cdelt[0] * (pc[0][0] * q1 + pc[0][1] * q2);
-            double y = cdelt[1] * (pc[1][0] * q1 + pc[1][1] * q2);
-            // SIN deprojection (Paper II eq. 59-60 with xi = eta = 0)
-            double r = sqrt(x * x + y * y) * D2R;
             size_t o = (size_t)yy * nx + xx;
-            if (r > 1.0) { X[o] = Y[o] = NAN; continue; }
-            double phi = (r == 0.0) ? 0.0 : atan2(x, -y);
-            double ct = r, st = sqrt((1.0 - r) * (1.0 + r));  // cos/sin of native latitude theta
-            double dphi = phi - pp;
-            double sdelta = st * sdp + ct * cdp * cos(dphi);
-            double yv = -ct * sin(dphi);
-            double xv = st * cdp - ct * sdp * cos(dphi);
-            double alpha = ap + atan2(yv, xv);
-            double delta = atan2(sdelta, sqrt(xv * xv + yv * yv));  // (xv, yv) = cos(delta) (cos, sin) of d-alpha
-            double a = fmod(alpha * R2D, 360.0);
-            if (a < 0) a += 360.0;
-            X[o] = a;
-            Y[o] = delta * R2D;
+            sin_pix2world(w, xx + 1.0, yy + 1.0, X[o], Y[o]);
         }
-    }
     return HCG_OK;
 }
 

@@ -132,6 +132,10 @@ hcg_status hcg_target_destroy(hcg_target *t);
 hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube, int layout,
                     float *weights_out, int mem, int engine);
 hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out);
+/* Upper bound (bytes) of the per-call candidate entry buffer of the
+ * multi-channel engine; larger jobs are processed in runs of tile rows
+ * (default 4 GiB). */
+hcg_status hcg_set_entry_budget(hcg_context *ctx, uint64_t bytes);
 
 /* Wait for all work queued on the context's stream. */
 hcg_status hcg_synchronize(hcg_context *ctx);
