@@ -29,6 +29,11 @@ class HcgError(RuntimeError):
         self.status = status
 
 
+class Job(C.Structure):
+    _fields_ = [("field", C.c_void_p), ("target", C.c_void_p), ("cube", C.c_void_p), ("weights", C.c_void_p),
+                ("layout", C.c_int)]
+
+
 class Info(C.Structure):
     _fields_ = [("nside", C.c_uint64), ("npix", C.c_uint64), ("firstring", C.c_uint64), ("usedrings", C.c_uint64),
                 ("resolution", C.c_double), ("disc_size", C.c_double), ("kernel_param0", C.c_double),
@@ -64,6 +69,14 @@ EXPORTS = {
     "hcg_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "hcg_synchronize": ([C.c_void_p], C.c_int),
     "hcg_set_entry_budget": ([C.c_void_p, C.c_uint64], C.c_int),
+    "hcg_grid_batch": ([C.c_void_p, C.c_uint32, C.c_void_p], C.c_int),
+    "hcg_server_create": ([C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)], C.c_int),
+    "hcg_server_submit": ([C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
+    "hcg_server_wait": ([C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+    "hcg_server_drain": ([C.c_void_p], C.c_int),
+    "hcg_server_stats": ([C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
+                          C.POINTER(C.c_uint32)], C.c_int),
+    "hcg_server_destroy": ([C.c_void_p], C.c_int),
     "hcg_fits_read_samples": ([C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
                                C.c_void_p], C.c_int),
     "hcg_fits_read_header": ([C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
@@ -245,8 +258,68 @@ class Context:
     def synchronize(self):
         self._check(self.L.hcg_synchronize(self.h))
 
+    def grid_batch(self, jobs):
+        """jobs: list of (field, target, cube_tensor, weights_tensor_or_None, layout) with CUDA tensors."""
+        arr = (Job * len(jobs))()
+        for i, (f, t, cube, w, layout) in enumerate(jobs):
+            if not (hasattr(cube, "is_cuda") and cube.is_cuda):
+                raise ValueError("batch outputs must be CUDA tensors")
+            arr[i] = Job(f.h.value, t.h.value, cube.data_ptr(), w.data_ptr() if w is not None else None, layout)
+        self._check(self.L.hcg_grid_batch(self.h, len(jobs), arr))
+
     def set_entry_budget(self, nbytes: int):
         self._check(self.L.hcg_set_entry_budget(self.h, nbytes))
+
+
+class Server:
+    """hcg_server: continuous-batching request loop over `lanes` contexts."""
+
+    def __init__(self, ctx: Context, lanes: int = 2, hbm_budget: int = 120 << 30, max_batch: int = 64,
+                 device: int = 0):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx._check(ctx.L.hcg_server_create(ctx.h, device, lanes, hbm_budget, max_batch, C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, field, target, cube, weights=None, layout: int = SAMPLE_MAJOR, footprint: int = 0) -> int:
+        job = Job(field.h.value, target.h.value, cube.data_ptr(), weights.data_ptr() if weights is not None else None,
+                  layout)
+        t = C.c_uint64()
+        st = self.ctx.L.hcg_server_submit(self.h, C.byref(job), footprint, C.byref(t))
+        if st != 0:
+            raise HcgError(st, "submit")
+        self._keep[t.value] = (cube, weights)
+        return t.value
+
+    def wait(self, ticket: int):
+        lat, q = C.c_double(), C.c_double()
+        st = self.ctx.L.hcg_server_wait(self.h, ticket, C.byref(lat), C.byref(q))
+        self._keep.pop(ticket, None)
+        if st != 0:
+            raise HcgError(st, "job %d" % ticket)
+        return lat.value, q.value
+
+    def drain(self):
+        st = self.ctx.L.hcg_server_drain(self.h)
+        if st != 0:
+            raise HcgError(st, "drain")
+
+    def stats(self):
+        p50, p99, n, b = C.c_double(), C.c_double(), C.c_uint64(), C.c_uint32()
+        self.ctx.L.hcg_server_stats(self.h, C.byref(p50), C.byref(p99), C.byref(n), C.byref(b))
+        return {"p50_s": p50.value, "p99_s": p99.value, "jobs": n.value, "batches": b.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.hcg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Field:

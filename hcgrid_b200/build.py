@@ -21,8 +21,8 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libhcgrid_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["hcg_field.cu", "hcg_grid.cu", "hcg_capi.cu"]
-CXX_SOURCES = ["hcg_wcs.cpp", "hcg_fits.cpp", "hcg_compat.cpp"]
+CU_SOURCES = ["hcg_field.cu", "hcg_grid.cu", "hcg_batch.cu", "hcg_capi.cu"]
+CXX_SOURCES = ["hcg_wcs.cpp", "hcg_fits.cpp", "hcg_compat.cpp", "hcg_server.cpp"]
 CLI = os.path.join(PKG, "bin", "HCGrid")
 
 
@@ -62,11 +62,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         objs.append(obj)
         if os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
             continue
-        cmd = ["g++", "-O2", "-fPIC", "-ffp-contract=off", "-std=c++17", *inc,
+        cmd = ["g++", "-O2", "-fPIC", "-ffp-contract=off", "-std=c++17", "-pthread", *inc,
                "-I", "/usr/local/cuda/include", "-c", os.path.join(CSRC, src), "-o", obj]
         log += _run(cmd)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        log += _run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"])
+        log += _run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static", "-Xlinker", "-lpthread"])
     # flag-compatible command line (HCGrid/HCGrid.cpp) linked against the library
     cli_src = os.path.join(CSRC, "hcg_cli.cpp")
     if not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB), os.path.getmtime(cli_src)):

@@ -1,0 +1,409 @@
+// Batched gridding: many independent jobs (field, target, cube) in one pass.
+//
+// Every phase is one persistent launch over the work of all jobs: a fixed
+// number of CTAs per SM pull work items (pixels, 2x2 groups, tiles, tile x
+// channel-slice pairs) from a device-side queue (an atomic head per phase)
+// and look the item's job up in a device job table. Launch shapes do not
+// depend on the batch, and all per-batch state (job table, queue heads,
+// totals, scratch pointers) lives in device memory, so the whole pass is
+// captured once into a CUDA graph and replayed for every batch; the host
+// only uploads the job table before the replay.
+//
+// Items run the same device functions as the single-job launches
+// (hcg_kernels.cuh), so each job's cube is identical to hcg_grid's. Entries
+// of all jobs share one pool; if a batch needs more than the pool holds, the
+// geometry phase skips the groups that do not fit, flags it, and the host
+// grows the pool and replays. A job whose tiles span more rings than the
+// tile table holds is re-run through hcg_grid.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "hcg_internal.h"
+#include "hcg_kernels.cuh"
+
+namespace hcg {
+namespace {
+
+struct JobDesc {
+    GridArgs a;       // per-job geometry (prep -> batch prep array + pixel base)
+    GroupArgs g;      // map shape; off/cnt/cap below are already offset to this job
+    TileArgs T;       // tile table slice of this job
+    const double *X, *Y;
+    uint64_t firstring, usedrings;
+    double disc;
+    const float *spec;
+    uint32_t nchan, cstride, nslices, ostride;  // ostride 0: [channel][pixel]
+    float *out, *wout;
+    uint32_t *cap, *cnt;
+    unsigned long long *off;
+    double *wsum;
+    PixPrep *prep;
+    // first item of this job in each phase's item space
+    unsigned long long pix_base, grp_base, tile_base, acc_base, c1_base;
+};
+
+enum { Q_TILE = 0, Q_COUNT, Q_GEOM, Q_ACC, Q_C1, Q_N };
+
+struct BatchHdr {
+    uint32_t njobs;
+    unsigned long long tot_pix, tot_grp, tot_tile, tot_acc, tot_c1;
+    unsigned long long head[Q_N];
+    unsigned long long entry_cap;      // entries the pool holds
+    unsigned long long entries_needed; // total entries of the batch (set by the scan)
+    unsigned long long pool_overflow;  // groups skipped for lack of pool space
+    uint32_t *e_idx;
+    float4 *e_w;
+    unsigned long long *off_all;       // [tot_grp + 1]
+    uint32_t *cap_all;
+};
+
+constexpr int kPersistPerSM = 8;
+
+// Job owning item `it` of a phase: last job whose base is <= it.
+template <typename F>
+__device__ __forceinline__ int find_job(const JobDesc *__restrict__ jobs, uint32_t njobs, unsigned long long it,
+                                        F base_of) {
+    int lo = 0, hi = (int)njobs;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (base_of(jobs[mid]) <= it) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) kb_prep(const BatchHdr *__restrict__ H, const JobDesc *__restrict__ jobs,
+                                               DevStats *stats) {
+    for (unsigned long long it = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; it < H->tot_pix;
+         it += (unsigned long long)gridDim.x * blockDim.x) {
+        int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.pix_base; });
+        const JobDesc &J = jobs[j];
+        prep_item(J.a.h, J.firstring, J.usedrings, J.disc, J.X, J.Y, J.prep, stats, it - J.pix_base);
+    }
+}
+
+__device__ __forceinline__ unsigned long long block_fetch(BatchHdr *H, int q) {
+    __shared__ unsigned long long s_item;
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(&H->head[q], 1ULL);
+    __syncthreads();
+    return s_item;
+}
+
+__device__ __forceinline__ unsigned long long warp_fetch(BatchHdr *H, int q) {
+    unsigned long long v = 0;
+    if ((threadIdx.x & 31) == 0) v = atomicAdd(&H->head[q], 1ULL);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+__global__ void __launch_bounds__(256) kb_tile_rings(BatchHdr *H, const JobDesc *__restrict__ jobs) {
+    for (;;) {
+        unsigned long long it = block_fetch(H, Q_TILE);
+        if (it >= H->tot_tile) return;
+        int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.tile_base; });
+        const JobDesc &J = jobs[j];
+        tile_rings_item(J.a, J.g, J.T, it - J.tile_base);
+    }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) kb_group(BatchHdr *H, const JobDesc *__restrict__ jobs) {
+    __shared__ PixPrep s_prep[8][4];
+    const int warp = threadIdx.x >> 5;
+    for (;;) {
+        unsigned long long it = warp_fetch(H, COUNT ? Q_COUNT : Q_GEOM);
+        if (it >= H->tot_grp) return;
+        int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.grp_base; });
+        const JobDesc &J = jobs[j];
+        uint64_t grp = it - J.grp_base;
+        if (!COUNT) {
+            // the pool must hold this group's entries; otherwise skip and report
+            unsigned long long end = J.off[grp] + J.cap[grp];
+            if (end > H->entry_cap) {
+                if ((threadIdx.x & 31) == 0) atomicAdd(&H->pool_overflow, 1ULL);
+                continue;
+            }
+        }
+        group_item<COUNT>(J.a, J.g, J.cap, J.off, H->e_idx, H->e_w, J.cnt, J.wsum, J.T, grp, s_prep[warp]);
+    }
+}
+
+// Exclusive scan of all jobs' group capacities (one block).
+__global__ void __launch_bounds__(1024) kb_scan(BatchHdr *H) {
+    __shared__ unsigned long long part[1024];
+    const unsigned long long n = H->tot_grp;
+    const uint32_t *in = H->cap_all;
+    unsigned long long *out = H->off_all;
+    unsigned long long per = (n + 1023) / 1024;
+    unsigned long long b = threadIdx.x * per, e = min(n, b + per);
+    unsigned long long s = 0;
+    for (unsigned long long i = b; i < e; ++i) s += in[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        unsigned long long v = (threadIdx.x >= o) ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned long long run = part[threadIdx.x] - s;
+    for (unsigned long long i = b; i < e; ++i) {
+        out[i] = run;
+        run += in[i];
+    }
+    if (threadIdx.x == 1023) {
+        out[n] = part[1023];
+        H->entries_needed = part[1023];
+    }
+}
+
+__global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobDesc *__restrict__ jobs) {
+    for (;;) {
+        unsigned long long it = block_fetch(H, Q_ACC);
+        if (it >= H->tot_acc) return;
+        int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.acc_base; });
+        const JobDesc &J = jobs[j];
+        unsigned long long local = it - J.acc_base;
+        uint64_t tile = local / J.nslices;
+        uint32_t c0 = (uint32_t)(local % J.nslices) * kSlice;
+        tile_accum_item(J.g, J.T, J.off, J.cnt, H->e_idx, H->e_w, J.wsum, J.spec, J.nchan, J.cstride, J.out,
+                        J.ostride, J.wout, tile, c0);
+    }
+}
+
+__global__ void __launch_bounds__(256) kb_1chan(BatchHdr *H, const JobDesc *__restrict__ jobs) {
+    for (;;) {
+        unsigned long long it = warp_fetch(H, Q_C1);
+        if (it >= H->tot_c1) return;
+        int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.c1_base; });
+        const JobDesc &J = jobs[j];
+        grid1_item(J.a, J.spec, J.cstride, J.out, J.wout, it - J.c1_base);
+    }
+}
+
+}  // namespace
+
+// Batch state kept by a context: device header + job table, scratch and the
+// captured graph.
+struct BatchState {
+    BatchHdr *d_hdr = nullptr;
+    BatchHdr *h_hdr = nullptr;  // pinned
+    JobDesc *d_jobs = nullptr;
+    JobDesc *h_jobs = nullptr;  // pinned
+    uint32_t job_cap = 0;
+    cudaGraphExec_t exec = nullptr;
+    int nsm = 0;
+    void *scratch[8] = {};
+    size_t scratch_size[8] = {};
+    unsigned long long entry_cap = 0;
+};
+
+static cudaError_t grow(BatchState &B, int slot, size_t bytes, cudaStream_t s, void **out) {
+    if (B.scratch_size[slot] < bytes) {
+        if (B.scratch[slot]) cudaFreeAsync(B.scratch[slot], s);
+        size_t want = bytes + bytes / 4 + 256;
+        cudaError_t e = cudaMallocAsync(&B.scratch[slot], want, s);
+        if (e != cudaSuccess) {
+            B.scratch[slot] = nullptr;
+            B.scratch_size[slot] = 0;
+            return e;
+        }
+        B.scratch_size[slot] = want;
+    }
+    *out = B.scratch[slot];
+    return cudaSuccess;
+}
+
+static cudaError_t capture(hcg_context *ctx, BatchState &B) {
+    cudaStream_t s = ctx->stream;
+    const int smem = kStageSlots * kSlice * (int)sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(kb_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t graph;
+    if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+    cudaMemsetAsync(&B.d_hdr->head[0], 0, sizeof(B.d_hdr->head), s);
+    cudaMemsetAsync(&B.d_hdr->pool_overflow, 0, sizeof(unsigned long long), s);
+    const int n = B.nsm;
+    kb_prep<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs, ctx->d_stats);
+    kb_tile_rings<<<n * 4, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+    kb_group<true><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+    kb_scan<<<1, 1024, 0, s>>>(B.d_hdr);
+    kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+    kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
+    kb_1chan<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) return ce;
+    e = cudaGraphInstantiate(&B.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    return e;
+}
+
+cudaError_t batch_release(hcg_context *ctx) {
+    BatchState *B = (BatchState *)ctx->batch;
+    if (!B) return cudaSuccess;
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    for (auto &p : B->scratch)
+        if (p) cudaFreeAsync(p, ctx->stream);
+    if (B->d_hdr) cudaFreeAsync(B->d_hdr, ctx->stream);
+    if (B->d_jobs) cudaFreeAsync(B->d_jobs, ctx->stream);
+    if (B->h_hdr) cudaFreeHost(B->h_hdr);
+    if (B->h_jobs) cudaFreeHost(B->h_jobs);
+    delete B;
+    ctx->batch = nullptr;
+    return cudaSuccess;
+}
+
+// Grid `njobs` jobs with device output buffers in one graph replay.
+// `fallback[j]` is set for jobs that must be re-run through hcg_grid.
+cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, std::vector<char> &fallback,
+                       std::string &why) {
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    if (!ctx->batch) {
+        BatchState *B = new BatchState();
+        cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+        if ((e = cudaMallocAsync(&B->d_hdr, sizeof(BatchHdr), s)) != cudaSuccess ||
+            (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess) {
+            delete B;
+            return e;
+        }
+        ctx->batch = B;
+    }
+    BatchState &B = *(BatchState *)ctx->batch;
+    if (njobs > B.job_cap) {
+        if (B.d_jobs) cudaFreeAsync(B.d_jobs, s);
+        if (B.h_jobs) cudaFreeHost(B.h_jobs);
+        B.job_cap = std::max<uint32_t>(njobs, 64);
+        if ((e = cudaMallocAsync(&B.d_jobs, B.job_cap * sizeof(JobDesc), s)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&B.h_jobs, B.job_cap * sizeof(JobDesc))) != cudaSuccess) return e;
+    }
+    // item spaces and scratch sizes
+    unsigned long long pix = 0, grp = 0, tile = 0, acc = 0, c1 = 0;
+    std::vector<JobDesc> J(njobs);
+    for (uint32_t i = 0; i < njobs; ++i) {
+        const hcg_field *f = jobs[i].field;
+        const hcg_target *t = jobs[i].target;
+        JobDesc &d = J[i];
+        memset(&d, 0, sizeof d);
+        uint64_t P = (uint64_t)t->nx * t->ny;
+        d.g.nx = t->nx;
+        d.g.ny = t->ny;
+        d.g.gx = (t->nx + 1) / 2;
+        d.g.ngroups = (f->nchan > 1) ? (uint64_t)d.g.gx * ((t->ny + 1) / 2) : 0;
+        d.g.g0 = 0;
+        d.g.g1 = d.g.ngroups;
+        d.g.ebase = 0;
+        d.T.ntx = (t->nx + kTileX - 1) / kTileX;
+        d.T.nty = (t->ny + kTileY - 1) / kTileY;
+        uint64_t ntiles = (f->nchan > 1) ? (uint64_t)d.T.ntx * d.T.nty : 0;
+        d.nslices = (f->cstride + kSlice - 1) / kSlice;
+        d.pix_base = pix;
+        d.grp_base = grp;
+        d.tile_base = tile;
+        d.acc_base = acc;
+        d.c1_base = c1;
+        pix += P;
+        grp += d.g.ngroups;
+        tile += ntiles;
+        acc += ntiles * d.nslices;
+        if (f->nchan == 1) c1 += P;
+    }
+    void *p_prep, *p_wsum, *p_cap, *p_cnt, *p_off, *p_tiles;
+    const size_t tile_words = 3 + kTileMaxRings + kTileMaxRings + 1;  // r0, nr, U, ulo[], base[]
+    if ((e = grow(B, 0, (pix + 1) * sizeof(PixPrep), s, &p_prep)) != cudaSuccess ||
+        (e = grow(B, 1, (pix + 1) * sizeof(double), s, &p_wsum)) != cudaSuccess ||
+        (e = grow(B, 2, (grp + 1) * sizeof(uint32_t), s, &p_cap)) != cudaSuccess ||
+        (e = grow(B, 3, (grp + 1) * sizeof(uint32_t), s, &p_cnt)) != cudaSuccess ||
+        (e = grow(B, 4, (grp + 2) * sizeof(unsigned long long), s, &p_off)) != cudaSuccess ||
+        (e = grow(B, 5, (tile + 1) * tile_words * sizeof(uint32_t), s, &p_tiles)) != cudaSuccess)
+        return e;
+    if (B.entry_cap == 0) B.entry_cap = 1ULL << 24;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        void *p_eidx, *p_ew;
+        if ((e = grow(B, 6, (B.entry_cap + 1) * sizeof(uint32_t), s, &p_eidx)) != cudaSuccess ||
+            (e = grow(B, 7, (B.entry_cap + 1) * sizeof(float4), s, &p_ew)) != cudaSuccess) {
+            why = "entry pool of " + std::to_string(B.entry_cap) + " entries";
+            return e;
+        }
+        int *t_r0 = (int *)p_tiles;
+        int *t_nr = t_r0 + (tile + 1);
+        uint32_t *t_U = (uint32_t *)(t_nr + (tile + 1));
+        uint32_t *t_ulo = t_U + (tile + 1);
+        uint32_t *t_base = t_ulo + (tile + 1) * kTileMaxRings;
+        for (uint32_t i = 0; i < njobs; ++i) {
+            const hcg_field *f = jobs[i].field;
+            const hcg_target *t = jobs[i].target;
+            JobDesc &d = J[i];
+            d.prep = (PixPrep *)p_prep + d.pix_base;
+            d.wsum = (double *)p_wsum + d.pix_base;
+            d.cap = (uint32_t *)p_cap + d.grp_base;
+            d.cnt = (uint32_t *)p_cnt + d.grp_base;
+            d.off = (unsigned long long *)p_off + d.grp_base;
+            d.a = GridArgs{f->hpx, f->d_rings, d.prep, f->d_keys, f->d_l2, f->d_b2, f->d_cb2, f->d_w,
+                           f->sphere_radius, f->kparam0, ctx->d_stats};
+            d.T.t0 = 0;
+            d.T.r0 = t_r0 + d.tile_base;
+            d.T.nr = t_nr + d.tile_base;
+            d.T.U = t_U + d.tile_base;
+            d.T.ulo = t_ulo + d.tile_base * kTileMaxRings;
+            d.T.base = t_base + d.tile_base * (kTileMaxRings + 1);
+            d.T.overflow = &ctx->d_stats->overflow;
+            d.X = t->d_x;
+            d.Y = t->d_y;
+            d.firstring = f->firstring;
+            d.usedrings = f->usedrings;
+            d.disc = f->disc_size;
+            d.spec = f->d_spec;
+            d.nchan = f->nchan;
+            d.cstride = f->cstride;
+            d.ostride = jobs[i].layout == HCG_LAYOUT_CHANNEL_MAJOR ? 0 : f->nchan;
+            d.out = jobs[i].cube;
+            d.wout = jobs[i].weights;
+        }
+        memcpy(B.h_jobs, J.data(), njobs * sizeof(JobDesc));
+        BatchHdr &h = *B.h_hdr;
+        memset(&h, 0, sizeof h);
+        h.njobs = njobs;
+        h.tot_pix = pix;
+        h.tot_grp = grp;
+        h.tot_tile = tile;
+        h.tot_acc = acc;
+        h.tot_c1 = c1;
+        h.entry_cap = B.entry_cap;
+        h.e_idx = (uint32_t *)p_eidx;
+        h.e_w = (float4 *)p_ew;
+        h.off_all = (unsigned long long *)p_off;
+        h.cap_all = (uint32_t *)p_cap;
+        if ((e = cudaMemcpyAsync(B.d_jobs, B.h_jobs, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, s)) !=
+                cudaSuccess ||
+            (e = cudaMemcpyAsync(B.d_hdr, B.h_hdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(&ctx->d_stats->overflow, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+            return e;
+        if (!B.exec && (e = capture(ctx, B)) != cudaSuccess) return e;
+        cudaEventRecord(ctx->ev0, s);
+        for (auto &ev : ctx->evp) cudaEventRecord(ev, s);  // one graph: phases are not separated
+        if ((e = cudaGraphLaunch(B.exec, s)) != cudaSuccess) return e;
+        cudaEventRecord(ctx->ev1, s);
+        if ((e = cudaMemcpyAsync(B.h_hdr, B.d_hdr, sizeof(BatchHdr), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+            return e;
+        unsigned long long tile_overflow = 0;
+        if ((e = cudaMemcpyAsync(&tile_overflow, &ctx->d_stats->overflow, sizeof tile_overflow,
+                                 cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        fallback.assign(njobs, 0);
+        if (tile_overflow) {
+            // some tile spans more rings than its table: those jobs' groups
+            // wrote sample indices, so re-run every multi-channel job singly
+            for (uint32_t i = 0; i < njobs; ++i)
+                if (jobs[i].field->nchan > 1) fallback[i] = 1;
+        }
+        if (B.h_hdr->pool_overflow == 0) return cudaSuccess;
+        B.entry_cap = B.h_hdr->entries_needed + (B.h_hdr->entries_needed >> 3) + 1024;  // grow and replay once
+    }
+    why = "entry pool still too small after growing";
+    return cudaErrorMemoryAllocation;
+}
+
+}  // namespace hcg

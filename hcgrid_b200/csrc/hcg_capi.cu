@@ -70,6 +70,13 @@ void healpix_params(double hpx_max_res, HpxParams &h) {
     h.resolution = sqrt(omega);
 }
 
+// Device buffers of a field (caller holds the context lock).
+void release_field(hcg_field *f, cudaStream_t s) {
+    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_lut, f->d_rings, f->d_spec};
+    for (void *p : ps)
+        if (p) cudaFreeAsync(p, s);
+}
+
 }  // namespace
 
 void *hcg::Scratch::get(int slot, size_t bytes, cudaStream_t s, cudaError_t &err) {
@@ -156,6 +163,7 @@ hcg_status hcg_context_destroy(hcg_context *ctx) {
     {
         Guard g(ctx);
         cudaStreamSynchronize(ctx->stream);
+        batch_release(ctx);
         ctx->scratch.release(ctx->stream);
         cudaStreamSynchronize(ctx->stream);
         cudaFree(ctx->d_stats);
@@ -230,6 +238,10 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
     f->ctx = ctx;
     f->n = n;
     f->hpx = ctx->hpx;
+    f->sphere_radius = ctx->sphere_radius;
+    f->kparam0 = ctx->kparams[0];
+    f->disc_size = ctx->disc_size;
+    f->kernel_type = ctx->kernel_type;
     const double *dl = lon, *db = lat, *dw = weights;
     double *tmp = nullptr;
     if (mem == HCG_MEM_HOST) {
@@ -249,7 +261,8 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
     if (e != cudaSuccess) {
         hcg_status st = cuda_fail(ctx, e, "field build", why);
         cudaStreamSynchronize(s);
-        hcg_field_destroy(f);
+        release_field(f, s);  // the context lock is already held here
+        delete f;
         return st;
     }
     *out = f;
@@ -296,10 +309,7 @@ hcg_status hcg_field_destroy(hcg_field *f) {
     hcg_context *ctx = f->ctx;
     {
         Guard g(ctx);
-        cudaStream_t s = ctx->stream;
-        void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_lut, f->d_rings, f->d_spec};
-        for (void *p : ps)
-            if (p) cudaFreeAsync(p, s);
+        release_field(f, ctx->stream);
     }
     delete f;
     return HCG_OK;
@@ -414,9 +424,7 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
     if (!ctx || !field || !target || !cube) return HCG_EINVAL;
     Guard g(ctx);
     if (!ctx->prepared) return fail(ctx, HCG_ESTATE, "hcg_prepare_grid_kernel must come first");
-    if (ctx->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
-    if (field->hpx.nside != ctx->hpx.nside)
-        return fail(ctx, HCG_ESTATE, "field was built for another HEALPix resolution; rebuild it");
+    if (field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
     if (!field->d_spec) return fail(ctx, HCG_ESTATE, "field has no spectra (hcg_field_set_spectra)");
     if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
         return fail(ctx, HCG_EINVAL, "unknown layout");
@@ -441,6 +449,35 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
             CK(ctx, cudaMemcpyAsync(weights_out, dw, P * sizeof(float), cudaMemcpyDeviceToHost, s), "weights download");
         CK(ctx, cudaStreamSynchronize(s), "grid");
     }
+    return HCG_OK;
+}
+
+hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs) {
+    if (!ctx || (njobs && !jobs)) return HCG_EINVAL;
+    Guard g(ctx);
+    if (njobs == 0) return HCG_OK;
+    for (uint32_t i = 0; i < njobs; ++i) {
+        const hcg_job &j = jobs[i];
+        if (!j.field || !j.target || !j.cube) return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " incomplete");
+        if (j.field->ctx->device != ctx->device || j.target->ctx->device != ctx->device)
+            return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " lives on another device");
+        if (!j.field->d_spec) return fail(ctx, HCG_ESTATE, "job " + std::to_string(i) + ": field has no spectra");
+        if (j.field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
+        if (j.layout != HCG_LAYOUT_SAMPLE_MAJOR && j.layout != HCG_LAYOUT_CHANNEL_MAJOR)
+            return fail(ctx, HCG_EINVAL, "unknown layout");
+    }
+    CK(ctx, cudaMemsetAsync(ctx->d_stats, 0, offsetof(DevStats, invalid_input), ctx->stream), "stats reset");
+    std::vector<char> fallback;
+    std::string why;
+    cudaError_t e = grid_batch(ctx, njobs, jobs, fallback, why);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch", why);
+    for (uint32_t i = 0; i < njobs; ++i) {
+        if (!fallback[i]) continue;
+        e = grid_field(ctx, jobs[i].field, jobs[i].target, jobs[i].cube, jobs[i].layout, jobs[i].weights,
+                       HCG_ENGINE_AUTO, why);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch fallback", why);
+    }
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "grid batch");
     return HCG_OK;
 }
 

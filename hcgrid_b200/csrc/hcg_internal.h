@@ -78,12 +78,15 @@ struct hcg_context {
     cudaEvent_t evp[4] = {nullptr, nullptr, nullptr, nullptr};  // phase boundaries inside hcg_grid
     float last_ms = 0.f;
     unsigned long long entry_budget = 4ULL << 30;  // bytes of (sample, weights) entries per launch run
+    void *batch = nullptr;                          // batch engine state (hcg_batch.cu)
 };
 
 struct hcg_field {
     hcg_context *ctx = nullptr;
     uint64_t n = 0;
     hcg::HpxParams hpx = {};
+    double sphere_radius = 0, kparam0 = 0, disc_size = 0;  // kernel setup the field was built with
+    uint32_t kernel_type = 0;
     uint64_t firstring = 0, usedrings = 0;
     uint64_t *d_keys = nullptr;   // n + 1, sorted, sentinel npix
     uint32_t *d_perm = nullptr;   // sorted position -> input index
@@ -112,6 +115,9 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
                        float *d_wts, int engine, std::string &why);
 int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny, std::vector<double> &x,
                       std::vector<double> &y, std::string &why);
+cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, std::vector<char> &fallback,
+                       std::string &why);
+cudaError_t batch_release(hcg_context *ctx);
 struct SinWcs;
 int parse_sin_header(const char *header, size_t len, uint32_t &nx, uint32_t &ny, SinWcs &w, std::string &why);
 cudaError_t sin_coords_device(const SinWcs &w, uint32_t nx, uint32_t ny, double *d_x, double *d_y, cudaStream_t s);

@@ -132,6 +132,42 @@ hcg_status hcg_target_destroy(hcg_target *t);
 hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube, int layout,
                     float *weights_out, int mem, int engine);
 hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out);
+
+/* One job of a batch: a field (with spectra), a target and DEVICE output
+ * buffers (cube in `layout`, weights optional). */
+typedef struct {
+    const hcg_field *field;
+    const hcg_target *target;
+    float *cube;
+    float *weights;
+    int layout;
+} hcg_job;
+
+/* Grid many independent jobs in one pass: each phase is one persistent
+ * launch over all jobs' work items fed by a device-side queue, and the pass
+ * is a CUDA graph replayed per batch. Jobs may differ in sample count, map
+ * size, channel count and kernel (each field grids with the kernel setup it
+ * was created under). Returns when all cubes are written; each cube equals
+ * what hcg_grid writes for that job. */
+hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs);
+
+/* Serving loop with continuous batching. `lanes` contexts on `device` (the
+ * first is ctx) each replay their own batch graph on their own stream, so a
+ * batch admitted while another runs overlaps with it on the GPU. Jobs are
+ * admitted in arrival order while the sum of their footprints (bytes,
+ * caller's estimate of output + scratch) stays within hbm_budget_bytes, at
+ * most max_batch per batch. Fields and targets must be ready (their upload
+ * finished: hcg_synchronize on their context) before submission; outputs
+ * are device buffers. hcg_server_wait returns the job's status and its
+ * latency (submit -> cube written) and queueing time in seconds. */
+typedef struct hcg_server hcg_server;
+hcg_status hcg_server_create(hcg_context *ctx, int device, uint32_t lanes, uint64_t hbm_budget_bytes,
+                             uint32_t max_batch, hcg_server **out);
+hcg_status hcg_server_submit(hcg_server *server, const hcg_job *job, uint64_t footprint_bytes, uint64_t *ticket);
+hcg_status hcg_server_wait(hcg_server *server, uint64_t ticket, double *latency_s, double *queue_s);
+hcg_status hcg_server_drain(hcg_server *server);
+hcg_status hcg_server_stats(hcg_server *server, double *p50_s, double *p99_s, uint64_t *jobs, uint32_t *batches);
+hcg_status hcg_server_destroy(hcg_server *server);
 /* Upper bound (bytes) of the per-call candidate entry buffer of the
  * multi-channel engine; larger jobs are processed in runs of tile rows
  * (default 4 GiB). */
