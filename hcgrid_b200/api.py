@@ -57,6 +57,7 @@ EXPORTS = {
     "hcg_field_set_spectra": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_field_sorted": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_destroy": ([C.c_void_p], C.c_int),
+    "hcg_field_share": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
     "hcg_target_create": ([C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int,
                            C.POINTER(C.c_void_p)], C.c_int),
     "hcg_target_from_header": ([C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
@@ -344,6 +345,15 @@ class Field:
             nchan = values.shape[0]
         self.ctx._check(self.ctx.L.hcg_field_set_spectra(self.h, nchan, vp, layout, mem))
         self.nchan = nchan
+
+    def share(self) -> "Field":
+        """Another handle on this field's resident geometry, without spectra."""
+        f = Field.__new__(Field)
+        f.ctx, f.n, f.nchan = self.ctx, self.n, 0
+        h = C.c_void_p()
+        self.ctx._check(self.ctx.L.hcg_field_share(self.h, C.byref(h)))
+        f.h = h
+        return f
 
     def sorted(self):
         inf = self.ctx.info(self)

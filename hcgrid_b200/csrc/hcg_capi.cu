@@ -70,11 +70,15 @@ void healpix_params(double hpx_max_res, HpxParams &h) {
     h.resolution = sqrt(omega);
 }
 
-// Device buffers of a field (caller holds the context lock).
+// Device buffers of a field (caller holds the context lock). The sorted
+// geometry is freed with the last field that shares it.
 void release_field(hcg_field *f, cudaStream_t s) {
-    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_lut, f->d_rings, f->d_spec};
+    if (f->d_spec) cudaFreeAsync(f->d_spec, s);
+    if (f->geom_refs && --*f->geom_refs > 0) return;
+    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_lut, f->d_rings};
     for (void *p : ps)
         if (p) cudaFreeAsync(p, s);
+    delete f->geom_refs;
 }
 
 }  // namespace
@@ -158,21 +162,35 @@ hcg_status hcg_context_create(int device, void *stream, hcg_context **out) {
     return HCG_OK;
 }
 
+// A context lives until it was destroyed and every field and target made on
+// it has been released.
+static void ctx_teardown(hcg_context *ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    batch_release(ctx);
+    ctx->scratch.release(ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_stats);
+    cudaEventDestroy(ctx->ev0);
+    cudaEventDestroy(ctx->ev1);
+    for (auto &ev : ctx->evp) cudaEventDestroy(ev);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+static void ctx_release(hcg_context *ctx) {
+    if (ctx->refs.fetch_sub(1) == 1) ctx_teardown(ctx);
+}
+
 hcg_status hcg_context_destroy(hcg_context *ctx) {
     if (!ctx) return HCG_EINVAL;
     {
         Guard g(ctx);
+        if (ctx->closed) return HCG_ESTATE;
+        ctx->closed = true;
         cudaStreamSynchronize(ctx->stream);
-        batch_release(ctx);
-        ctx->scratch.release(ctx->stream);
-        cudaStreamSynchronize(ctx->stream);
-        cudaFree(ctx->d_stats);
-        cudaEventDestroy(ctx->ev0);
-        cudaEventDestroy(ctx->ev1);
-        for (auto &ev : ctx->evp) cudaEventDestroy(ev);
-        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     }
-    delete ctx;
+    ctx_release(ctx);
     return HCG_OK;
 }
 
@@ -242,6 +260,8 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
     f->kparam0 = ctx->kparams[0];
     f->disc_size = ctx->disc_size;
     f->kernel_type = ctx->kernel_type;
+    f->geom_refs = new (std::nothrow) int(1);
+    if (!f->geom_refs) { delete f; return fail(ctx, HCG_ENOMEM, "host allocation"); }
     const double *dl = lon, *db = lat, *dw = weights;
     double *tmp = nullptr;
     if (mem == HCG_MEM_HOST) {
@@ -265,6 +285,7 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
         delete f;
         return st;
     }
+    ctx->refs.fetch_add(1);
     *out = f;
     return HCG_OK;
 }
@@ -304,6 +325,20 @@ hcg_status hcg_field_sorted(const hcg_field *field, uint64_t *keys, uint32_t *pe
     return HCG_OK;
 }
 
+hcg_status hcg_field_share(const hcg_field *src, hcg_field **out) {
+    if (!src || !out) return HCG_EINVAL;
+    hcg_context *ctx = src->ctx;
+    Guard g(ctx);
+    hcg_field *f = new (std::nothrow) hcg_field(*src);
+    if (!f) return fail(ctx, HCG_ENOMEM, "host allocation");
+    f->d_spec = nullptr;
+    f->nchan = f->cstride = 0;
+    ++*f->geom_refs;
+    ctx->refs.fetch_add(1);
+    *out = f;
+    return HCG_OK;
+}
+
 hcg_status hcg_field_destroy(hcg_field *f) {
     if (!f) return HCG_EINVAL;
     hcg_context *ctx = f->ctx;
@@ -312,6 +347,7 @@ hcg_status hcg_field_destroy(hcg_field *f) {
         release_field(f, ctx->stream);
     }
     delete f;
+    ctx_release(ctx);
     return HCG_OK;
 }
 
@@ -335,6 +371,7 @@ static hcg_status make_target(hcg_context *ctx, uint32_t nx, uint32_t ny, const 
         delete t;
         return cuda_fail(ctx, e, "target upload");
     }
+    ctx->refs.fetch_add(1);
     *out = t;
     return HCG_OK;
 }
@@ -375,6 +412,7 @@ hcg_status hcg_target_from_header(hcg_context *ctx, const char *header, size_t l
         delete t;
         return cuda_fail(ctx, e, "target");
     }
+    ctx->refs.fetch_add(1);
     *out = t;
     return HCG_OK;
 }
@@ -416,6 +454,7 @@ hcg_status hcg_target_destroy(hcg_target *t) {
         if (t->d_y) cudaFreeAsync(t->d_y, ctx->stream);
     }
     delete t;
+    ctx_release(ctx);
     return HCG_OK;
 }
 

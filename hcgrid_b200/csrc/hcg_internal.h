@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -59,6 +60,8 @@ struct Scratch {
 }  // namespace hcg
 
 struct hcg_context {
+    std::atomic<int> refs{1};  // the context itself + each field and target made on it
+    bool closed = false;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -98,6 +101,7 @@ struct hcg_field {
     hcg::RingRec *d_rings = nullptr;
     float *d_spec = nullptr;      // [n][cstride], sorted
     uint32_t nchan = 0, cstride = 0;
+    int *geom_refs = nullptr;     // fields sharing the arrays above except d_spec (hcg_field_share)
 };
 
 struct hcg_target {

@@ -226,3 +226,42 @@ def block_job(shape: dict, build_values: bool = True) -> GridJob:
     if build_values:
         job.values = spectra_cpu(G, L, 0.05, rng)
     return job
+
+
+def job_work(shape: dict) -> float:
+    """Estimated multiply-adds of one job: pixels x candidates x channels
+    (candidates = density x disc area x 1.4 for the ring windows)."""
+    sig = shape["fwhm"] / 3600.0 * FWHM_TO_SIGMA
+    r = 3.0 * sig
+    dens = shape["n"] / shape["size_deg"] ** 2
+    return shape["grid"] ** 2 * math.pi * r * r * dens * 1.4 * shape["nchan"]
+
+
+def config5_requests(njobs: int = 2000, seed: int = 3, reuse: float = 0.3, max_grid: int = 2048,
+                     max_values: int = 1 << 62, max_work: float = float("inf")):
+    """Request stream of the served form: shapes drawn as in config 4 (seed
+    `seed`), a fraction `reuse` of requests re-gridding an earlier request's
+    field (same samples, new spectra). Caps, when given, redraw shapes whose
+    grid, sample-channel count or estimated work exceed them. Returns dicts
+    with the shape, the field id it uses and the seed of its spectra."""
+    rng = np.random.default_rng(seed)
+    shapes = []
+    draws = config4_shapes(nblocks=max(4 * njobs, 64), seed=seed)
+    for s in draws:
+        if s["grid"] > max_grid or s["n"] * s["nchan"] > max_values or job_work(s) > max_work:
+            continue
+        shapes.append(s)
+    out = []
+    fields = []
+    k = 0
+    for i in range(njobs):
+        if fields and rng.uniform() < reuse:
+            fid = int(rng.integers(0, len(fields)))
+            shape = dict(fields[fid])
+        else:
+            shape = dict(shapes[k % len(shapes)])
+            k += 1
+            fid = len(fields)
+            fields.append(shape)
+        out.append(dict(request=i, field=fid, shape=shape, spectra_seed=int(rng.integers(0, 2**31 - 1))))
+    return out

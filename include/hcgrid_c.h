@@ -111,6 +111,10 @@ hcg_status hcg_field_set_spectra(hcg_field *field, uint32_t nchan, const float *
  * (usedrings+1); any pointer may be NULL. Host memory. */
 hcg_status hcg_field_sorted(const hcg_field *field, uint64_t *keys, uint32_t *perm, uint32_t *lut);
 hcg_status hcg_field_destroy(hcg_field *field);
+/* A second handle on the same resident geometry (sorted samples, LUT, ring
+ * table) without spectra: new spectra on known sample positions skip the
+ * sort. The geometry is freed with the last handle. */
+hcg_status hcg_field_share(const hcg_field *field, hcg_field **out);
 
 /* Target pixel centres in degrees, indexed yy*nx + xx. */
 hcg_status hcg_target_create(hcg_context *ctx, uint32_t nx, uint32_t ny, const double *xwcs, const double *ywcs,
