@@ -71,6 +71,7 @@ EXPORTS = {
     "hcg_synchronize": ([C.c_void_p], C.c_int),
     "hcg_set_entry_budget": ([C.c_void_p, C.c_uint64], C.c_int),
     "hcg_grid_batch": ([C.c_void_p, C.c_uint32, C.c_void_p], C.c_int),
+    "hcg_grid_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_server_create": ([C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)], C.c_int),
     "hcg_server_submit": ([C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
     "hcg_server_wait": ([C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),

@@ -180,6 +180,21 @@ hcg_status hcg_set_entry_budget(hcg_context *ctx, uint64_t bytes);
 /* Wait for all work queued on the context's stream. */
 hcg_status hcg_synchronize(hcg_context *ctx);
 
+/* hcg_grid for single-channel fields without any allocation, for callers
+ * that cannot allocate device memory when they grid (a pipeline that fixed
+ * its device memory at start-up, or code running inside an open stream
+ * capture, where cudaMalloc is not allowed). No counterpart in the
+ * reference. Its per-pixel scratch is a fixed array inside the library of
+ * 131072 pixels (12 MiB, held on every GPU that loads the library until the
+ * process exits): larger targets are rejected with HCG_EINVAL. cube and
+ * weights_out (optional) are device buffers of nx*ny floats. The first call
+ * on a device looks up the array's device address; make it before any stream
+ * capture. Calls share the array, so calls whose work overlaps on the GPU
+ * race: issue them one after another. Asynchronous on the context's stream,
+ * like hcg_grid with device buffers. */
+hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube,
+                            float *weights_out);
+
 /* FITS boundary, host only, in the reference's formats (HCGrid/gmap.cpp):
  *   hcg_fits_read_samples   read_input_map (gmap.cpp:102-148): values from the
  *                           primary image (N = NAXIS1*NAXIS2 samples, NAXIS3
