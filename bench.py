@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--workload", default="config2", choices=["config2", "config1"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # reduced cases (profiling, quick checks); the headline run uses none of these
+    ap.add_argument("--samples", type=int, default=None)
+    ap.add_argument("--channels", type=int, default=None)
+    ap.add_argument("--pixels-x", type=int, default=None)
+    ap.add_argument("--field-deg", type=float, default=None)
     return ap.parse_args()
 
 
@@ -66,11 +71,20 @@ def peaks():
 # ---------------------------------------------------------------------------
 # workload
 
-def job_for(name):
+def job_for(args):
     from hcgrid_b200 import synth
-    if name == "config1":
-        return synth.config1()
-    return synth.config2()
+    kw = {}
+    if args.samples:
+        kw["n"] = args.samples
+    if args.pixels_x:
+        kw["nx"] = args.pixels_x
+    if args.workload == "config1":
+        return synth.config1(**kw)
+    if args.channels:
+        kw["nchan"] = args.channels
+    if args.field_deg:
+        kw["size_deg"] = args.field_deg
+    return synth.config2(**kw)
 
 
 def algorithmic_bytes(n, c, p):
@@ -228,7 +242,7 @@ def reduce_max(torch, dist, v):
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
-    job = job_for(args.workload)
+    job = job_for(args)
     P = job.nx * job.ny
     if args.impl == "reference":
         if rank == 0:

@@ -89,8 +89,10 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_accum(GroupArgs g, TileAr
                                                             const float *__restrict__ spec, uint32_t nchan,
                                                             uint32_t cstride, float *__restrict__ out,
                                                             uint32_t ostride, float *__restrict__ wout) {
-    tile_accum_item(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan, cstride, out, ostride, wout, T.t0 + blockIdx.x,
-                    blockIdx.y * kSlice);
+    // slices of a tile are adjacent blocks: they run together and share the
+    // tile's entries through L2
+    tile_accum_item(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan, cstride, out, ostride, wout, T.t0 + blockIdx.y,
+                    blockIdx.x * kSlice);
 }
 
 // Exclusive scan of n uint32 counts into uint64 offsets (out[n] = total),
@@ -220,7 +222,8 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         unsigned long long most = 1;
         for (uint32_t ra = 0; ra < T.nty;) {
             uint32_t rb = ra + 1;
-            while (rb < T.nty && ro[rb + 1] - ro[ra] <= budget) ++rb;
+            // a run fits the entry budget and the 65535 limit of the grid's y dimension
+            while (rb < T.nty && ro[rb + 1] - ro[ra] <= budget && (uint64_t)(rb + 1 - ra) * T.ntx <= 65535) ++rb;
             chunks.push_back({ra, rb});
             most = std::max(most, ro[rb] - ro[ra]);
             ra = rb;
@@ -255,7 +258,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             if (tiled) {
                 TileArgs Tc = T;
                 Tc.t0 = (uint64_t)ch.first * T.ntx;
-                dim3 grid((unsigned)((uint64_t)(ch.second - ch.first) * T.ntx), (f->cstride + kSlice - 1) / kSlice);
+                dim3 grid((f->cstride + kSlice - 1) / kSlice, (unsigned)((uint64_t)(ch.second - ch.first) * T.ntx));
                 k_tile_accum<<<grid, kTileThreads, smem, s>>>(gc, Tc, off, cnt, e_idx, e_w, wsum, f->d_spec,
                                                                f->nchan, f->cstride, dst, ostride, d_wts);
             } else {

@@ -553,9 +553,26 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
 // chunk; 16 threads per 2x2 group each own 4 channels of the slice, so a
 // staged value is used for 4 pixels. Output [pixel][channel].
 constexpr int kSlice = 64, kTileThreads = (kTileX / 2) * (kTileY / 2) * (kSlice / 4);
-constexpr int kStageSlots = 768;
-// Block-collective (every thread of a kTileThreads block; needs
-// kStageSlots * kSlice floats of dynamic shared memory).
+constexpr int kStageSlots = 768;              // rows of staged spectra (two buffers of kStageSlots / 2)
+constexpr int kChunk = kStageSlots / 2;
+
+// 16-byte asynchronous global -> shared copy (zero-filled when !valid).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Channel sums of one tile for one slice of kSlice channels. The tile's
+// union of candidate spectra (its slots) is staged in shared memory in
+// chunks of kChunk rows, double-buffered: while the entries of one chunk are
+// summed, the next chunk streams in through cp.async. 16 threads per 2x2
+// group each own 4 channels of the slice, so a staged value feeds 4 pixels.
+// Block-collective (every thread of a kTileThreads block; kStageSlots *
+// kSlice floats of dynamic shared memory).
 __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileArgs &T,
                                                 const unsigned long long *__restrict__ off,
                                                 const uint32_t *__restrict__ cnt,
@@ -564,7 +581,7 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
                                                 const float *__restrict__ spec, uint32_t nchan, uint32_t cstride,
                                                 float *__restrict__ out, uint32_t ostride,
                                                 float *__restrict__ wout, uint64_t tile, uint32_t c0) {
-    extern __shared__ float4 s_spec[];  // [kStageSlots][kSlice / 4]
+    extern __shared__ float4 s_spec[];  // [2][kChunk][kSlice / 4]
     __shared__ uint32_t s_ulo[kTileMaxRings], s_base[kTileMaxRings + 1];
     __syncthreads();  // shared state of a previous item is no longer read
     const int tid = threadIdx.x, q = tid & (kSlice / 4 - 1), gl = tid / (kSlice / 4);
@@ -585,9 +602,10 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
-    for (uint32_t cs = 0; cs < U; cs += kStageSlots) {
-        const uint32_t ce = min(U, cs + kStageSlots);
-        // stage rows [cs, ce): 16 threads per row, one float4 each
+    // stage rows [cs, min(U, cs + kChunk)) into buffer b: 16 threads per row
+    auto stage = [&](uint32_t cs, int b) {
+        const uint32_t ce = min(U, cs + kChunk);
+        float4 *dst = s_spec + (size_t)b * kChunk * (kSlice / 4);
         for (uint32_t i = tid; i < (ce - cs) * (kSlice / 4); i += kTileThreads) {
             uint32_t row = i / (kSlice / 4), part = i % (kSlice / 4);
             uint32_t slot = cs + row;
@@ -598,30 +616,61 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
             }
             uint32_t idx = s_ulo[lo] + (slot - s_base[lo]);
             uint32_t c = c0 + 4 * part;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (c < cstride) v = __ldg(reinterpret_cast<const float4 *>(spec + (uint64_t)idx * cstride + c));
-            s_spec[row * (kSlice / 4) + part] = v;
+            bool ok = c < cstride;
+            const float *src = spec + (uint64_t)idx * cstride + (ok ? c : 0);
+            cp_async16(dst + row * (kSlice / 4) + part, src, ok);
+        }
+        cp_async_commit();
+    };
+    const uint32_t nchunks = (U + kChunk - 1) / kChunk;
+    if (nchunks > 0) stage(0, 0);
+    for (uint32_t k = 0; k < nchunks; ++k) {
+        const uint32_t cs = k * kChunk, ce = min(U, cs + kChunk);
+        if (k + 1 < nchunks) {
+            stage(cs + kChunk, (k + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
-        for (; e + 4 <= e_end; e += 4) {
-            uint32_t sl[4];
-            float4 w[4];
+        const float4 *buf = s_spec + (size_t)(k & 1) * kChunk * (kSlice / 4);
+        // entries four at a time, the next four loaded while these are summed
+        uint32_t sl[4], nsl[4];
+        float4 w[4], nw[4];
+        bool have = e + 4 <= e_end;
+        if (have) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                sl[u] = __ldg(e_slot + e + u);
-                w[u] = __ldg(e_w + e + u);
+                nsl[u] = __ldg(e_slot + e + u);
+                nw[u] = __ldg(e_w + e + u);
+            }
+        }
+        while (have) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                sl[u] = nsl[u];
+                w[u] = nw[u];
             }
             if (sl[3] >= ce) break;
+            e += 4;
+            have = e + 4 <= e_end;
+            if (have) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    nsl[u] = __ldg(e_slot + e + u);
+                    nw[u] = __ldg(e_w + e + u);
+                }
+            }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const float4 sv = s_spec[(sl[u] - cs) * (kSlice / 4) + q];
+                const float4 sv = buf[(sl[u] - cs) * (kSlice / 4) + q];
                 const float wv[4] = {w[u].x, w[u].y, w[u].z, w[u].w};
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    acc[k].x = fmaf(wv[k], sv.x, acc[k].x);
-                    acc[k].y = fmaf(wv[k], sv.y, acc[k].y);
-                    acc[k].z = fmaf(wv[k], sv.z, acc[k].z);
-                    acc[k].w = fmaf(wv[k], sv.w, acc[k].w);
+                for (int kk = 0; kk < 4; ++kk) {
+                    acc[kk].x = fmaf(wv[kk], sv.x, acc[kk].x);
+                    acc[kk].y = fmaf(wv[kk], sv.y, acc[kk].y);
+                    acc[kk].z = fmaf(wv[kk], sv.z, acc[kk].z);
+                    acc[kk].w = fmaf(wv[kk], sv.w, acc[kk].w);
                 }
             }
         }
@@ -629,17 +678,17 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
             uint32_t sl = __ldg(e_slot + e);
             if (sl >= ce) break;
             const float4 w = __ldg(e_w + e);
-            const float4 sv = s_spec[(sl - cs) * (kSlice / 4) + q];
+            const float4 sv = buf[(sl - cs) * (kSlice / 4) + q];
             const float wv[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                acc[k].x = fmaf(wv[k], sv.x, acc[k].x);
-                acc[k].y = fmaf(wv[k], sv.y, acc[k].y);
-                acc[k].z = fmaf(wv[k], sv.z, acc[k].z);
-                acc[k].w = fmaf(wv[k], sv.w, acc[k].w);
+            for (int kk = 0; kk < 4; ++kk) {
+                acc[kk].x = fmaf(wv[kk], sv.x, acc[kk].x);
+                acc[kk].y = fmaf(wv[kk], sv.y, acc[kk].y);
+                acc[kk].z = fmaf(wv[kk], sv.z, acc[kk].z);
+                acc[kk].w = fmaf(wv[kk], sv.w, acc[kk].w);
             }
         }
-        __syncthreads();
+        __syncthreads();  // buffer k & 1 is restaged at iteration k + 1
     }
     if (!gvalid) return;
     const uint32_t c = c0 + 4 * q;

@@ -172,11 +172,14 @@ def test_invalid_inputs_are_rejected(ctx):
     with pytest.raises(api.HcgError) as e:
         ctx.grid(f, t)  # no spectra yet
     assert e.value.status == 7
+    # a field grids with the kernel set up when it was created: GAUSS2D is
+    # accepted by the setup (as in the reference) but not gridded
     kp = np.array([0.02, 0.02, 0.0])
     ctx.prepare_grid_kernel(api.GAUSS2D, kp, 0.06, 0.01)
-    f.set_spectra(np.ones(3, np.float32))
+    f2 = ctx.field(lon, np.array([10.0, 10.05, 10.1]))
+    f2.set_spectra(np.ones(3, np.float32))
     with pytest.raises(api.HcgError) as e:
-        ctx.grid(f, t)
+        ctx.grid(f2, t)
     assert e.value.status == 6
 
 
