@@ -49,9 +49,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config1"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config5"])
+    ap.add_argument("--jobs", type=int, default=200, help="config5: requests in the stream (the full form has 2000)")
+    ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--engine", default="fp32", choices=list(ENGINES),
+                    help="channel-sum engine: FP32 CUDA cores or tensor cores with a 16-bit hi/lo split")
     # reduced cases (profiling, quick checks); the headline run uses none of these
     ap.add_argument("--samples", type=int, default=None)
     ap.add_argument("--channels", type=int, default=None)
@@ -60,12 +64,28 @@ def parse():
     return ap.parse_args()
 
 
+ENGINES = {"fp32": 1, "tc-f16": 3, "tc-bf16": 2}
+ENGINE_TEXT = {"fp32": "FP32 CUDA-core channel sums, FP64 geometry",
+               "tc-f16": "tcgen05 channel sums, compensated FP16 hi/lo (3 products, FP32 accumulate), FP64 geometry",
+               "tc-bf16": "tcgen05 channel sums, compensated BF16 hi/lo (3 products, FP32 accumulate), FP64 geometry"}
+
+
 def peaks():
     try:
         d = json.load(open(MEASURED))
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def tensor_peak():
+    """Dense bf16 TFLOP/s (f16 runs at the same rate): the burst figure, for
+    a kernel timed on its own."""
+    try:
+        d = json.load(open(MEASURED))
+        return float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
 
 
 # ---------------------------------------------------------------------------
@@ -239,8 +259,194 @@ def reduce_max(torch, dist, v):
     return float(t.item())
 
 
+# ---------------------------------------------------------------------------
+# served form (config 5): request stream through hcg_server vs plain per-call
+
+def device_block_spectra(lon_d, lat_d, shape, nchan, seed, torch, dev):
+    """[n][nchan] float32 spectra of one request on the device: 20 Gaussian
+    sources of the block's field with seeded line profiles, plus N(0, 0.05)."""
+    from hcgrid_b200 import synth
+    rng = np.random.default_rng(seed)
+    src = synth.make_sources(20, shape["ra"], shape["dec"], shape["size_deg"], rng)
+    ra = torch.tensor(src.ra, device=dev)
+    dec = torch.tensor(src.dec, device=dev)
+    amp = torch.tensor(src.amp, device=dev)
+    sig = torch.tensor(src.sigma_deg, device=dev)
+    c0 = rng.uniform(0.1, 0.9, len(src.amp)) * nchan
+    w = rng.uniform(0.01, 0.05, len(src.amp)) * nchan
+    ch = np.arange(nchan)
+    L = torch.tensor(np.exp(-((ch[None, :] - c0[:, None]) ** 2) / (2.0 * w[:, None] ** 2)), device=dev,
+                     dtype=torch.float32)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    n = lon_d.shape[0]
+    S = torch.empty((n, nchan), dtype=torch.float32, device=dev)
+    step = max(1, (1 << 26) // max(nchan, 1))
+    for i in range(0, n, step):
+        lo, la = lon_d[i:i + step, None], lat_d[i:i + step, None]
+        dx = torch.remainder(lo - ra[None, :] + 180.0, 360.0) - 180.0
+        dx = dx * torch.cos(torch.deg2rad(dec))[None, :]
+        dy = la - dec[None, :]
+        G = (amp[None, :] * torch.exp(-(dx * dx + dy * dy) / (2.0 * sig[None, :] ** 2))).float()
+        torch.matmul(G, L, out=S[i:i + step])
+        S[i:i + step].add_(torch.randn((G.shape[0], nchan), generator=gen, device=dev), alpha=0.05)
+    return S
+
+
+def served_main(args):
+    """Config 5: a stream of gridding requests with config-4 shapes (seed 3),
+    30% of them re-gridding an earlier request's field with new spectra.
+    Fields (sorted samples, ring LUT) and targets stay resident; each request
+    brings its spectra (generated on the device) and output buffers.
+
+    served: requests go through hcg_server (continuous batching over 2 lanes,
+    persistent batch kernels, tensor-core channel sums on FP16 hi/lo spectra,
+    HBM admission budget). Capacity = closed-loop throughput; then Poisson
+    arrivals at 80% of it give p50/p99 latency (submit -> cube written).
+    plain: the same requests one hcg_grid call at a time on the FP32 engine.
+    Both time the gridding only; spectra generation and upload are outside
+    the latency (they overlap the server's work in the served run)."""
+    import torch
+    from hcgrid_b200 import api, synth
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    api.load(build_if_missing=True)
+    budget = int(args.hbm_budget_gb * (1 << 30))
+    reqs = synth.config5_requests(njobs=args.jobs, seed=3, reuse=0.3, max_grid=2048, max_values=1 << 29,
+                                  max_cube=1 << 30)
+    ctx = api.Context(0)
+    # resident fields and targets (built once, outside the timed runs)
+    base = {}
+    for r in reqs:
+        fid = r["field"]
+        if fid in base:
+            continue
+        sh = r["shape"]
+        rng = np.random.default_rng(sh["seed"])
+        lon, lat = synth.raster_scan(sh["n"], sh["ra"], sh["dec"], sh["size_deg"], 2.0, rng)
+        sigma = sh["fwhm"] / 3600.0 * synth.FWHM_TO_SIGMA
+        ctx.prepare_grid_kernel(api.GAUSS1D, np.array([sigma, 0.0, 0.0]), 3.0 * sigma, sigma / 2.0)
+        f = ctx.field(lon, lat)
+        hdr = synth.sin_header(sh["grid"], sh["grid"], sh["ra"], sh["dec"], sh["size_deg"] / sh["grid"])
+        t = ctx.target_from_header(hdr)
+        base[fid] = (f, t, torch.from_numpy(lon).to(dev), torch.from_numpy(lat).to(dev))
+    ctx.synchronize()
+
+    def work(r):
+        return r["shape"]["n"] * r["shape"]["nchan"]
+
+    def footprint(r, split):
+        sh = r["shape"]
+        P = sh["grid"] ** 2
+        return sh["n"] * sh["nchan"] * 4 + P * (sh["nchan"] + 1) * 4 + P * 160
+
+    def prepare(r, tc):
+        sh = r["shape"]
+        f0, t, lon_d, lat_d = base[r["field"]]
+        S = device_block_spectra(lon_d, lat_d, sh, sh["nchan"], r["spectra_seed"], torch, dev)
+        torch.cuda.synchronize(dev)
+        f = f0.share()
+        f.set_spectra(S)
+        del S
+        if tc and sh["nchan"] > 1:
+            f.split_spectra(api.ENGINE_TC_F16, keep_fp32=False)
+        P = t.nx * t.ny
+        cube = torch.empty((P * sh["nchan"],), dtype=torch.float32, device=dev)
+        wts = torch.empty((P,), dtype=torch.float32, device=dev)
+        ctx.synchronize()
+        return f, t, cube, wts
+
+    # plain per-call FP32 path
+    plain_lat = []
+    t_plain = 0.0
+    for r in reqs:
+        f, t, cube, wts = prepare(r, tc=False)
+        t0 = time.perf_counter()
+        ctx.grid(f, t, cube, wts, engine=api.ENGINE_FP32)
+        ctx.synchronize()
+        dt = time.perf_counter() - t0
+        plain_lat.append(dt)
+        t_plain += dt
+        f.close()
+        del cube, wts
+    tot_work = sum(work(r) for r in reqs)
+
+    def run_served(arrivals):
+        srv = api.Server(ctx, lanes=2, hbm_budget=budget, max_batch=64)
+        inflight = []  # (ticket, bytes, field, buffers)
+        used = 0
+        lats, queues = [], []
+        t_start = time.perf_counter()
+        for i, r in enumerate(reqs):
+            fp = footprint(r, True)
+            while inflight and used + fp > budget:
+                tk, b, f, bufs = inflight.pop(0)
+                lt, q = srv.wait(tk)
+                lats.append(lt)
+                queues.append(q)
+                used -= b
+                f.close()
+            if arrivals is not None:
+                delay = t_start + arrivals[i] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+            f, t, cube, wts = prepare(r, tc=True)
+            tk = srv.submit(f, t, cube, wts, api.SAMPLE_MAJOR, footprint=fp)
+            inflight.append((tk, fp, f, (cube, wts)))
+            used += fp
+        for tk, b, f, bufs in inflight:
+            lt, q = srv.wait(tk)
+            lats.append(lt)
+            queues.append(q)
+            f.close()
+        makespan = time.perf_counter() - t_start
+        st = srv.stats()
+        srv.close()
+        return makespan, lats, queues, st
+
+    run_served(None)  # warm-up: captures the lanes' batch graphs
+    makespan, lats_cl, _, st_cl = run_served(None)
+    capacity = tot_work / makespan
+    rate = 0.8 * len(reqs) / makespan  # requests per second at 80% of capacity
+    rng = np.random.default_rng(3)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    arrivals -= arrivals[0]
+    makespan_p, lats, queues, st = run_served(arrivals)
+    pct = lambda v, q: float(np.percentile(np.asarray(v), q))
+    out = {"metric": METRIC, "value": capacity, "unit": UNIT, "n_gpus": 1, "steps": len(reqs), "warmup": 1,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp16 hi/lo tensor-core channel sums (FP64 geometry)",
+           "data": "synthetic (seeded config-5 request stream, hcgrid_b200/synth.py)",
+           "config": {"workload": "config5: %d requests, config-4 shapes (seed 3), 30%% field reuse, HBM budget "
+                                  "%.0f GB" % (len(reqs), args.hbm_budget_gb),
+                      "unique_fields": len(base), "total_sample_channels": tot_work,
+                      "caps": "grid <= 2048, samples x channels <= 2^29, grid^2 x channels <= 2^30",
+                      "engine": "served: hcg_server (2 lanes, batch graphs, tensor cores FP16 hi/lo); "
+                                "plain: hcg_grid FP32 engine per call"},
+           "served": {"capacity": capacity, "closed_loop_s": round(makespan, 4),
+                      "p50_s_closed_loop": pct(lats_cl, 50), "p99_s_closed_loop": pct(lats_cl, 99),
+                      "poisson_rate_per_s": round(rate, 3), "throughput_at_80pct": tot_work / makespan_p,
+                      "p50_s": pct(lats, 50), "p99_s": pct(lats, 99), "queue_p99_s": pct(queues, 99),
+                      "batches": st["batches"]},
+           "plain": {"value": tot_work / t_plain, "p50_s": pct(plain_lat, 50), "p99_s": pct(plain_lat, 99),
+                     "total_s": round(t_plain, 4)},
+           "served_over_plain": round(capacity / (tot_work / t_plain), 3),
+           "gpu_launches": None, "e2e": None, "cpu_baseline": None}
+    print(json.dumps(out))
+    for f, t, _, _ in base.values():
+        f.close()
+        t.close()
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.workload == "config5":
+        if args.impl == "ours":
+            return served_main(args)
+        print(json.dumps({"impl": "reference", "unavailable": "the served form runs the B200 request loop; the "
+                          "reference's CPU path is timed on config2 and config1"}))
+        return
     world, rank, local = dist_setup(args)
     job = job_for(args)
     P = job.nx * job.ny
@@ -284,8 +490,11 @@ def main():
         lat_d = torch.from_numpy(job.lat).to(dev)
         S = device_spectra(job, torch, dev)
     stream.synchronize()
+    engine = ENGINES[args.engine]
     field = ctx.field(lon_d, lat_d)
     field.set_spectra(S)
+    if engine != api.ENGINE_FP32 and job.nchan > 1:
+        field.split_spectra(engine, keep_fp32=False)
     target = ctx.target_from_header(job.header)
     ctx.synchronize()
     S_host = None
@@ -296,10 +505,10 @@ def main():
     torch.cuda.empty_cache()
     cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
     wts = torch.empty(P, dtype=torch.float32, device=dev)
-    launches_per_step = 2 if job.nchan == 1 else 5
+    launches_per_step = 2 if job.nchan == 1 else 7  # prep, tile rings, count, scan, row offsets, weights, sums
 
     for _ in range(args.warmup):
-        ctx.grid(field, target, cube, wts)
+        ctx.grid(field, target, cube, wts, engine=engine)
     ctx.synchronize()
     stats = ctx.stats()
 
@@ -314,7 +523,7 @@ def main():
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         for _ in range(args.steps):
-            ctx.grid(field, target, cube, wts)
+            ctx.grid(field, target, cube, wts, engine=engine)
             st = ctx.stats()  # phase times of this step (device events on the launching stream)
             for i in range(4):
                 phase_ms[i].append(st.ms_phase[i])
@@ -331,8 +540,10 @@ def main():
     st = ctx.stats()
 
     # dominant kernel and its roofline
-    phase_names = ["pixel setup", "candidate count+scan", "FP64 weights (k_group)", "channel sums (k_group_accum)"]
-    kernels = ["k_pixel_prep", "k_group<true>+k_scan_offsets", "k_group<false>", "k_group_accum"]
+    tc = engine != api.ENGINE_FP32 and job.nchan > 1
+    phase_names = ["pixel setup", "candidate count+scan", "FP64 weights (k_group)",
+                   "channel sums (k_tile_tc)" if tc else "channel sums (k_tile_accum)"]
+    kernels = ["k_pixel_prep", "k_group<true>+k_scan_offsets", "k_group<false>", "k_tile_tc" if tc else "k_tile_accum"]
     if job.nchan == 1:
         phase_names[3] = "single-channel gridding (k_grid_1chan)"
         kernels[3] = "k_grid_1chan"
@@ -360,6 +571,15 @@ def main():
                 "phase_ms": {n: round(a, 3) for n, a in zip(phase_names, avg)},
                 "whole_step_hbm_frac": round(algorithmic_bytes(job.n, job.nchan, P) / (ms_per_step * 1e-3) / 1e9 / peak, 4),
                 "pairs_within": int(st.pairs_within), "pairs_candidate": int(st.pairs_candidate)}
+    if tc and dom == 3:
+        tpk, tkind = tensor_peak()
+        tflops = 2.0 * st.tc_macs / (avg[3] * 1e-3) / 1e12
+        roofline["tensor"] = {"achieved": round(tflops, 1), "peak": tpk, "unit": "TFLOP/s",
+                              "frac": round(tflops / tpk, 4), "issued_macs": int(st.tc_macs),
+                              "useful_macs": int(st.pairs_within) * job.nchan,
+                              "peak_source": tkind + " (MEASURED_PEAKS.json bf16_tflops, burst)"}
+        if tflops / tpk > roofline["frac"]:
+            roofline["bound"] = "tensor"
 
     # end to end through the C ABI from host buffers
     e2e = None
@@ -374,8 +594,10 @@ def main():
             t0 = time.perf_counter()
             f2 = ctx.field(lon_h, lat_h)
             f2.set_spectra(S_host)
+            if tc:
+                f2.split_spectra(engine, keep_fp32=False)
             t2 = ctx.target_from_header(job.header)
-            ctx.grid(f2, t2, cube_h, w_h)
+            ctx.grid(f2, t2, cube_h, w_h, engine=engine)
             dt = time.perf_counter() - t0
             f2.close()
             t2.close()
@@ -386,7 +608,8 @@ def main():
         d2h = 4 * P * job.nchan + 4 * P
         e2e = {"value": work * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "s_per_step": round(t_e2e, 4),
-               "path": "hcg_field_create + hcg_field_set_spectra + hcg_target_from_header + hcg_grid, host pinned"}
+               "path": "hcg_field_create + hcg_field_set_spectra%s + hcg_target_from_header + hcg_grid, host pinned"
+                       % (" + hcg_field_split_spectra" if tc else "")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -406,7 +629,7 @@ def main():
                           "samples": job.n, "channels": job.nchan, "pixels": P, "nside": ctx.info(field).nside,
                           "parallelism": "replica per GPU" if world > 1 else "single GPU",
                           "l2": "inputs larger than L2 (spectra %.1f GB), no flush" % (4 * job.n * job.nchan / 1e9),
-                          "engine": "FP32 CUDA-core channel sums, FP64 geometry"},
+                          "engine": ENGINE_TEXT[args.engine] if job.nchan > 1 else ENGINE_TEXT["fp32"]},
                "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,
                "e2e": e2e, "cpu_baseline": cpu}
         print(json.dumps(out))

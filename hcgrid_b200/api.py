@@ -17,7 +17,7 @@ from . import build as _build
 GAUSS1D, GAUSS2D, TAPERED_SINC = 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
 SAMPLE_MAJOR, CHANNEL_MAJOR = 0, 1
-ENGINE_AUTO, ENGINE_FP32 = 0, 1
+ENGINE_AUTO, ENGINE_FP32, ENGINE_TC_BF16, ENGINE_TC_F16 = 0, 1, 2, 3
 
 STATUS = {0: "HCG_OK", 1: "HCG_EINVAL", 2: "HCG_ENOMEM", 3: "HCG_ETIMEOUT", 4: "HCG_EDEVICE", 5: "HCG_EIO",
           6: "HCG_EUNSUPPORTED", 7: "HCG_ESTATE"}
@@ -42,7 +42,8 @@ class Info(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("pairs_candidate", C.c_uint64), ("pairs_within", C.c_uint64), ("ring_skips", C.c_uint64),
-                ("hard_roundings", C.c_uint64), ("ms_total", C.c_double), ("ms_phase", C.c_double * 4)]
+                ("hard_roundings", C.c_uint64), ("ms_total", C.c_double), ("ms_phase", C.c_double * 4),
+                ("tc_macs", C.c_uint64)]
 
 
 EXPORTS = {
@@ -55,6 +56,7 @@ EXPORTS = {
     "hcg_field_create": ([C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                           C.POINTER(C.c_void_p)], C.c_int),
     "hcg_field_set_spectra": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_field_split_spectra": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_field_sorted": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_destroy": ([C.c_void_p], C.c_int),
     "hcg_field_share": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
@@ -346,6 +348,10 @@ class Field:
             nchan = values.shape[0]
         self.ctx._check(self.ctx.L.hcg_field_set_spectra(self.h, nchan, vp, layout, mem))
         self.nchan = nchan
+
+    def split_spectra(self, engine: int = ENGINE_TC_F16, keep_fp32: bool = True):
+        """16-bit hi/lo copy of the spectra for a tensor-core engine."""
+        self.ctx._check(self.ctx.L.hcg_field_split_spectra(self.h, engine, 1 if keep_fp32 else 0))
 
     def share(self) -> "Field":
         """Another handle on this field's resident geometry, without spectra."""

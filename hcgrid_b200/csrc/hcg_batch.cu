@@ -22,6 +22,7 @@
 
 #include "hcg_internal.h"
 #include "hcg_kernels.cuh"
+#include "hcg_tc.cuh"
 
 namespace hcg {
 namespace {
@@ -41,14 +42,15 @@ struct JobDesc {
     double *wsum;
     PixPrep *prep;
     // first item of this job in each phase's item space
-    unsigned long long pix_base, grp_base, tile_base, acc_base, c1_base;
+    unsigned long long pix_base, grp_base, tile_base, acc_base, c1_base, tc_base;
+    TcJob tc;  // tensor-core engine arguments (jobs whose field holds split spectra)
 };
 
-enum { Q_TILE = 0, Q_COUNT, Q_GEOM, Q_ACC, Q_C1, Q_N };
+enum { Q_TILE = 0, Q_COUNT, Q_GEOM, Q_ACC, Q_C1, Q_TC, Q_N };
 
 struct BatchHdr {
     uint32_t njobs;
-    unsigned long long tot_pix, tot_grp, tot_tile, tot_acc, tot_c1;
+    unsigned long long tot_pix, tot_grp, tot_tile, tot_acc, tot_c1, tot_tc;
     unsigned long long head[Q_N];
     unsigned long long entry_cap;      // entries the pool holds
     unsigned long long entries_needed; // total entries of the batch (set by the scan)
@@ -119,9 +121,13 @@ __global__ void __launch_bounds__(256) kb_group(BatchHdr *H, const JobDesc *__re
         uint64_t grp = it - J.grp_base;
         if (!COUNT) {
             // the pool must hold this group's entries; otherwise skip and report
+            // (no entries recorded: the pass is replayed once the pool has grown)
             unsigned long long end = J.off[grp] + J.cap[grp];
             if (end > H->entry_cap) {
-                if ((threadIdx.x & 31) == 0) atomicAdd(&H->pool_overflow, 1ULL);
+                if ((threadIdx.x & 31) == 0) {
+                    J.cnt[grp] = 0;
+                    atomicAdd(&H->pool_overflow, 1ULL);
+                }
                 continue;
             }
         }
@@ -159,6 +165,7 @@ __global__ void __launch_bounds__(1024) kb_scan(BatchHdr *H) {
 }
 
 __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobDesc *__restrict__ jobs) {
+    if (H->pool_overflow) return;  // entries incomplete: this pass is replayed after the pool grows
     for (;;) {
         unsigned long long it = block_fetch(H, Q_ACC);
         if (it >= H->tot_acc) return;
@@ -170,6 +177,34 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
         tile_accum_item(J.g, J.T, J.off, J.cnt, H->e_idx, H->e_w, J.wsum, J.spec, J.nchan, J.cstride, J.out,
                         J.ostride, J.wout, tile, c0);
     }
+}
+
+// Tensor-core channel sums: one CTA per SM takes (job, channel block, tile)
+// items from the queue; barrier phases and TMEM persist across items.
+__global__ void __launch_bounds__(kTcThreads, 1)
+    kb_tc(BatchHdr *H, const JobDesc *__restrict__ jobs, const void *zero_page, unsigned long long *timeouts,
+          unsigned long long *macs) {
+    __shared__ TcShared S;
+    if (H->pool_overflow) return;  // entries incomplete: this pass is replayed after the pool grows
+    tc_setup(S);
+    uint32_t gk = 0, itn = 0;
+    for (;;) {
+        if (threadIdx.x == 0) S.item = S.abort ? ~0ULL : atomicAdd(&H->head[Q_TC], 1ULL);
+        __syncthreads();
+        const unsigned long long it = S.item;
+        if (it >= H->tot_tc) break;
+        const int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.tc_base; });
+        const TcJob &J = jobs[j].tc;
+        const unsigned long long local = it - jobs[j].tc_base;
+        const uint64_t ntiles = (uint64_t)J.T.ntx * J.T.nty;
+        const uint64_t tile = local % ntiles;  // tiles fastest: neighbours share staged samples in L2
+        tc_load_rings(S, J.T, tile);
+        __syncthreads();
+        tc_item(S, J, tile, (uint32_t)(local / ntiles), gk, itn, zero_page, timeouts, macs);
+        ++itn;
+        __syncthreads();  // every role is done with the item's ring table and accumulator
+    }
+    tc_teardown(S, gk, timeouts);
 }
 
 __global__ void __launch_bounds__(256) kb_1chan(BatchHdr *H, const JobDesc *__restrict__ jobs) {
@@ -184,6 +219,8 @@ __global__ void __launch_bounds__(256) kb_1chan(BatchHdr *H, const JobDesc *__re
 
 }  // namespace
 
+static bool batch_uses_tc(const hcg_field *f) { return auto_engine(f) != HCG_ENGINE_FP32; }
+
 // Batch state kept by a context: device header + job table, scratch and the
 // captured graph.
 struct BatchState {
@@ -196,6 +233,10 @@ struct BatchState {
     int nsm = 0;
     void *scratch[8] = {};
     size_t scratch_size[8] = {};
+    CUtensorMap *d_maps = nullptr, *h_maps = nullptr;  // 2 per job: hi, lo
+    unsigned long long *d_jovf = nullptr, *h_jovf = nullptr;  // per job: tiles beyond the ring table
+    uint32_t map_cap = 0;
+    void *zero_page = nullptr;  // the tensor-core engine's zero page
     unsigned long long entry_cap = 0;
 };
 
@@ -220,6 +261,7 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     const int smem = kStageSlots * kSlice * (int)sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(kb_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
+    if ((e = tc_set_smem((const void *)kb_tc)) != cudaSuccess) return e;
     cudaGraph_t graph;
     if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
     cudaMemsetAsync(&B.d_hdr->head[0], 0, sizeof(B.d_hdr->head), s);
@@ -231,6 +273,8 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     kb_scan<<<1, 1024, 0, s>>>(B.d_hdr);
     kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
     kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
+    kb_tc<<<n, kTcThreads, kTcSmem, s>>>(B.d_hdr, B.d_jobs, B.zero_page, &ctx->d_stats->timeouts,
+                                          &ctx->d_stats->tc_macs);
     kb_1chan<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (ce != cudaSuccess) return ce;
@@ -247,6 +291,11 @@ cudaError_t batch_release(hcg_context *ctx) {
         if (p) cudaFreeAsync(p, ctx->stream);
     if (B->d_hdr) cudaFreeAsync(B->d_hdr, ctx->stream);
     if (B->d_jobs) cudaFreeAsync(B->d_jobs, ctx->stream);
+    if (B->d_maps) cudaFreeAsync(B->d_maps, ctx->stream);
+    if (B->zero_page) cudaFreeAsync(B->zero_page, ctx->stream);
+    if (B->h_maps) cudaFreeHost(B->h_maps);
+    if (B->d_jovf) cudaFreeAsync(B->d_jovf, ctx->stream);
+    if (B->h_jovf) cudaFreeHost(B->h_jovf);
     if (B->h_hdr) cudaFreeHost(B->h_hdr);
     if (B->h_jobs) cudaFreeHost(B->h_jobs);
     delete B;
@@ -264,7 +313,12 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         BatchState *B = new BatchState();
         cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
         if ((e = cudaMallocAsync(&B->d_hdr, sizeof(BatchHdr), s)) != cudaSuccess ||
-            (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess) {
+            (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess ||
+            (e = cudaMallocAsync(&B->zero_page, 2 * kAHalf, s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(B->zero_page, 0, 2 * kAHalf, s)) != cudaSuccess) {
+            if (B->d_hdr) cudaFreeAsync(B->d_hdr, s);
+            if (B->h_hdr) cudaFreeHost(B->h_hdr);
+            if (B->zero_page) cudaFreeAsync(B->zero_page, s);
             delete B;
             return e;
         }
@@ -274,12 +328,23 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
     if (njobs > B.job_cap) {
         if (B.d_jobs) cudaFreeAsync(B.d_jobs, s);
         if (B.h_jobs) cudaFreeHost(B.h_jobs);
+        if (B.d_jovf) cudaFreeAsync(B.d_jovf, s);
+        if (B.h_jovf) cudaFreeHost(B.h_jovf);
         B.job_cap = std::max<uint32_t>(njobs, 64);
         if ((e = cudaMallocAsync(&B.d_jobs, B.job_cap * sizeof(JobDesc), s)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jobs, B.job_cap * sizeof(JobDesc))) != cudaSuccess) return e;
+        if ((e = cudaMallocAsync(&B.d_jovf, B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&B.h_jovf, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
+    }
+    if (2 * njobs > B.map_cap) {
+        if (B.d_maps) cudaFreeAsync(B.d_maps, s);
+        if (B.h_maps) cudaFreeHost(B.h_maps);
+        B.map_cap = std::max<uint32_t>(2 * njobs, 128);
+        if ((e = cudaMallocAsync(&B.d_maps, B.map_cap * sizeof(CUtensorMap), s)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&B.h_maps, B.map_cap * sizeof(CUtensorMap))) != cudaSuccess) return e;
     }
     // item spaces and scratch sizes
-    unsigned long long pix = 0, grp = 0, tile = 0, acc = 0, c1 = 0;
+    unsigned long long pix = 0, grp = 0, tile = 0, acc = 0, c1 = 0, tcn = 0;
     std::vector<JobDesc> J(njobs);
     for (uint32_t i = 0; i < njobs; ++i) {
         const hcg_field *f = jobs[i].field;
@@ -297,16 +362,26 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         d.T.ntx = (t->nx + kTileX - 1) / kTileX;
         d.T.nty = (t->ny + kTileY - 1) / kTileY;
         uint64_t ntiles = (f->nchan > 1) ? (uint64_t)d.T.ntx * d.T.nty : 0;
-        d.nslices = (f->cstride + kSlice - 1) / kSlice;
+        const bool tc = batch_uses_tc(f);
+        d.nslices = tc ? 0 : (f->cstride + kSlice - 1) / kSlice;
+        if (tc) {
+            d.T.pad = 8;  // ring runs as boxes of 8 samples
+            if (!tc_prepare_job(f, &B.h_maps[2 * i], &B.h_maps[2 * i + 1], d.tc)) {
+                why = "cuTensorMapEncodeTiled";
+                return cudaErrorInvalidValue;
+            }
+        }
         d.pix_base = pix;
         d.grp_base = grp;
         d.tile_base = tile;
         d.acc_base = acc;
         d.c1_base = c1;
+        d.tc_base = tcn;
         pix += P;
         grp += d.g.ngroups;
         tile += ntiles;
         acc += ntiles * d.nslices;
+        if (tc) tcn += ntiles * d.tc.ncb;
         if (f->nchan == 1) c1 += P;
     }
     void *p_prep, *p_wsum, *p_cap, *p_cnt, *p_off, *p_tiles;
@@ -348,7 +423,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             d.T.U = t_U + d.tile_base;
             d.T.ulo = t_ulo + d.tile_base * kTileMaxRings;
             d.T.base = t_base + d.tile_base * (kTileMaxRings + 1);
-            d.T.overflow = &ctx->d_stats->overflow;
+            d.T.overflow = B.d_jovf + i;
             d.X = t->d_x;
             d.Y = t->d_y;
             d.firstring = f->firstring;
@@ -360,6 +435,21 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             d.ostride = jobs[i].layout == HCG_LAYOUT_CHANNEL_MAJOR ? 0 : f->nchan;
             d.out = jobs[i].cube;
             d.wout = jobs[i].weights;
+            if (d.tc.nb) {
+                TcJob &c = d.tc;
+                c.map_hi = B.d_maps + 2 * i;
+                c.map_lo = B.d_maps + 2 * i + 1;
+                c.g = d.g;
+                c.T = d.T;
+                c.off = d.off;
+                c.cnt = d.cnt;
+                c.e_slot = (const uint32_t *)p_eidx;
+                c.e_w = (const float4 *)p_ew;
+                c.wsum = d.wsum;
+                c.out = d.out;
+                c.ostride = d.ostride;
+                c.wout = d.wout;
+            }
         }
         memcpy(B.h_jobs, J.data(), njobs * sizeof(JobDesc));
         BatchHdr &h = *B.h_hdr;
@@ -370,6 +460,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         h.tot_tile = tile;
         h.tot_acc = acc;
         h.tot_c1 = c1;
+        h.tot_tc = tcn;
         h.entry_cap = B.entry_cap;
         h.e_idx = (uint32_t *)p_eidx;
         h.e_w = (float4 *)p_ew;
@@ -378,7 +469,11 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if ((e = cudaMemcpyAsync(B.d_jobs, B.h_jobs, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, s)) !=
                 cudaSuccess ||
             (e = cudaMemcpyAsync(B.d_hdr, B.h_hdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(&ctx->d_stats->overflow, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+            (e = cudaMemsetAsync(&ctx->d_stats->overflow, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(B.d_jovf, 0, njobs * sizeof(unsigned long long), s)) != cudaSuccess)
+            return e;
+        if (tcn && (e = cudaMemcpyAsync(B.d_maps, B.h_maps, 2 * njobs * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                                        s)) != cudaSuccess)
             return e;
         if (!B.exec && (e = capture(ctx, B)) != cudaSuccess) return e;
         cudaEventRecord(ctx->ev0, s);
@@ -387,18 +482,22 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         cudaEventRecord(ctx->ev1, s);
         if ((e = cudaMemcpyAsync(B.h_hdr, B.d_hdr, sizeof(BatchHdr), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
             return e;
-        unsigned long long tile_overflow = 0;
-        if ((e = cudaMemcpyAsync(&tile_overflow, &ctx->d_stats->overflow, sizeof tile_overflow,
-                                 cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        unsigned long long timeouts = 0;
+        if ((e = cudaMemcpyAsync(&timeouts, &ctx->d_stats->timeouts, sizeof timeouts, cudaMemcpyDeviceToHost,
+                                 s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(B.h_jovf, B.d_jovf, njobs * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 s)) != cudaSuccess)
             return e;
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-        fallback.assign(njobs, 0);
-        if (tile_overflow) {
-            // some tile spans more rings than its table: those jobs' groups
-            // wrote sample indices, so re-run every multi-channel job singly
-            for (uint32_t i = 0; i < njobs; ++i)
-                if (jobs[i].field->nchan > 1) fallback[i] = 1;
+        if (timeouts) {
+            why = std::to_string(timeouts) + " tensor-core pipeline waits ran out";
+            return cudaErrorTimeout;
         }
+        // a job with a tile spanning more rings than its table wrote sample
+        // indices for that tile's groups: it is re-run on its own
+        fallback.assign(njobs, 0);
+        for (uint32_t i = 0; i < njobs; ++i)
+            if (B.h_jovf[i] && jobs[i].field->nchan > 1) fallback[i] = 1;
         if (B.h_hdr->pool_overflow == 0) return cudaSuccess;
         B.entry_cap = B.h_hdr->entries_needed + (B.h_hdr->entries_needed >> 3) + 1024;  // grow and replay once
     }

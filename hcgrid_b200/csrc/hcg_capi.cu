@@ -74,6 +74,7 @@ void healpix_params(double hpx_max_res, HpxParams &h) {
 // geometry is freed with the last field that shares it.
 void release_field(hcg_field *f, cudaStream_t s) {
     if (f->d_spec) cudaFreeAsync(f->d_spec, s);
+    free_split(f, s);
     if (f->geom_refs && --*f->geom_refs > 0) return;
     void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_lut, f->d_rings};
     for (void *p : ps)
@@ -307,9 +308,27 @@ hcg_status hcg_field_set_spectra(hcg_field *field, uint32_t nchan, const float *
         CK(ctx, cudaMemcpyAsync(tmp, values, nb, cudaMemcpyHostToDevice, s), "spectra upload");
         dv = tmp;
     }
+    free_split(field, s);  // the split, if any, described the previous spectra
     cudaError_t e = permute_spectra(ctx, field, dv, nchan, layout);
     if (tmp) cudaFreeAsync(tmp, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "spectra permute");
+    return HCG_OK;
+}
+
+hcg_status hcg_field_split_spectra(hcg_field *field, int engine, int keep_fp32) {
+    if (!field) return HCG_EINVAL;
+    hcg_context *ctx = field->ctx;
+    Guard g(ctx);
+    if (engine != HCG_ENGINE_TC_BF16 && engine != HCG_ENGINE_TC_F16)
+        return fail(ctx, HCG_EINVAL, "split engine must be HCG_ENGINE_TC_BF16 or HCG_ENGINE_TC_F16");
+    if (!field->d_spec) return fail(ctx, HCG_ESTATE, "field has no FP32 spectra (hcg_field_set_spectra)");
+    std::string why;
+    cudaError_t e = split_spectra(ctx, field, engine, why);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "spectra split", why);
+    if (!keep_fp32) {
+        cudaFreeAsync(field->d_spec, ctx->stream);
+        field->d_spec = nullptr;
+    }
     return HCG_OK;
 }
 
@@ -333,6 +352,11 @@ hcg_status hcg_field_share(const hcg_field *src, hcg_field **out) {
     if (!f) return fail(ctx, HCG_ENOMEM, "host allocation");
     f->d_spec = nullptr;
     f->nchan = f->cstride = 0;
+    f->d_xhi = f->d_xlo = nullptr;
+    f->d_xinv = nullptr;
+    f->xcpad = 0;
+    f->xfmt = 0;
+    f->xnonfinite = 0;
     ++*f->geom_refs;
     ctx->refs.fetch_add(1);
     *out = f;
@@ -464,10 +488,19 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
     Guard g(ctx);
     if (!ctx->prepared) return fail(ctx, HCG_ESTATE, "hcg_prepare_grid_kernel must come first");
     if (field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
-    if (!field->d_spec) return fail(ctx, HCG_ESTATE, "field has no spectra (hcg_field_set_spectra)");
+    if (!field->d_spec && !field->xfmt) return fail(ctx, HCG_ESTATE, "field has no spectra (hcg_field_set_spectra)");
     if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
         return fail(ctx, HCG_EINVAL, "unknown layout");
-    if (engine != HCG_ENGINE_AUTO && engine != HCG_ENGINE_FP32) return fail(ctx, HCG_EINVAL, "unknown engine");
+    if (engine < HCG_ENGINE_AUTO || engine > HCG_ENGINE_TC_F16) return fail(ctx, HCG_EINVAL, "unknown engine");
+    if (engine == HCG_ENGINE_AUTO) engine = auto_engine(field);
+    const bool tc = engine != HCG_ENGINE_FP32 && field->nchan > 1;
+    if (tc && field->xfmt != engine)
+        return fail(ctx, HCG_ESTATE, "the tensor-core engine needs hcg_field_split_spectra with the same engine");
+    if (tc && field->xnonfinite)
+        return fail(ctx, HCG_EINVAL,
+                    std::to_string(field->xnonfinite) + " non-finite spectrum values: grid with HCG_ENGINE_FP32");
+    if (!tc && !field->d_spec)
+        return fail(ctx, HCG_ESTATE, "the FP32 spectra were dropped by hcg_field_split_spectra");
     cudaStream_t s = ctx->stream;
     const size_t P = (size_t)target->nx * target->ny;
     const size_t cube_bytes = P * field->nchan * sizeof(float);
@@ -482,6 +515,12 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
     std::string why;
     cudaError_t e = grid_field(ctx, field, target, dc, layout, dw, engine, why);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "grid", why);
+    if (tc) {
+        unsigned long long to = 0;
+        CK(ctx, cudaMemcpyAsync(&to, &ctx->d_stats->timeouts, sizeof(to), cudaMemcpyDeviceToHost, s), "timeouts");
+        CK(ctx, cudaStreamSynchronize(s), "grid");
+        if (to) return fail(ctx, HCG_ETIMEOUT, std::to_string(to) + " tensor-core pipeline waits ran out");
+    }
     if (mem == HCG_MEM_HOST) {
         CK(ctx, cudaMemcpyAsync(cube, dc, cube_bytes, cudaMemcpyDeviceToHost, s), "cube download");
         if (weights_out)
@@ -500,7 +539,8 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
         if (!j.field || !j.target || !j.cube) return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " incomplete");
         if (j.field->ctx->device != ctx->device || j.target->ctx->device != ctx->device)
             return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " lives on another device");
-        if (!j.field->d_spec) return fail(ctx, HCG_ESTATE, "job " + std::to_string(i) + ": field has no spectra");
+        if (!j.field->d_spec && auto_engine(j.field) == HCG_ENGINE_FP32)
+            return fail(ctx, HCG_ESTATE, "job " + std::to_string(i) + ": field has no spectra for its engine");
         if (j.field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
         if (j.layout != HCG_LAYOUT_SAMPLE_MAJOR && j.layout != HCG_LAYOUT_CHANNEL_MAJOR)
             return fail(ctx, HCG_EINVAL, "unknown layout");
@@ -509,11 +549,12 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
     std::vector<char> fallback;
     std::string why;
     cudaError_t e = grid_batch(ctx, njobs, jobs, fallback, why);
+    if (e == cudaErrorTimeout) return fail(ctx, HCG_ETIMEOUT, why);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch", why);
     for (uint32_t i = 0; i < njobs; ++i) {
         if (!fallback[i]) continue;
         e = grid_field(ctx, jobs[i].field, jobs[i].target, jobs[i].cube, jobs[i].layout, jobs[i].weights,
-                       HCG_ENGINE_AUTO, why);
+                       auto_engine(jobs[i].field), why);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch fallback", why);
     }
     CK(ctx, cudaStreamSynchronize(ctx->stream), "grid batch");
@@ -530,6 +571,7 @@ hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out) {
     out->pairs_within = d.pairs_within;
     out->ring_skips = d.ring_skips;
     out->hard_roundings = d.hard_roundings;
+    out->tc_macs = d.tc_macs;
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) != cudaSuccess) {
         cudaGetLastError();

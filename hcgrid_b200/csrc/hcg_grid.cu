@@ -150,10 +150,12 @@ cudaError_t sin_coords_device(const SinWcs &w, uint32_t nx, uint32_t ny, double 
 
 cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t, float *d_cube, int layout,
                        float *d_wts, int engine, std::string &why) {
-    (void)engine;
+    // engine: HCG_ENGINE_FP32 or a tensor-core engine whose split the field holds
+    const bool tc = (engine == HCG_ENGINE_TC_BF16 || engine == HCG_ENGINE_TC_F16) && f->nchan > 1;
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaSuccess;
     const uint64_t P = (uint64_t)t->nx * t->ny;
+    if ((e = cudaMemsetAsync(&ctx->d_stats->timeouts, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
     PixPrep *prep = (PixPrep *)ctx->scratch.get(0, P * sizeof(PixPrep), s, e);
     if (e != cudaSuccess) return e;
     cudaEventRecord(ctx->ev0, s);
@@ -197,8 +199,9 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         unsigned long long *rowoff =
             (unsigned long long *)ctx->scratch.get(13, (T.nty + 2) * sizeof(unsigned long long), s, e);
         T.overflow = &ctx->d_stats->overflow;
+        T.pad = tc ? 8 : 1;  // the tensor-core engine loads ring runs as boxes of 8 samples
         if (e != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(T.overflow, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(T.overflow, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
         k_tile_rings<<<(unsigned)ntiles, 256, 0, s>>>(a, g, T);
         TileArgs none{};
         k_group<true><<<gblocks, 256, 0, s>>>(a, g, cap, nullptr, nullptr, nullptr, nullptr, nullptr, none);
@@ -217,6 +220,11 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             return e;
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
         const bool tiled = ro[T.nty + 1] == 0;  // every tile's ring span fits the tile table
+        if (tc && !tiled && !f->d_spec) {
+            why = "a tile spans more than " + std::to_string(kTileMaxRings) +
+                  " rings: the FP32 fallback needs the FP32 spectra";
+            return cudaErrorInvalidValue;
+        }
         const unsigned long long budget = ctx->entry_budget / (sizeof(uint32_t) + sizeof(float4));
         std::vector<std::pair<uint32_t, uint32_t>> chunks;
         unsigned long long most = 1;
@@ -255,7 +263,13 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             k_group<false><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tiled ? T : none);
             if (first) cudaEventRecord(ctx->evp[2], s);  // phase marks are exact for a single chunk
             first = false;
-            if (tiled) {
+            if (tiled && tc) {
+                TileArgs Tc = T;
+                Tc.t0 = (uint64_t)ch.first * T.ntx;
+                e = tc_accum(ctx, f, gc, Tc, (uint64_t)(ch.second - ch.first) * T.ntx, off, cnt, e_idx, e_w, wsum, dst,
+                             ostride, d_wts, why);
+                if (e != cudaSuccess) return e;
+            } else if (tiled) {
                 TileArgs Tc = T;
                 Tc.t0 = (uint64_t)ch.first * T.ntx;
                 dim3 grid((f->cstride + kSlice - 1) / kSlice, (unsigned)((uint64_t)(ch.second - ch.first) * T.ntx));

@@ -22,6 +22,8 @@ struct DevStats {
     unsigned long long hard_roundings;
     unsigned long long invalid_input;
     unsigned long long overflow;
+    unsigned long long timeouts;  // bounded device waits that ran out (tensor-core engine)
+    unsigned long long tc_macs;   // tensor-core multiply-adds issued (tensor-core engine)
 };
 
 // One HEALPix ring that holds samples, with the ring half of loc2pix
@@ -101,6 +103,12 @@ struct hcg_field {
     hcg::RingRec *d_rings = nullptr;
     float *d_spec = nullptr;      // [n][cstride], sorted
     uint32_t nchan = 0, cstride = 0;
+    // 16-bit hi/lo split of the sorted spectra for the tensor-core engine
+    uint16_t *d_xhi = nullptr, *d_xlo = nullptr;  // [n][xcpad]
+    float *d_xinv = nullptr;      // [xcpad]: 1 / (channel scale * weight scale)
+    uint32_t xcpad = 0;           // nchan rounded up to 64
+    int xfmt = 0;                 // HCG_ENGINE_TC_BF16 / HCG_ENGINE_TC_F16, 0: no split
+    unsigned long long xnonfinite = 0;  // non-finite spectrum values seen by the split
     int *geom_refs = nullptr;     // fields sharing the arrays above except d_spec (hcg_field_share)
 };
 
@@ -112,11 +120,19 @@ struct hcg_target {
 
 // Launchers (hcg_field.cu, hcg_grid.cu). All return cudaGetLastError().
 namespace hcg {
+// HCG_ENGINE_AUTO: the tensor-core engine of the field's split spectra
+// (multi-channel fields with finite spectra), else the FP32 engine.
+inline int auto_engine(const hcg_field *f) {
+    return (f->xfmt && f->nchan > 1 && f->xnonfinite == 0) ? f->xfmt : HCG_ENGINE_FP32;
+}
 cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, const double *d_lat,
                         const double *d_w, std::string &why);
 cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, uint32_t nchan, int layout);
 cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t, float *d_cube, int layout,
                        float *d_wts, int engine, std::string &why);
+// hcg_tc.cu: hi/lo split of a field's spectra; tensor-core accumulation
+cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::string &why);
+void free_split(hcg_field *f, cudaStream_t s);
 int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny, std::vector<double> &x,
                       std::vector<double> &y, std::string &why);
 cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, std::vector<char> &fallback,

@@ -222,6 +222,9 @@ __device__ __forceinline__ void grid1_item(const GridArgs &a, const float *__res
     }
 }
 
+}  // namespace
+
+// Launch arguments shared by the kernels of several translation units.
 struct GroupArgs {
     uint32_t nx, ny, gx;
     uint64_t ngroups;
@@ -233,14 +236,23 @@ struct GroupArgs {
 // ring windows is staged in shared memory by k_tile_accum. Per tile: first
 // ring, ring count (0 = no samples), union size U and, per ring j, the union
 // interval start ulo[j] and its slot base[j] in the staged list.
-constexpr int kTileX = 16, kTileY = 8, kTileMaxRings = 256;
+constexpr int kTileX = 16, kTileY = 8, kTileMaxRings = 1024;
 struct TileArgs {
     uint32_t ntx, nty;
     uint64_t t0;  // first tile of this launch
     int *r0, *nr;
     uint32_t *U, *ulo, *base;  // ulo: [tile][kTileMaxRings], base: [tile][kTileMaxRings + 1]
     unsigned long long *overflow;
+    uint32_t pad;  // ring runs take a multiple of `pad` slots (> 1: the tensor-core engine's 8-row boxes)
 };
+
+// hcg_tc.cu: tensor-core accumulation of `ntiles` tiles from T.t0, after
+// k_group emitted the entries (slot mode) and the weight sums.
+cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, const TileArgs &T, uint64_t ntiles,
+                     const unsigned long long *off, const uint32_t *cnt, const uint32_t *e_slot, const float4 *e_w,
+                     const double *wsum, float *out, uint32_t ostride, float *wout, std::string &why);
+
+namespace {
 
 // One warp per 2x2 pixel group. COUNT: number of union candidates (upper
 // bound of the entries). Otherwise: FP64 weights of every union candidate
@@ -528,6 +540,7 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
         for (int jb = 0; jb < nrt; jb += 32) {
             int j = jb + tid;
             uint32_t len = (j < nrt && s_lo[j] < s_hi[j]) ? s_hi[j] - s_lo[j] : 0;
+            if (T.pad > 1) len = (len + T.pad - 1) / T.pad * T.pad;
             uint32_t incl = len;
             for (int o = 1; o < 32; o <<= 1) {
                 uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -561,6 +574,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool va
     unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid ? 16 : 0)
                  : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>

@@ -1,0 +1,253 @@
+// Tensor-core engine, host side and the single-job launch: the hi/lo split
+// of a field's spectra and k_tile_tc, one CTA per (tile, channel block). The
+// per-tile pipeline (tcgen05 MMAs fed by TMA) is in hcg_tc.cuh.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+#include <string>
+
+#include "hcg_internal.h"
+#include "hcg_kernels.cuh"
+#include "hcg_tc.cuh"
+
+namespace hcg {
+namespace {
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_tile_tc(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, TcJob J,
+              const void *zero_page, unsigned long long *timeouts, unsigned long long *macs) {
+    __shared__ TcShared S;
+    J.map_hi = &tm_hi;
+    J.map_lo = &tm_lo;
+    const uint64_t tile = J.T.t0 + blockIdx.x;
+    tc_load_rings(S, J.T, tile);
+    tc_setup(S);  // ends with a CTA barrier
+    if (threadIdx.x == 0) {
+        sm100::prefetch_tensormap(&tm_hi);
+        sm100::prefetch_tensormap(&tm_lo);
+    }
+    uint32_t gk = 0;
+    tc_item(S, J, tile, blockIdx.y, gk, 0, zero_page, timeouts, macs);
+    tc_teardown(S, gk, timeouts);
+}
+
+// ------------------------------------------------------------ spectra split
+// Per-channel largest magnitude and the count of non-finite values.
+__global__ void k_split_amax(const float *__restrict__ spec, uint64_t n, uint32_t nchan, uint32_t cstride,
+                             uint32_t rows_per_block, unsigned int *amax_bits,
+                             unsigned long long *nonfinite) {
+    const uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ch >= nchan) return;
+    const uint64_t r0 = (uint64_t)blockIdx.y * rows_per_block;
+    const uint64_t r1 = r0 + rows_per_block < n ? r0 + rows_per_block : n;
+    unsigned int m = 0;
+    unsigned long long bad = 0;
+    for (uint64_t r = r0; r < r1; ++r) {
+        const float v = spec[r * cstride + ch];
+        if (!isfinite(v)) {
+            ++bad;
+            continue;
+        }
+        m = max(m, __float_as_uint(fabsf(v)));
+    }
+    atomicMax(amax_bits + ch, m);
+    if (bad) atomicAdd(nonfinite, bad);
+}
+
+// Channel scales: FP16 keeps |x| * scale in [2^13, 2^14); BF16 needs none.
+__global__ void k_split_scales(const unsigned int *amax_bits, uint32_t nchan, uint32_t cpad, uint32_t fmt,
+                               float wscale, float *scale, float *inv_scale) {
+    const uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ch >= cpad) return;
+    float s = 1.f;
+    if (fmt == 0 && ch < nchan) {
+        const float a = __uint_as_float(amax_bits[ch]);
+        if (a > 0.f) {
+            int ex;
+            frexpf(a, &ex);  // a = f * 2^ex, f in [0.5, 1)
+            s = ldexpf(1.f, max(-126, min(127, 14 - ex)));
+        }
+    }
+    scale[ch] = s;
+    inv_scale[ch] = 1.f / (s * wscale);  // powers of two: exact
+}
+
+// hi/lo halves, channel-blocked: element (row r, channel c) at
+// [c / 64][r][c % 64], so 8 consecutive rows of one 64-channel block are one
+// contiguous kilobyte (one TMA box row group).
+__global__ void k_split(const float *__restrict__ spec, uint64_t n, uint32_t nchan, uint32_t cstride, uint32_t cpad,
+                        uint32_t fmt, const float *__restrict__ scale, uint16_t *hi, uint16_t *lo) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= n * cpad) return;
+    const uint64_t r = i / cpad;
+    const uint32_t ch = (uint32_t)(i % cpad);
+    float v = ch < nchan ? spec[r * cstride + ch] : 0.f;
+    if (!isfinite(v)) v = 0.f;  // such fields are refused by the engine; keep the arrays finite
+    v *= scale[ch];
+    const uint16_t h = tc_to16(v, fmt);
+    const uint64_t o = ((uint64_t)(ch >> 6) * n + r) * 64 + (ch & 63);
+    hi[o] = h;
+    lo[o] = tc_to16(v - tc_from16(h, fmt), fmt);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// [cpad / 64][rows][64] 16-bit array: boxes of 64 channels x 8 rows x nb
+// channel blocks, 128-byte swizzle (each 64 x 8 slab is one MN-major atom)
+bool make_map(CUtensorMap *m, const uint16_t *base, uint64_t rows, uint32_t cpad, uint32_t nb) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {64, rows, cpad / 64};
+    cuuint64_t strides[2] = {128, (cuuint64_t)rows * 128};
+    cuuint32_t box[3] = {64, 8, nb};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, (void *)base, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+void free_split(hcg_field *f, cudaStream_t s) {
+    if (f->d_xhi) cudaFreeAsync(f->d_xhi, s);
+    if (f->d_xlo) cudaFreeAsync(f->d_xlo, s);
+    if (f->d_xinv) cudaFreeAsync(f->d_xinv, s);
+    f->d_xhi = f->d_xlo = nullptr;
+    f->d_xinv = nullptr;
+    f->xcpad = 0;
+    f->xfmt = 0;
+    f->xnonfinite = 0;
+}
+
+cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::string &why) {
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    const uint32_t fmt = fmt_engine == HCG_ENGINE_TC_BF16 ? 1u : 0u;
+    const uint32_t cpad = (f->nchan + 63) / 64 * 64;
+    const uint64_t n = f->n;
+    uint16_t *hi = nullptr, *lo = nullptr;
+    float *scale = nullptr, *inv = nullptr;
+    unsigned int *amax = nullptr;
+    unsigned long long *bad = nullptr;
+    const size_t nb = (size_t)n * cpad * sizeof(uint16_t);
+    if ((e = cudaMallocAsync(&hi, nb ? nb : 16, s)) != cudaSuccess ||
+        (e = cudaMallocAsync(&lo, nb ? nb : 16, s)) != cudaSuccess ||
+        (e = cudaMallocAsync(&scale, cpad * sizeof(float), s)) != cudaSuccess ||
+        (e = cudaMallocAsync(&inv, cpad * sizeof(float), s)) != cudaSuccess ||
+        (e = cudaMallocAsync(&amax, cpad * sizeof(unsigned int) + sizeof(unsigned long long), s)) != cudaSuccess) {
+        why = "split spectra of " + std::to_string(2 * nb) + " bytes";
+        if (hi) cudaFreeAsync(hi, s);
+        if (lo) cudaFreeAsync(lo, s);
+        if (scale) cudaFreeAsync(scale, s);
+        if (inv) cudaFreeAsync(inv, s);
+        return e;
+    }
+    bad = (unsigned long long *)(amax + cpad);  // cpad is a multiple of 64: 8-byte aligned
+    cudaMemsetAsync(amax, 0, cpad * sizeof(unsigned int) + sizeof(unsigned long long), s);
+    const float wscale = fmt ? 1.f : 32768.f;
+    if (n > 0) {
+        const uint32_t rpb = 4096;
+        dim3 grid((f->nchan + 255) / 256, (unsigned)((n + rpb - 1) / rpb));
+        k_split_amax<<<grid, 256, 0, s>>>(f->d_spec, n, f->nchan, f->cstride, rpb, amax, bad);
+    }
+    k_split_scales<<<(cpad + 255) / 256, 256, 0, s>>>(amax, f->nchan, cpad, fmt, wscale, scale, inv);
+    if (n > 0) {
+        const uint64_t tot = n * cpad;
+        k_split<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(f->d_spec, n, f->nchan, f->cstride, cpad, fmt, scale,
+                                                              hi, lo);
+    }
+    unsigned long long nonfinite = 0;
+    cudaMemcpyAsync(&nonfinite, bad, sizeof(nonfinite), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(amax, s);
+    cudaFreeAsync(scale, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) {
+        cudaFreeAsync(hi, s);
+        cudaFreeAsync(lo, s);
+        cudaFreeAsync(inv, s);
+        return e;
+    }
+    free_split(f, s);
+    f->d_xhi = hi;
+    f->d_xlo = lo;
+    f->d_xinv = inv;
+    f->xcpad = cpad;
+    f->xfmt = fmt_engine;
+    f->xnonfinite = nonfinite;
+    return cudaSuccess;
+}
+
+bool tc_prepare_job(const hcg_field *f, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J) {
+    const uint32_t nblk64 = f->xcpad / 64;
+    J.nb = nblk64 < 4 ? nblk64 : 4;
+    J.ncb = (nblk64 + J.nb - 1) / J.nb;
+    if (!make_map(map_hi, f->d_xhi, f->n, f->xcpad, J.nb) || !make_map(map_lo, f->d_xlo, f->n, f->xcpad, J.nb))
+        return false;
+    J.nchan = f->nchan;
+    J.nrows = (uint32_t)f->n;
+    J.fmt = f->xfmt == HCG_ENGINE_TC_BF16 ? 1u : 0u;
+    J.wscale = J.fmt ? 1.f : 32768.f;
+    J.inv_scale = f->d_xinv;
+    return true;
+}
+
+cudaError_t tc_set_smem(const void *kernel) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+}
+
+cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, const TileArgs &T, uint64_t ntiles,
+                     const unsigned long long *off, const uint32_t *cnt, const uint32_t *e_slot, const float4 *e_w,
+                     const double *wsum, float *out, uint32_t ostride, float *wout, std::string &why) {
+    cudaStream_t s = ctx->stream;
+    CUtensorMap mh, ml;
+    TcJob J{};
+    if (!tc_prepare_job(f, &mh, &ml, J)) {
+        why = "cuTensorMapEncodeTiled";
+        return cudaErrorInvalidValue;
+    }
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = tc_set_smem((const void *)k_tile_tc);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    cudaError_t e = cudaSuccess;
+    void *zero = ctx->scratch.get(20, 2 * kAHalf, s, e);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(zero, 0, 2 * kAHalf, s)) != cudaSuccess) return e;
+    J.g = g;
+    J.off = off;
+    J.cnt = cnt;
+    J.e_slot = e_slot;
+    J.e_w = e_w;
+    J.wsum = wsum;
+    J.out = out;
+    J.ostride = ostride;
+    J.wout = wout;
+    for (uint64_t t0 = 0; t0 < ntiles; t0 += 0x7fffffffull) {
+        J.T = T;
+        J.T.t0 = T.t0 + t0;
+        dim3 grid((unsigned)std::min<uint64_t>(ntiles - t0, 0x7fffffffull), J.ncb);
+        k_tile_tc<<<grid, kTcThreads, kTcSmem, s>>>(mh, ml, J, zero, &ctx->d_stats->timeouts,
+                                                     &ctx->d_stats->tc_macs);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace hcg

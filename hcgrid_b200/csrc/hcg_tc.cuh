@@ -1,0 +1,383 @@
+// Tensor-core channel accumulation (tcgen05, sm_100a): the per-tile device
+// code shared by the single-job kernel (hcg_tc.cu) and the persistent batch
+// kernel (hcg_batch.cu).
+//
+// For one 16x8-pixel tile the gridded cube is a dense product
+//     cube[pixel][channel] = sum_slot W[pixel][slot] * X[slot][channel]
+// where the slots are the tile's staged samples (the union of the ring
+// windows of its pixels, one contiguous run of sorted samples per HEALPix
+// ring, padded to a multiple of 8) and W holds the FP64-evaluated GAUSS1D
+// weights of the pairs inside sphere_radius (zero elsewhere): the weights the
+// FP32 engine sums. The product runs on the 5th-generation tensor cores as a
+// compensated 16-bit split, W = Wh + Wl and X = Xh + Xl with
+// hi = round(x), lo = round(x - hi):
+//     W X ~= Wh Xh + Wh Xl + Wl Xh
+// three kind::f16 MMAs per K step into one FP32 accumulator in tensor memory.
+// Split formats: BF16 hi/lo (8 + 8 significant bits, per-term relative error
+// <= 3 * 2^-16) or FP16 hi/lo (11 + 11 bits) with power-of-two scales per
+// channel and for the weights that keep both halves in FP16's normal range
+// (per-term error ~3 * 2^-22). Scales are powers of two: exact.
+//
+// One work item = one tile x up to 256 channels (nb 64-channel blocks).
+// Warp roles in a 192-thread CTA:
+//   warp 0    producer: per 64-slot K chunk, one bulk copy of a zero page
+//             over the chunk's weight operand, then the spectra: 8 runs of 8
+//             sorted samples, each one 3-D TMA box (64 channels x 8 rows x nb
+//             channel blocks, 128-byte swizzle: the MN-major B atoms) of the
+//             hi and of the lo array;
+//   warp 1    TMEM allocation and MMA issue (one thread);
+//   warps 2-5 write the weights of the chunk's entries into the zeroed
+//             K-major operand (128-byte swizzle), then run the epilogue:
+//             tcgen05.ld of the accumulator, multiplication by the inverse
+//             scales and by 1 / (FP64 weight sum), store.
+// Two pipeline stages (A hi/lo 32 KB + B hi/lo 64 KB each). Pipeline
+// counters run on across the items a CTA processes. Every wait is bounded
+// (1 s of global time): a wait that runs out counts a timeout and sets the
+// CTA's abort flag; the roles wind down, the producer waits (bounded) for its
+// copies, TMEM is freed and the host reports HCG_ETIMEOUT.
+//
+// Padding slots of a ring run hold real neighbouring samples (or TMA zero
+// fill past the last sample) with zero weight; a non-finite spectrum value
+// would turn 0 * x into NaN across the tile, so fields with non-finite
+// spectra are refused by the tensor-core engines (the FP32 engine grids them).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "hcg_kernels.cuh"
+#include "hcg_sm100.cuh"
+
+namespace hcg {
+
+constexpr int kTcM = kTileX * kTileY;  // 128 pixels: the MMA's M
+constexpr int kTcK = 64;               // slots per K chunk (one 128-byte swizzle row of 16-bit values)
+constexpr int kTcStages = 2;
+constexpr int kTcThreads = 192;
+constexpr int kTcBuilders = 128;
+constexpr uint32_t kTcMaxN = 256;                         // channels per item
+constexpr uint32_t kAHalf = kTcM * kTcK * 2;              // 16 KB
+constexpr uint32_t kBHalf = kTcK * kTcMaxN * 2;           // 32 KB
+constexpr uint32_t kStageBytes = 2 * kAHalf + 2 * kBHalf;
+constexpr uint32_t kTcSmem = kTcStages * kStageBytes + 1024;  // + alignment of the swizzle atoms
+constexpr uint64_t kTcWaitNs = 1000000000ull;
+constexpr uint32_t kTmemCols = 256;
+static_assert(kTcM == 128, "a tile is one M=128 MMA");
+static_assert(kTcK == 64, "a chunk is 8 row boxes of 8 slots and one 128-byte swizzle row");
+
+// One job's tensor-core arguments.
+struct TcJob {
+    const CUtensorMap *map_hi, *map_lo;  // [ncb64][n][64] 16-bit arrays, boxes 64 x 8 x nb
+    GroupArgs g;
+    TileArgs T;
+    const unsigned long long *off;  // entry offset of each group (minus g.ebase)
+    const uint32_t *cnt;
+    const uint32_t *e_slot;
+    const float4 *e_w;
+    const double *wsum;
+    uint32_t nb;        // 64-channel blocks per item (1..4)
+    uint32_t ncb;       // items per tile (channel blocks of nb * 64)
+    uint32_t nchan;
+    uint32_t nrows;     // samples
+    uint32_t fmt;       // 0: f16, 1: bf16
+    float wscale;       // weight scale (power of two)
+    const float *inv_scale;  // [cpad]: 1 / (channel scale * wscale)
+    float *out;
+    uint32_t ostride;   // 0: [channel][pixel]; else [pixel][ostride]
+    float *wout;
+};
+
+constexpr int kTcRing = 8;  // entries in flight per builder thread
+
+struct TcShared {
+    uint64_t full_a[kTcStages], full_b[kTcStages], empty[kTcStages], zfill[kTcStages], acc_full;
+    uint32_t tmem;
+    volatile int abort;
+    unsigned long long item;
+    uint32_t ulo[kTileMaxRings], base[kTileMaxRings + 1];
+    float4 ring_w[kTcRing * kTcBuilders];  // builders' entry rings, [position][thread]
+    uint32_t ring_slot[kTcRing * kTcBuilders];
+};
+
+// hcg_tc.cu: the tensor maps and format fields of a field with split
+// spectra (false: the maps could not be encoded); the shared-memory opt-in of
+// a kernel built on tc_item.
+bool tc_prepare_job(const hcg_field *f, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J);
+cudaError_t tc_set_smem(const void *kernel);
+
+namespace {
+
+__device__ __forceinline__ uint16_t tc_to16(float v, uint32_t fmt) {
+    return fmt ? __bfloat16_as_ushort(__float2bfloat16_rn(v)) : __half_as_ushort(__float2half_rn(v));
+}
+
+__device__ __forceinline__ float tc_from16(uint16_t b, uint32_t fmt) {
+    return fmt ? __bfloat162float(__ushort_as_bfloat16(b)) : __half2float(__ushort_as_half(b));
+}
+
+// byte offset of element (row m, column k) of a K-major 128-row x 64-column
+// 16-bit operand in 128-byte-swizzled 8-row atoms
+__device__ __forceinline__ uint32_t tc_a_offset(uint32_t m, uint32_t k) {
+    return (m >> 3) * 1024u + (m & 7u) * 128u + ((((k >> 3) ^ (m & 7u)) << 4) | ((k & 7u) << 1));
+}
+
+__device__ __forceinline__ uint8_t *tc_smem_base() {
+    extern __shared__ uint8_t s_tc_raw[];
+    return (uint8_t *)(((uintptr_t)s_tc_raw + 1023) & ~(uintptr_t)1023);
+}
+
+// Whole CTA: barriers and TMEM.
+__device__ __forceinline__ void tc_setup(TcShared &S) {
+    using namespace sm100;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            mbar_init(&S.full_a[s], kTcBuilders);
+            mbar_init(&S.full_b[s], 1);
+            mbar_init(&S.empty[s], 1);
+            mbar_init(&S.zfill[s], 1);
+        }
+        mbar_init(&S.acc_full, 1);
+        S.abort = 0;
+        mbar_fence_init();
+    }
+    if ((tid >> 5) == 1) {
+        tmem_alloc(&S.tmem, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+
+__device__ __forceinline__ void tc_give_up(TcShared &S, unsigned long long *timeouts) {
+    atomicAdd(timeouts, 1ULL);
+    S.abort = 1;
+}
+
+// Whole CTA, after its last item: the producer waits (bounded) for the copies
+// of the last chunks of each stage, then TMEM is freed.
+__device__ __forceinline__ void tc_teardown(TcShared &S, uint32_t gk, unsigned long long *timeouts) {
+    using namespace sm100;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (uint32_t g = gk > kTcStages ? gk - kTcStages : 0; g < gk; ++g) {
+            const uint32_t s = g & 1, ph = (g >> 1) & 1;
+            if (!mbar_wait(&S.full_b[s], ph, kTcWaitNs) || !mbar_wait(&S.zfill[s], ph, kTcWaitNs)) {
+                tc_give_up(S, timeouts);
+                break;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if ((tid >> 5) == 1) {
+        tc_fence_after();
+        tmem_dealloc(S.tmem, kTmemCols);
+    }
+}
+
+// Whole CTA: the tile's ring table into shared memory (caller syncs after).
+__device__ __forceinline__ void tc_load_rings(TcShared &S, const TileArgs &T, uint64_t tile) {
+    const int nrt = T.nr[tile];
+    for (int j = threadIdx.x; j < nrt; j += kTcThreads) S.ulo[j] = T.ulo[tile * kTileMaxRings + j];
+    for (int j = threadIdx.x; j <= nrt; j += kTcThreads) S.base[j] = T.base[tile * (kTileMaxRings + 1) + j];
+}
+
+// Whole CTA: one item. `gk` counts the K chunks this CTA has run (all items),
+// `itn` its items; both advance identically in every thread.
+__device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t tile, uint32_t cblk, uint32_t &gk,
+                                        uint32_t itn, const void *zero_page, unsigned long long *timeouts,
+                                        unsigned long long *macs) {
+    using namespace sm100;
+    uint8_t *smem = tc_smem_base();
+    auto A_hi = [&](uint32_t s) { return smem + s * kStageBytes; };
+    auto A_lo = [&](uint32_t s) { return smem + s * kStageBytes + kAHalf; };
+    auto B_hi = [&](uint32_t s) { return smem + s * kStageBytes + 2 * kAHalf; };
+    auto B_lo = [&](uint32_t s) { return smem + s * kStageBytes + 2 * kAHalf + kBHalf; };
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const TileArgs &T = J.T;
+    const uint32_t U = T.U[tile];
+    const uint32_t nchunks = (U + kTcK - 1) / kTcK;
+    const uint32_t taddr = S.tmem;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------------------------------------------- producer
+            const uint32_t bytes = 2u * 8u * J.nb * 1024u;
+            int j = 0;
+            for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
+                const uint32_t g = gk + k, s = g & 1;
+                if (g >= kTcStages && !mbar_wait(&S.empty[s], ((g >> 1) - 1) & 1, kTcWaitNs)) {
+                    tc_give_up(S, timeouts);
+                    break;
+                }
+                mbar_arrive_expect_tx(&S.zfill[s], 2 * kAHalf);
+                bulk_copy_g2s(A_hi(s), zero_page, 2 * kAHalf, &S.zfill[s]);
+                mbar_arrive_expect_tx(&S.full_b[s], bytes);
+                for (int b = 0; b < 8; ++b) {
+                    const uint32_t slot0 = k * kTcK + 8 * b;
+                    int row;
+                    if (slot0 >= U) {
+                        row = (int)J.nrows;  // past the last sample: zero fill
+                    } else {
+                        while (S.base[j + 1] <= slot0) ++j;
+                        row = (int)(S.ulo[j] + (slot0 - S.base[j]));
+                    }
+                    const int cz = (int)(cblk * J.nb);
+                    tma_load_3d(B_hi(s) + b * 4096, J.map_hi, &S.full_b[s], 0, row, cz);
+                    tma_load_3d(B_lo(s) + b * 4096, J.map_lo, &S.full_b[s], 0, row, cz);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------------------------------------------- MMA issue
+            const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
+            uint32_t acc = 0;
+            for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
+                const uint32_t g = gk + k, s = g & 1, ph = (g >> 1) & 1;
+                if (!mbar_wait(&S.full_a[s], ph, kTcWaitNs) || !mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
+                    tc_give_up(S, timeouts);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ah = smem_u32(A_hi(s)), al = smem_u32(A_lo(s));
+                const uint32_t bh = smem_u32(B_hi(s)), bl = smem_u32(B_lo(s));
+#pragma unroll
+                for (int kk = 0; kk < kTcK / 16; ++kk) {
+                    const uint64_t adh = smem_desc_sw128(ah + kk * 32, 16, 1024);
+                    const uint64_t adl = smem_desc_sw128(al + kk * 32, 16, 1024);
+                    const uint64_t bdh = smem_desc_sw128(bh + kk * 8192, 1024, 4096);
+                    const uint64_t bdl = smem_desc_sw128(bl + kk * 8192, 1024, 4096);
+                    mma_f16_ss(taddr, adh, bdh, idesc, acc);
+                    mma_f16_ss(taddr, adh, bdl, idesc, 1);
+                    mma_f16_ss(taddr, adl, bdh, idesc, 1);
+                    acc = 1;
+                }
+                mma_commit(&S.empty[s]);
+            }
+            if (acc) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)kTcK * nchunks);
+            if (nchunks == 0)
+                mbar_arrive(&S.acc_full);
+            else
+                mma_commit(&S.acc_full);  // also after a timeout: every MMA issued has completed once it fires
+        }
+    } else {
+        // -------------------------------------------------------- weight operand
+        const GroupArgs &G = J.g;
+        const int bt = tid - 64, gq = bt >> 2, sub = bt & 3;
+        const uint32_t gxl = gq & 7, gyl = gq >> 3;
+        const uint32_t gxi = (uint32_t)(tile % T.ntx) * (kTileX / 2) + gxl;
+        const uint32_t gyi = (uint32_t)(tile / T.ntx) * (kTileY / 2) + gyl;
+        const uint64_t grp = (uint64_t)gyi * G.gx + gxi;
+        uint64_t e = 0, e_end = 0;
+        if (gxi < G.gx && grp < G.ngroups) {
+            e = J.off[grp] - G.ebase;
+            e_end = e + J.cnt[grp];
+        }
+        e += sub;
+        // This thread takes every 4th entry of its group. Its next eight
+        // entries sit in a private ring in shared memory filled by cp.async:
+        // the copy of an entry is issued eight entries before it is read, and
+        // reading the ring at a per-thread position needs neither register
+        // moves nor divergent branches.
+        uint32_t *rs = S.ring_slot + bt;  // [kTcRing][kTcBuilders]
+        float4 *rw = S.ring_w + bt;
+        auto issue = [&](int i) {
+            if (e < e_end) {
+                cp_async4(rs + i * kTcBuilders, J.e_slot + e);
+                cp_async16(rw + i * kTcBuilders, J.e_w + e, true);
+            } else {
+                rs[i * kTcBuilders] = 0xffffffffu;
+            }
+            cp_async_commit();
+            e += 4;
+        };
+#pragma unroll
+        for (int i = 0; i < kTcRing; ++i) issue(i);
+        int head = 0;
+        uint32_t mrow[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) mrow[q] = (2 * gyl + (q >> 1)) * kTileX + 2 * gxl + (q & 1);
+        for (uint32_t k = 0; k < nchunks; ++k) {
+            const uint32_t g = gk + k, s = g & 1;
+            if (S.abort) break;
+            if (!mbar_wait(&S.zfill[s], (g >> 1) & 1, kTcWaitNs)) {  // zeroed operand: the stage is free
+                tc_give_up(S, timeouts);
+                break;
+            }
+            const uint32_t cs = k * kTcK, ce = cs + kTcK;
+            uint8_t *ah = A_hi(s), *al = A_lo(s);
+            for (;;) {
+                cp_async_wait<kTcRing - 1>();  // the ring's oldest copy has landed
+                const uint32_t slot = rs[head * kTcBuilders];
+                if (slot >= ce) break;
+                const float4 wq = rw[head * kTcBuilders];
+                const uint32_t col = slot - cs;
+                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float w = wv[q] * J.wscale;
+                    const uint16_t h = tc_to16(w, J.fmt);
+                    const uint16_t l = tc_to16(w - tc_from16(h, J.fmt), J.fmt);
+                    const uint32_t o = tc_a_offset(mrow[q], col);
+                    *(uint16_t *)(ah + o) = h;
+                    *(uint16_t *)(al + o) = l;
+                }
+                issue(head);
+                head = (head + 1) & (kTcRing - 1);
+            }
+            fence_proxy_async_smem();
+            mbar_arrive(&S.full_a[s]);
+        }
+        cp_async_wait<0>();  // no copy into the ring outlives the item
+        // -------------------------------------------------------- epilogue
+        const bool ok = mbar_wait(&S.acc_full, itn & 1, kTcWaitNs);
+        if (!ok) tc_give_up(S, timeouts);
+        tc_fence_after();
+        const uint32_t q4 = warp & 3;  // TMEM lane quarter this warp may access
+        const uint32_t m = q4 * 32 + lane;
+        const uint32_t xx = (uint32_t)(tile % T.ntx) * kTileX + (m & (kTileX - 1));
+        const uint32_t yy = (uint32_t)(tile / T.ntx) * kTileY + m / kTileX;
+        const bool valid = xx < G.nx && yy < G.ny;
+        const uint64_t P = (uint64_t)G.nx * G.ny;
+        const uint64_t p = (uint64_t)yy * G.nx + xx;
+        const double ws = valid ? J.wsum[p] : 0.0;
+        const float inv = (float)(1.0 / ws);
+        if (valid && cblk == 0 && J.wout) J.wout[p] = (float)ws;
+        const bool store = ok && !S.abort && valid;
+        for (uint32_t cb = 0; cb < 2 * J.nb; ++cb) {
+            uint32_t r[32];
+            if (nchunks > 0) {
+                tmem_ld_32x32b_x32(taddr + ((q4 * 32u) << 16) + cb * 32u, r);
+                tmem_wait_ld();
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) r[i] = 0u;
+            }
+            const uint32_t c0 = cblk * J.nb * 64 + cb * 32;
+            if (!store) continue;
+            if (J.ostride == 0) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const uint32_t ch = c0 + i;
+                    if (ch < J.nchan) J.out[(uint64_t)ch * P + p] = (__uint_as_float(r[i]) * J.inv_scale[ch]) * inv;
+                }
+            } else {
+                float *dst = J.out + p * J.ostride;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const uint32_t ch = c0 + i;
+                    if (ch < J.nchan) dst[ch] = (__uint_as_float(r[i]) * J.inv_scale[ch]) * inv;
+                }
+            }
+        }
+        tc_fence_before();
+    }
+    gk += nchunks;
+}
+
+}  // namespace
+}  // namespace hcg

@@ -238,17 +238,18 @@ def job_work(shape: dict) -> float:
 
 
 def config5_requests(njobs: int = 2000, seed: int = 3, reuse: float = 0.3, max_grid: int = 2048,
-                     max_values: int = 1 << 62, max_work: float = float("inf")):
+                     max_values: int = 1 << 62, max_work: float = float("inf"), max_cube: int = 1 << 62):
     """Request stream of the served form: shapes drawn as in config 4 (seed
     `seed`), a fraction `reuse` of requests re-gridding an earlier request's
     field (same samples, new spectra). Caps, when given, redraw shapes whose
-    grid, sample-channel count or estimated work exceed them. Returns dicts
+    grid, sample-channel count, cube size or estimated work exceed them. Returns dicts
     with the shape, the field id it uses and the seed of its spectra."""
     rng = np.random.default_rng(seed)
     shapes = []
     draws = config4_shapes(nblocks=max(4 * njobs, 64), seed=seed)
     for s in draws:
-        if s["grid"] > max_grid or s["n"] * s["nchan"] > max_values or job_work(s) > max_work:
+        if (s["grid"] > max_grid or s["n"] * s["nchan"] > max_values or job_work(s) > max_work
+                or s["grid"] ** 2 * s["nchan"] > max_cube):
             continue
         shapes.append(s)
     out = []

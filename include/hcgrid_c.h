@@ -61,6 +61,12 @@ typedef enum {
 /* Gridding engines. */
 #define HCG_ENGINE_AUTO 0
 #define HCG_ENGINE_FP32 1 /* FP64 geometry, FP32 CUDA-core channel accumulation */
+/* FP64 geometry and weights, channel sums on the tensor cores (tcgen05) as a
+ * compensated 16-bit split W X ~= Wh Xh + Wh Xl + Wl Xh with FP32
+ * accumulation. Needs hcg_field_split_spectra with the same engine first;
+ * single-channel fields always use the FP32 single-channel kernel. */
+#define HCG_ENGINE_TC_BF16 2 /* BF16 hi/lo: per-term relative error <= 3 * 2^-16 */
+#define HCG_ENGINE_TC_F16 3  /* FP16 hi/lo with power-of-two channel scales: ~3 * 2^-22 */
 
 typedef struct hcg_context hcg_context;
 typedef struct hcg_field hcg_field;
@@ -81,6 +87,7 @@ typedef struct {
     uint64_t hard_roundings;  /* cos/sin roundings the double-double test could not decide */
     double ms_total;          /* device time of the last hcg_grid call */
     double ms_phase[4];       /* of which: pixel setup, candidate count + scan, FP64 weights, channel sums */
+    uint64_t tc_macs;         /* tensor-core multiply-adds issued (3 per compensated product; 0 on the FP32 engine) */
 } hcg_stats;
 
 const char *hcg_status_string(hcg_status s);
@@ -107,6 +114,15 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
 /* Attach spectra (float32) in either layout; permuted into sorted order on
  * the device and kept resident. */
 hcg_status hcg_field_set_spectra(hcg_field *field, uint32_t nchan, const float *values, int layout, int mem);
+
+/* Store the field's spectra a second time as 16-bit hi/lo pairs (per-channel
+ * power-of-two scale for HCG_ENGINE_TC_F16) for the tensor-core engine
+ * `engine`. keep_fp32 = 0 frees the FP32 copy (the FP32 engine is then not
+ * available for this field until hcg_field_set_spectra). Non-finite values
+ * are counted: such fields are refused by the tensor-core engines
+ * (HCG_EINVAL). hcg_field_set_spectra drops the split. No reference
+ * counterpart (the reference grids FP64 on CUDA cores). */
+hcg_status hcg_field_split_spectra(hcg_field *field, int engine, int keep_fp32);
 /* Sorted keys (n+1 with the npix sentinel), permutation (n) and ring LUT
  * (usedrings+1); any pointer may be NULL. Host memory. */
 hcg_status hcg_field_sorted(const hcg_field *field, uint64_t *keys, uint32_t *perm, uint32_t *lut);

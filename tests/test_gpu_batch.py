@@ -108,3 +108,42 @@ def test_batch_jobs_match_oracle(ctx, jobs):
             r = ref[~nan[:, ch], ch]
             if r.size:
                 assert np.abs(c[~nan[:, ch], ch] - r).max() / np.abs(r).max() <= tol
+
+
+@pytest.fixture(scope="module")
+def tc_jobs(ctx):
+    """Fresh fields of the same shapes; the multi-channel ones hold split
+    spectra (FP16 hi/lo for blocks 1 and 3, BF16 hi/lo for block 2), so the
+    batch runs them on the persistent tensor-core kernel."""
+    items = [make(ctx, s) for s in SHAPES]
+    for i, eng in ((1, api.ENGINE_TC_F16), (2, api.ENGINE_TC_BF16), (3, api.ENGINE_TC_F16)):
+        items[i][1].split_spectra(eng)
+    return items
+
+
+def test_tensor_core_batch_equals_single_calls(ctx, tc_jobs, jobs):
+    layouts = [api.CHANNEL_MAJOR, api.SAMPLE_MAJOR, api.CHANNEL_MAJOR, api.SAMPLE_MAJOR, api.CHANNEL_MAJOR]
+    got = run_batch(ctx, tc_jobs, layouts)
+    st = ctx.stats()
+    assert st.tc_macs > 0
+    for i, ((job, f, t), lay, (cube, w)) in enumerate(zip(tc_jobs, layouts, got)):
+        ref_cube, ref_w = single(ctx, job, f, t, lay)  # hcg_grid, engine of the field's split
+        np.testing.assert_array_equal(cube, ref_cube)
+        np.testing.assert_array_equal(w, ref_w)
+        # and within the split's precision of the FP32 engine
+        j32, f32, t32 = jobs[i]
+        c32, w32 = single(ctx, j32, f32, t32, lay)
+        np.testing.assert_array_equal(w, w32)
+        if job.nchan > 1:
+            nan = np.isnan(c32)
+            np.testing.assert_array_equal(np.isnan(cube), nan)
+            scale = np.abs(c32[~nan]).max()
+            assert np.abs(cube[~nan] - c32[~nan]).max() <= 5e-5 * scale
+
+
+def test_tensor_core_job_alone_equals_job_in_mix(ctx, tc_jobs):
+    mix = run_batch(ctx, tc_jobs, [api.SAMPLE_MAJOR] * len(tc_jobs))
+    for i in (1, 2, 3):
+        alone = run_batch(ctx, [tc_jobs[i]], [api.SAMPLE_MAJOR])[0]
+        np.testing.assert_array_equal(alone[0], mix[i][0])
+        np.testing.assert_array_equal(alone[1], mix[i][1])

@@ -1,0 +1,164 @@
+"""Tensor-core engines (tcgen05, compensated 16-bit hi/lo products) against
+the FP64 oracle and the FP32 engine, through the C ABI.
+
+Tolerances, relative to the largest |value| of each channel plane (the
+measure of the FP32 parity tests):
+  * FP16 hi/lo: 1e-5 (per-term error of the three-product split ~3 * 2^-22,
+    plus FP32 accumulation);
+  * BF16 hi/lo: 5e-5 (per-term bound 3 * 2^-16 = 4.6e-5).
+Weights are the FP64 sums of the same entries the FP32 engine uses, so the
+weight map is bit-identical to the FP32 engine's, as is the NaN pattern of
+empty pixels."""
+import numpy as np
+import pytest
+
+from hcgrid_b200 import api, synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = {api.ENGINE_TC_F16: 1e-5, api.ENGINE_TC_BF16: 5e-5}
+ENGINES = [api.ENGINE_TC_F16, api.ENGINE_TC_BF16]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def prepare(ctx, job):
+    ctx.prepare_grid_kernel(api.GAUSS1D, np.array([job.sigma_deg, 0.0, 0.0]), job.sphere_radius, job.hpx_max_res)
+
+
+def plane_errors(cube, ref):
+    """max over channels of max|cube - ref| / max|ref| (NaN patterns equal)."""
+    nan = np.isnan(ref)
+    assert np.array_equal(np.isnan(cube), nan)
+    worst = 0.0
+    for c in range(ref.shape[1]):
+        r = ref[~nan[:, c], c]
+        if r.size == 0:
+            continue
+        g = cube[~nan[:, c], c].astype(np.float64)
+        worst = max(worst, np.abs(g - r).max() / max(np.abs(r).max(), 1e-30))
+    return worst
+
+
+@pytest.fixture(scope="module")
+def small(ctx):
+    """Config-2 generator, 150k samples over 2 deg, 100 channels (not a
+    multiple of 64), 120x120 map: several tiles, ring runs of all lengths."""
+    job = synth.config2(n=150_000, nchan=100, nx=120, size_deg=2.0, build_values=True)
+    prepare(ctx, job)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(job.values)
+    t = ctx.target_from_header(job.header)
+    xw, yw = t.coords()
+    g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    ps = O.presort(g.hpx, job.lon, job.lat)
+    oc, ow, _ = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], job.values[ps.perm].astype(np.float64), xw, yw)
+    ref = oc / ow[:, None]
+    c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+    yield job, f, t, ref, c32, w32
+    f.close()
+    t.close()
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("layout", [api.SAMPLE_MAJOR, api.CHANNEL_MAJOR])
+def test_tc_matches_oracle(ctx, small, engine, layout):
+    job, f, t, ref, c32, w32 = small
+    prepare(ctx, job)
+    f.split_spectra(engine)
+    cube, w = ctx.grid(f, t, layout=layout, engine=engine)
+    if layout == api.CHANNEL_MAJOR:
+        cube = cube.T
+    np.testing.assert_array_equal(w, w32)
+    err = plane_errors(cube, ref)
+    print(f"engine {engine} layout {layout}: max plane-relative error vs FP64 oracle {err:.3e}")
+    assert err <= TOL[engine]
+    assert plane_errors(c32, ref) <= 1e-5
+
+
+def test_auto_engine_uses_the_split(ctx, small):
+    job, f, t, ref, c32, w32 = small
+    prepare(ctx, job)
+    f.split_spectra(api.ENGINE_TC_F16)
+    a, _ = ctx.grid(f, t)
+    b, _ = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+    np.testing.assert_array_equal(a, b)
+    # deterministic: the same launch twice gives the same bits
+    c, _ = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+    np.testing.assert_array_equal(b, c)
+
+
+@pytest.mark.parametrize("nchan", [64, 300])
+def test_tc_channel_blocks(ctx, nchan):
+    """64 channels (one 64-channel block) and 300 (two CTAs per tile, the
+    second partly past the last channel)."""
+    job = synth.config2(n=60_000, nchan=nchan, nx=64, size_deg=1.2, build_values=True)
+    prepare(ctx, job)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(job.values)
+    t = ctx.target_from_header(job.header)
+    c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+    f.split_spectra(api.ENGINE_TC_F16)
+    ct, wt = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+    np.testing.assert_array_equal(wt, w32)
+    # FP32 engine and FP16 hi/lo engine agree to the split's precision
+    assert plane_errors(ct, c32.astype(np.float64)) <= 1e-5
+
+
+def test_tc_empty_tiles_and_padding(ctx):
+    """A map larger than the field: whole tiles without samples come out NaN
+    with zero weight, exactly where the FP32 engine puts them."""
+    job = synth.config2(n=30_000, nchan=64, nx=96, size_deg=1.0, build_values=True)
+    prepare(ctx, job)
+    hdr = synth.sin_header(96, 96, 180.0, 30.0, 2.0 / 96)  # config2 is centred at (180, 30)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(job.values)
+    t = ctx.target_from_header(hdr)
+    c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+    f.split_spectra(api.ENGINE_TC_BF16)
+    ct, wt = ctx.grid(f, t, engine=api.ENGINE_TC_BF16)
+    assert np.isnan(ct).any() and (~np.isnan(ct)).any()
+    np.testing.assert_array_equal(np.isnan(ct), np.isnan(c32))
+    np.testing.assert_array_equal(wt, w32)
+    assert plane_errors(ct, c32.astype(np.float64)) <= 5e-5
+
+
+def test_tc_state_and_input_checks(ctx):
+    job = synth.config2(n=20_000, nchan=64, nx=32, size_deg=0.6, build_values=True)
+    prepare(ctx, job)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(job.values)
+    t = ctx.target_from_header(job.header)
+    with pytest.raises(RuntimeError, match="HCG_ESTATE"):  # no split yet
+        ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+    f.split_spectra(api.ENGINE_TC_BF16)
+    with pytest.raises(RuntimeError, match="HCG_ESTATE"):  # split of the other format
+        ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+    with pytest.raises(RuntimeError, match="HCG_EINVAL"):
+        ctx.grid(f, t, engine=7)
+    with pytest.raises(RuntimeError, match="HCG_EINVAL"):
+        f.split_spectra(api.ENGINE_FP32)
+    ref, _ = ctx.grid(f, t, engine=api.ENGINE_TC_BF16)
+    # dropping the FP32 copy keeps the tensor-core result and closes the FP32 engine
+    f.split_spectra(api.ENGINE_TC_BF16, keep_fp32=False)
+    again, _ = ctx.grid(f, t)
+    np.testing.assert_array_equal(ref, again)
+    with pytest.raises(RuntimeError, match="HCG_ESTATE"):
+        ctx.grid(f, t, engine=api.ENGINE_FP32)
+    # new spectra drop the split; non-finite values are refused by the tensor-core engines
+    bad = job.values.copy()
+    bad[::50, 3] = np.nan
+    f.set_spectra(bad)
+    with pytest.raises(RuntimeError, match="HCG_ESTATE"):
+        ctx.grid(f, t, engine=api.ENGINE_TC_BF16)
+    f.split_spectra(api.ENGINE_TC_BF16)
+    with pytest.raises(RuntimeError, match="HCG_EINVAL"):
+        ctx.grid(f, t, engine=api.ENGINE_TC_BF16)
+    c32, _ = ctx.grid(f, t, engine=api.ENGINE_FP32)  # the FP32 engine grids them
+    assert np.isnan(c32[:, 3]).any()
