@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--engine", default="fp32", choices=list(ENGINES),
                     help="channel-sum engine: FP32 CUDA cores or tensor cores with a 16-bit hi/lo split")
+    ap.add_argument("--tc-config", type=int, default=None,
+                    help="tensor-core pipeline shape (0: 256 ch x 2 stages, 1: 128 x 3, 2: 64 x 4); "
+                         "default: autotuned on the workload before the timed steps")
     # reduced cases (profiling, quick checks); the headline run uses none of these
     ap.add_argument("--samples", type=int, default=None)
     ap.add_argument("--channels", type=int, default=None)
@@ -297,15 +300,19 @@ def served_main(args):
     """Config 5: a stream of gridding requests with config-4 shapes (seed 3),
     30% of them re-gridding an earlier request's field with new spectra.
     Fields (sorted samples, ring LUT) and targets stay resident; each request
-    brings its spectra (generated on the device) and output buffers.
+    brings its spectra (generated on the device, permuted into the request's
+    field share and, for the tensor-core engine, split into FP16 hi/lo) and
+    its output buffers. Requests are staged in windows that fit the HBM
+    admission budget; only the gridding is timed.
 
-    served: requests go through hcg_server (continuous batching over 2 lanes,
-    persistent batch kernels, tensor-core channel sums on FP16 hi/lo spectra,
-    HBM admission budget). Capacity = closed-loop throughput; then Poisson
-    arrivals at 80% of it give p50/p99 latency (submit -> cube written).
-    plain: the same requests one hcg_grid call at a time on the FP32 engine.
-    Both time the gridding only; spectra generation and upload are outside
-    the latency (they overlap the server's work in the served run)."""
+    served: each window's requests go through hcg_server (continuous
+    batching over 2 lanes, persistent batch kernels replayed from a CUDA
+    graph, tensor-core channel sums, footprint admission). Capacity = work /
+    time from a window's first submit to its last completion (closed loop);
+    then Poisson arrivals at 80% of capacity give p50/p99 latency (submit ->
+    cube written). Arms beside it on the same requests: plain = one hcg_grid
+    call at a time on the FP32 engine; tc_per_call = one hcg_grid call at a
+    time on the tensor-core engine."""
     import torch
     from hcgrid_b200 import api, synth
     dev = torch.device("cuda", 0)
@@ -315,9 +322,8 @@ def served_main(args):
     reqs = synth.config5_requests(njobs=args.jobs, seed=3, reuse=0.3, max_grid=2048, max_values=1 << 29,
                                   max_cube=1 << 30)
     ctx = api.Context(0)
-    # resident fields and targets (built once, outside the timed runs)
     base = {}
-    for r in reqs:
+    for r in reqs:  # resident fields and targets, built once
         fid = r["field"]
         if fid in base:
             continue
@@ -335,102 +341,124 @@ def served_main(args):
     def work(r):
         return r["shape"]["n"] * r["shape"]["nchan"]
 
-    def footprint(r, split):
+    def footprint(r):
+        """device bytes of one request: spectra (FP32 during the upload, then
+        the hi/lo split), cube and weights, and the per-pixel scratch of the
+        batch engine (pixel setup, weight sums, tile tables, entries)."""
         sh = r["shape"]
         P = sh["grid"] ** 2
-        return sh["n"] * sh["nchan"] * 4 + P * (sh["nchan"] + 1) * 4 + P * 160
+        return 2 * sh["n"] * sh["nchan"] * 4 + P * (sh["nchan"] + 1) * 4 + P * 600
 
-    def prepare(r, tc):
-        sh = r["shape"]
-        f0, t, lon_d, lat_d = base[r["field"]]
-        S = device_block_spectra(lon_d, lat_d, sh, sh["nchan"], r["spectra_seed"], torch, dev)
-        torch.cuda.synchronize(dev)
-        f = f0.share()
-        f.set_spectra(S)
-        del S
-        if tc and sh["nchan"] > 1:
-            f.split_spectra(api.ENGINE_TC_F16, keep_fp32=False)
-        P = t.nx * t.ny
-        cube = torch.empty((P * sh["nchan"],), dtype=torch.float32, device=dev)
-        wts = torch.empty((P,), dtype=torch.float32, device=dev)
-        ctx.synchronize()
-        return f, t, cube, wts
-
-    # plain per-call FP32 path
-    plain_lat = []
-    t_plain = 0.0
+    windows, cur, used = [], [], 0
+    stage_budget = min(budget, 64 << 30)  # staged requests; the rest of HBM is the lanes' working memory
     for r in reqs:
-        f, t, cube, wts = prepare(r, tc=False)
-        t0 = time.perf_counter()
-        ctx.grid(f, t, cube, wts, engine=api.ENGINE_FP32)
+        fp = footprint(r)
+        if cur and used + fp > stage_budget:
+            windows.append(cur)
+            cur, used = [], 0
+        cur.append(r)
+        used += fp
+    if cur:
+        windows.append(cur)
+
+    def stage(win, tc):
+        out = []
+        for r in win:
+            sh = r["shape"]
+            f0, t, lon_d, lat_d = base[r["field"]]
+            S = device_block_spectra(lon_d, lat_d, sh, sh["nchan"], r["spectra_seed"], torch, dev)
+            torch.cuda.synchronize(dev)
+            f = f0.share()
+            f.set_spectra(S)
+            del S
+            if tc and sh["nchan"] > 1:
+                f.split_spectra(api.ENGINE_TC_F16, keep_fp32=False)
+            P = t.nx * t.ny
+            cube = torch.empty((P * sh["nchan"],), dtype=torch.float32, device=dev)
+            wts = torch.empty((P,), dtype=torch.float32, device=dev)
+            out.append((r, f, t, cube, wts))
         ctx.synchronize()
-        dt = time.perf_counter() - t0
-        plain_lat.append(dt)
-        t_plain += dt
-        f.close()
-        del cube, wts
-    tot_work = sum(work(r) for r in reqs)
+        return out
 
-    def run_served(arrivals):
-        srv = api.Server(ctx, lanes=2, hbm_budget=budget, max_batch=64)
-        inflight = []  # (ticket, bytes, field, buffers)
-        used = 0
-        lats, queues = [], []
-        t_start = time.perf_counter()
-        for i, r in enumerate(reqs):
-            fp = footprint(r, True)
-            while inflight and used + fp > budget:
-                tk, b, f, bufs = inflight.pop(0)
-                lt, q = srv.wait(tk)
-                lats.append(lt)
-                queues.append(q)
-                used -= b
-                f.close()
-            if arrivals is not None:
-                delay = t_start + arrivals[i] - time.perf_counter()
-                if delay > 0:
-                    time.sleep(delay)
-            f, t, cube, wts = prepare(r, tc=True)
-            tk = srv.submit(f, t, cube, wts, api.SAMPLE_MAJOR, footprint=fp)
-            inflight.append((tk, fp, f, (cube, wts)))
-            used += fp
-        for tk, b, f, bufs in inflight:
-            lt, q = srv.wait(tk)
-            lats.append(lt)
-            queues.append(q)
+    def release(staged):
+        for _, f, _, _, _ in staged:
             f.close()
-        makespan = time.perf_counter() - t_start
-        st = srv.stats()
-        srv.close()
-        return makespan, lats, queues, st
+        staged.clear()
+        ctx.synchronize()
+        torch.cuda.empty_cache()
 
-    run_served(None)  # warm-up: captures the lanes' batch graphs
-    makespan, lats_cl, _, st_cl = run_served(None)
-    capacity = tot_work / makespan
-    rate = 0.8 * len(reqs) / makespan  # requests per second at 80% of capacity
-    rng = np.random.default_rng(3)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
-    arrivals -= arrivals[0]
-    makespan_p, lats, queues, st = run_served(arrivals)
+    def per_call(tc):
+        lat = []
+        for win in windows:
+            staged = stage(win, tc)
+            for r, f, t, cube, wts in staged:
+                eng = api.ENGINE_TC_F16 if (tc and r["shape"]["nchan"] > 1) else api.ENGINE_FP32
+                t0 = time.perf_counter()
+                ctx.grid(f, t, cube, wts, engine=eng)
+                ctx.synchronize()
+                lat.append(time.perf_counter() - t0)
+            release(staged)
+        return lat
+
+    def served(rate):
+        srv = api.Server(ctx, lanes=2, hbm_budget=budget, max_batch=64)
+        lats, queues, busy = [], [], 0.0
+        rng = np.random.default_rng(3)
+        try:
+            for win in windows:
+                staged = stage(win, True)
+                arr = None
+                if rate:
+                    arr = np.cumsum(rng.exponential(1.0 / rate, len(staged)))
+                    arr -= arr[0]
+                tickets = []
+                t0 = time.perf_counter()
+                for i, (r, f, t, cube, wts) in enumerate(staged):
+                    if arr is not None:
+                        d = t0 + arr[i] - time.perf_counter()
+                        if d > 0:
+                            time.sleep(d)
+                    tickets.append(srv.submit(f, t, cube, wts, api.SAMPLE_MAJOR, footprint=footprint(r)))
+                for tk in tickets:
+                    lt, q = srv.wait(tk)
+                    lats.append(lt)
+                    queues.append(q)
+                busy += time.perf_counter() - t0
+                release(staged)
+            st = srv.stats()
+        finally:
+            srv.close()
+        return busy, lats, queues, st
+
+    tot_work = sum(work(r) for r in reqs)
+    plain_lat = per_call(False)
+    tc_lat = per_call(True)
+    served(None)  # warm-up: each lane captures its batch graph
+    busy, lats_cl, _, st_cl = served(None)
+    capacity = tot_work / busy
+    rate = 0.8 * len(reqs) / busy
+    busy_p, lats, queues, st = served(rate)
     pct = lambda v, q: float(np.percentile(np.asarray(v), q))
+    plain = tot_work / sum(plain_lat)
     out = {"metric": METRIC, "value": capacity, "unit": UNIT, "n_gpus": 1, "steps": len(reqs), "warmup": 1,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "fp16 hi/lo tensor-core channel sums (FP64 geometry)",
            "data": "synthetic (seeded config-5 request stream, hcgrid_b200/synth.py)",
            "config": {"workload": "config5: %d requests, config-4 shapes (seed 3), 30%% field reuse, HBM budget "
                                   "%.0f GB" % (len(reqs), args.hbm_budget_gb),
-                      "unique_fields": len(base), "total_sample_channels": tot_work,
+                      "unique_fields": len(base), "windows": len(windows), "total_sample_channels": tot_work,
                       "caps": "grid <= 2048, samples x channels <= 2^29, grid^2 x channels <= 2^30",
                       "engine": "served: hcg_server (2 lanes, batch graphs, tensor cores FP16 hi/lo); "
                                 "plain: hcg_grid FP32 engine per call"},
-           "served": {"capacity": capacity, "closed_loop_s": round(makespan, 4),
+           "served": {"capacity": capacity, "busy_s": round(busy, 4), "batches_closed_loop": st_cl["batches"],
                       "p50_s_closed_loop": pct(lats_cl, 50), "p99_s_closed_loop": pct(lats_cl, 99),
-                      "poisson_rate_per_s": round(rate, 3), "throughput_at_80pct": tot_work / makespan_p,
-                      "p50_s": pct(lats, 50), "p99_s": pct(lats, 99), "queue_p99_s": pct(queues, 99),
-                      "batches": st["batches"]},
-           "plain": {"value": tot_work / t_plain, "p50_s": pct(plain_lat, 50), "p99_s": pct(plain_lat, 99),
-                     "total_s": round(t_plain, 4)},
-           "served_over_plain": round(capacity / (tot_work / t_plain), 3),
+                      "poisson_rate_per_s": round(rate, 3), "throughput_at_80pct": tot_work / busy_p,
+                      "p50_s": pct(lats, 50), "p99_s": pct(lats, 99), "queue_p99_s": pct(queues, 99)},
+           "plain": {"value": plain, "p50_s": pct(plain_lat, 50), "p99_s": pct(plain_lat, 99),
+                     "total_s": round(sum(plain_lat), 4)},
+           "tc_per_call": {"value": tot_work / sum(tc_lat), "p50_s": pct(tc_lat, 50), "p99_s": pct(tc_lat, 99),
+                           "total_s": round(sum(tc_lat), 4)},
+           "served_over_plain": round(capacity / plain, 3),
            "gpu_launches": None, "e2e": None, "cpu_baseline": None}
     print(json.dumps(out))
     for f, t, _, _ in base.values():
@@ -507,6 +535,15 @@ def main():
     wts = torch.empty(P, dtype=torch.float32, device=dev)
     launches_per_step = 2 if job.nchan == 1 else 7  # prep, tile rings, count, scan, row offsets, weights, sums
 
+    tune = None
+    if engine != api.ENGINE_FP32 and job.nchan > 1:
+        if args.tc_config is not None:
+            ctx.tc_set_config(args.tc_config)
+            tune = {"config": args.tc_config, "how": "fixed by --tc-config"}
+        else:
+            best, ms = ctx.autotune(field, target, reps=2)
+            tune = {"config": best, "ms_per_config": [round(m, 3) for m in ms],
+                    "how": "hcg_autotune: best of 2 timed runs per pipeline shape"}
     for _ in range(args.warmup):
         ctx.grid(field, target, cube, wts, engine=engine)
     ctx.synchronize()
@@ -629,7 +666,8 @@ def main():
                           "samples": job.n, "channels": job.nchan, "pixels": P, "nside": ctx.info(field).nside,
                           "parallelism": "replica per GPU" if world > 1 else "single GPU",
                           "l2": "inputs larger than L2 (spectra %.1f GB), no flush" % (4 * job.n * job.nchan / 1e9),
-                          "engine": ENGINE_TEXT[args.engine] if job.nchan > 1 else ENGINE_TEXT["fp32"]},
+                          "engine": ENGINE_TEXT[args.engine] if job.nchan > 1 else ENGINE_TEXT["fp32"],
+                          "tc_pipeline": tune},
                "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,
                "e2e": e2e, "cpu_baseline": cpu}
         print(json.dumps(out))

@@ -57,6 +57,8 @@ EXPORTS = {
                           C.POINTER(C.c_void_p)], C.c_int),
     "hcg_field_set_spectra": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_field_split_spectra": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_tc_set_config": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_autotune": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_sorted": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_destroy": ([C.c_void_p], C.c_int),
     "hcg_field_share": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
@@ -93,7 +95,9 @@ _lib = None
 
 
 def lib_path() -> str:
-    return _build.LIB
+    """The library this process loads: HCGRID_B200_LIB when set (another
+    build of the same library), else the in-tree build."""
+    return os.environ.get("HCGRID_B200_LIB") or _build.LIB
 
 
 def load(build_if_missing: bool = False):
@@ -261,6 +265,17 @@ class Context:
 
     def synchronize(self):
         self._check(self.L.hcg_synchronize(self.h))
+
+    def tc_set_config(self, config: int, channel_class: int = -1):
+        self._check(self.L.hcg_tc_set_config(self.h, channel_class, config))
+
+    def autotune(self, field: "Field", target: "Target", reps: int = 2):
+        """Time each tensor-core pipeline shape on (field, target); keeps and
+        returns the fastest with the per-shape best times (ms)."""
+        best = C.c_int()
+        ms = (C.c_float * 3)()
+        self._check(self.L.hcg_autotune(self.h, field.h, target.h, reps, C.byref(best), ms))
+        return best.value, list(ms)
 
     def grid_batch(self, jobs):
         """jobs: list of (field, target, cube_tensor, weights_tensor_or_None, layout) with CUDA tensors."""

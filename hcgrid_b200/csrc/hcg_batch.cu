@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(256) kb_tile_rings(BatchHdr *H, const JobDesc 
 template <bool COUNT>
 __global__ void __launch_bounds__(256) kb_group(BatchHdr *H, const JobDesc *__restrict__ jobs) {
     __shared__ PixPrep s_prep[8][4];
+    __shared__ PixHalf s_half[8][4];
     const int warp = threadIdx.x >> 5;
     for (;;) {
         unsigned long long it = warp_fetch(H, COUNT ? Q_COUNT : Q_GEOM);
@@ -131,7 +132,8 @@ __global__ void __launch_bounds__(256) kb_group(BatchHdr *H, const JobDesc *__re
                 continue;
             }
         }
-        group_item<COUNT>(J.a, J.g, J.cap, J.off, H->e_idx, H->e_w, J.cnt, J.wsum, J.T, grp, s_prep[warp]);
+        group_item<COUNT>(J.a, J.g, J.cap, J.off, H->e_idx, H->e_w, J.cnt, J.wsum, J.T, grp, s_prep[warp],
+                          s_half[warp]);
     }
 }
 
@@ -181,12 +183,15 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
 
 // Tensor-core channel sums: one CTA per SM takes (job, channel block, tile)
 // items from the queue; barrier phases and TMEM persist across items.
+using KbTcCfg = TcCfgN4S2;  // the batch kernel's pipeline shape
+constexpr int kKbTcConfig = 0;
+
 __global__ void __launch_bounds__(kTcThreads, 1)
     kb_tc(BatchHdr *H, const JobDesc *__restrict__ jobs, const void *zero_page, unsigned long long *timeouts,
           unsigned long long *macs) {
     __shared__ TcShared S;
     if (H->pool_overflow) return;  // entries incomplete: this pass is replayed after the pool grows
-    tc_setup(S);
+    tc_setup<KbTcCfg>(S);
     uint32_t gk = 0, itn = 0;
     for (;;) {
         if (threadIdx.x == 0) S.item = S.abort ? ~0ULL : atomicAdd(&H->head[Q_TC], 1ULL);
@@ -200,11 +205,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint64_t tile = local % ntiles;  // tiles fastest: neighbours share staged samples in L2
         tc_load_rings(S, J.T, tile);
         __syncthreads();
-        tc_item(S, J, tile, (uint32_t)(local / ntiles), gk, itn, zero_page, timeouts, macs);
+        tc_item<KbTcCfg>(S, J, tile, (uint32_t)(local / ntiles), gk, itn, zero_page, timeouts, macs);
         ++itn;
         __syncthreads();  // every role is done with the item's ring table and accumulator
     }
-    tc_teardown(S, gk, timeouts);
+    tc_teardown<KbTcCfg>(S, gk, timeouts);
 }
 
 __global__ void __launch_bounds__(256) kb_1chan(BatchHdr *H, const JobDesc *__restrict__ jobs) {
@@ -231,8 +236,8 @@ struct BatchState {
     uint32_t job_cap = 0;
     cudaGraphExec_t exec = nullptr;
     int nsm = 0;
-    void *scratch[8] = {};
-    size_t scratch_size[8] = {};
+    void *scratch[9] = {};
+    size_t scratch_size[9] = {};
     CUtensorMap *d_maps = nullptr, *h_maps = nullptr;  // 2 per job: hi, lo
     unsigned long long *d_jovf = nullptr, *h_jovf = nullptr;  // per job: tiles beyond the ring table
     uint32_t map_cap = 0;
@@ -261,7 +266,7 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     const int smem = kStageSlots * kSlice * (int)sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(kb_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    if ((e = tc_set_smem((const void *)kb_tc)) != cudaSuccess) return e;
+    if ((e = tc_set_smem((const void *)kb_tc, KbTcCfg::kSmem)) != cudaSuccess) return e;
     cudaGraph_t graph;
     if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
     cudaMemsetAsync(&B.d_hdr->head[0], 0, sizeof(B.d_hdr->head), s);
@@ -273,7 +278,7 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     kb_scan<<<1, 1024, 0, s>>>(B.d_hdr);
     kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
     kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
-    kb_tc<<<n, kTcThreads, kTcSmem, s>>>(B.d_hdr, B.d_jobs, B.zero_page, &ctx->d_stats->timeouts,
+    kb_tc<<<n, kTcThreads, KbTcCfg::kSmem, s>>>(B.d_hdr, B.d_jobs, B.zero_page, &ctx->d_stats->timeouts,
                                           &ctx->d_stats->tc_macs);
     kb_1chan<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -314,8 +319,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
         if ((e = cudaMallocAsync(&B->d_hdr, sizeof(BatchHdr), s)) != cudaSuccess ||
             (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess ||
-            (e = cudaMallocAsync(&B->zero_page, 2 * kAHalf, s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(B->zero_page, 0, 2 * kAHalf, s)) != cudaSuccess) {
+            (e = cudaMallocAsync(&B->zero_page, (size_t)kTcZeroWindows * 2 * kAHalf, s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(B->zero_page, 0, (size_t)kTcZeroWindows * 2 * kAHalf, s)) != cudaSuccess) {
             if (B->d_hdr) cudaFreeAsync(B->d_hdr, s);
             if (B->h_hdr) cudaFreeHost(B->h_hdr);
             if (B->zero_page) cudaFreeAsync(B->zero_page, s);
@@ -366,7 +371,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         d.nslices = tc ? 0 : (f->cstride + kSlice - 1) / kSlice;
         if (tc) {
             d.T.pad = 8;  // ring runs as boxes of 8 samples
-            if (!tc_prepare_job(f, &B.h_maps[2 * i], &B.h_maps[2 * i + 1], d.tc)) {
+            if (!tc_prepare_job(f, KbTcCfg::kNb, &B.h_maps[2 * i], &B.h_maps[2 * i + 1], d.tc)) {
                 why = "cuTensorMapEncodeTiled";
                 return cudaErrorInvalidValue;
             }
@@ -384,14 +389,15 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if (tc) tcn += ntiles * d.tc.ncb;
         if (f->nchan == 1) c1 += P;
     }
-    void *p_prep, *p_wsum, *p_cap, *p_cnt, *p_off, *p_tiles;
+    void *p_prep, *p_wsum, *p_cap, *p_cnt, *p_off, *p_tiles, *p_ridx;
     const size_t tile_words = 3 + kTileMaxRings + kTileMaxRings + 1;  // r0, nr, U, ulo[], base[]
     if ((e = grow(B, 0, (pix + 1) * sizeof(PixPrep), s, &p_prep)) != cudaSuccess ||
         (e = grow(B, 1, (pix + 1) * sizeof(double), s, &p_wsum)) != cudaSuccess ||
         (e = grow(B, 2, (grp + 1) * sizeof(uint32_t), s, &p_cap)) != cudaSuccess ||
         (e = grow(B, 3, (grp + 1) * sizeof(uint32_t), s, &p_cnt)) != cudaSuccess ||
         (e = grow(B, 4, (grp + 2) * sizeof(unsigned long long), s, &p_off)) != cudaSuccess ||
-        (e = grow(B, 5, (tile + 1) * tile_words * sizeof(uint32_t), s, &p_tiles)) != cudaSuccess)
+        (e = grow(B, 5, (tile + 1) * tile_words * sizeof(uint32_t), s, &p_tiles)) != cudaSuccess ||
+        (e = grow(B, 8, (tile + 1) * kTileMaxSpan * sizeof(uint16_t), s, &p_ridx)) != cudaSuccess)
         return e;
     if (B.entry_cap == 0) B.entry_cap = 1ULL << 24;
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -415,14 +421,14 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             d.cap = (uint32_t *)p_cap + d.grp_base;
             d.cnt = (uint32_t *)p_cnt + d.grp_base;
             d.off = (unsigned long long *)p_off + d.grp_base;
-            d.a = GridArgs{f->hpx, f->d_rings, d.prep, f->d_keys, f->d_l2, f->d_b2, f->d_cb2, f->d_w,
-                           f->sphere_radius, f->kparam0, ctx->d_stats};
+            d.a = grid_args(f, d.prep, ctx->d_stats);
             d.T.t0 = 0;
             d.T.r0 = t_r0 + d.tile_base;
             d.T.nr = t_nr + d.tile_base;
             d.T.U = t_U + d.tile_base;
             d.T.ulo = t_ulo + d.tile_base * kTileMaxRings;
             d.T.base = t_base + d.tile_base * (kTileMaxRings + 1);
+            d.T.ring_idx = (uint16_t *)p_ridx + d.tile_base * kTileMaxSpan;
             d.T.overflow = B.d_jovf + i;
             d.X = t->d_x;
             d.Y = t->d_y;
@@ -499,7 +505,50 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         for (uint32_t i = 0; i < njobs; ++i)
             if (B.h_jovf[i] && jobs[i].field->nchan > 1) fallback[i] = 1;
         if (B.h_hdr->pool_overflow == 0) return cudaSuccess;
-        B.entry_cap = B.h_hdr->entries_needed + (B.h_hdr->entries_needed >> 3) + 1024;  // grow and replay once
+        const unsigned long long need = B.h_hdr->entries_needed + (B.h_hdr->entries_needed >> 3) + 1024;
+        const unsigned long long max_pool = ctx->entry_budget / (sizeof(uint32_t) + sizeof(float4));
+        if (need <= max_pool) {
+            B.entry_cap = need;  // grow and replay once
+            continue;
+        }
+        // The batch's entries exceed the context's entry budget: the jobs with
+        // the most entries go to the single-job path (which runs them in
+        // budget-sized passes) and the others are batched again.
+        std::vector<unsigned long long> lo(njobs), hi(njobs);
+        for (uint32_t i = 0; i < njobs; ++i) {
+            const unsigned long long *o = (const unsigned long long *)p_off;
+            if ((e = cudaMemcpyAsync(&lo[i], o + J[i].grp_base, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                     s)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(&hi[i], o + J[i].grp_base + J[i].g.ngroups, sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+                return e;
+        }
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        std::vector<uint32_t> order(njobs);
+        for (uint32_t i = 0; i < njobs; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return hi[a] - lo[a] > hi[b] - lo[b]; });
+        unsigned long long total = B.h_hdr->entries_needed;
+        std::vector<char> out(njobs, 0);
+        for (uint32_t k = 0; k < njobs && total + (total >> 3) + 1024 > max_pool; ++k) {
+            out[order[k]] = 1;
+            total -= hi[order[k]] - lo[order[k]];
+        }
+        std::vector<hcg_job> rest;
+        std::vector<uint32_t> rest_idx;
+        for (uint32_t i = 0; i < njobs; ++i)
+            if (!out[i]) {
+                rest.push_back(jobs[i]);
+                rest_idx.push_back(i);
+            }
+        std::vector<char> sub_fallback;
+        if (!rest.empty()) {
+            B.entry_cap = total + (total >> 3) + 1024;
+            if ((e = grid_batch(ctx, (uint32_t)rest.size(), rest.data(), sub_fallback, why)) != cudaSuccess) return e;
+        }
+        fallback = out;
+        for (size_t k = 0; k < rest_idx.size(); ++k)
+            if (sub_fallback[k]) fallback[rest_idx[k]] = 1;
+        return cudaSuccess;
     }
     why = "entry pool still too small after growing";
     return cudaErrorMemoryAllocation;

@@ -76,7 +76,7 @@ void release_field(hcg_field *f, cudaStream_t s) {
     if (f->d_spec) cudaFreeAsync(f->d_spec, s);
     free_split(f, s);
     if (f->geom_refs && --*f->geom_refs > 0) return;
-    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_lut, f->d_rings};
+    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_half, f->d_lut, f->d_rings};
     for (void *p : ps)
         if (p) cudaFreeAsync(p, s);
     delete f->geom_refs;
@@ -527,6 +527,65 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
             CK(ctx, cudaMemcpyAsync(weights_out, dw, P * sizeof(float), cudaMemcpyDeviceToHost, s), "weights download");
         CK(ctx, cudaStreamSynchronize(s), "grid");
     }
+    return HCG_OK;
+}
+
+hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    if (config < -1 || config >= kTcConfigCount || channel_class < -1 || channel_class >= kTcClasses)
+        return fail(ctx, HCG_EINVAL, "unknown tensor-core pipeline shape or channel class");
+    for (int c = 0; c < kTcClasses; ++c)
+        if (channel_class < 0 || c == channel_class) ctx->tc_config[c] = config;
+    return HCG_OK;
+}
+
+hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, int *best,
+                        float *ms) {
+    if (!ctx || !field || !target || reps < 1) return HCG_EINVAL;
+    int cls;
+    {
+        Guard g(ctx);
+        if (!field->xfmt || field->nchan < 2)
+            return fail(ctx, HCG_ESTATE, "autotune needs a multi-channel field with split spectra");
+        cls = tc_class_of(field->xcpad);
+    }
+    const size_t P = (size_t)target->nx * target->ny;
+    float *cube = nullptr, *wts = nullptr;
+    {
+        Guard g(ctx);
+        cudaError_t e = cudaSuccess;
+        cube = (float *)ctx->scratch.get(16, P * field->nchan * sizeof(float), ctx->stream, e);
+        wts = (float *)ctx->scratch.get(17, P * sizeof(float), ctx->stream, e);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "autotune buffers");
+    }
+    float t[kTcConfigCount];
+    int pick = 0;
+    for (int c = 0; c < kTcConfigCount; ++c) {
+        {
+            Guard g(ctx);
+            ctx->tc_config[cls] = c;
+        }
+        t[c] = 3.4e38f;
+        for (int r = 0; r < reps + 1; ++r) {  // the first run is a warm-up
+            hcg_status st = hcg_grid(ctx, field, target, cube, HCG_LAYOUT_SAMPLE_MAJOR, wts, HCG_MEM_DEVICE,
+                                     field->xfmt);
+            if (st != HCG_OK) return st;
+            Guard g(ctx);
+            CK(ctx, cudaStreamSynchronize(ctx->stream), "autotune");
+            float m = 0.f;
+            if (cudaEventElapsedTime(&m, ctx->ev0, ctx->ev1) != cudaSuccess) cudaGetLastError();
+            if (r > 0 && m < t[c]) t[c] = m;
+        }
+        if (t[c] < t[pick]) pick = c;
+    }
+    {
+        Guard g(ctx);
+        ctx->tc_config[cls] = pick;
+    }
+    if (best) *best = pick;
+    if (ms)
+        for (int c = 0; c < kTcConfigCount; ++c) ms[c] = t[c];
     return HCG_OK;
 }
 

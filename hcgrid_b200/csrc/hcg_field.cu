@@ -233,15 +233,20 @@ __global__ void k_ring_table(HpxParams h, uint64_t firstring, uint64_t usedrings
 __global__ void k_permute_geometry(uint64_t n, const uint32_t *__restrict__ perm, const double *__restrict__ lon,
                                    const double *__restrict__ lat, const double *__restrict__ w,
                                    double *__restrict__ l2, double *__restrict__ b2, double *__restrict__ cb2,
-                                   double *__restrict__ wout) {
+                                   double *__restrict__ wout, double4 *__restrict__ half) {
     uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t i = perm[j];
     double b = dmul(lat[i], kDeg2Rad);
-    l2[j] = dmul(lon[i], kDeg2Rad);
+    double l = dmul(lon[i], kDeg2Rad);
+    l2[j] = l;
     b2[j] = b;
     cb2[j] = cos(b);
     wout[j] = w ? w[i] : 1.0;
+    double4 q;
+    sincos(l * 0.5, &q.x, &q.y);
+    sincos(b * 0.5, &q.z, &q.w);
+    half[j] = q;
 }
 
 // out[j][0..cstride) = in[perm[j]][0..nchan), zero padded; one warp per row.
@@ -353,9 +358,10 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
     TRY(cudaMallocAsync(&f->d_l2, n * sizeof(double), s));
     TRY(cudaMallocAsync(&f->d_b2, n * sizeof(double), s));
     TRY(cudaMallocAsync(&f->d_cb2, n * sizeof(double), s));
+    TRY(cudaMallocAsync(&f->d_half, n * sizeof(double4), s));
     TRY(cudaMallocAsync(&f->d_w, n * sizeof(double), s));
     k_permute_geometry<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, f->d_perm, d_lon, d_lat, d_w, f->d_l2, f->d_b2,
-                                                                   f->d_cb2, f->d_w);
+                                                                   f->d_cb2, f->d_w, f->d_half);
     TRY(cudaGetLastError());
 fail:
     if (k0) cudaFreeAsync(k0, s);

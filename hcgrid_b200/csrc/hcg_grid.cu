@@ -59,9 +59,10 @@ __global__ void __launch_bounds__(256) k_group(GridArgs a, GroupArgs g, uint32_t
                                                uint32_t *__restrict__ cnt, double *__restrict__ wsum,
                                                TileArgs tiles) {
     __shared__ PixPrep s_prep[8][4];
+    __shared__ PixHalf s_half[8][4];
     int warp = threadIdx.x >> 5;
     uint64_t grp = g.g0 + blockIdx.x * 8ull + warp;
-    if (grp < g.g1) group_item<COUNT>(a, g, cap, off, e_idx, e_w, cnt, wsum, tiles, grp, s_prep[warp]);
+    if (grp < g.g1) group_item<COUNT>(a, g, cap, off, e_idx, e_w, cnt, wsum, tiles, grp, s_prep[warp], s_half[warp]);
 }
 
 __global__ void __launch_bounds__(256) k_group_accum(GroupArgs g, const unsigned long long *__restrict__ off,
@@ -162,8 +163,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
     k_pixel_prep<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(f->hpx, f->firstring, f->usedrings, f->disc_size, P,
                                                               t->d_x, t->d_y, prep, ctx->d_stats);
     cudaEventRecord(ctx->evp[0], s);
-    GridArgs a{f->hpx, f->d_rings, prep, f->d_keys, f->d_l2, f->d_b2, f->d_cb2, f->d_w,
-               f->sphere_radius, f->kparam0, ctx->d_stats};
+    const GridArgs a = grid_args(f, prep, ctx->d_stats);
     if (f->nchan == 1) {
         cudaEventRecord(ctx->evp[1], s);
         cudaEventRecord(ctx->evp[2], s);
@@ -196,6 +196,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         T.U = (uint32_t *)ctx->scratch.get(10, ntiles * sizeof(uint32_t), s, e);
         T.ulo = (uint32_t *)ctx->scratch.get(11, ntiles * kTileMaxRings * sizeof(uint32_t), s, e);
         T.base = (uint32_t *)ctx->scratch.get(12, ntiles * (kTileMaxRings + 1) * sizeof(uint32_t), s, e);
+        T.ring_idx = (uint16_t *)ctx->scratch.get(14, ntiles * kTileMaxSpan * sizeof(uint16_t), s, e);
         unsigned long long *rowoff =
             (unsigned long long *)ctx->scratch.get(13, (T.nty + 2) * sizeof(unsigned long long), s, e);
         T.overflow = &ctx->d_stats->overflow;
@@ -221,8 +222,8 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
         const bool tiled = ro[T.nty + 1] == 0;  // every tile's ring span fits the tile table
         if (tc && !tiled && !f->d_spec) {
-            why = "a tile spans more than " + std::to_string(kTileMaxRings) +
-                  " rings: the FP32 fallback needs the FP32 spectra";
+            why = "a tile spans more than " + std::to_string(kTileMaxSpan) + " rings or holds samples in more than " +
+                  std::to_string(kTileMaxRings) + ": the FP32 fallback needs the FP32 spectra";
             return cudaErrorInvalidValue;
         }
         const unsigned long long budget = ctx->entry_budget / (sizeof(uint32_t) + sizeof(float4));

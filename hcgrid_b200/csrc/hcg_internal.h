@@ -83,6 +83,7 @@ struct hcg_context {
     cudaEvent_t evp[4] = {nullptr, nullptr, nullptr, nullptr};  // phase boundaries inside hcg_grid
     float last_ms = 0.f;
     unsigned long long entry_budget = 4ULL << 30;  // bytes of (sample, weights) entries per launch run
+    int tc_config[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // tensor-core pipeline shape per channel class (-1: default)
     void *batch = nullptr;                          // batch engine state (hcg_batch.cu)
 };
 
@@ -99,6 +100,7 @@ struct hcg_field {
     double *d_b2 = nullptr;
     double *d_cb2 = nullptr;      // cos(b2)
     double *d_w = nullptr;        // per-sample input weight, sorted
+    double4 *d_half = nullptr;    // sorted: sin(l/2), cos(l/2), sin(b/2), cos(b/2) of each sample
     uint32_t *d_lut = nullptr;    // usedrings + 1
     hcg::RingRec *d_rings = nullptr;
     float *d_spec = nullptr;      // [n][cstride], sorted
@@ -120,6 +122,15 @@ struct hcg_target {
 
 // Launchers (hcg_field.cu, hcg_grid.cu). All return cudaGetLastError().
 namespace hcg {
+constexpr int kTcClasses = 8;
+constexpr int kTcConfigCount = 3;  // tensor-core pipeline shapes (hcg_tc_set_config)
+// channel class of a split field: 64-channel blocks 1, 2, 3-4, 5-8, ... -> 0, 1, 2, 3, ...
+inline int tc_class_of(uint32_t cpad) {
+    const uint32_t b = cpad / 64;
+    int c = 0;
+    while ((1u << c) < b && c < kTcClasses - 1) ++c;
+    return c;
+}
 // HCG_ENGINE_AUTO: the tensor-core engine of the field's split spectra
 // (multi-channel fields with finite spectra), else the FP32 engine.
 inline int auto_engine(const hcg_field *f) {

@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "hcg_internal.h"
 
 namespace hcg {
@@ -165,7 +167,77 @@ struct GridArgs {
     const double *l2, *b2, *cb2, *w;
     double sphere_radius, p0;
     DevStats *stats;
+    const double4 *half;  // per sorted sample: sin(l/2), cos(l/2), sin(b/2), cos(b/2)
+    double hlo, hhi;      // haversine thresholds bracketing sphere_radius (see pair_weight)
+    int series;           // d^2 from the arcsine-squared series (small sphere_radius)
 };
+
+// Host: GridArgs of a field. The cutoff d < r (d = 2 asin(sqrt(h)) in degrees,
+// helpers.cu:128-130) is decided from the haversine h alone when h is outside
+// [h* (1 - 1e-9), h* (1 + 1e-9)], h* = sin^2(r / 2): the device's h and d carry
+// relative errors below 1e-12 there, so the decision is the one the full
+// formula takes. Inside the band the full formula decides.
+inline GridArgs grid_args(const hcg_field *f, const PixPrep *prep, DevStats *stats) {
+    GridArgs a{f->hpx, f->d_rings, prep, f->d_keys, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->sphere_radius,
+               f->kparam0, stats, f->d_half, 0.0, 0.0, 0};
+    const double s = std::sin(f->sphere_radius * kDeg2Rad * 0.5);
+    const double hstar = s * s;
+    a.hlo = hstar * (1.0 - 1e-9);
+    a.hhi = hstar * (1.0 + 1e-9);
+    a.series = hstar < 1e-3;
+    return a;
+}
+
+// 32-byte read-only load (no double4 overload of __ldg)
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Pixel side of the pair test: half-angle sines and cosines.
+struct PixHalf {
+    double sl, cl, sb, cb;
+};
+__device__ __forceinline__ PixHalf pix_half(const PixPrep &P) {
+    PixHalf q;
+    sincos(P.l1 * 0.5, &q.sl, &q.cl);
+    sincos(P.b1 * 0.5, &q.sb, &q.cb);
+    return q;
+}
+
+// Weight of sample idx for the pixel (0 outside sphere_radius): the
+// haversine h = sin^2(db/2) + cos b1 cos b2 sin^2(dl/2) with the half-angle
+// differences expanded from precomputed sines and cosines; d^2 for accepted
+// pairs from asin^2(x) = sum_n (2x)^(2n) / (2 n^2 C(2n, n)) at x = sqrt(h)
+// (five terms; used when h* < 1e-3, truncation below 1e-16 relative), else
+// from asin itself. Pairs inside the threshold band take the full formula.
+__device__ __forceinline__ double pair_weight_s(const GridArgs &a, const PixPrep &P, const PixHalf &q,
+                                                const double4 &s, double cb2, double win, uint32_t idx) {
+    const double sb = q.sb * s.w - q.cb * s.z;  // sin((b1 - b2) / 2)
+    const double sl = q.sl * s.y - q.cl * s.x;  // sin((l1 - l2) / 2)
+    const double h = sb * sb + P.cb1 * cb2 * (sl * sl);
+    if (h > a.hhi) return 0.0;
+    double d2;
+    if (h < a.hlo) {
+        if (a.series) {
+            const double t = h * (1.0 + h * (1.0 / 3.0 + h * (8.0 / 45.0 + h * (4.0 / 35.0 + h * (128.0 / 1575.0)))));
+            d2 = 4.0 * t * (kRad2Deg * kRad2Deg);
+        } else {
+            const double d = 2.0 * asin(sqrt(h)) * kRad2Deg;
+            d2 = d * d;
+        }
+    } else {
+        const double d = dist_deg(P.l1, P.b1, P.cb1, __ldg(a.l2 + idx), __ldg(a.b2 + idx), cb2);
+        if (!(d < a.sphere_radius)) return 0.0;
+        d2 = d * d;
+    }
+    return win * exp(-d2 * a.p0);
+}
+
+__device__ __forceinline__ double pair_weight(const GridArgs &a, const PixPrep &P, const PixHalf &q, uint32_t idx) {
+    return pair_weight_s(a, P, q, ldg4(a.half + idx), __ldg(a.cb2 + idx), __ldg(a.w + idx), idx);
+}
 
 // Single channel: one warp per pixel, FP64 throughout.
 // Warp-collective: every lane passes the same pixel p.
@@ -173,6 +245,7 @@ __device__ __forceinline__ void grid1_item(const GridArgs &a, const float *__res
                                            float *__restrict__ out, float *__restrict__ wout, uint64_t p) {
     int lane = threadIdx.x & 31;
     const PixPrep P = a.prep[p];
+    const PixHalf ph = pix_half(P);
     double acc = 0.0, ws = 0.0;
     unsigned long long cand = 0, within = 0, skips = 0;
     for (int rb = 0; rb < P.nr; rb += 32) {
@@ -197,10 +270,9 @@ __device__ __forceinline__ void grid1_item(const GridArgs &a, const float *__res
             uint32_t s_len = __shfl_sync(0xffffffffu, len, src);
             if (t < total) {
                 uint32_t idx = s_lo + (t - (s_incl - s_len));
-                double d = dist_deg(P.l1, P.b1, P.cb1, __ldg(a.l2 + idx), __ldg(a.b2 + idx), __ldg(a.cb2 + idx));
+                const double wt = pair_weight(a, P, ph, idx);
                 ++cand;
-                if (d < a.sphere_radius) {
-                    double wt = __ldg(a.w + idx) * exp(-d * d * a.p0);
+                if (wt > 0.0) {
                     acc += (double)__ldg(data + (uint64_t)idx * cstride) * wt;
                     ws += wt;
                     ++within;
@@ -233,15 +305,19 @@ struct GroupArgs {
 };
 
 // Tiles of kTileX x kTileY pixels (kTileX/2 x kTileY/2 groups) whose union of
-// ring windows is staged in shared memory by k_tile_accum. Per tile: first
-// ring, ring count (0 = no samples), union size U and, per ring j, the union
-// interval start ulo[j] and its slot base[j] in the staged list.
-constexpr int kTileX = 16, kTileY = 8, kTileMaxRings = 1024;
+// ring windows is staged in shared memory by the accumulation kernels. Per
+// tile: first ring r0 of its ring span, the number nr of rings of the span
+// that hold union candidates (0 = no samples), the union size U and, per such
+// ring c (in ring order), the union interval start ulo[c] and its slot
+// base[c] in the staged list; ring_idx maps ring r0 + j of the span to c.
+// Pixels much larger than the kernel give long spans with few occupied rings.
+constexpr int kTileX = 16, kTileY = 8, kTileMaxRings = 1024, kTileMaxSpan = 4096;
 struct TileArgs {
     uint32_t ntx, nty;
     uint64_t t0;  // first tile of this launch
     int *r0, *nr;
     uint32_t *U, *ulo, *base;  // ulo: [tile][kTileMaxRings], base: [tile][kTileMaxRings + 1]
+    uint16_t *ring_idx;        // [tile][kTileMaxSpan]: index c of ring r0 + j (0xffff: no candidates)
     unsigned long long *overflow;
     uint32_t pad;  // ring runs take a multiple of `pad` slots (> 1: the tensor-core engine's 8-row boxes)
 };
@@ -266,7 +342,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
                                            const unsigned long long *__restrict__ off,
                                            uint32_t *__restrict__ e_idx, float4 *__restrict__ e_w,
                                            uint32_t *__restrict__ cnt, double *__restrict__ wsum,
-                                           const TileArgs &tiles, uint64_t grp, PixPrep *s_prep) {
+                                           const TileArgs &tiles, uint64_t grp, PixPrep *s_prep, PixHalf *s_half) {
     int lane = threadIdx.x & 31;
     __syncwarp();
     uint32_t gyi = (uint32_t)(grp / g.gx), gxi = (uint32_t)(grp % g.gx);
@@ -278,7 +354,10 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
         valid[q] = xx < g.nx && yy < g.ny;
         pix[q] = (uint64_t)yy * g.nx + xx;
     }
-    if (lane < 4 && valid[lane]) s_prep[lane] = a.prep[pix[lane]];
+    if (lane < 4 && valid[lane]) {
+        s_prep[lane] = a.prep[pix[lane]];
+        if (!COUNT) s_half[lane] = pix_half(s_prep[lane]);
+    }
     __syncwarp();
     int R0 = 1 << 30, R1 = -1;
 #pragma unroll
@@ -307,8 +386,10 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
         uint32_t glo = 0xffffffffu, ghi = 0;
         long long slot_shift = 0;  // slot = idx + slot_shift for this lane's ring
         if (slots && k <= R1) {
-            uint64_t j = tile * kTileMaxRings + (uint64_t)(k - tr0);
-            slot_shift = (long long)tiles.base[tile * (kTileMaxRings + 1) + (k - tr0)] - (long long)tiles.ulo[j];
+            const uint32_t c = tiles.ring_idx[tile * kTileMaxSpan + (uint64_t)(k - tr0)];
+            if (c < kTileMaxRings)  // rings without tile candidates have none for the group either
+                slot_shift = (long long)tiles.base[tile * (kTileMaxRings + 1) + c] -
+                             (long long)tiles.ulo[tile * kTileMaxRings + c];
         }
         if (k <= R1) {
             const RingRec R = a.rings[k];
@@ -354,16 +435,14 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
             bool any = false;
             if (t < total) {
                 idx = s_glo + (t - s_excl);
-                double l2 = __ldg(a.l2 + idx), b2 = __ldg(a.b2 + idx), cb2 = __ldg(a.cb2 + idx);
-                double win = __ldg(a.w + idx);
+                const double4 hs = ldg4(a.half + idx);
+                const double cb2 = __ldg(a.cb2 + idx), win = __ldg(a.w + idx);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if (idx >= s_lo[q] && idx < s_hi[q]) {
-                        const PixPrep &P = s_prep[q];
-                        double d = dist_deg(P.l1, P.b1, P.cb1, l2, b2, cb2);
+                        const double wt = pair_weight_s(a, s_prep[q], s_half[q], hs, cb2, win, idx);
                         ++cand;
-                        if (d < a.sphere_radius) {
-                            double wt = win * exp(-d * d * a.p0);
+                        if (wt > 0.0) {
                             ws[q] += wt;
                             wq[q] = (float)wt;
                             any = true;
@@ -486,7 +565,7 @@ __device__ __forceinline__ void group_accum_item(const GroupArgs &g, const unsig
 __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupArgs &g, const TileArgs &T,
                                                 uint64_t tile) {
     __shared__ PixPrep s_prep[kTileX * kTileY];
-    __shared__ uint32_t s_lo[kTileMaxRings], s_hi[kTileMaxRings];
+    __shared__ uint32_t s_lo[kTileMaxSpan], s_hi[kTileMaxSpan];
     __shared__ int s_r0, s_r1;
     const uint32_t tx0 = (uint32_t)(tile % T.ntx) * kTileX, ty0 = (uint32_t)(tile / T.ntx) * kTileY;
     const int tid = threadIdx.x;
@@ -510,12 +589,12 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
     }
     __syncthreads();
     const int r0 = s_r0, nrt = s_r1 - s_r0 + 1;
-    if (nrt <= 0 || nrt > kTileMaxRings) {
+    if (nrt <= 0 || nrt > kTileMaxSpan) {
         if (tid == 0) {
             T.r0[tile] = 0;
             T.nr[tile] = 0;
             T.U[tile] = 0;
-            if (nrt > kTileMaxRings) atomicAdd(T.overflow, 1ULL);
+            if (nrt > kTileMaxSpan) atomicAdd(T.overflow, 1ULL);
         }
         return;
     }
@@ -535,28 +614,40 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
         }
     }
     __syncthreads();
-    if (tid < 32) {  // one warp: prefix sums of the union lengths
-        uint32_t run = 0;
+    if (tid < 32) {  // one warp: compaction of the occupied rings and prefix sums of their lengths
+        uint32_t run = 0, count = 0;
         for (int jb = 0; jb < nrt; jb += 32) {
-            int j = jb + tid;
-            uint32_t len = (j < nrt && s_lo[j] < s_hi[j]) ? s_hi[j] - s_lo[j] : 0;
+            const int j = jb + tid;
+            const bool occ = j < nrt && s_lo[j] < s_hi[j];
+            uint32_t len = occ ? s_hi[j] - s_lo[j] : 0;
             if (T.pad > 1) len = (len + T.pad - 1) / T.pad * T.pad;
             uint32_t incl = len;
             for (int o = 1; o < 32; o <<= 1) {
                 uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
                 if (tid >= o) incl += v;
             }
-            if (j < nrt) {
-                T.ulo[tile * kTileMaxRings + j] = (s_lo[j] < s_hi[j]) ? s_lo[j] : 0;
-                T.base[tile * (kTileMaxRings + 1) + j] = run + incl - len;
+            const unsigned ball = __ballot_sync(0xffffffffu, occ);
+            const uint32_t c = count + __popc(ball & ((1u << tid) - 1u));
+            if (j < nrt) T.ring_idx[tile * kTileMaxSpan + j] = (occ && c < kTileMaxRings) ? (uint16_t)c : 0xffff;
+            if (occ && c < kTileMaxRings) {
+                T.ulo[tile * kTileMaxRings + c] = s_lo[j];
+                T.base[tile * (kTileMaxRings + 1) + c] = run + incl - len;
             }
             run += __shfl_sync(0xffffffffu, incl, 31);
+            count += __popc(ball);
         }
         if (tid == 0) {
-            T.base[tile * (kTileMaxRings + 1) + nrt] = run;
-            T.r0[tile] = r0;
-            T.nr[tile] = nrt;
-            T.U[tile] = run;
+            if (count > kTileMaxRings) {  // more occupied rings than the table holds
+                T.r0[tile] = 0;
+                T.nr[tile] = 0;
+                T.U[tile] = 0;
+                atomicAdd(T.overflow, 1ULL);
+            } else {
+                T.base[tile * (kTileMaxRings + 1) + count] = run;
+                T.r0[tile] = r0;
+                T.nr[tile] = (int)count;
+                T.U[tile] = run;
+            }
         }
     }
 }

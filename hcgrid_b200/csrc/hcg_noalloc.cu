@@ -116,8 +116,7 @@ extern "C" hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field,
                                                                     field->disc_size, P, target->d_x, target->d_y,
                                                                     prep, ctx->d_stats);
         for (auto &ev : ctx->evp) cudaEventRecord(ev, s);
-        GridArgs a{field->hpx, field->d_rings, prep, field->d_keys, field->d_l2, field->d_b2, field->d_cb2,
-                   field->d_w, field->sphere_radius, field->kparam0, ctx->d_stats};
+        const GridArgs a = grid_args(field, prep, ctx->d_stats);
         k_noalloc_grid<<<(unsigned)((P * 32 + 255) / 256), 256, 0, s>>>(a, P, field->d_spec, field->cstride, cube,
                                                                         weights_out);
         cudaEventRecord(ctx->ev1, s);

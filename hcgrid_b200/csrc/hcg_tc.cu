@@ -17,6 +17,7 @@
 namespace hcg {
 namespace {
 
+template <class Cfg>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tile_tc(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, TcJob J,
               const void *zero_page, unsigned long long *timeouts, unsigned long long *macs) {
@@ -25,14 +26,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     J.map_lo = &tm_lo;
     const uint64_t tile = J.T.t0 + blockIdx.x;
     tc_load_rings(S, J.T, tile);
-    tc_setup(S);  // ends with a CTA barrier
+    tc_setup<Cfg>(S);  // ends with a CTA barrier
     if (threadIdx.x == 0) {
         sm100::prefetch_tensormap(&tm_hi);
         sm100::prefetch_tensormap(&tm_lo);
     }
     uint32_t gk = 0;
-    tc_item(S, J, tile, blockIdx.y, gk, 0, zero_page, timeouts, macs);
-    tc_teardown(S, gk, timeouts);
+    tc_item<Cfg>(S, J, tile, blockIdx.y, gk, 0, zero_page, timeouts, macs);
+    tc_teardown<Cfg>(S, gk, timeouts);
 }
 
 // ------------------------------------------------------------ spectra split
@@ -193,9 +194,9 @@ cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::s
     return cudaSuccess;
 }
 
-bool tc_prepare_job(const hcg_field *f, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J) {
+bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J) {
     const uint32_t nblk64 = f->xcpad / 64;
-    J.nb = nblk64 < 4 ? nblk64 : 4;
+    J.nb = nblk64 < (uint32_t)nb_max ? nblk64 : (uint32_t)nb_max;
     J.ncb = (nblk64 + J.nb - 1) / J.nb;
     if (!make_map(map_hi, f->d_xhi, f->n, f->xcpad, J.nb) || !make_map(map_lo, f->d_xlo, f->n, f->xcpad, J.nb))
         return false;
@@ -207,30 +208,55 @@ bool tc_prepare_job(const hcg_field *f, CUtensorMap *map_hi, CUtensorMap *map_lo
     return true;
 }
 
-cudaError_t tc_set_smem(const void *kernel) {
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+cudaError_t tc_set_smem(const void *kernel, uint32_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
+
+// Pipeline shape for a field: the autotuned choice of its channel class,
+// else the widest item its channels fill.
+int tc_pick(const hcg_context *ctx, const hcg_field *f) {
+    const int t = ctx->tc_config[tc_class_of(f->xcpad)];
+    if (t >= 0 && t < kTcConfigCount) return t;
+    const uint32_t b = f->xcpad / 64;
+    return b >= 4 ? 0 : (b >= 2 ? 1 : 2);
+}
+
+namespace {
+template <class Cfg>
+cudaError_t launch_tc(hcg_context *ctx, const hcg_field *f, TcJob &J, const TileArgs &T, uint64_t ntiles,
+                      const void *zero, std::string &why) {
+    cudaStream_t s = ctx->stream;
+    CUtensorMap mh, ml;
+    if (!tc_prepare_job(f, Cfg::kNb, &mh, &ml, J)) {
+        why = "cuTensorMapEncodeTiled";
+        return cudaErrorInvalidValue;
+    }
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set) {
+        cudaError_t e = tc_set_smem((const void *)k_tile_tc<Cfg>, Cfg::kSmem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    for (uint64_t t0 = 0; t0 < ntiles; t0 += 0x7fffffffull) {
+        J.T = T;
+        J.T.t0 = T.t0 + t0;
+        dim3 grid((unsigned)std::min<uint64_t>(ntiles - t0, 0x7fffffffull), J.ncb);
+        k_tile_tc<Cfg><<<grid, kTcThreads, Cfg::kSmem, s>>>(mh, ml, J, zero, &ctx->d_stats->timeouts,
+                                                            &ctx->d_stats->tc_macs);
+    }
+    return cudaGetLastError();
+}
+}  // namespace
 
 cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, const TileArgs &T, uint64_t ntiles,
                      const unsigned long long *off, const uint32_t *cnt, const uint32_t *e_slot, const float4 *e_w,
                      const double *wsum, float *out, uint32_t ostride, float *wout, std::string &why) {
     cudaStream_t s = ctx->stream;
-    CUtensorMap mh, ml;
     TcJob J{};
-    if (!tc_prepare_job(f, &mh, &ml, J)) {
-        why = "cuTensorMapEncodeTiled";
-        return cudaErrorInvalidValue;
-    }
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = tc_set_smem((const void *)k_tile_tc);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
     cudaError_t e = cudaSuccess;
-    void *zero = ctx->scratch.get(20, 2 * kAHalf, s, e);
+    void *zero = ctx->scratch.get(20, (size_t)kTcZeroWindows * 2 * kAHalf, s, e);
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(zero, 0, 2 * kAHalf, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(zero, 0, (size_t)kTcZeroWindows * 2 * kAHalf, s)) != cudaSuccess) return e;
     J.g = g;
     J.off = off;
     J.cnt = cnt;
@@ -240,14 +266,11 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
     J.out = out;
     J.ostride = ostride;
     J.wout = wout;
-    for (uint64_t t0 = 0; t0 < ntiles; t0 += 0x7fffffffull) {
-        J.T = T;
-        J.T.t0 = T.t0 + t0;
-        dim3 grid((unsigned)std::min<uint64_t>(ntiles - t0, 0x7fffffffull), J.ncb);
-        k_tile_tc<<<grid, kTcThreads, kTcSmem, s>>>(mh, ml, J, zero, &ctx->d_stats->timeouts,
-                                                     &ctx->d_stats->tc_macs);
+    switch (tc_pick(ctx, f)) {
+        case 1: return launch_tc<TcCfgN2S3>(ctx, f, J, T, ntiles, zero, why);
+        case 2: return launch_tc<TcCfgN1S4>(ctx, f, J, T, ntiles, zero, why);
+        default: return launch_tc<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
     }
-    return cudaGetLastError();
 }
 
 }  // namespace hcg

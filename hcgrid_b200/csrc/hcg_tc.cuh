@@ -53,18 +53,31 @@ namespace hcg {
 
 constexpr int kTcM = kTileX * kTileY;  // 128 pixels: the MMA's M
 constexpr int kTcK = 64;               // slots per K chunk (one 128-byte swizzle row of 16-bit values)
-constexpr int kTcStages = 2;
 constexpr int kTcThreads = 192;
 constexpr int kTcBuilders = 128;
-constexpr uint32_t kTcMaxN = 256;                         // channels per item
-constexpr uint32_t kAHalf = kTcM * kTcK * 2;              // 16 KB
-constexpr uint32_t kBHalf = kTcK * kTcMaxN * 2;           // 32 KB
-constexpr uint32_t kStageBytes = 2 * kAHalf + 2 * kBHalf;
-constexpr uint32_t kTcSmem = kTcStages * kStageBytes + 1024;  // + alignment of the swizzle atoms
+constexpr uint32_t kAHalf = kTcM * kTcK * 2;  // 16 KB
 constexpr uint64_t kTcWaitNs = 1000000000ull;
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTcZeroWindows = 160;  // zero region: kTcZeroWindows x 32 KB (5 MB)
 static_assert(kTcM == 128, "a tile is one M=128 MMA");
 static_assert(kTcK == 64, "a chunk is 8 row boxes of 8 slots and one 128-byte swizzle row");
+
+// Pipeline shapes: NB 64-channel blocks per item (the MMA's N = 64 NB) and ST
+// stages, all in 192 KB of operand buffers. More channels per item build the
+// weight operand fewer times per channel; more stages hide more copy latency.
+template <int NB, int ST>
+struct TcCfg {
+    static constexpr int kNb = NB;
+    static constexpr int kStages = ST;
+    static constexpr uint32_t kBHalf = kTcK * 64 * NB * 2;  // one of hi / lo
+    static constexpr uint32_t kStageBytes = 2 * kAHalf + 2 * kBHalf;
+    static constexpr uint32_t kSmem = ST * kStageBytes + 1024;  // + alignment of the swizzle atoms
+    static constexpr uint32_t kTmemCols = NB * 64 <= 64 ? 64 : (NB * 64 <= 128 ? 128 : 256);
+    static_assert(ST * kStageBytes <= 192 * 1024, "operand buffers fit shared memory");
+};
+using TcCfgN4S2 = TcCfg<4, 2>;  // 256 channels per item, 2 stages
+using TcCfgN2S3 = TcCfg<2, 3>;  // 128 channels, 3 stages
+using TcCfgN1S4 = TcCfg<1, 4>;  // 64 channels, 4 stages
+static_assert(kTcConfigCount == 3, "hcg_tc_set_config numbers the three shapes above 0, 1, 2");
 
 // One job's tensor-core arguments.
 struct TcJob {
@@ -89,9 +102,10 @@ struct TcJob {
 };
 
 constexpr int kTcRing = 8;  // entries in flight per builder thread
+constexpr int kTcMaxStages = 4;
 
 struct TcShared {
-    uint64_t full_a[kTcStages], full_b[kTcStages], empty[kTcStages], zfill[kTcStages], acc_full;
+    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], zfill[kTcMaxStages], acc_full;
     uint32_t tmem;
     volatile int abort;
     unsigned long long item;
@@ -103,8 +117,9 @@ struct TcShared {
 // hcg_tc.cu: the tensor maps and format fields of a field with split
 // spectra (false: the maps could not be encoded); the shared-memory opt-in of
 // a kernel built on tc_item.
-bool tc_prepare_job(const hcg_field *f, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J);
-cudaError_t tc_set_smem(const void *kernel);
+bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J);
+cudaError_t tc_set_smem(const void *kernel, uint32_t bytes);
+int tc_pick(const hcg_context *ctx, const hcg_field *f);
 
 namespace {
 
@@ -128,11 +143,12 @@ __device__ __forceinline__ uint8_t *tc_smem_base() {
 }
 
 // Whole CTA: barriers and TMEM.
+template <class Cfg>
 __device__ __forceinline__ void tc_setup(TcShared &S) {
     using namespace sm100;
     const int tid = threadIdx.x;
     if (tid == 0) {
-        for (int s = 0; s < kTcStages; ++s) {
+        for (int s = 0; s < Cfg::kStages; ++s) {
             mbar_init(&S.full_a[s], kTcBuilders);
             mbar_init(&S.full_b[s], 1);
             mbar_init(&S.empty[s], 1);
@@ -143,7 +159,7 @@ __device__ __forceinline__ void tc_setup(TcShared &S) {
         mbar_fence_init();
     }
     if ((tid >> 5) == 1) {
-        tmem_alloc(&S.tmem, kTmemCols);
+        tmem_alloc(&S.tmem, Cfg::kTmemCols);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -158,12 +174,14 @@ __device__ __forceinline__ void tc_give_up(TcShared &S, unsigned long long *time
 
 // Whole CTA, after its last item: the producer waits (bounded) for the copies
 // of the last chunks of each stage, then TMEM is freed.
+template <class Cfg>
 __device__ __forceinline__ void tc_teardown(TcShared &S, uint32_t gk, unsigned long long *timeouts) {
     using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages;
     const int tid = threadIdx.x;
     if (tid == 0) {
-        for (uint32_t g = gk > kTcStages ? gk - kTcStages : 0; g < gk; ++g) {
-            const uint32_t s = g & 1, ph = (g >> 1) & 1;
+        for (uint32_t g = gk > ST ? gk - ST : 0; g < gk; ++g) {
+            const uint32_t s = g % ST, ph = (g / ST) & 1;
             if (!mbar_wait(&S.full_b[s], ph, kTcWaitNs) || !mbar_wait(&S.zfill[s], ph, kTcWaitNs)) {
                 tc_give_up(S, timeouts);
                 break;
@@ -174,7 +192,7 @@ __device__ __forceinline__ void tc_teardown(TcShared &S, uint32_t gk, unsigned l
     __syncthreads();
     if ((tid >> 5) == 1) {
         tc_fence_after();
-        tmem_dealloc(S.tmem, kTmemCols);
+        tmem_dealloc(S.tmem, Cfg::kTmemCols);
     }
 }
 
@@ -187,15 +205,17 @@ __device__ __forceinline__ void tc_load_rings(TcShared &S, const TileArgs &T, ui
 
 // Whole CTA: one item. `gk` counts the K chunks this CTA has run (all items),
 // `itn` its items; both advance identically in every thread.
+template <class Cfg>
 __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t tile, uint32_t cblk, uint32_t &gk,
                                         uint32_t itn, const void *zero_page, unsigned long long *timeouts,
                                         unsigned long long *macs) {
     using namespace sm100;
     uint8_t *smem = tc_smem_base();
-    auto A_hi = [&](uint32_t s) { return smem + s * kStageBytes; };
-    auto A_lo = [&](uint32_t s) { return smem + s * kStageBytes + kAHalf; };
-    auto B_hi = [&](uint32_t s) { return smem + s * kStageBytes + 2 * kAHalf; };
-    auto B_lo = [&](uint32_t s) { return smem + s * kStageBytes + 2 * kAHalf + kBHalf; };
+    constexpr uint32_t ST = Cfg::kStages;
+    auto A_hi = [&](uint32_t s) { return smem + s * Cfg::kStageBytes; };
+    auto A_lo = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + kAHalf; };
+    auto B_hi = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + 2 * kAHalf; };
+    auto B_lo = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + 2 * kAHalf + Cfg::kBHalf; };
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileArgs &T = J.T;
     const uint32_t U = T.U[tile];
@@ -208,13 +228,16 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
             const uint32_t bytes = 2u * 8u * J.nb * 1024u;
             int j = 0;
             for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
-                const uint32_t g = gk + k, s = g & 1;
-                if (g >= kTcStages && !mbar_wait(&S.empty[s], ((g >> 1) - 1) & 1, kTcWaitNs)) {
+                const uint32_t g = gk + k, s = g % ST;
+                if (g >= ST && !mbar_wait(&S.empty[s], ((g / ST) - 1) & 1, kTcWaitNs)) {
                     tc_give_up(S, timeouts);
                     break;
                 }
                 mbar_arrive_expect_tx(&S.zfill[s], 2 * kAHalf);
-                bulk_copy_g2s(A_hi(s), zero_page, 2 * kAHalf, &S.zfill[s]);
+                // each CTA copies from its own window of the zero region, so the
+                // copies of all SMs spread over the L2 slices
+                bulk_copy_g2s(A_hi(s), (const uint8_t *)zero_page + (blockIdx.x % kTcZeroWindows) * (2 * kAHalf),
+                              2 * kAHalf, &S.zfill[s]);
                 mbar_arrive_expect_tx(&S.full_b[s], bytes);
                 for (int b = 0; b < 8; ++b) {
                     const uint32_t slot0 = k * kTcK + 8 * b;
@@ -226,8 +249,8 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                         row = (int)(S.ulo[j] + (slot0 - S.base[j]));
                     }
                     const int cz = (int)(cblk * J.nb);
-                    tma_load_3d(B_hi(s) + b * 4096, J.map_hi, &S.full_b[s], 0, row, cz);
-                    tma_load_3d(B_lo(s) + b * 4096, J.map_lo, &S.full_b[s], 0, row, cz);
+                    tma_load_3d(B_hi(s) + b * (1024 * Cfg::kNb), J.map_hi, &S.full_b[s], 0, row, cz);
+                    tma_load_3d(B_lo(s) + b * (1024 * Cfg::kNb), J.map_lo, &S.full_b[s], 0, row, cz);
                 }
             }
         }
@@ -237,7 +260,7 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
             const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
             uint32_t acc = 0;
             for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
-                const uint32_t g = gk + k, s = g & 1, ph = (g >> 1) & 1;
+                const uint32_t g = gk + k, s = g % ST, ph = (g / ST) & 1;
                 if (!mbar_wait(&S.full_a[s], ph, kTcWaitNs) || !mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
                     tc_give_up(S, timeouts);
                     break;
@@ -249,8 +272,9 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                 for (int kk = 0; kk < kTcK / 16; ++kk) {
                     const uint64_t adh = smem_desc_sw128(ah + kk * 32, 16, 1024);
                     const uint64_t adl = smem_desc_sw128(al + kk * 32, 16, 1024);
-                    const uint64_t bdh = smem_desc_sw128(bh + kk * 8192, 1024, 4096);
-                    const uint64_t bdl = smem_desc_sw128(bl + kk * 8192, 1024, 4096);
+                    // 8-slot row groups at 1024 * kNb bytes; 64-channel atoms at 1024
+                    const uint64_t bdh = smem_desc_sw128(bh + kk * 2 * 1024 * Cfg::kNb, 1024, 1024 * Cfg::kNb);
+                    const uint64_t bdl = smem_desc_sw128(bl + kk * 2 * 1024 * Cfg::kNb, 1024, 1024 * Cfg::kNb);
                     mma_f16_ss(taddr, adh, bdh, idesc, acc);
                     mma_f16_ss(taddr, adh, bdl, idesc, 1);
                     mma_f16_ss(taddr, adl, bdh, idesc, 1);
@@ -302,9 +326,9 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
 #pragma unroll
         for (int q = 0; q < 4; ++q) mrow[q] = (2 * gyl + (q >> 1)) * kTileX + 2 * gxl + (q & 1);
         for (uint32_t k = 0; k < nchunks; ++k) {
-            const uint32_t g = gk + k, s = g & 1;
+            const uint32_t g = gk + k, s = g % ST;
             if (S.abort) break;
-            if (!mbar_wait(&S.zfill[s], (g >> 1) & 1, kTcWaitNs)) {  // zeroed operand: the stage is free
+            if (!mbar_wait(&S.zfill[s], (g / ST) & 1, kTcWaitNs)) {  // zeroed operand: the stage is free
                 tc_give_up(S, timeouts);
                 break;
             }

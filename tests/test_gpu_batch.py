@@ -147,3 +147,19 @@ def test_tensor_core_job_alone_equals_job_in_mix(ctx, tc_jobs):
         alone = run_batch(ctx, [tc_jobs[i]], [api.SAMPLE_MAJOR])[0]
         np.testing.assert_array_equal(alone[0], mix[i][0])
         np.testing.assert_array_equal(alone[1], mix[i][1])
+
+
+def test_batch_over_entry_budget_routes_jobs_to_single_path(ctx, jobs):
+    """When a batch's entries exceed the context's entry budget, the jobs
+    with the most entries run on the single-job path (in budget-sized
+    passes) and the rest are batched: every cube still equals its single
+    call."""
+    ctx.set_entry_budget(2_000_000)  # bytes: 100,000 entries
+    try:
+        got = run_batch(ctx, jobs, [api.SAMPLE_MAJOR] * len(jobs))
+    finally:
+        ctx.set_entry_budget(4 << 30)
+    for (job, f, t), (cube, w) in zip(jobs, got):
+        ref_cube, ref_w = single(ctx, job, f, t, api.SAMPLE_MAJOR)
+        np.testing.assert_array_equal(cube, ref_cube)
+        np.testing.assert_array_equal(w, ref_w)

@@ -162,3 +162,48 @@ def test_tc_state_and_input_checks(ctx):
         ctx.grid(f, t, engine=api.ENGINE_TC_BF16)
     c32, _ = ctx.grid(f, t, engine=api.ENGINE_FP32)  # the FP32 engine grids them
     assert np.isnan(c32[:, 3]).any()
+
+
+def test_pipeline_shapes_and_autotune(ctx, small):
+    """Every tensor-core pipeline shape (256 channels x 2 stages, 128 x 3,
+    64 x 4) gives the same weights and stays within tolerance of the oracle;
+    the autotuner times them and keeps one."""
+    job, f, t, ref, c32, w32 = small
+    prepare(ctx, job)
+    f.split_spectra(api.ENGINE_TC_F16)
+    outs = []
+    try:
+        for cfg in range(3):
+            ctx.tc_set_config(cfg)
+            c, w = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+            np.testing.assert_array_equal(w, w32)
+            err = plane_errors(c, ref)
+            print(f"pipeline shape {cfg}: max plane-relative error {err:.3e}")
+            assert err <= TOL[api.ENGINE_TC_F16]
+            outs.append(c)
+        ctx.tc_set_config(-1)
+        best, ms = ctx.autotune(f, t, reps=1)
+        print("autotune", best, ms)
+        assert best in (0, 1, 2) and all(m > 0 for m in ms)
+        with pytest.raises(RuntimeError, match="HCG_EINVAL"):
+            ctx.tc_set_config(5)
+    finally:
+        ctx.tc_set_config(-1)
+
+
+def test_coarse_pixels_many_rings(ctx):
+    """Pixels 12x the kernel (64x64 map over 13 deg, FWHM 60"): a tile's ring
+    span exceeds a thousand HEALPix rings but few of them hold candidates;
+    the compacted tile table keeps the tensor-core and FP32 tile engines on."""
+    shape = dict(block=0, n=26_206, size_deg=13.016, ra=154.57, dec=7.25, grid=64, nchan=64, fwhm=60.0, seed=5)
+    job = synth.block_job(shape)
+    prepare(ctx, job)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(np.ascontiguousarray(job.values.reshape(job.n, -1)))
+    f.nchan = job.nchan
+    t = ctx.target_from_header(job.header)
+    c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+    f.split_spectra(api.ENGINE_TC_F16, keep_fp32=False)
+    ct, wt = ctx.grid(f, t)
+    np.testing.assert_array_equal(wt, w32)
+    assert plane_errors(ct, c32.astype(np.float64)) <= 1e-5
