@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--engine", default="fp32", choices=list(ENGINES),
                     help="channel-sum engine: FP32 CUDA cores or tensor cores with a 16-bit hi/lo split")
     ap.add_argument("--tc-config", type=int, default=None,
-                    help="tensor-core pipeline shape (0: 256 ch x 2 stages, 1: 128 x 3, 2: 64 x 4); "
+                    help="tensor-core pipeline shape (0: 256 ch x 64-sample chunks x 2 stages, 1: 128 x 64 x 3, "
+                         "2: 64 x 64 x 4, 3: 256 x 32 x 4); "
                          "default: autotuned on the workload before the timed steps")
     # reduced cases (profiling, quick checks); the headline run uses none of these
     ap.add_argument("--samples", type=int, default=None)

@@ -59,6 +59,7 @@ struct BatchHdr {
     float4 *e_w;
     unsigned long long *off_all;       // [tot_grp + 1]
     uint32_t *cap_all;
+    unsigned long long *scan_part;     // [kBatchScanParts + 1]
 };
 
 constexpr int kPersistPerSM = 8;
@@ -137,33 +138,18 @@ __global__ void __launch_bounds__(256) kb_group(BatchHdr *H, const JobDesc *__re
     }
 }
 
-// Exclusive scan of all jobs' group capacities (one block).
-__global__ void __launch_bounds__(1024) kb_scan(BatchHdr *H) {
-    __shared__ unsigned long long part[1024];
-    const unsigned long long n = H->tot_grp;
-    const uint32_t *in = H->cap_all;
-    unsigned long long *out = H->off_all;
-    unsigned long long per = (n + 1023) / 1024;
-    unsigned long long b = threadIdx.x * per, e = min(n, b + per);
-    unsigned long long s = 0;
-    for (unsigned long long i = b; i < e; ++i) s += in[i];
-    part[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        unsigned long long v = (threadIdx.x >= o) ? part[threadIdx.x - o] : 0;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
-    }
-    unsigned long long run = part[threadIdx.x] - s;
-    for (unsigned long long i = b; i < e; ++i) {
-        out[i] = run;
-        run += in[i];
-    }
-    if (threadIdx.x == 1023) {
-        out[n] = part[1023];
-        H->entries_needed = part[1023];
-    }
+// Exclusive scan of all jobs' group capacities: three fixed-shape passes
+// over kBatchScanParts parts (graph-captured; the count is read on the device).
+constexpr uint32_t kBatchScanParts = 296;
+__global__ void __launch_bounds__(kScanThreads) kb_scan_sums(BatchHdr *H) {
+    scan_sums_item(H->cap_all, H->tot_grp, kBatchScanParts, H->scan_part, blockIdx.x);
+}
+__global__ void __launch_bounds__(kScanThreads) kb_scan_psum(BatchHdr *H) {
+    scan_psum_item(H->scan_part, kBatchScanParts);
+    if (threadIdx.x == 0) H->entries_needed = H->scan_part[kBatchScanParts];
+}
+__global__ void __launch_bounds__(kScanThreads) kb_scan_apply(BatchHdr *H) {
+    scan_apply_item(H->cap_all, H->tot_grp, kBatchScanParts, H->scan_part, H->off_all, blockIdx.x);
 }
 
 __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobDesc *__restrict__ jobs) {
@@ -183,7 +169,7 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
 
 // Tensor-core channel sums: one CTA per SM takes (job, channel block, tile)
 // items from the queue; barrier phases and TMEM persist across items.
-using KbTcCfg = TcCfgN4S2;  // the batch kernel's pipeline shape
+using KbTcCfg = TcCfgN4K32;  // the batch kernel's pipeline shape
 constexpr int kKbTcConfig = 0;
 
 __global__ void __launch_bounds__(kTcThreads, 1)
@@ -236,9 +222,9 @@ struct BatchState {
     uint32_t job_cap = 0;
     cudaGraphExec_t exec = nullptr;
     int nsm = 0;
-    void *scratch[9] = {};
-    size_t scratch_size[9] = {};
-    CUtensorMap *d_maps = nullptr, *h_maps = nullptr;  // 2 per job: hi, lo
+    void *scratch[10] = {};
+    size_t scratch_size[10] = {};
+    CUtensorMap *d_maps = nullptr, *h_maps = nullptr;  // two per job: spectra (hi and lo halves), cube
     unsigned long long *d_jovf = nullptr, *h_jovf = nullptr;  // per job: tiles beyond the ring table
     uint32_t map_cap = 0;
     void *zero_page = nullptr;  // the tensor-core engine's zero page
@@ -275,7 +261,9 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     kb_prep<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs, ctx->d_stats);
     kb_tile_rings<<<n * 4, 256, 0, s>>>(B.d_hdr, B.d_jobs);
     kb_group<true><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
-    kb_scan<<<1, 1024, 0, s>>>(B.d_hdr);
+    kb_scan_sums<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
+    kb_scan_psum<<<1, kScanThreads, 0, s>>>(B.d_hdr);
+    kb_scan_apply<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
     kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
     kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
     kb_tc<<<n, kTcThreads, KbTcCfg::kSmem, s>>>(B.d_hdr, B.d_jobs, B.zero_page, &ctx->d_stats->timeouts,
@@ -319,8 +307,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
         if ((e = cudaMallocAsync(&B->d_hdr, sizeof(BatchHdr), s)) != cudaSuccess ||
             (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess ||
-            (e = cudaMallocAsync(&B->zero_page, (size_t)kTcZeroWindows * 2 * kAHalf, s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(B->zero_page, 0, (size_t)kTcZeroWindows * 2 * kAHalf, s)) != cudaSuccess) {
+            (e = cudaMallocAsync(&B->zero_page, (size_t)kTcZeroWindows * kTcMaxA, s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(B->zero_page, 0, (size_t)kTcZeroWindows * kTcMaxA, s)) != cudaSuccess) {
             if (B->d_hdr) cudaFreeAsync(B->d_hdr, s);
             if (B->h_hdr) cudaFreeHost(B->h_hdr);
             if (B->zero_page) cudaFreeAsync(B->zero_page, s);
@@ -371,7 +359,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         d.nslices = tc ? 0 : (f->cstride + kSlice - 1) / kSlice;
         if (tc) {
             d.T.pad = 8;  // ring runs as boxes of 8 samples
-            if (!tc_prepare_job(f, KbTcCfg::kNb, &B.h_maps[2 * i], &B.h_maps[2 * i + 1], d.tc)) {
+            if (!tc_prepare_job(f, KbTcCfg::kNb, &B.h_maps[2 * i], d.tc)) {
                 why = "cuTensorMapEncodeTiled";
                 return cudaErrorInvalidValue;
             }
@@ -389,7 +377,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if (tc) tcn += ntiles * d.tc.ncb;
         if (f->nchan == 1) c1 += P;
     }
-    void *p_prep, *p_wsum, *p_cap, *p_cnt, *p_off, *p_tiles, *p_ridx;
+    void *p_prep, *p_wsum, *p_cap, *p_cnt, *p_off, *p_tiles, *p_ridx, *p_scan;
     const size_t tile_words = 3 + kTileMaxRings + kTileMaxRings + 1;  // r0, nr, U, ulo[], base[]
     if ((e = grow(B, 0, (pix + 1) * sizeof(PixPrep), s, &p_prep)) != cudaSuccess ||
         (e = grow(B, 1, (pix + 1) * sizeof(double), s, &p_wsum)) != cudaSuccess ||
@@ -397,7 +385,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         (e = grow(B, 3, (grp + 1) * sizeof(uint32_t), s, &p_cnt)) != cudaSuccess ||
         (e = grow(B, 4, (grp + 2) * sizeof(unsigned long long), s, &p_off)) != cudaSuccess ||
         (e = grow(B, 5, (tile + 1) * tile_words * sizeof(uint32_t), s, &p_tiles)) != cudaSuccess ||
-        (e = grow(B, 8, (tile + 1) * kTileMaxSpan * sizeof(uint16_t), s, &p_ridx)) != cudaSuccess)
+        (e = grow(B, 8, (tile + 1) * kTileMaxSpan * sizeof(uint16_t), s, &p_ridx)) != cudaSuccess ||
+        (e = grow(B, 9, (kBatchScanParts + 1) * sizeof(unsigned long long), s, &p_scan)) != cudaSuccess)
         return e;
     if (B.entry_cap == 0) B.entry_cap = 1ULL << 24;
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -429,6 +418,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             d.T.ulo = t_ulo + d.tile_base * kTileMaxRings;
             d.T.base = t_base + d.tile_base * (kTileMaxRings + 1);
             d.T.ring_idx = (uint16_t *)p_ridx + d.tile_base * kTileMaxSpan;
+            d.T.cap = d.cap;  // the tile pass counts each group's candidates
             d.T.overflow = B.d_jovf + i;
             d.X = t->d_x;
             d.Y = t->d_y;
@@ -443,8 +433,10 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             d.wout = jobs[i].weights;
             if (d.tc.nb) {
                 TcJob &c = d.tc;
-                c.map_hi = B.d_maps + 2 * i;
-                c.map_lo = B.d_maps + 2 * i + 1;
+                c.map = B.d_maps + 2 * i;
+                c.out_map = tc_out_map(&B.h_maps[2 * i + 1], d.out, d.ostride, d.g.nx, d.g.ny, c.nchan, c.nb)
+                                ? B.d_maps + 2 * i + 1
+                                : nullptr;
                 c.g = d.g;
                 c.T = d.T;
                 c.off = d.off;
@@ -472,6 +464,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         h.e_w = (float4 *)p_ew;
         h.off_all = (unsigned long long *)p_off;
         h.cap_all = (uint32_t *)p_cap;
+        h.scan_part = (unsigned long long *)p_scan;
         if ((e = cudaMemcpyAsync(B.d_jobs, B.h_jobs, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, s)) !=
                 cudaSuccess ||
             (e = cudaMemcpyAsync(B.d_hdr, B.h_hdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s)) != cudaSuccess ||

@@ -98,27 +98,17 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_accum(GroupArgs g, TileAr
 
 // Exclusive scan of n uint32 counts into uint64 offsets (out[n] = total),
 // one block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_scan_offsets(const uint32_t *__restrict__ in, uint64_t n,
-                                                       unsigned long long *__restrict__ out) {
-    __shared__ unsigned long long part[1024];
-    uint64_t per = (n + 1023) / 1024;
-    uint64_t b = threadIdx.x * per, e = min(n, b + per);
-    unsigned long long s = 0;
-    for (uint64_t i = b; i < e; ++i) s += in[i];
-    part[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        unsigned long long v = (threadIdx.x >= o) ? part[threadIdx.x - o] : 0;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
-    }
-    unsigned long long run = part[threadIdx.x] - s;
-    for (uint64_t i = b; i < e; ++i) {
-        out[i] = run;
-        run += in[i];
-    }
-    if (threadIdx.x == 1023) out[n] = part[1023];
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(const uint32_t *__restrict__ in, uint64_t n,
+                                                            uint32_t parts, unsigned long long *__restrict__ psum) {
+    scan_sums_item(in, n, parts, psum, blockIdx.x);
+}
+__global__ void __launch_bounds__(kScanThreads) k_scan_psum(unsigned long long *__restrict__ psum, uint32_t parts) {
+    scan_psum_item(psum, parts);
+}
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t *__restrict__ in, uint64_t n,
+                                                             uint32_t parts, const unsigned long long *__restrict__ psum,
+                                                             unsigned long long *__restrict__ out) {
+    scan_apply_item(in, n, parts, psum, out, blockIdx.x);
 }
 
 
@@ -199,14 +189,21 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         T.ring_idx = (uint16_t *)ctx->scratch.get(14, ntiles * kTileMaxSpan * sizeof(uint16_t), s, e);
         unsigned long long *rowoff =
             (unsigned long long *)ctx->scratch.get(13, (T.nty + 2) * sizeof(unsigned long long), s, e);
+        const uint32_t parts = (uint32_t)std::min<uint64_t>(1024, (g.ngroups + 4095) / 4096 + 1);
+        unsigned long long *psum =
+            (unsigned long long *)ctx->scratch.get(15, (parts + 1) * sizeof(unsigned long long), s, e);
+        T.cap = cap;  // the tile pass counts each group's candidates
         T.overflow = &ctx->d_stats->overflow;
         T.pad = tc ? 8 : 1;  // the tensor-core engine loads ring runs as boxes of 8 samples
         if (e != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(T.overflow, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
         k_tile_rings<<<(unsigned)ntiles, 256, 0, s>>>(a, g, T);
         TileArgs none{};
+        // groups of tiles whose ring span exceeds the table (cap unknown) are counted here
         k_group<true><<<gblocks, 256, 0, s>>>(a, g, cap, nullptr, nullptr, nullptr, nullptr, nullptr, none);
-        k_scan_offsets<<<1, 1024, 0, s>>>(cap, g.ngroups, off);
+        k_scan_sums<<<parts, kScanThreads, 0, s>>>(cap, g.ngroups, parts, psum);
+        k_scan_psum<<<1, kScanThreads, 0, s>>>(psum, parts);
+        k_scan_apply<<<parts, kScanThreads, 0, s>>>(cap, g.ngroups, parts, psum, off);
         // entry offsets at tile-row boundaries: the work is split into runs of
         // tile rows whose entries fit the context's entry budget
         const uint64_t groups_per_row = (uint64_t)(kTileY / 2) * g.gx;

@@ -123,7 +123,7 @@ struct hcg_target {
 // Launchers (hcg_field.cu, hcg_grid.cu). All return cudaGetLastError().
 namespace hcg {
 constexpr int kTcClasses = 8;
-constexpr int kTcConfigCount = 3;  // tensor-core pipeline shapes (hcg_tc_set_config)
+constexpr int kTcConfigCount = 4;  // tensor-core pipeline shapes (hcg_tc_set_config)
 // channel class of a split field: 64-channel blocks 1, 2, 3-4, 5-8, ... -> 0, 1, 2, 3, ...
 inline int tc_class_of(uint32_t cpad) {
     const uint32_t b = cpad / 64;

@@ -312,12 +312,15 @@ struct GroupArgs {
 // base[c] in the staged list; ring_idx maps ring r0 + j of the span to c.
 // Pixels much larger than the kernel give long spans with few occupied rings.
 constexpr int kTileX = 16, kTileY = 8, kTileMaxRings = 1024, kTileMaxSpan = 4096;
+constexpr uint32_t kCapUnknown = 0xffffffffu;
+constexpr int kTileGroups = (kTileX / 2) * (kTileY / 2);
 struct TileArgs {
     uint32_t ntx, nty;
     uint64_t t0;  // first tile of this launch
     int *r0, *nr;
     uint32_t *U, *ulo, *base;  // ulo: [tile][kTileMaxRings], base: [tile][kTileMaxRings + 1]
     uint16_t *ring_idx;        // [tile][kTileMaxSpan]: index c of ring r0 + j (0xffff: no candidates)
+    uint32_t *cap;             // per 2x2 group: union candidate count (kCapUnknown: left to k_group<true>)
     unsigned long long *overflow;
     uint32_t pad;  // ring runs take a multiple of `pad` slots (> 1: the tensor-core engine's 8-row boxes)
 };
@@ -345,6 +348,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
                                            const TileArgs &tiles, uint64_t grp, PixPrep *s_prep, PixHalf *s_half) {
     int lane = threadIdx.x & 31;
     __syncwarp();
+    if (COUNT && cap[grp] != kCapUnknown) return;  // counted by the tile pass
     uint32_t gyi = (uint32_t)(grp / g.gx), gxi = (uint32_t)(grp % g.gx);
     uint64_t pix[4];
     bool valid[4];
@@ -481,6 +485,91 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
     }
 }
 
+// Exclusive scan of n u32 counts into u64 offsets (out[n] = the total), in
+// three passes over `parts` contiguous parts of the input, each swept by a
+// block of kScanThreads threads in coalesced rows: the part sums, a scan of
+// the part sums (one block), then the scan of each part from its base.
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ void scan_part(uint64_t n, uint32_t parts, uint32_t p, uint64_t &b, uint64_t &e) {
+    const uint64_t per = (n + parts - 1) / parts;
+    b = min(n, (uint64_t)p * per);
+    e = min(n, b + per);
+}
+
+// Block-wide exclusive scan of one value per thread; returns the exclusive
+// prefix and sets `total`. Every thread of the block calls it.
+__device__ __forceinline__ unsigned long long block_exclusive_scan(unsigned long long v, unsigned long long &total) {
+    __shared__ unsigned long long s_warp[kScanThreads / 32];
+    __shared__ unsigned long long s_total;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned long long incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __syncthreads();  // the shared values of a previous call are no longer read
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const unsigned long long x = lane < nw ? s_warp[lane] : 0ULL;
+        unsigned long long xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long t = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += t;
+        }
+        if (lane < nw) s_warp[lane] = xi - x;  // exclusive over the warps
+        if (lane == 31) s_total = xi;
+    }
+    __syncthreads();
+    total = s_total;
+    return s_warp[w] + incl - v;
+}
+
+__device__ __forceinline__ void scan_sums_item(const uint32_t *__restrict__ in, uint64_t n, uint32_t parts,
+                                               unsigned long long *__restrict__ psum, uint32_t p) {
+    uint64_t b, e;
+    scan_part(n, parts, p, b, e);
+    unsigned long long v = 0;
+    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) v += in[i];
+    unsigned long long tot;
+    block_exclusive_scan(v, tot);
+    if (threadIdx.x == 0) psum[p] = tot;
+}
+
+// One block: psum[0..parts) -> exclusive prefix sums, psum[parts] = total.
+__device__ __forceinline__ void scan_psum_item(unsigned long long *__restrict__ psum, uint32_t parts) {
+    unsigned long long run = 0;
+    for (uint32_t c = 0; c < parts; c += blockDim.x) {
+        const uint32_t i = c + threadIdx.x;
+        const unsigned long long v = i < parts ? psum[i] : 0ULL;
+        unsigned long long tot;
+        const unsigned long long ex = block_exclusive_scan(v, tot);
+        if (i < parts) psum[i] = run + ex;
+        run += tot;
+    }
+    if (threadIdx.x == 0) psum[parts] = run;
+}
+
+__device__ __forceinline__ void scan_apply_item(const uint32_t *__restrict__ in, uint64_t n, uint32_t parts,
+                                                const unsigned long long *__restrict__ psum,
+                                                unsigned long long *__restrict__ out, uint32_t p) {
+    uint64_t b, e;
+    scan_part(n, parts, p, b, e);
+    unsigned long long run = psum[p];
+    for (uint64_t c = b; c < e; c += blockDim.x) {
+        const uint64_t i = c + threadIdx.x;
+        const unsigned long long v = i < e ? in[i] : 0ULL;
+        unsigned long long tot;
+        const unsigned long long ex = block_exclusive_scan(v, tot);
+        if (i < e) out[i] = run + ex;
+        run += tot;
+    }
+    if (p == parts - 1 && threadIdx.x == 0) out[n] = psum[parts];
+}
+
 // FP32 channel accumulation of a group's entries; lane owns 4 channels per
 // 128-channel pass. Output [pixel][channel] with row stride `ostride`.
 // Warp-collective: every lane passes the same group.
@@ -566,11 +655,13 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
                                                 uint64_t tile) {
     __shared__ PixPrep s_prep[kTileX * kTileY];
     __shared__ uint32_t s_lo[kTileMaxSpan], s_hi[kTileMaxSpan];
+    __shared__ uint32_t s_cnt[kTileGroups];
     __shared__ int s_r0, s_r1;
     const uint32_t tx0 = (uint32_t)(tile % T.ntx) * kTileX, ty0 = (uint32_t)(tile / T.ntx) * kTileY;
     const int tid = threadIdx.x;
     __syncthreads();  // shared state of a previous item is no longer read
     if (tid == 0) { s_r0 = 1 << 30; s_r1 = -1; }
+    if (tid < kTileGroups) s_cnt[tid] = 0;
     __syncthreads();
     if (tid < kTileX * kTileY) {
         uint32_t xx = tx0 + tid % kTileX, yy = ty0 + tid / kTileX;
@@ -589,6 +680,14 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
     }
     __syncthreads();
     const int r0 = s_r0, nrt = s_r1 - s_r0 + 1;
+    // candidate counts of the tile's 2x2 groups (the entries k_group<false> may emit)
+    auto write_caps = [&](bool known) {
+        if (!T.cap || tid >= kTileGroups) return;
+        const uint32_t gxi = (uint32_t)(tile % T.ntx) * (kTileX / 2) + tid % (kTileX / 2);
+        const uint32_t gyi = (uint32_t)(tile / T.ntx) * (kTileY / 2) + tid / (kTileX / 2);
+        const uint64_t grp = (uint64_t)gyi * g.gx + gxi;
+        if (gxi < g.gx && grp < g.ngroups) T.cap[grp] = known ? s_cnt[tid] : kCapUnknown;
+    };
     if (nrt <= 0 || nrt > kTileMaxSpan) {
         if (tid == 0) {
             T.r0[tile] = 0;
@@ -596,24 +695,38 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
             T.U[tile] = 0;
             if (nrt > kTileMaxSpan) atomicAdd(T.overflow, 1ULL);
         }
+        write_caps(nrt <= 0);  // no samples: nothing to count
         return;
     }
     for (int j = tid; j < nrt; j += blockDim.x) { s_lo[j] = 0xffffffffu; s_hi[j] = 0; }
     __syncthreads();
-    const int npx = kTileX * kTileY;
-    for (int i = tid; i < npx * nrt; i += blockDim.x) {
-        int p = i % npx, j = i / npx;
-        const PixPrep &P = s_prep[p];
-        int k = r0 + j;
-        if (P.nr > 0 && k >= P.ur && k < P.ur + P.nr) {
-            uint32_t lo, hi;
-            if (ring_window(a.h, a.rings[k], P, a.keys, lo, hi) && hi > lo) {
-                atomicMin(&s_lo[j], lo);
-                atomicMax(&s_hi[j], hi);
+    // one (group, ring) pair per thread: the union of the group's four
+    // windows (group_item's count) and the tile union (min / max over groups)
+    for (int i = tid; i < kTileGroups * nrt; i += blockDim.x) {
+        const int gq = i % kTileGroups, j = i / kTileGroups;
+        const int k = r0 + j;
+        uint32_t glo = 0xffffffffu, ghi = 0;
+        const RingRec R = a.rings[k];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int p = (2 * (gq / (kTileX / 2)) + (q >> 1)) * kTileX + 2 * (gq % (kTileX / 2)) + (q & 1);
+            const PixPrep &P = s_prep[p];
+            if (P.nr > 0 && k >= P.ur && k < P.ur + P.nr) {
+                uint32_t lo, hi;
+                if (ring_window(a.h, R, P, a.keys, lo, hi) && hi > lo) {
+                    glo = min(glo, lo);
+                    ghi = max(ghi, hi);
+                }
             }
+        }
+        if (glo < ghi) {
+            atomicAdd(&s_cnt[gq], ghi - glo);
+            atomicMin(&s_lo[j], glo);
+            atomicMax(&s_hi[j], ghi);
         }
     }
     __syncthreads();
+    write_caps(true);
     if (tid < 32) {  // one warp: compaction of the occupied rings and prefix sums of their lengths
         uint32_t run = 0, count = 0;
         for (int jb = 0; jb < nrt; jb += 32) {

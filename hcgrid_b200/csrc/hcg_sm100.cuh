@@ -87,6 +87,16 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// 4-D tiled load (c0 innermost).
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, "
+        "%6}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
 // Untiled bulk copy global -> shared (16-byte aligned addresses, size a
 // multiple of 16), completing on `bar` by bytes.
 __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
@@ -95,6 +105,21 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32
             smem_u32(dst)),
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
+}
+
+// 3-D tiled store of a shared-memory box to global memory (elements outside
+// the tensor are not written). Completion is tracked by bulk groups.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(map),
+                 "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit_group() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Wait until the bulk stores of this thread have read their shared-memory sources.
+__device__ __forceinline__ void bulk_wait_group_read0() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *map) {
@@ -188,18 +213,20 @@ __device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Shared-memory matrix descriptor, 128-byte swizzle (layout type 2),
-// descriptor version 1, base offset 0 (operand atoms are 1024-byte aligned).
+// Shared-memory matrix descriptor, swizzled layout (type 2: 128-byte, 4:
+// 64-byte), descriptor version 1, base offset 0 (operand atoms are aligned to
+// their swizzle period).
 // Offsets in bytes. K-major operands: `sbo` = stride between 8-row groups,
 // `lbo` unused (1). MN-major operands: `lbo` = stride between 64-element
 // (128-byte) blocks along M/N, `sbo` = stride between 8-row groups along K.
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes,
+                                              uint32_t layout) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
     d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // version
-    d |= (uint64_t)2 << 61;  // SWIZZLE_128B
+    d |= (uint64_t)1 << 46;                 // version
+    d |= (uint64_t)(layout & 7u) << 61;     // 2: SWIZZLE_128B, 4: SWIZZLE_64B
     return d;
 }
 

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -19,18 +20,15 @@ namespace {
 
 template <class Cfg>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_tile_tc(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, TcJob J,
+    k_tile_tc(const __grid_constant__ CUtensorMap tm, const __grid_constant__ CUtensorMap tm_out, int has_out, TcJob J,
               const void *zero_page, unsigned long long *timeouts, unsigned long long *macs) {
     __shared__ TcShared S;
-    J.map_hi = &tm_hi;
-    J.map_lo = &tm_lo;
+    J.map = &tm;
+    J.out_map = has_out ? &tm_out : nullptr;
     const uint64_t tile = J.T.t0 + blockIdx.x;
     tc_load_rings(S, J.T, tile);
     tc_setup<Cfg>(S);  // ends with a CTA barrier
-    if (threadIdx.x == 0) {
-        sm100::prefetch_tensormap(&tm_hi);
-        sm100::prefetch_tensormap(&tm_lo);
-    }
+    if (threadIdx.x == 0) sm100::prefetch_tensormap(&tm);
     uint32_t gk = 0;
     tc_item<Cfg>(S, J, tile, blockIdx.y, gk, 0, zero_page, timeouts, macs);
     tc_teardown<Cfg>(S, gk, timeouts);
@@ -77,9 +75,9 @@ __global__ void k_split_scales(const unsigned int *amax_bits, uint32_t nchan, ui
     inv_scale[ch] = 1.f / (s * wscale);  // powers of two: exact
 }
 
-// hi/lo halves, channel-blocked: element (row r, channel c) at
-// [c / 64][r][c % 64], so 8 consecutive rows of one 64-channel block are one
-// contiguous kilobyte (one TMA box row group).
+// hi/lo halves in one array, channel-blocked: element (row r, channel c) of
+// half h at [h][c / 64][r][c % 64], so 8 consecutive rows of one 64-channel
+// block are one contiguous kilobyte and one 4-D TMA box brings both halves.
 __global__ void k_split(const float *__restrict__ spec, uint64_t n, uint32_t nchan, uint32_t cstride, uint32_t cpad,
                         uint32_t fmt, const float *__restrict__ scale, uint16_t *hi, uint16_t *lo) {
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -92,7 +90,7 @@ __global__ void k_split(const float *__restrict__ spec, uint64_t n, uint32_t nch
     const uint16_t h = tc_to16(v, fmt);
     const uint64_t o = ((uint64_t)(ch >> 6) * n + r) * 64 + (ch & 63);
     hi[o] = h;
-    lo[o] = tc_to16(v - tc_from16(h, fmt), fmt);
+    lo[o] = tc_to16(v - tc_from16(h, fmt), fmt);  // lo = hi + (cpad / 64) n 64
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -110,16 +108,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// [cpad / 64][rows][64] 16-bit array: boxes of 64 channels x 8 rows x nb
-// channel blocks, 128-byte swizzle (each 64 x 8 slab is one MN-major atom)
+// [2][cpad / 64][rows][64] 16-bit array: boxes of 64 channels x 8 rows x nb
+// channel blocks x 2 halves, 128-byte swizzle (each 64 x 8 slab is one
+// MN-major atom)
 bool make_map(CUtensorMap *m, const uint16_t *base, uint64_t rows, uint32_t cpad, uint32_t nb) {
     auto fn = encode_fn();
     if (!fn) return false;
-    cuuint64_t dims[3] = {64, rows, cpad / 64};
-    cuuint64_t strides[2] = {128, (cuuint64_t)rows * 128};
-    cuuint32_t box[3] = {64, 8, nb};
-    cuuint32_t estr[3] = {1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, (void *)base, dims, strides, box, estr,
+    cuuint64_t dims[4] = {64, rows, cpad / 64, 2};
+    cuuint64_t strides[3] = {128, (cuuint64_t)rows * 128, (cuuint64_t)rows * 128 * (cpad / 64)};
+    cuuint32_t box[4] = {64, 8, nb, 2};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, (void *)base, dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -127,8 +126,7 @@ bool make_map(CUtensorMap *m, const uint16_t *base, uint64_t rows, uint32_t cpad
 }  // namespace
 
 void free_split(hcg_field *f, cudaStream_t s) {
-    if (f->d_xhi) cudaFreeAsync(f->d_xhi, s);
-    if (f->d_xlo) cudaFreeAsync(f->d_xlo, s);
+    if (f->d_xhi) cudaFreeAsync(f->d_xhi, s);  // the lo half lives in the same allocation
     if (f->d_xinv) cudaFreeAsync(f->d_xinv, s);
     f->d_xhi = f->d_xlo = nullptr;
     f->d_xinv = nullptr;
@@ -148,18 +146,17 @@ cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::s
     unsigned int *amax = nullptr;
     unsigned long long *bad = nullptr;
     const size_t nb = (size_t)n * cpad * sizeof(uint16_t);
-    if ((e = cudaMallocAsync(&hi, nb ? nb : 16, s)) != cudaSuccess ||
-        (e = cudaMallocAsync(&lo, nb ? nb : 16, s)) != cudaSuccess ||
+    if ((e = cudaMallocAsync(&hi, nb ? 2 * nb : 16, s)) != cudaSuccess ||
         (e = cudaMallocAsync(&scale, cpad * sizeof(float), s)) != cudaSuccess ||
         (e = cudaMallocAsync(&inv, cpad * sizeof(float), s)) != cudaSuccess ||
         (e = cudaMallocAsync(&amax, cpad * sizeof(unsigned int) + sizeof(unsigned long long), s)) != cudaSuccess) {
         why = "split spectra of " + std::to_string(2 * nb) + " bytes";
         if (hi) cudaFreeAsync(hi, s);
-        if (lo) cudaFreeAsync(lo, s);
         if (scale) cudaFreeAsync(scale, s);
         if (inv) cudaFreeAsync(inv, s);
         return e;
     }
+    lo = hi + (size_t)n * cpad;  // [2][cpad / 64][n][64]: the lo half follows the hi half
     bad = (unsigned long long *)(amax + cpad);  // cpad is a multiple of 64: 8-byte aligned
     cudaMemsetAsync(amax, 0, cpad * sizeof(unsigned int) + sizeof(unsigned long long), s);
     const float wscale = fmt ? 1.f : 32768.f;
@@ -180,7 +177,6 @@ cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::s
     cudaFreeAsync(scale, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) {
         cudaFreeAsync(hi, s);
-        cudaFreeAsync(lo, s);
         cudaFreeAsync(inv, s);
         return e;
     }
@@ -194,12 +190,39 @@ cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::s
     return cudaSuccess;
 }
 
-bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J) {
+// The cube as a 3-D tensor whose box is one item (tile x channel block):
+// [y][x][channel] for sample-major cubes, [channel][y][x] for channel-major
+// ones. false when a stride is not a multiple of 16 bytes (the kernel then
+// stores directly).
+bool tc_out_map(CUtensorMap *m, float *out, uint32_t ostride, uint32_t nx, uint32_t ny, uint32_t nchan,
+                uint32_t nb) {
+    auto fn = encode_fn();
+    if (!fn || ((uintptr_t)out & 15)) return false;
+    cuuint64_t dims[3];
+    cuuint64_t strides[2];
+    cuuint32_t box[3];
+    if (ostride) {
+        if (ostride != nchan || (nchan & 3)) return false;
+        dims[0] = nchan; dims[1] = nx; dims[2] = ny;
+        strides[0] = (cuuint64_t)nchan * 4; strides[1] = (cuuint64_t)nx * nchan * 4;
+        box[0] = 64 * nb; box[1] = kTileX; box[2] = kTileY;
+    } else {
+        if (nx & 3) return false;
+        dims[0] = nx; dims[1] = ny; dims[2] = nchan;
+        strides[0] = (cuuint64_t)nx * 4; strides[1] = (cuuint64_t)nx * ny * 4;
+        box[0] = kTileX; box[1] = kTileY; box[2] = 64 * nb;
+    }
+    cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)out, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map, TcJob &J) {
     const uint32_t nblk64 = f->xcpad / 64;
     J.nb = nblk64 < (uint32_t)nb_max ? nblk64 : (uint32_t)nb_max;
     J.ncb = (nblk64 + J.nb - 1) / J.nb;
-    if (!make_map(map_hi, f->d_xhi, f->n, f->xcpad, J.nb) || !make_map(map_lo, f->d_xlo, f->n, f->xcpad, J.nb))
-        return false;
+    if (!make_map(map, f->d_xhi, f->n, f->xcpad, J.nb)) return false;
     J.nchan = f->nchan;
     J.nrows = (uint32_t)f->n;
     J.fmt = f->xfmt == HCG_ENGINE_TC_BF16 ? 1u : 0u;
@@ -218,7 +241,7 @@ int tc_pick(const hcg_context *ctx, const hcg_field *f) {
     const int t = ctx->tc_config[tc_class_of(f->xcpad)];
     if (t >= 0 && t < kTcConfigCount) return t;
     const uint32_t b = f->xcpad / 64;
-    return b >= 4 ? 0 : (b >= 2 ? 1 : 2);
+    return b >= 4 ? 3 : (b >= 2 ? 1 : 2);
 }
 
 namespace {
@@ -226,11 +249,13 @@ template <class Cfg>
 cudaError_t launch_tc(hcg_context *ctx, const hcg_field *f, TcJob &J, const TileArgs &T, uint64_t ntiles,
                       const void *zero, std::string &why) {
     cudaStream_t s = ctx->stream;
-    CUtensorMap mh, ml;
-    if (!tc_prepare_job(f, Cfg::kNb, &mh, &ml, J)) {
+    CUtensorMap tm, tm_out;
+    if (!tc_prepare_job(f, Cfg::kNb, &tm, J)) {
         why = "cuTensorMapEncodeTiled";
         return cudaErrorInvalidValue;
     }
+    const int has_out = tc_out_map(&tm_out, J.out, J.ostride, J.g.nx, J.g.ny, J.nchan, J.nb) ? 1 : 0;
+    if (!has_out) memset(&tm_out, 0, sizeof tm_out);
     static bool attr_set = false;  // per instantiation
     if (!attr_set) {
         cudaError_t e = tc_set_smem((const void *)k_tile_tc<Cfg>, Cfg::kSmem);
@@ -241,7 +266,7 @@ cudaError_t launch_tc(hcg_context *ctx, const hcg_field *f, TcJob &J, const Tile
         J.T = T;
         J.T.t0 = T.t0 + t0;
         dim3 grid((unsigned)std::min<uint64_t>(ntiles - t0, 0x7fffffffull), J.ncb);
-        k_tile_tc<Cfg><<<grid, kTcThreads, Cfg::kSmem, s>>>(mh, ml, J, zero, &ctx->d_stats->timeouts,
+        k_tile_tc<Cfg><<<grid, kTcThreads, Cfg::kSmem, s>>>(tm, tm_out, has_out, J, zero, &ctx->d_stats->timeouts,
                                                             &ctx->d_stats->tc_macs);
     }
     return cudaGetLastError();
@@ -254,9 +279,9 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
     cudaStream_t s = ctx->stream;
     TcJob J{};
     cudaError_t e = cudaSuccess;
-    void *zero = ctx->scratch.get(20, (size_t)kTcZeroWindows * 2 * kAHalf, s, e);
+    void *zero = ctx->scratch.get(20, (size_t)kTcZeroWindows * kTcMaxA, s, e);
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(zero, 0, (size_t)kTcZeroWindows * 2 * kAHalf, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(zero, 0, (size_t)kTcZeroWindows * kTcMaxA, s)) != cudaSuccess) return e;
     J.g = g;
     J.off = off;
     J.cnt = cnt;
@@ -267,9 +292,10 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
     J.ostride = ostride;
     J.wout = wout;
     switch (tc_pick(ctx, f)) {
+        case 0: return launch_tc<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
         case 1: return launch_tc<TcCfgN2S3>(ctx, f, J, T, ntiles, zero, why);
         case 2: return launch_tc<TcCfgN1S4>(ctx, f, J, T, ntiles, zero, why);
-        default: return launch_tc<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
+        default: return launch_tc<TcCfgN4K32>(ctx, f, J, T, ntiles, zero, why);
     }
 }
 

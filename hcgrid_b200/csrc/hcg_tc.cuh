@@ -20,18 +20,22 @@
 //
 // One work item = one tile x up to 256 channels (nb 64-channel blocks).
 // Warp roles in a 192-thread CTA:
-//   warp 0    producer: per 64-slot K chunk, one bulk copy of a zero page
-//             over the chunk's weight operand, then the spectra: 8 runs of 8
-//             sorted samples, each one 3-D TMA box (64 channels x 8 rows x nb
-//             channel blocks, 128-byte swizzle: the MN-major B atoms) of the
-//             hi and of the lo array;
+//   warp 0    producer: per K chunk (64 or 32 slots), one bulk copy of a
+//             zero page over the chunk's weight operand, then the spectra:
+//             runs of 8 sorted samples, each one 4-D TMA box (64 channels x 8
+//             rows x nb channel blocks x hi/lo, 128-byte swizzle: the
+//             MN-major B atoms);
 //   warp 1    TMEM allocation and MMA issue (one thread);
 //   warps 2-5 write the weights of the chunk's entries into the zeroed
-//             K-major operand (128-byte swizzle), then run the epilogue:
-//             tcgen05.ld of the accumulator, multiplication by the inverse
-//             scales and by 1 / (FP64 weight sum), store.
-// Two pipeline stages (A hi/lo 32 KB + B hi/lo 64 KB each). Pipeline
-// counters run on across the items a CTA processes. Every wait is bounded
+//             K-major operand (swizzled), then run the epilogue: tcgen05.ld
+//             of the accumulator, multiplication by the inverse channel
+//             scales and by 1 / (FP64 weight sum) into a shared-memory tile
+//             laid out as the cube's box, written by one TMA bulk tensor
+//             store (direct stores where the cube's strides do not allow
+//             TMA).
+// The pipeline shapes (channels per item, chunk size, stages) are the
+// TcCfg instances below. Pipeline counters run on across the items a CTA
+// processes. Every wait is bounded
 // (1 s of global time): a wait that runs out counts a timeout and sets the
 // CTA's abort flag; the roles wind down, the producer waits (bounded) for its
 // copies, TMEM is freed and the host reports HCG_ETIMEOUT.
@@ -52,36 +56,46 @@
 namespace hcg {
 
 constexpr int kTcM = kTileX * kTileY;  // 128 pixels: the MMA's M
-constexpr int kTcK = 64;               // slots per K chunk (one 128-byte swizzle row of 16-bit values)
 constexpr int kTcThreads = 192;
 constexpr int kTcBuilders = 128;
-constexpr uint32_t kAHalf = kTcM * kTcK * 2;  // 16 KB
+constexpr uint32_t kTcMaxA = kTcM * 64 * 2 * 2;  // largest weight operand (hi + lo) of a chunk: 32 KB
 constexpr uint64_t kTcWaitNs = 1000000000ull;
 constexpr uint32_t kTcZeroWindows = 160;  // zero region: kTcZeroWindows x 32 KB (5 MB)
+constexpr uint32_t kTcMaxN = 256;         // channels per item (the MMA's largest N)
 static_assert(kTcM == 128, "a tile is one M=128 MMA");
-static_assert(kTcK == 64, "a chunk is 8 row boxes of 8 slots and one 128-byte swizzle row");
 
-// Pipeline shapes: NB 64-channel blocks per item (the MMA's N = 64 NB) and ST
-// stages, all in 192 KB of operand buffers. More channels per item build the
-// weight operand fewer times per channel; more stages hide more copy latency.
-template <int NB, int ST>
+// Pipeline shapes: NB 64-channel blocks per item (the MMA's N = 64 NB), K
+// slots per chunk (64: 128-byte rows of the weight operand, 128-byte
+// swizzle; 32: 64-byte rows, 64-byte swizzle) and ST stages, in 192 KB of
+// operand buffers. More channels per item build the weight operand fewer
+// times per channel; more (smaller) stages hide more copy latency.
+template <int NB, int ST, int KC>
 struct TcCfg {
     static constexpr int kNb = NB;
     static constexpr int kStages = ST;
-    static constexpr uint32_t kBHalf = kTcK * 64 * NB * 2;  // one of hi / lo
-    static constexpr uint32_t kStageBytes = 2 * kAHalf + 2 * kBHalf;
+    static constexpr int kK = KC;
+    static constexpr uint32_t kAHalf = kTcM * KC * 2;          // weight operand hi (or lo)
+    static constexpr uint32_t kARow = KC * 2;                  // bytes per operand row
+    static constexpr uint32_t kAAtom = 8 * kARow;              // 8-row swizzle atom
+    static constexpr uint32_t kALayout = KC == 64 ? 2u : 4u;   // descriptor layout: SWIZZLE_128B / _64B
+    static constexpr uint32_t kBGroup = 2 * NB * 1024;         // one 8-slot row group: hi blocks, lo blocks
+    static constexpr uint32_t kBBytes = (KC / 8) * kBGroup;
+    static constexpr uint32_t kStageBytes = 2 * kAHalf + kBBytes;
     static constexpr uint32_t kSmem = ST * kStageBytes + 1024;  // + alignment of the swizzle atoms
     static constexpr uint32_t kTmemCols = NB * 64 <= 64 ? 64 : (NB * 64 <= 128 ? 128 : 256);
+    static_assert(KC == 64 || KC == 32, "chunks of 64 or 32 slots");
     static_assert(ST * kStageBytes <= 192 * 1024, "operand buffers fit shared memory");
+    static_assert(2 * kAHalf <= kTcMaxA, "zero page covers the weight operand");
 };
-using TcCfgN4S2 = TcCfg<4, 2>;  // 256 channels per item, 2 stages
-using TcCfgN2S3 = TcCfg<2, 3>;  // 128 channels, 3 stages
-using TcCfgN1S4 = TcCfg<1, 4>;  // 64 channels, 4 stages
-static_assert(kTcConfigCount == 3, "hcg_tc_set_config numbers the three shapes above 0, 1, 2");
+using TcCfgN4S2 = TcCfg<4, 2, 64>;  // 256 channels per item, 64-slot chunks, 2 stages
+using TcCfgN2S3 = TcCfg<2, 3, 64>;  // 128 channels, 64-slot chunks, 3 stages
+using TcCfgN1S4 = TcCfg<1, 4, 64>;  // 64 channels, 64-slot chunks, 4 stages
+using TcCfgN4K32 = TcCfg<4, 4, 32>;  // 256 channels, 32-slot chunks, 4 stages
+static_assert(kTcConfigCount == 4, "hcg_tc_set_config numbers the shapes above 0, 1, 2, 3");
 
 // One job's tensor-core arguments.
 struct TcJob {
-    const CUtensorMap *map_hi, *map_lo;  // [ncb64][n][64] 16-bit arrays, boxes 64 x 8 x nb
+    const CUtensorMap *map;  // [2][ncb64][n][64] 16-bit hi/lo arrays, boxes 64 x 8 x nb x 2
     GroupArgs g;
     TileArgs T;
     const unsigned long long *off;  // entry offset of each group (minus g.ebase)
@@ -99,6 +113,7 @@ struct TcJob {
     float *out;
     uint32_t ostride;   // 0: [channel][pixel]; else [pixel][ostride]
     float *wout;
+    const CUtensorMap *out_map;  // 3-D map of the cube (null: direct stores); box = one item
 };
 
 constexpr int kTcRing = 8;  // entries in flight per builder thread
@@ -110,6 +125,7 @@ struct TcShared {
     volatile int abort;
     unsigned long long item;
     uint32_t ulo[kTileMaxRings], base[kTileMaxRings + 1];
+    float inv_scale[kTcMaxN];              // the item's channels: 1 / (channel scale * weight scale)
     float4 ring_w[kTcRing * kTcBuilders];  // builders' entry rings, [position][thread]
     uint32_t ring_slot[kTcRing * kTcBuilders];
 };
@@ -117,7 +133,8 @@ struct TcShared {
 // hcg_tc.cu: the tensor maps and format fields of a field with split
 // spectra (false: the maps could not be encoded); the shared-memory opt-in of
 // a kernel built on tc_item.
-bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map_hi, CUtensorMap *map_lo, TcJob &J);
+bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map, TcJob &J);
+bool tc_out_map(CUtensorMap *m, float *out, uint32_t ostride, uint32_t nx, uint32_t ny, uint32_t nchan, uint32_t nb);
 cudaError_t tc_set_smem(const void *kernel, uint32_t bytes);
 int tc_pick(const hcg_context *ctx, const hcg_field *f);
 
@@ -131,10 +148,13 @@ __device__ __forceinline__ float tc_from16(uint16_t b, uint32_t fmt) {
     return fmt ? __bfloat162float(__ushort_as_bfloat16(b)) : __half2float(__ushort_as_half(b));
 }
 
-// byte offset of element (row m, column k) of a K-major 128-row x 64-column
-// 16-bit operand in 128-byte-swizzled 8-row atoms
+// byte offset of element (row m, column k) of a K-major 128-row x KC-column
+// 16-bit operand in swizzled 8-row atoms (the 16-byte chunk index is XORed
+// with address bits 7-9 for the 128-byte swizzle, 7-8 for the 64-byte one)
+template <int KC>
 __device__ __forceinline__ uint32_t tc_a_offset(uint32_t m, uint32_t k) {
-    return (m >> 3) * 1024u + (m & 7u) * 128u + ((((k >> 3) ^ (m & 7u)) << 4) | ((k & 7u) << 1));
+    if (KC == 64) return (m >> 3) * 1024u + (m & 7u) * 128u + ((((k >> 3) ^ (m & 7u)) << 4) | ((k & 7u) << 1));
+    return (m >> 3) * 512u + (m & 7u) * 64u + ((((k >> 3) ^ ((m >> 1) & 3u)) << 4) | ((k & 7u) << 1));
 }
 
 __device__ __forceinline__ uint8_t *tc_smem_base() {
@@ -212,20 +232,20 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
     using namespace sm100;
     uint8_t *smem = tc_smem_base();
     constexpr uint32_t ST = Cfg::kStages;
+    constexpr uint32_t KC = Cfg::kK;
     auto A_hi = [&](uint32_t s) { return smem + s * Cfg::kStageBytes; };
-    auto A_lo = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + kAHalf; };
-    auto B_hi = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + 2 * kAHalf; };
-    auto B_lo = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + 2 * kAHalf + Cfg::kBHalf; };
+    auto A_lo = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + Cfg::kAHalf; };
+    auto B_of = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + 2 * Cfg::kAHalf; };
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileArgs &T = J.T;
     const uint32_t U = T.U[tile];
-    const uint32_t nchunks = (U + kTcK - 1) / kTcK;
+    const uint32_t nchunks = (U + KC - 1) / KC;
     const uint32_t taddr = S.tmem;
 
     if (warp == 0) {
         if (lane == 0) {
             // ---------------------------------------------------- producer
-            const uint32_t bytes = 2u * 8u * J.nb * 1024u;
+            const uint32_t bytes = (KC / 8) * 2u * J.nb * 1024u;
             int j = 0;
             for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
                 const uint32_t g = gk + k, s = g % ST;
@@ -233,14 +253,15 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                     tc_give_up(S, timeouts);
                     break;
                 }
-                mbar_arrive_expect_tx(&S.zfill[s], 2 * kAHalf);
+                mbar_arrive_expect_tx(&S.zfill[s], 2 * Cfg::kAHalf);
                 // each CTA copies from its own window of the zero region, so the
                 // copies of all SMs spread over the L2 slices
-                bulk_copy_g2s(A_hi(s), (const uint8_t *)zero_page + (blockIdx.x % kTcZeroWindows) * (2 * kAHalf),
-                              2 * kAHalf, &S.zfill[s]);
+                bulk_copy_g2s(A_hi(s), (const uint8_t *)zero_page + (blockIdx.x % kTcZeroWindows) * kTcMaxA,
+                              2 * Cfg::kAHalf, &S.zfill[s]);
                 mbar_arrive_expect_tx(&S.full_b[s], bytes);
-                for (int b = 0; b < 8; ++b) {
-                    const uint32_t slot0 = k * kTcK + 8 * b;
+#pragma unroll
+                for (int b = 0; b < (int)(KC / 8); ++b) {
+                    const uint32_t slot0 = k * KC + 8 * b;
                     int row;
                     if (slot0 >= U) {
                         row = (int)J.nrows;  // past the last sample: zero fill
@@ -248,9 +269,7 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                         while (S.base[j + 1] <= slot0) ++j;
                         row = (int)(S.ulo[j] + (slot0 - S.base[j]));
                     }
-                    const int cz = (int)(cblk * J.nb);
-                    tma_load_3d(B_hi(s) + b * (1024 * Cfg::kNb), J.map_hi, &S.full_b[s], 0, row, cz);
-                    tma_load_3d(B_lo(s) + b * (1024 * Cfg::kNb), J.map_lo, &S.full_b[s], 0, row, cz);
+                    tma_load_4d(B_of(s) + b * Cfg::kBGroup, J.map, &S.full_b[s], 0, row, (int)(cblk * J.nb), 0);
                 }
             }
         }
@@ -267,14 +286,14 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                 }
                 tc_fence_after();
                 const uint32_t ah = smem_u32(A_hi(s)), al = smem_u32(A_lo(s));
-                const uint32_t bh = smem_u32(B_hi(s)), bl = smem_u32(B_lo(s));
+                const uint32_t bh = smem_u32(B_of(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
 #pragma unroll
-                for (int kk = 0; kk < kTcK / 16; ++kk) {
-                    const uint64_t adh = smem_desc_sw128(ah + kk * 32, 16, 1024);
-                    const uint64_t adl = smem_desc_sw128(al + kk * 32, 16, 1024);
-                    // 8-slot row groups at 1024 * kNb bytes; 64-channel atoms at 1024
-                    const uint64_t bdh = smem_desc_sw128(bh + kk * 2 * 1024 * Cfg::kNb, 1024, 1024 * Cfg::kNb);
-                    const uint64_t bdl = smem_desc_sw128(bl + kk * 2 * 1024 * Cfg::kNb, 1024, 1024 * Cfg::kNb);
+                for (int kk = 0; kk < (int)(KC / 16); ++kk) {
+                    const uint64_t adh = smem_desc(ah + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
+                    const uint64_t adl = smem_desc(al + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
+                    // two 8-slot row groups per K step; 64-channel atoms 1 KB apart
+                    const uint64_t bdh = smem_desc(bh + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
+                    const uint64_t bdl = smem_desc(bl + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
                     mma_f16_ss(taddr, adh, bdh, idesc, acc);
                     mma_f16_ss(taddr, adh, bdl, idesc, 1);
                     mma_f16_ss(taddr, adl, bdh, idesc, 1);
@@ -282,7 +301,7 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                 }
                 mma_commit(&S.empty[s]);
             }
-            if (acc) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)kTcK * nchunks);
+            if (acc) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)KC * nchunks);
             if (nchunks == 0)
                 mbar_arrive(&S.acc_full);
             else
@@ -332,7 +351,7 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                 tc_give_up(S, timeouts);
                 break;
             }
-            const uint32_t cs = k * kTcK, ce = cs + kTcK;
+            const uint32_t cs = k * KC, ce = cs + KC;
             uint8_t *ah = A_hi(s), *al = A_lo(s);
             for (;;) {
                 cp_async_wait<kTcRing - 1>();  // the ring's oldest copy has landed
@@ -346,7 +365,7 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                     const float w = wv[q] * J.wscale;
                     const uint16_t h = tc_to16(w, J.fmt);
                     const uint16_t l = tc_to16(w - tc_from16(h, J.fmt), J.fmt);
-                    const uint32_t o = tc_a_offset(mrow[q], col);
+                    const uint32_t o = tc_a_offset<KC>(mrow[q], col);
                     *(uint16_t *)(ah + o) = h;
                     *(uint16_t *)(al + o) = l;
                 }
@@ -358,20 +377,28 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
         }
         cp_async_wait<0>();  // no copy into the ring outlives the item
         // -------------------------------------------------------- epilogue
+        const uint32_t c_item = cblk * J.nb * 64;  // first channel of the item
+        const uint32_t ncols = 64 * J.nb;
+        for (uint32_t c = bt; c < ncols; c += kTcBuilders)
+            S.inv_scale[c] = c_item + c < J.nchan ? J.inv_scale[c_item + c] : 0.f;
         const bool ok = mbar_wait(&S.acc_full, itn & 1, kTcWaitNs);
         if (!ok) tc_give_up(S, timeouts);
         tc_fence_after();
+        // inv_scale staged; the store decision is the same in every builder
+        const bool store = !named_barrier_or(2, kTcBuilders, !ok || S.abort);
         const uint32_t q4 = warp & 3;  // TMEM lane quarter this warp may access
         const uint32_t m = q4 * 32 + lane;
-        const uint32_t xx = (uint32_t)(tile % T.ntx) * kTileX + (m & (kTileX - 1));
-        const uint32_t yy = (uint32_t)(tile / T.ntx) * kTileY + m / kTileX;
+        const uint32_t tx0 = (uint32_t)(tile % T.ntx) * kTileX, ty0 = (uint32_t)(tile / T.ntx) * kTileY;
+        const uint32_t xx = tx0 + (m & (kTileX - 1));
+        const uint32_t yy = ty0 + m / kTileX;
         const bool valid = xx < G.nx && yy < G.ny;
         const uint64_t P = (uint64_t)G.nx * G.ny;
         const uint64_t p = (uint64_t)yy * G.nx + xx;
         const double ws = valid ? J.wsum[p] : 0.0;
         const float inv = (float)(1.0 / ws);
         if (valid && cblk == 0 && J.wout) J.wout[p] = (float)ws;
-        const bool store = ok && !S.abort && valid;
+        // the item's operand buffers are idle now: the staging tile of the cube
+        float *stage = (float *)tc_smem_base();
         for (uint32_t cb = 0; cb < 2 * J.nb; ++cb) {
             uint32_t r[32];
             if (nchunks > 0) {
@@ -381,21 +408,53 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
 #pragma unroll
                 for (int i = 0; i < 32; ++i) r[i] = 0u;
             }
-            const uint32_t c0 = cblk * J.nb * 64 + cb * 32;
+            float v[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = (__uint_as_float(r[i]) * S.inv_scale[cb * 32 + i]) * inv;
             if (!store) continue;
-            if (J.ostride == 0) {
+            if (J.out_map) {
+                if (J.ostride) {
+                    // box [y][x][channel]: this pixel's 32 values, 16-byte pieces in a
+                    // lane-rotated order (fewer bank conflicts)
+                    float4 *row = (float4 *)(stage + (size_t)m * ncols + cb * 32);
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const uint32_t ch = c0 + i;
-                    if (ch < J.nchan) J.out[(uint64_t)ch * P + p] = (__uint_as_float(r[i]) * J.inv_scale[ch]) * inv;
-                }
-            } else {
-                float *dst = J.out + p * J.ostride;
+                    for (int u = 0; u < 8; ++u) {
+                        const int k = (u + lane) & 7;  // 16-byte bank group of this lane's piece
+                        float4 q = make_float4(v[0], v[1], v[2], v[3]);
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const uint32_t ch = c0 + i;
-                    if (ch < J.nchan) dst[ch] = (__uint_as_float(r[i]) * J.inv_scale[ch]) * inv;
+                        for (int kk = 1; kk < 8; ++kk)  // lane-dependent index into registers: selects
+                            if (kk == k) q = make_float4(v[4 * kk], v[4 * kk + 1], v[4 * kk + 2], v[4 * kk + 3]);
+                        row[k] = q;
+                    }
+                } else {
+                    // box [channel][y][x]
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) stage[(size_t)(cb * 32 + i) * kTcM + m] = v[i];
                 }
+            } else if (valid) {
+                const uint32_t c0 = c_item + cb * 32;
+                if (J.ostride == 0) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (c0 + i < J.nchan) J.out[(uint64_t)(c0 + i) * P + p] = v[i];
+                } else {
+                    float *dst = J.out + p * J.ostride;
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (c0 + i < J.nchan) dst[c0 + i] = v[i];
+                }
+            }
+        }
+        if (store && J.out_map) {
+            fence_proxy_async_smem();
+            named_barrier(2, kTcBuilders);  // the staging tile is complete
+            if (bt == 0) {
+                if (J.ostride)
+                    tma_store_3d(J.out_map, stage, (int)c_item, (int)tx0, (int)ty0);
+                else
+                    tma_store_3d(J.out_map, stage, (int)tx0, (int)ty0, (int)c_item);
+                bulk_commit_group();
+                bulk_wait_group_read0();  // the staging tile may be overwritten after this
             }
         }
         tc_fence_before();

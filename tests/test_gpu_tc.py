@@ -94,10 +94,11 @@ def test_auto_engine_uses_the_split(ctx, small):
     np.testing.assert_array_equal(b, c)
 
 
-@pytest.mark.parametrize("nchan", [64, 300])
+@pytest.mark.parametrize("nchan", [64, 98, 300])
 def test_tc_channel_blocks(ctx, nchan):
-    """64 channels (one 64-channel block) and 300 (two CTAs per tile, the
-    second partly past the last channel)."""
+    """64 channels (one 64-channel block), 98 (rows not a multiple of 16
+    bytes: direct stores instead of the TMA store) and 300 (two CTAs per
+    tile, the second partly past the last channel)."""
     job = synth.config2(n=60_000, nchan=nchan, nx=64, size_deg=1.2, build_values=True)
     prepare(ctx, job)
     f = ctx.field(job.lon, job.lat)
@@ -111,18 +112,23 @@ def test_tc_channel_blocks(ctx, nchan):
     assert plane_errors(ct, c32.astype(np.float64)) <= 1e-5
 
 
-def test_tc_empty_tiles_and_padding(ctx):
-    """A map larger than the field: whole tiles without samples come out NaN
-    with zero weight, exactly where the FP32 engine puts them."""
-    job = synth.config2(n=30_000, nchan=64, nx=96, size_deg=1.0, build_values=True)
+@pytest.mark.parametrize("layout", [api.SAMPLE_MAJOR, api.CHANNEL_MAJOR])
+def test_tc_empty_tiles_and_padding(ctx, layout):
+    """A 97x97 map larger than the field: partial edge tiles (the TMA store
+    clips them; channel-major rows of 97 floats take direct stores) and
+    whole tiles without samples, which come out NaN with zero weight exactly
+    where the FP32 engine puts them."""
+    job = synth.config2(n=30_000, nchan=64, nx=97, size_deg=1.0, build_values=True)
     prepare(ctx, job)
-    hdr = synth.sin_header(96, 96, 180.0, 30.0, 2.0 / 96)  # config2 is centred at (180, 30)
+    hdr = synth.sin_header(97, 97, 180.0, 30.0, 2.0 / 97)  # config2 is centred at (180, 30)
     f = ctx.field(job.lon, job.lat)
     f.set_spectra(job.values)
     t = ctx.target_from_header(hdr)
-    c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+    c32, w32 = ctx.grid(f, t, layout=layout, engine=api.ENGINE_FP32)
     f.split_spectra(api.ENGINE_TC_BF16)
-    ct, wt = ctx.grid(f, t, engine=api.ENGINE_TC_BF16)
+    ct, wt = ctx.grid(f, t, layout=layout, engine=api.ENGINE_TC_BF16)
+    if layout == api.CHANNEL_MAJOR:
+        ct, c32 = ct.T, c32.T
     assert np.isnan(ct).any() and (~np.isnan(ct)).any()
     np.testing.assert_array_equal(np.isnan(ct), np.isnan(c32))
     np.testing.assert_array_equal(wt, w32)
@@ -165,15 +171,16 @@ def test_tc_state_and_input_checks(ctx):
 
 
 def test_pipeline_shapes_and_autotune(ctx, small):
-    """Every tensor-core pipeline shape (256 channels x 2 stages, 128 x 3,
-    64 x 4) gives the same weights and stays within tolerance of the oracle;
-    the autotuner times them and keeps one."""
+    """Every tensor-core pipeline shape (256 channels x 64-sample chunks x 2
+    stages, 128 x 64 x 3, 64 x 64 x 4, 256 x 32 x 4) gives the same weights
+    and stays within tolerance of the oracle; the autotuner times them and
+    keeps one."""
     job, f, t, ref, c32, w32 = small
     prepare(ctx, job)
     f.split_spectra(api.ENGINE_TC_F16)
     outs = []
     try:
-        for cfg in range(3):
+        for cfg in range(4):
             ctx.tc_set_config(cfg)
             c, w = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
             np.testing.assert_array_equal(w, w32)
@@ -184,7 +191,7 @@ def test_pipeline_shapes_and_autotune(ctx, small):
         ctx.tc_set_config(-1)
         best, ms = ctx.autotune(f, t, reps=1)
         print("autotune", best, ms)
-        assert best in (0, 1, 2) and all(m > 0 for m in ms)
+        assert best in (0, 1, 2, 3) and all(m > 0 for m in ms)
         with pytest.raises(RuntimeError, match="HCG_EINVAL"):
             ctx.tc_set_config(5)
     finally:
