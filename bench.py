@@ -54,8 +54,10 @@ def parse():
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--engine", default="fp32", choices=list(ENGINES),
-                    help="channel-sum engine: FP32 CUDA cores or tensor cores with a 16-bit hi/lo split")
+    ap.add_argument("--engine", default="tc-f16", choices=list(ENGINES),
+                    help="channel-sum engine: tensor cores with a 16-bit hi/lo split, or FP32 CUDA cores")
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="also time this many steps of the plain FP32 engine on the same field (0: skip)")
     ap.add_argument("--tc-config", type=int, default=None,
                     help="tensor-core pipeline shape (0: 256 ch x 64-sample chunks x 2 stages, 1: 128 x 64 x 3, "
                          "2: 64 x 64 x 4, 3: 256 x 32 x 4); "
@@ -69,6 +71,9 @@ def parse():
 
 
 ENGINES = {"fp32": 1, "tc-f16": 3, "tc-bf16": 2}
+DTYPE_TEXT = {"fp32": "f32 (FP64 geometry)",
+              "tc-f16": "f16 hi/lo x3, f32 accumulate (FP64 geometry)",
+              "tc-bf16": "bf16 hi/lo x3, f32 accumulate (FP64 geometry)"}
 ENGINE_TEXT = {"fp32": "FP32 CUDA-core channel sums, FP64 geometry",
                "tc-f16": "tcgen05 channel sums, compensated FP16 hi/lo (3 products, FP32 accumulate), FP64 geometry",
                "tc-bf16": "tcgen05 channel sums, compensated BF16 hi/lo (3 products, FP32 accumulate), FP64 geometry"}
@@ -200,6 +205,25 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baselines (the reference's own host build, else the oracle port)
 
+class CStdoutToStderr:
+    """Send what C code prints to stdout (the reference's host pre-sort
+    prints its timings) to stderr, so stdout carries only the JSON line."""
+
+    def __enter__(self):
+        import ctypes
+        sys.stdout.flush()
+        self.libc = ctypes.CDLL(None)
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *a):
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def cpu_baseline(job, budget_s=20.0):
     """Reference CPU path on a bounded sample: full pre-sort of all samples
     plus the kernel body for one channel on a central square of the target;
@@ -217,25 +241,26 @@ def cpu_baseline(job, budget_s=20.0):
     x0 = (nx - side) // 2
     sel = (np.arange(side)[:, None] + x0) * nx + (np.arange(side)[None, :] + x0)
     sx, sy = np.ascontiguousarray(xw[sel.ravel()]), np.ascontiguousarray(yw[sel.ravel()])
-    if O.have_ref():
-        kind = "reference"
-        O.ref_prepare(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
-        t0 = time.perf_counter()
-        keys, slon, slat, sdat, fr, ur, lut = O.ref_presort(job.lon, job.lat, vals, 2)
-        t_sort = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        O.ref_grid(keys, slon, slat, sdat, lut, fr, ur, side, side, sx, sy)
-        t_sub = time.perf_counter() - t0
-    else:
-        kind = "port"
-        g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
-        t0 = time.perf_counter()
-        ps = O.presort(g.hpx, job.lon, job.lat)
-        t_sort = time.perf_counter() - t0
-        sl, sb, sd = job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm]
-        t0 = time.perf_counter()
-        O.grid(g, ps, sl, sb, sd, sx, sy)
-        t_sub = time.perf_counter() - t0
+    with CStdoutToStderr():
+        if O.have_ref():
+            kind = "reference"
+            O.ref_prepare(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+            t0 = time.perf_counter()
+            keys, slon, slat, sdat, fr, ur, lut = O.ref_presort(job.lon, job.lat, vals, 2)
+            t_sort = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            O.ref_grid(keys, slon, slat, sdat, lut, fr, ur, side, side, sx, sy)
+            t_sub = time.perf_counter() - t0
+        else:
+            kind = "port"
+            g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+            t0 = time.perf_counter()
+            ps = O.presort(g.hpx, job.lon, job.lat)
+            t_sort = time.perf_counter() - t0
+            sl, sb, sd = job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm]
+            t0 = time.perf_counter()
+            O.grid(g, ps, sl, sb, sd, sx, sy)
+            t_sub = time.perf_counter() - t0
     t_kernel = t_sub * P / (side * side)
     t_job = t_sort + job.nchan * t_kernel
     value = job.n * job.nchan / t_job
@@ -522,8 +547,9 @@ def main():
     engine = ENGINES[args.engine]
     field = ctx.field(lon_d, lat_d)
     field.set_spectra(S)
+    plain_steps = args.plain_steps if (engine != api.ENGINE_FP32 and job.nchan > 1) else 0
     if engine != api.ENGINE_FP32 and job.nchan > 1:
-        field.split_spectra(engine, keep_fp32=False)
+        field.split_spectra(engine, keep_fp32=plain_steps > 0)
     target = ctx.target_from_header(job.header)
     ctx.synchronize()
     S_host = None
@@ -534,7 +560,8 @@ def main():
     torch.cuda.empty_cache()
     cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
     wts = torch.empty(P, dtype=torch.float32, device=dev)
-    launches_per_step = 2 if job.nchan == 1 else 7  # prep, tile rings, count, scan, row offsets, weights, sums
+    # prep, tile rings, count of overflowed tiles, 3-pass scan, row offsets, weights, sums
+    launches_per_step = 2 if job.nchan == 1 else 9
 
     tune = None
     if engine != api.ENGINE_FP32 and job.nchan > 1:
@@ -573,9 +600,27 @@ def main():
         dist.barrier()
     ms_per_step = reduce_max(torch, dist, total_ms / args.steps)
     clocks = clk.summary()
+    st = ctx.stats()  # counters of the last timed step (before the plain engine runs)
+    plain = None
+    if plain_steps > 0:
+        # the plain FP32 CUDA-core engine on the same resident field, same timing rules
+        for _ in range(2):
+            ctx.grid(field, target, cube, wts, engine=api.ENGINE_FP32)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        pe0 = torch.cuda.Event(enable_timing=True)
+        pe1 = torch.cuda.Event(enable_timing=True)
+        pe0.record(stream)
+        for _ in range(plain_steps):
+            ctx.grid(field, target, cube, wts, engine=api.ENGINE_FP32)
+        pe1.record(stream)
+        torch.cuda.synchronize(dev)
+        pms = reduce_max(torch, dist, pe0.elapsed_time(pe1) / plain_steps)
+        plain = {"engine": ENGINE_TEXT["fp32"], "value": job.n * job.nchan * world / (pms * 1e-3),
+                 "ms_per_step": round(pms, 3), "steps": plain_steps, "warmup": 2}
     work = job.n * job.nchan
     value = work * world / (ms_per_step * 1e-3)
-    st = ctx.stats()
 
     # dominant kernel and its roofline
     tc = engine != api.ENGINE_FP32 and job.nchan > 1
@@ -598,7 +643,7 @@ def main():
     traffic = None
     try:
         tr = json.load(open(TRAFFIC))
-        t = tr.get(job.name, {}).get(kernels[dom])
+        t = tr.get("%s:%dx%d:%d" % (job.name, job.n, job.nchan, job.nx), {}).get(kernels[dom])
         traffic = t if t is None else float(t)
     except Exception:
         pass
@@ -659,7 +704,8 @@ def main():
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 geometry)",
+               "scaling": "weak", "vs_baseline": None,
+               "dtype": DTYPE_TEXT[args.engine] if job.nchan > 1 else DTYPE_TEXT["fp32"],
                "data": "synthetic (seeded %s generator, hcgrid_b200/synth.py)" % job.name,
                "config": {"workload": "%s: %d samples x %d channels -> %dx%d RA---SIN/DEC--SIN, GAUSS1D FWHM %g\", "
                                       "sphere_radius 3 sigma" % (job.name, job.n, job.nchan, job.nx, job.ny,
@@ -670,7 +716,8 @@ def main():
                           "engine": ENGINE_TEXT[args.engine] if job.nchan > 1 else ENGINE_TEXT["fp32"],
                           "tc_pipeline": tune},
                "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,
-               "e2e": e2e, "cpu_baseline": cpu}
+               "e2e": e2e, "cpu_baseline": cpu, "plain_fp32": plain,
+               "over_plain_fp32": round(value / plain["value"], 3) if plain else None}
         print(json.dumps(out))
     field.close()
     target.close()
