@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(256) kb_tile_rings(BatchHdr *H, const JobDesc 
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256) kb_group(BatchHdr *H, const JobDesc *__restrict__ jobs) {
+__global__ void __launch_bounds__(256, 3) kb_group(BatchHdr *H, const JobDesc *__restrict__ jobs) {
     __shared__ PixPrep s_prep[8][4];
     __shared__ PixHalf s_half[8][4];
     const int warp = threadIdx.x >> 5;
@@ -222,8 +222,8 @@ struct BatchState {
     uint32_t job_cap = 0;
     cudaGraphExec_t exec = nullptr;
     int nsm = 0;
-    void *scratch[10] = {};
-    size_t scratch_size[10] = {};
+    void *scratch[11] = {};
+    size_t scratch_size[11] = {};
     CUtensorMap *d_maps = nullptr, *h_maps = nullptr;  // two per job: spectra (hi and lo halves), cube
     unsigned long long *d_jovf = nullptr, *h_jovf = nullptr;  // per job: tiles beyond the ring table
     uint32_t map_cap = 0;
@@ -388,6 +388,13 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         (e = grow(B, 8, (tile + 1) * kTileMaxSpan * sizeof(uint16_t), s, &p_ridx)) != cudaSuccess ||
         (e = grow(B, 9, (kBatchScanParts + 1) * sizeof(unsigned long long), s, &p_scan)) != cudaSuccess)
         return e;
+    // per-group windows kept by the tile pass for the weight pass (up to 4 GiB of them)
+    void *p_win = nullptr;
+    const size_t wbytes = (size_t)(tile + 1) * kWinSpan * kTileGroups * 2 * sizeof(uint4);
+    if (wbytes <= (4ull << 30) && grow(B, 10, wbytes, s, &p_win) != cudaSuccess) {
+        cudaGetLastError();
+        p_win = nullptr;
+    }
     if (B.entry_cap == 0) B.entry_cap = 1ULL << 24;
     for (int attempt = 0; attempt < 2; ++attempt) {
         void *p_eidx, *p_ew;
@@ -419,6 +426,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             d.T.base = t_base + d.tile_base * (kTileMaxRings + 1);
             d.T.ring_idx = (uint16_t *)p_ridx + d.tile_base * kTileMaxSpan;
             d.T.cap = d.cap;  // the tile pass counts each group's candidates
+            d.T.win = p_win ? (uint4 *)p_win + d.tile_base * kWinSpan * kTileGroups * 2 : nullptr;
             d.T.overflow = B.d_jovf + i;
             d.X = t->d_x;
             d.Y = t->d_y;

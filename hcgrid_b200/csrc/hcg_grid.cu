@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(256) k_grid_1chan(GridArgs a, uint64_t npixmap
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_group(GridArgs a, GroupArgs g, uint32_t *__restrict__ cap,
+__global__ void __launch_bounds__(256, 3) k_group(GridArgs a, GroupArgs g, uint32_t *__restrict__ cap,
                                                const unsigned long long *__restrict__ off,
                                                uint32_t *__restrict__ e_idx, float4 *__restrict__ e_w,
                                                uint32_t *__restrict__ cnt, double *__restrict__ wsum,
@@ -193,6 +193,16 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         unsigned long long *psum =
             (unsigned long long *)ctx->scratch.get(15, (parts + 1) * sizeof(unsigned long long), s, e);
         T.cap = cap;  // the tile pass counts each group's candidates
+        {
+            // the tile pass keeps each group's windows for the weight pass (up to 4 GiB of them)
+            const size_t wbytes = (size_t)ntiles * kWinSpan * kTileGroups * 2 * sizeof(uint4);
+            cudaError_t ew = cudaSuccess;
+            T.win = wbytes <= (4ull << 30) ? (uint4 *)ctx->scratch.get(18, wbytes, s, ew) : nullptr;
+            if (ew != cudaSuccess) {
+                cudaGetLastError();
+                T.win = nullptr;
+            }
+        }
         T.overflow = &ctx->d_stats->overflow;
         T.pad = tc ? 8 : 1;  // the tensor-core engine loads ring runs as boxes of 8 samples
         if (e != cudaSuccess) return e;

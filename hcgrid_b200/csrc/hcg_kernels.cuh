@@ -314,6 +314,10 @@ struct GroupArgs {
 constexpr int kTileX = 16, kTileY = 8, kTileMaxRings = 1024, kTileMaxSpan = 4096;
 constexpr uint32_t kCapUnknown = 0xffffffffu;
 constexpr int kTileGroups = (kTileX / 2) * (kTileY / 2);
+// Rings of a tile's span whose per-group windows the tile pass keeps for the
+// weight pass (wider spans: the weight pass computes its windows itself).
+// A kept window is (lo, hi); lo > hi marks a ring the reference would spin on.
+constexpr int kWinSpan = 64;
 struct TileArgs {
     uint32_t ntx, nty;
     uint64_t t0;  // first tile of this launch
@@ -321,6 +325,7 @@ struct TileArgs {
     uint32_t *U, *ulo, *base;  // ulo: [tile][kTileMaxRings], base: [tile][kTileMaxRings + 1]
     uint16_t *ring_idx;        // [tile][kTileMaxSpan]: index c of ring r0 + j (0xffff: no candidates)
     uint32_t *cap;             // per 2x2 group: union candidate count (kCapUnknown: left to k_group<true>)
+    uint4 *win;                // [tile][kWinSpan][kTileGroups][2]: the group's 4 pixel windows per ring (or null)
     unsigned long long *overflow;
     uint32_t pad;  // ring runs take a multiple of `pad` slots (> 1: the tensor-core engine's 8-row boxes)
 };
@@ -395,7 +400,26 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
                 slot_shift = (long long)tiles.base[tile * (kTileMaxRings + 1) + c] -
                              (long long)tiles.ulo[tile * kTileMaxRings + c];
         }
-        if (k <= R1) {
+        if (k <= R1 && !COUNT && slots && tiles.win && k - tr0 < kWinSpan) {
+            // the tile pass kept this group's windows for the ring
+            const uint4 *w = tiles.win + ((tile * kWinSpan + (uint64_t)(k - tr0)) * kTileGroups +
+                                          (uint64_t)((gyi % (kTileY / 2)) * (kTileX / 2) + gxi % (kTileX / 2))) * 2;
+            const uint4 w0 = __ldg(w), w1 = __ldg(w + 1);
+            const uint32_t kl[4] = {w0.x, w0.z, w1.x, w1.z}, kh[4] = {w0.y, w0.w, w1.y, w1.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (kl[q] > kh[q]) {
+                    ++skips;
+                } else {
+                    lo[q] = kl[q];
+                    hi[q] = kh[q];
+                    if (hi[q] > lo[q]) {
+                        glo = min(glo, lo[q]);
+                        ghi = max(ghi, hi[q]);
+                    }
+                }
+            }
+        } else if (k <= R1) {
             const RingRec R = a.rings[k];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -707,17 +731,29 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
         const int k = r0 + j;
         uint32_t glo = 0xffffffffu, ghi = 0;
         const RingRec R = a.rings[k];
+        uint32_t wlo[4] = {0, 0, 0, 0}, whi[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int p = (2 * (gq / (kTileX / 2)) + (q >> 1)) * kTileX + 2 * (gq % (kTileX / 2)) + (q & 1);
             const PixPrep &P = s_prep[p];
             if (P.nr > 0 && k >= P.ur && k < P.ur + P.nr) {
                 uint32_t lo, hi;
-                if (ring_window(a.h, R, P, a.keys, lo, hi) && hi > lo) {
-                    glo = min(glo, lo);
-                    ghi = max(ghi, hi);
+                if (!ring_window(a.h, R, P, a.keys, lo, hi)) {
+                    wlo[q] = 1;  // lo > hi: the reference would spin on this ring
+                } else {
+                    wlo[q] = lo;
+                    whi[q] = hi;
+                    if (hi > lo) {
+                        glo = min(glo, lo);
+                        ghi = max(ghi, hi);
+                    }
                 }
             }
+        }
+        if (T.win && j < kWinSpan) {
+            uint4 *w = T.win + ((tile * kWinSpan + j) * kTileGroups + gq) * 2;
+            w[0] = make_uint4(wlo[0], whi[0], wlo[1], whi[1]);
+            w[1] = make_uint4(wlo[2], whi[2], wlo[3], whi[3]);
         }
         if (glo < ghi) {
             atomicAdd(&s_cnt[gq], ghi - glo);
