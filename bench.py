@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config5"])
     ap.add_argument("--jobs", type=int, default=200, help="config5: requests in the stream (the full form has 2000)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
+    ap.add_argument("--detail", default=None, help="config5: write per-request times of the per-call arms here")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--engine", default="tc-f16", choices=list(ENGINES),
@@ -60,7 +61,7 @@ def parse():
                     help="also time this many steps of the plain FP32 engine on the same field (0: skip)")
     ap.add_argument("--tc-config", type=int, default=None,
                     help="tensor-core pipeline shape (0: 256 ch x 64-sample chunks x 2 stages, 1: 128 x 64 x 3, "
-                         "2: 64 x 64 x 4, 3: 256 x 32 x 4); "
+                         "2: 64 x 64 x 4, 3: 256 x 32 x 4, 4/5: 0/3 persistent); "
                          "default: autotuned on the workload before the timed steps")
     # reduced cases (profiling, quick checks); the headline run uses none of these
     ap.add_argument("--samples", type=int, default=None)
@@ -413,6 +414,8 @@ def served_main(args):
         ctx.synchronize()
         torch.cuda.empty_cache()
 
+    detail = []  # per request: arm, shape, seconds, device phase times
+
     def per_call(tc):
         lat = []
         for win in windows:
@@ -423,6 +426,10 @@ def served_main(args):
                 ctx.grid(f, t, cube, wts, engine=eng)
                 ctx.synchronize()
                 lat.append(time.perf_counter() - t0)
+                st = ctx.stats()
+                detail.append({"arm": "tc" if tc else "plain", "request": r["request"], "shape": r["shape"],
+                               "s": lat[-1], "phase_ms": [round(x, 3) for x in st.ms_phase],
+                               "pairs_within": int(st.pairs_within)})
             release(staged)
         return lat
 
@@ -445,10 +452,12 @@ def served_main(args):
                         if d > 0:
                             time.sleep(d)
                     tickets.append(srv.submit(f, t, cube, wts, api.SAMPLE_MAJOR, footprint=footprint(r)))
-                for tk in tickets:
+                for (r, *_), tk in zip(staged, tickets):
                     lt, q = srv.wait(tk)
                     lats.append(lt)
                     queues.append(q)
+                    detail.append({"arm": "served" if rate is None else "poisson", "request": r["request"],
+                                   "shape": r["shape"], "latency_s": lt, "queue_s": q})
                 busy += time.perf_counter() - t0
                 release(staged)
             st = srv.stats()
@@ -486,6 +495,9 @@ def served_main(args):
                            "total_s": round(sum(tc_lat), 4)},
            "served_over_plain": round(capacity / plain, 3),
            "gpu_launches": None, "e2e": None, "cpu_baseline": None}
+    if args.detail:
+        with open(args.detail, "w") as fh:
+            json.dump(detail, fh)
     print(json.dumps(out))
     for f, t, _, _ in base.values():
         f.close()

@@ -273,7 +273,7 @@ class Context:
         """Time each tensor-core pipeline shape on (field, target); keeps and
         returns the fastest with the per-shape best times (ms)."""
         best = C.c_int()
-        ms = (C.c_float * 4)()
+        ms = (C.c_float * 6)()
         self._check(self.L.hcg_autotune(self.h, field.h, target.h, reps, C.byref(best), ms))
         return best.value, list(ms)
 

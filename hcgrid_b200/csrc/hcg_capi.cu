@@ -76,7 +76,7 @@ void release_field(hcg_field *f, cudaStream_t s) {
     if (f->d_spec) cudaFreeAsync(f->d_spec, s);
     free_split(f, s);
     if (f->geom_refs && --*f->geom_refs > 0) return;
-    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_half, f->d_lut, f->d_rings};
+    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_half, f->d_lut, f->d_rings, f->d_ptab};
     for (void *p : ps)
         if (p) cudaFreeAsync(p, s);
     delete f->geom_refs;

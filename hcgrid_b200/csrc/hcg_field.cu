@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <vector>
 
 #include "hcg_internal.h"
 
@@ -199,7 +201,7 @@ __global__ void k_ring_lut(HpxParams h, uint64_t n, const uint64_t *__restrict__
 // (gridding.cu:330-334: ring info, pix2ang of startpix, then the theta used
 // by ang2pix for lpix and rpix).
 __global__ void k_ring_table(HpxParams h, uint64_t firstring, uint64_t usedrings, const uint32_t *__restrict__ lut,
-                             RingRec *__restrict__ rings, DevStats *stats) {
+                             const uint64_t *__restrict__ keys, RingRec *__restrict__ rings, DevStats *stats) {
     uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (k >= usedrings) return;
     RingRec R;
@@ -227,7 +229,25 @@ __global__ void k_ring_table(HpxParams h, uint64_t firstring, uint64_t usedrings
         R.t2 = ddiv(dmul(ns, s), dsqrt(ddiv(dadd(1., za), 3.)));
     R.lut_lo = lut[k];
     R.lut_hi = lut[k + 1];
+    // pixel range of the ring's samples; the table offsets are set on the host
+    R.pmin = 0;
+    R.span = 0;
+    R.tbl = 0;
+    if (R.lut_lo != 0 && R.lut_hi > R.lut_lo) {
+        R.pmin = (uint32_t)(keys[R.lut_lo] - R.startpix);
+        R.span = (uint32_t)(keys[R.lut_hi - 1] - keys[R.lut_lo] + 1);
+    }
     rings[k] = R;
+}
+
+// Per-ring pixel tables: entry q of ring k is the first sorted sample of the
+// ring whose pixel is >= startpix + pmin + q (one block per ring).
+__global__ void __launch_bounds__(256) k_ring_ptab(const RingRec *__restrict__ rings, const uint64_t *__restrict__ keys,
+                                                   uint32_t *__restrict__ ptab) {
+    const RingRec R = rings[blockIdx.x];
+    const uint64_t p0 = R.startpix + R.pmin;
+    for (uint32_t q = threadIdx.x; q < R.span; q += blockDim.x)
+        ptab[R.tbl + q] = lower_bound_u64(keys, R.lut_lo, R.lut_hi, p0 + q);
 }
 
 __global__ void k_permute_geometry(uint64_t n, const uint32_t *__restrict__ perm, const double *__restrict__ lon,
@@ -354,7 +374,35 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
     k_ring_lut<<<(unsigned)((f->usedrings + 1 + 255) / 256), 256, 0, s>>>(f->hpx, n, f->d_keys, f->firstring,
                                                                           f->usedrings, f->d_lut);
     k_ring_table<<<(unsigned)((f->usedrings + 255) / 256), 256, 0, s>>>(f->hpx, f->firstring, f->usedrings, f->d_lut,
-                                                                        f->d_rings, ctx->d_stats);
+                                                                        f->d_keys, f->d_rings, ctx->d_stats);
+    TRY(cudaGetLastError());
+    {
+        // Pixel tables: one u32 per HEALPix pixel between the first and last
+        // sample of each ring, when they fit in max(2^24, 4n) entries
+        // (HCG_RING_TABLE_MAX overrides; 0 keeps the binary searches).
+        uint64_t cap = std::max<uint64_t>(1ull << 24, 4 * n);
+        if (const char *v = getenv("HCG_RING_TABLE_MAX")) cap = strtoull(v, nullptr, 10);
+        std::vector<RingRec> hr(f->usedrings);
+        TRY(cudaMemcpyAsync(hr.data(), f->d_rings, hr.size() * sizeof(RingRec), cudaMemcpyDeviceToHost, s));
+        TRY(cudaStreamSynchronize(s));
+        uint64_t total = 0;
+        for (RingRec &R : hr) {
+            R.tbl = total;
+            total += R.span;
+        }
+        if (total > 0 && total <= cap && cudaMallocAsync(&f->d_ptab, total * sizeof(uint32_t), s) == cudaSuccess) {
+            TRY(cudaMemcpyAsync(f->d_rings, hr.data(), hr.size() * sizeof(RingRec), cudaMemcpyHostToDevice, s));
+            k_ring_ptab<<<(unsigned)f->usedrings, 256, 0, s>>>(f->d_rings, f->d_keys, f->d_ptab);
+            TRY(cudaGetLastError());
+            TRY(cudaStreamSynchronize(s));  // the host copy of the table must outlive the upload
+        } else {
+            cudaGetLastError();
+            for (RingRec &R : hr) R.span = 0, R.tbl = 0;
+            TRY(cudaMemcpyAsync(f->d_rings, hr.data(), hr.size() * sizeof(RingRec), cudaMemcpyHostToDevice, s));
+            TRY(cudaStreamSynchronize(s));
+        }
+        f->ptab_entries = f->d_ptab ? total : 0;
+    }
     TRY(cudaMallocAsync(&f->d_l2, n * sizeof(double), s));
     TRY(cudaMallocAsync(&f->d_b2, n * sizeof(double), s));
     TRY(cudaMallocAsync(&f->d_cb2, n * sizeof(double), s));

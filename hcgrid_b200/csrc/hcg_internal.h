@@ -36,6 +36,12 @@ struct RingRec {
     uint32_t lut_hi; // first sample of the next ring (end_int)
     int eq;          // |z| <= 2/3
     int zpos;        // z > 0
+    // Pixel table of the ring (span > 0): entry q at tbl + q is the first
+    // sorted sample whose pixel is >= startpix + pmin + q, for the pixels
+    // pmin .. pmin + span - 1 between the ring's first and last sample.
+    uint32_t pmin;
+    uint32_t span;
+    uint64_t tbl;
 };
 
 // One target pixel: its coordinates and the phi half of loc2pix for the two
@@ -102,6 +108,8 @@ struct hcg_field {
     double *d_w = nullptr;        // per-sample input weight, sorted
     double4 *d_half = nullptr;    // sorted: sin(l/2), cos(l/2), sin(b/2), cos(b/2) of each sample
     uint32_t *d_lut = nullptr;    // usedrings + 1
+    uint32_t *d_ptab = nullptr;   // per-ring pixel tables (RingRec::tbl), or none when too large
+    uint64_t ptab_entries = 0;
     hcg::RingRec *d_rings = nullptr;
     float *d_spec = nullptr;      // [n][cstride], sorted
     uint32_t nchan = 0, cstride = 0;
@@ -123,7 +131,7 @@ struct hcg_target {
 // Launchers (hcg_field.cu, hcg_grid.cu). All return cudaGetLastError().
 namespace hcg {
 constexpr int kTcClasses = 8;
-constexpr int kTcConfigCount = 4;  // tensor-core pipeline shapes (hcg_tc_set_config)
+constexpr int kTcConfigCount = 6;  // tensor-core pipeline shapes (hcg_tc_set_config)
 // channel class of a split field: 64-channel blocks 1, 2, 3-4, 5-8, ... -> 0, 1, 2, 3, ...
 inline int tc_class_of(uint32_t cpad) {
     const uint32_t b = cpad / 64;

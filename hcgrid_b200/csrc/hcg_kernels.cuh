@@ -99,13 +99,23 @@ __device__ __forceinline__ uint64_t edge_pix(const HpxParams &h, const RingRec &
 // Candidate interval [lo, hi) of one ring for one pixel
 // (gridding.cu:329-367). Returns false where the reference would spin.
 __device__ __forceinline__ bool ring_window(const HpxParams &h, const RingRec &R, const PixPrep &P,
-                                            const uint64_t *__restrict__ keys, uint32_t &lo, uint32_t &hi) {
+                                            const uint64_t *__restrict__ keys, const uint32_t *__restrict__ ptab,
+                                            uint32_t &lo, uint32_t &hi) {
     lo = hi = 0;
     uint64_t lpix = P.polar ? R.startpix : edge_pix(h, R, P, 0);
     if (!(lpix >= R.startpix && lpix < R.startpix + R.npr)) return false;
     uint64_t rpix = P.polar ? R.startpix + R.npr - 1 : edge_pix(h, R, P, 1);
     if (!(rpix >= R.startpix && rpix < R.startpix + R.npr)) return false;
     if (R.lut_lo == 0) return true;  // first used ring: the reference's search returns "none"
+    if (R.span) {
+        // the ring's pixel table gives the same bounds as the searches below
+        const int64_t q0 = (int64_t)(lpix - R.startpix) - (int64_t)R.pmin;
+        lo = q0 <= 0 ? R.lut_lo : (q0 >= (int64_t)R.span ? R.lut_hi : __ldg(ptab + R.tbl + q0));
+        const int64_t q1 = (int64_t)(rpix - R.startpix) - (int64_t)R.pmin + 1;  // first pixel > rpix
+        const uint32_t h1 = q1 <= 0 ? R.lut_lo : (q1 >= (int64_t)R.span ? R.lut_hi : __ldg(ptab + R.tbl + q1));
+        hi = h1 > lo ? h1 : lo;
+        return true;
+    }
     lo = lower_bound_u64(keys, R.lut_lo, R.lut_hi, lpix);
     hi = upper_bound_u64(keys, lo, R.lut_hi, rpix);
     return true;
@@ -168,6 +178,7 @@ struct GridArgs {
     double sphere_radius, p0;
     DevStats *stats;
     const double4 *half;  // per sorted sample: sin(l/2), cos(l/2), sin(b/2), cos(b/2)
+    const uint32_t *ptab; // per-ring pixel tables (RingRec::tbl)
     double hlo, hhi;      // haversine thresholds bracketing sphere_radius (see pair_weight)
     int series;           // d^2 from the arcsine-squared series (small sphere_radius)
 };
@@ -179,7 +190,7 @@ struct GridArgs {
 // formula takes. Inside the band the full formula decides.
 inline GridArgs grid_args(const hcg_field *f, const PixPrep *prep, DevStats *stats) {
     GridArgs a{f->hpx, f->d_rings, prep, f->d_keys, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->sphere_radius,
-               f->kparam0, stats, f->d_half, 0.0, 0.0, 0};
+               f->kparam0, stats, f->d_half, f->d_ptab, 0.0, 0.0, 0};
     const double s = std::sin(f->sphere_radius * kDeg2Rad * 0.5);
     const double hstar = s * s;
     a.hlo = hstar * (1.0 - 1e-9);
@@ -252,7 +263,7 @@ __device__ __forceinline__ void grid1_item(const GridArgs &a, const float *__res
         int r = rb + lane;
         uint32_t lo = 0, hi = 0;
         if (r < P.nr) {
-            if (!ring_window(a.h, a.rings[P.ur + r], P, a.keys, lo, hi)) ++skips;
+            if (!ring_window(a.h, a.rings[P.ur + r], P, a.keys, a.ptab, lo, hi)) ++skips;
         }
         uint32_t len = hi > lo ? hi - lo : 0;
         uint32_t incl = len;
@@ -425,7 +436,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
             for (int q = 0; q < 4; ++q) {
                 const PixPrep &P = s_prep[q];
                 if (valid[q] && k >= P.ur && k < P.ur + P.nr) {
-                    if (!ring_window(a.h, R, P, a.keys, lo[q], hi[q])) {
+                    if (!ring_window(a.h, R, P, a.keys, a.ptab, lo[q], hi[q])) {
                         ++skips;
                     } else if (hi[q] > lo[q]) {
                         glo = min(glo, lo[q]);
@@ -738,7 +749,7 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
             const PixPrep &P = s_prep[p];
             if (P.nr > 0 && k >= P.ur && k < P.ur + P.nr) {
                 uint32_t lo, hi;
-                if (!ring_window(a.h, R, P, a.keys, lo, hi)) {
+                if (!ring_window(a.h, R, P, a.keys, a.ptab, lo, hi)) {
                     wlo[q] = 1;  // lo > hi: the reference would spin on this ring
                 } else {
                     wlo[q] = lo;

@@ -34,6 +34,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_teardown<Cfg>(S, gk, timeouts);
 }
 
+template <class Cfg>
+__global__ void __launch_bounds__(kTcPersistThreads, 1)
+    k_tile_tc_persist(const __grid_constant__ CUtensorMap tm, TcJob J, uint64_t nitems, uint64_t ntiles,
+                      const void *zero_page, unsigned long long *timeouts, unsigned long long *macs) {
+    __shared__ TcPShared S;
+    J.map = &tm;
+    J.out_map = nullptr;
+    if (threadIdx.x == 0) sm100::prefetch_tensormap(&tm);
+    tc_persist<Cfg>(S, J, nitems, ntiles, zero_page, timeouts, macs);
+}
+
 // ------------------------------------------------------------ spectra split
 // Per-channel largest magnitude and the count of non-finite values.
 __global__ void k_split_amax(const float *__restrict__ spec, uint64_t n, uint32_t nchan, uint32_t cstride,
@@ -241,10 +252,36 @@ int tc_pick(const hcg_context *ctx, const hcg_field *f) {
     const int t = ctx->tc_config[tc_class_of(f->xcpad)];
     if (t >= 0 && t < kTcConfigCount) return t;
     const uint32_t b = f->xcpad / 64;
-    return b >= 4 ? 3 : (b >= 2 ? 1 : 2);
+    return b >= 4 ? 4 : (b >= 2 ? 1 : 2);
 }
 
 namespace {
+template <class Cfg>
+cudaError_t launch_tc_persist(hcg_context *ctx, const hcg_field *f, TcJob &J, const TileArgs &T, uint64_t ntiles,
+                              const void *zero, std::string &why) {
+    cudaStream_t s = ctx->stream;
+    CUtensorMap tm;
+    if (!tc_prepare_job(f, Cfg::kNb, &tm, J)) {
+        why = "cuTensorMapEncodeTiled";
+        return cudaErrorInvalidValue;
+    }
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set) {
+        cudaError_t e = tc_set_smem((const void *)k_tile_tc_persist<Cfg>, Cfg::kSmem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    J.T = T;
+    const uint64_t nitems = ntiles * J.ncb;
+    const unsigned grid = (unsigned)std::min<uint64_t>(nitems, (uint64_t)(nsm > 0 ? nsm : 148));
+    if (grid == 0) return cudaSuccess;
+    k_tile_tc_persist<Cfg><<<grid, kTcPersistThreads, Cfg::kSmem, s>>>(tm, J, nitems, ntiles, zero,
+                                                                      &ctx->d_stats->timeouts, &ctx->d_stats->tc_macs);
+    return cudaGetLastError();
+}
+
 template <class Cfg>
 cudaError_t launch_tc(hcg_context *ctx, const hcg_field *f, TcJob &J, const TileArgs &T, uint64_t ntiles,
                       const void *zero, std::string &why) {
@@ -295,7 +332,9 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
         case 0: return launch_tc<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
         case 1: return launch_tc<TcCfgN2S3>(ctx, f, J, T, ntiles, zero, why);
         case 2: return launch_tc<TcCfgN1S4>(ctx, f, J, T, ntiles, zero, why);
-        default: return launch_tc<TcCfgN4K32>(ctx, f, J, T, ntiles, zero, why);
+        case 3: return launch_tc<TcCfgN4K32>(ctx, f, J, T, ntiles, zero, why);
+        case 4: return launch_tc_persist<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
+        default: return launch_tc_persist<TcCfgN4K32>(ctx, f, J, T, ntiles, zero, why);
     }
 }
 

@@ -91,7 +91,9 @@ using TcCfgN4S2 = TcCfg<4, 2, 64>;  // 256 channels per item, 64-slot chunks, 2 
 using TcCfgN2S3 = TcCfg<2, 3, 64>;  // 128 channels, 64-slot chunks, 3 stages
 using TcCfgN1S4 = TcCfg<1, 4, 64>;  // 64 channels, 64-slot chunks, 4 stages
 using TcCfgN4K32 = TcCfg<4, 4, 32>;  // 256 channels, 32-slot chunks, 4 stages
-static_assert(kTcConfigCount == 4, "hcg_tc_set_config numbers the shapes above 0, 1, 2, 3");
+// 4, 5: shapes 0 and 3 in the persistent kernel (one CTA per SM, epilogue
+// overlapped with the next item)
+static_assert(kTcConfigCount == 6, "hcg_tc_set_config numbers the shapes 0-3 above and 4-5 persistent");
 
 // One job's tensor-core arguments.
 struct TcJob {
@@ -187,7 +189,8 @@ __device__ __forceinline__ void tc_setup(TcShared &S) {
     tc_fence_after();
 }
 
-__device__ __forceinline__ void tc_give_up(TcShared &S, unsigned long long *timeouts) {
+template <class SH>
+__device__ __forceinline__ void tc_give_up(SH &S, unsigned long long *timeouts) {
     atomicAdd(timeouts, 1ULL);
     S.abort = 1;
 }
@@ -202,7 +205,7 @@ __device__ __forceinline__ void tc_teardown(TcShared &S, uint32_t gk, unsigned l
     if (tid == 0) {
         for (uint32_t g = gk > ST ? gk - ST : 0; g < gk; ++g) {
             const uint32_t s = g % ST, ph = (g / ST) & 1;
-            if (!mbar_wait(&S.full_b[s], ph, kTcWaitNs) || !mbar_wait(&S.zfill[s], ph, kTcWaitNs)) {
+            if (!mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
                 tc_give_up(S, timeouts);
                 break;
             }
@@ -223,6 +226,199 @@ __device__ __forceinline__ void tc_load_rings(TcShared &S, const TileArgs &T, ui
     for (int j = threadIdx.x; j <= nrt; j += kTcThreads) S.base[j] = T.base[tile * (kTileMaxRings + 1) + j];
 }
 
+// Operand buffers of one pipeline stage.
+template <class Cfg>
+struct TcStage {
+    uint8_t *smem;
+    __device__ __forceinline__ uint8_t *A_hi(uint32_t s) const { return smem + s * Cfg::kStageBytes; }
+    __device__ __forceinline__ uint8_t *A_lo(uint32_t s) const { return smem + s * Cfg::kStageBytes + Cfg::kAHalf; }
+    __device__ __forceinline__ uint8_t *B(uint32_t s) const { return smem + s * Cfg::kStageBytes + 2 * Cfg::kAHalf; }
+};
+
+// Producer (the whole warp 0), one item: per chunk one 4-D TMA box per run of
+// 8 slots, issued by lanes 0..KC/8-1 in parallel, while lanes KC/8..2KC/8-1
+// prefetch the boxes of chunk k + stages into L2. S.ulo / S.base hold the
+// item's ring table (nrt rings); `gk` is the CTA's chunk count before the item.
+template <class Cfg, class SH>
+__device__ __forceinline__ void tc_produce(SH &S, const TcJob &J, uint32_t cblk, uint32_t U, uint32_t nchunks,
+                                           uint32_t gk, int nrt, unsigned long long *timeouts) {
+    using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
+    constexpr int NB8 = (int)(KC / 8);
+    const TcStage<Cfg> st{tc_smem_base()};
+    const int lane = threadIdx.x & 31;
+    const uint32_t bytes = NB8 * 2u * J.nb * 1024u;
+    // TMA row of slot0: the ring run j with base[j] <= slot0 < base[j + 1]
+    auto row_of = [&](uint32_t slot0) -> int {
+        if (slot0 >= U) return (int)J.nrows;  // past the last sample: zero fill
+        int lo = 0, hi = nrt;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (S.base[mid] <= slot0) lo = mid; else hi = mid;
+        }
+        return (int)(S.ulo[lo] + (slot0 - S.base[lo]));
+    };
+    for (uint32_t k = 0; k < nchunks; ++k) {
+        const uint32_t g = gk + k, s = g % ST;
+        int go = 1;
+        if (lane == 0) {
+            if (S.abort) {
+                go = 0;
+            } else if (g >= ST && !mbar_wait(&S.empty[s], ((g / ST) - 1) & 1, kTcWaitNs)) {
+                tc_give_up(S, timeouts);
+                go = 0;
+            } else {
+                mbar_arrive_expect_tx(&S.full_b[s], bytes);
+            }
+        }
+        if (!__shfl_sync(0xffffffffu, go, 0)) break;
+        const int b = lane % NB8;
+        const uint32_t kk = lane < NB8 ? k : k + ST;
+        if (lane < 2 * NB8 && kk < nchunks) {
+            const int row = row_of(kk * KC + 8 * b);
+            if (lane < NB8)
+                tma_load_4d(st.B(s) + b * Cfg::kBGroup, J.map, &S.full_b[s], 0, row, (int)(cblk * J.nb), 0);
+            else
+                tma_prefetch_4d(J.map, 0, row, (int)(cblk * J.nb), 0);
+        }
+    }
+}
+
+// MMA issue (one thread), one item into the accumulator at `d_tmem`; every
+// chunk's stage is released on its `empty` barrier when its MMAs complete.
+// Returns false if a wait ran out.
+template <class Cfg, class SH>
+__device__ __forceinline__ bool tc_mma(SH &S, const TcJob &J, uint32_t nchunks, uint32_t gk, uint32_t d_tmem,
+                                       unsigned long long *timeouts, unsigned long long *macs) {
+    using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
+    const TcStage<Cfg> st{tc_smem_base()};
+    const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
+    uint32_t acc = 0;
+    bool ok = true;
+    for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
+        const uint32_t g = gk + k, s = g % ST, ph = (g / ST) & 1;
+        if (!mbar_wait(&S.full_a[s], ph, kTcWaitNs) || !mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
+            tc_give_up(S, timeouts);
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        const uint32_t ah = smem_u32(st.A_hi(s)), al = smem_u32(st.A_lo(s));
+        const uint32_t bh = smem_u32(st.B(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
+#pragma unroll
+        for (int kk = 0; kk < (int)(KC / 16); ++kk) {
+            const uint64_t adh = smem_desc(ah + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
+            const uint64_t adl = smem_desc(al + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
+            // two 8-slot row groups per K step; 64-channel atoms 1 KB apart
+            const uint64_t bdh = smem_desc(bh + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
+            const uint64_t bdl = smem_desc(bl + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
+            mma_f16_ss(d_tmem, adh, bdh, idesc, acc);
+            mma_f16_ss(d_tmem, adh, bdl, idesc, 1);
+            mma_f16_ss(d_tmem, adl, bdh, idesc, 1);
+            acc = 1;
+        }
+        mma_commit(&S.empty[s]);
+    }
+    if (acc) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)KC * nchunks);
+    return ok;
+}
+
+// Builders (kTcBuilders threads, index bt), one item: the weights of the
+// chunk's entries into the zeroed K-major operand.
+template <class Cfg, class SH>
+__device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, uint32_t nchunks, uint32_t gk, int bt,
+                                         unsigned long long *timeouts) {
+    using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
+    const TcStage<Cfg> st{tc_smem_base()};
+    const TileArgs &T = J.T;
+    const GroupArgs &G = J.g;
+    const int gq = bt >> 2, sub = bt & 3;
+    const uint32_t gxl = gq & 7, gyl = gq >> 3;
+    const uint32_t gxi = (uint32_t)(tile % T.ntx) * (kTileX / 2) + gxl;
+    const uint32_t gyi = (uint32_t)(tile / T.ntx) * (kTileY / 2) + gyl;
+    const uint64_t grp = (uint64_t)gyi * G.gx + gxi;
+    uint64_t e = 0, e_end = 0;
+    if (gxi < G.gx && grp < G.ngroups) {
+        e = J.off[grp] - G.ebase;
+        e_end = e + J.cnt[grp];
+    }
+    e += sub;
+    // This thread takes every 4th entry of its group. Its next eight entries
+    // sit in a private ring in shared memory filled by cp.async: the copy of
+    // an entry is issued eight entries before it is read, and reading the ring
+    // at a per-thread position needs neither register moves nor divergent
+    // branches.
+    uint32_t *rs = S.ring_slot + bt;  // [kTcRing][kTcBuilders]
+    float4 *rw = S.ring_w + bt;
+    auto issue = [&](int i) {
+        if (e < e_end) {
+            cp_async4(rs + i * kTcBuilders, J.e_slot + e);
+            cp_async16(rw + i * kTcBuilders, J.e_w + e, true);
+        } else {
+            rs[i * kTcBuilders] = 0xffffffffu;
+        }
+        cp_async_commit();
+        e += 4;
+    };
+#pragma unroll
+    for (int i = 0; i < kTcRing; ++i) issue(i);
+    int head = 0;
+    uint32_t mrow[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) mrow[q] = (2 * gyl + (q >> 1)) * kTileX + 2 * gxl + (q & 1);
+    for (uint32_t k = 0; k < nchunks; ++k) {
+        const uint32_t g = gk + k, s = g % ST;
+        // warp-uniform exits: the zeroing below ends with __syncwarp
+        if (__any_sync(0xffffffffu, S.abort)) break;
+        const bool free = g < ST || mbar_wait(&S.empty[s], ((g / ST) - 1) & 1, kTcWaitNs);
+        if (__any_sync(0xffffffffu, !free)) {
+            if (!free) tc_give_up(S, timeouts);
+            break;
+        }
+        uint8_t *ah = st.A_hi(s), *al = st.A_lo(s);
+        {
+            // the group's four threads zero the group's four operand rows (hi and
+            // lo); the scatter below writes only into these rows
+            constexpr int kPieces = Cfg::kARow / 16;
+            const uint32_t m = mrow[sub];
+            uint4 *rh = (uint4 *)(ah + (m >> 3) * Cfg::kAAtom + (m & 7) * Cfg::kARow);
+            uint4 *rl = (uint4 *)(al + (m >> 3) * Cfg::kAAtom + (m & 7) * Cfg::kARow);
+#pragma unroll
+            for (int i = 0; i < kPieces; ++i) {
+                const int c = (i + bt) & (kPieces - 1);  // rotated: fewer bank conflicts
+                rh[c] = make_uint4(0, 0, 0, 0);
+                rl[c] = make_uint4(0, 0, 0, 0);
+            }
+            __syncwarp();
+        }
+        const uint32_t cs = k * KC, ce = cs + KC;
+        for (;;) {
+            cp_async_wait<kTcRing - 1>();  // the ring's oldest copy has landed
+            const uint32_t slot = rs[head * kTcBuilders];
+            if (slot >= ce) break;
+            const float4 wq = rw[head * kTcBuilders];
+            const uint32_t col = slot - cs;
+            const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float w = wv[q] * J.wscale;
+                const uint16_t h = tc_to16(w, J.fmt);
+                const uint16_t l = tc_to16(w - tc_from16(h, J.fmt), J.fmt);
+                const uint32_t o = tc_a_offset<KC>(mrow[q], col);
+                *(uint16_t *)(ah + o) = h;
+                *(uint16_t *)(al + o) = l;
+            }
+            issue(head);
+            head = (head + 1) & (kTcRing - 1);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(&S.full_a[s]);
+    }
+    cp_async_wait<0>();  // no copy into the ring outlives the item
+}
+
 // Whole CTA: one item. `gk` counts the K chunks this CTA has run (all items),
 // `itn` its items; both advance identically in every thread.
 template <class Cfg>
@@ -230,152 +426,25 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
                                         uint32_t itn, const void *zero_page, unsigned long long *timeouts,
                                         unsigned long long *macs) {
     using namespace sm100;
-    uint8_t *smem = tc_smem_base();
-    constexpr uint32_t ST = Cfg::kStages;
-    constexpr uint32_t KC = Cfg::kK;
-    auto A_hi = [&](uint32_t s) { return smem + s * Cfg::kStageBytes; };
-    auto A_lo = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + Cfg::kAHalf; };
-    auto B_of = [&](uint32_t s) { return smem + s * Cfg::kStageBytes + 2 * Cfg::kAHalf; };
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileArgs &T = J.T;
     const uint32_t U = T.U[tile];
-    const uint32_t nchunks = (U + KC - 1) / KC;
+    const uint32_t nchunks = (U + Cfg::kK - 1) / Cfg::kK;
     const uint32_t taddr = S.tmem;
-
     if (warp == 0) {
-        if (lane == 0) {
-            // ---------------------------------------------------- producer
-            const uint32_t bytes = (KC / 8) * 2u * J.nb * 1024u;
-            int j = 0;
-            for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
-                const uint32_t g = gk + k, s = g % ST;
-                if (g >= ST && !mbar_wait(&S.empty[s], ((g / ST) - 1) & 1, kTcWaitNs)) {
-                    tc_give_up(S, timeouts);
-                    break;
-                }
-                mbar_arrive_expect_tx(&S.zfill[s], 2 * Cfg::kAHalf);
-                // each CTA copies from its own window of the zero region, so the
-                // copies of all SMs spread over the L2 slices
-                bulk_copy_g2s(A_hi(s), (const uint8_t *)zero_page + (blockIdx.x % kTcZeroWindows) * kTcMaxA,
-                              2 * Cfg::kAHalf, &S.zfill[s]);
-                mbar_arrive_expect_tx(&S.full_b[s], bytes);
-#pragma unroll
-                for (int b = 0; b < (int)(KC / 8); ++b) {
-                    const uint32_t slot0 = k * KC + 8 * b;
-                    int row;
-                    if (slot0 >= U) {
-                        row = (int)J.nrows;  // past the last sample: zero fill
-                    } else {
-                        while (S.base[j + 1] <= slot0) ++j;
-                        row = (int)(S.ulo[j] + (slot0 - S.base[j]));
-                    }
-                    tma_load_4d(B_of(s) + b * Cfg::kBGroup, J.map, &S.full_b[s], 0, row, (int)(cblk * J.nb), 0);
-                }
-            }
-        }
+        tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, T.nr[tile], timeouts);
     } else if (warp == 1) {
         if (lane == 0) {
-            // ---------------------------------------------------- MMA issue
-            const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
-            uint32_t acc = 0;
-            for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
-                const uint32_t g = gk + k, s = g % ST, ph = (g / ST) & 1;
-                if (!mbar_wait(&S.full_a[s], ph, kTcWaitNs) || !mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
-                    tc_give_up(S, timeouts);
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t ah = smem_u32(A_hi(s)), al = smem_u32(A_lo(s));
-                const uint32_t bh = smem_u32(B_of(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
-#pragma unroll
-                for (int kk = 0; kk < (int)(KC / 16); ++kk) {
-                    const uint64_t adh = smem_desc(ah + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
-                    const uint64_t adl = smem_desc(al + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
-                    // two 8-slot row groups per K step; 64-channel atoms 1 KB apart
-                    const uint64_t bdh = smem_desc(bh + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
-                    const uint64_t bdl = smem_desc(bl + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
-                    mma_f16_ss(taddr, adh, bdh, idesc, acc);
-                    mma_f16_ss(taddr, adh, bdl, idesc, 1);
-                    mma_f16_ss(taddr, adl, bdh, idesc, 1);
-                    acc = 1;
-                }
-                mma_commit(&S.empty[s]);
-            }
-            if (acc) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)KC * nchunks);
+            tc_mma<Cfg>(S, J, nchunks, gk, taddr, timeouts, macs);
             if (nchunks == 0)
                 mbar_arrive(&S.acc_full);
             else
                 mma_commit(&S.acc_full);  // also after a timeout: every MMA issued has completed once it fires
         }
     } else {
-        // -------------------------------------------------------- weight operand
         const GroupArgs &G = J.g;
-        const int bt = tid - 64, gq = bt >> 2, sub = bt & 3;
-        const uint32_t gxl = gq & 7, gyl = gq >> 3;
-        const uint32_t gxi = (uint32_t)(tile % T.ntx) * (kTileX / 2) + gxl;
-        const uint32_t gyi = (uint32_t)(tile / T.ntx) * (kTileY / 2) + gyl;
-        const uint64_t grp = (uint64_t)gyi * G.gx + gxi;
-        uint64_t e = 0, e_end = 0;
-        if (gxi < G.gx && grp < G.ngroups) {
-            e = J.off[grp] - G.ebase;
-            e_end = e + J.cnt[grp];
-        }
-        e += sub;
-        // This thread takes every 4th entry of its group. Its next eight
-        // entries sit in a private ring in shared memory filled by cp.async:
-        // the copy of an entry is issued eight entries before it is read, and
-        // reading the ring at a per-thread position needs neither register
-        // moves nor divergent branches.
-        uint32_t *rs = S.ring_slot + bt;  // [kTcRing][kTcBuilders]
-        float4 *rw = S.ring_w + bt;
-        auto issue = [&](int i) {
-            if (e < e_end) {
-                cp_async4(rs + i * kTcBuilders, J.e_slot + e);
-                cp_async16(rw + i * kTcBuilders, J.e_w + e, true);
-            } else {
-                rs[i * kTcBuilders] = 0xffffffffu;
-            }
-            cp_async_commit();
-            e += 4;
-        };
-#pragma unroll
-        for (int i = 0; i < kTcRing; ++i) issue(i);
-        int head = 0;
-        uint32_t mrow[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) mrow[q] = (2 * gyl + (q >> 1)) * kTileX + 2 * gxl + (q & 1);
-        for (uint32_t k = 0; k < nchunks; ++k) {
-            const uint32_t g = gk + k, s = g % ST;
-            if (S.abort) break;
-            if (!mbar_wait(&S.zfill[s], (g / ST) & 1, kTcWaitNs)) {  // zeroed operand: the stage is free
-                tc_give_up(S, timeouts);
-                break;
-            }
-            const uint32_t cs = k * KC, ce = cs + KC;
-            uint8_t *ah = A_hi(s), *al = A_lo(s);
-            for (;;) {
-                cp_async_wait<kTcRing - 1>();  // the ring's oldest copy has landed
-                const uint32_t slot = rs[head * kTcBuilders];
-                if (slot >= ce) break;
-                const float4 wq = rw[head * kTcBuilders];
-                const uint32_t col = slot - cs;
-                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float w = wv[q] * J.wscale;
-                    const uint16_t h = tc_to16(w, J.fmt);
-                    const uint16_t l = tc_to16(w - tc_from16(h, J.fmt), J.fmt);
-                    const uint32_t o = tc_a_offset<KC>(mrow[q], col);
-                    *(uint16_t *)(ah + o) = h;
-                    *(uint16_t *)(al + o) = l;
-                }
-                issue(head);
-                head = (head + 1) & (kTcRing - 1);
-            }
-            fence_proxy_async_smem();
-            mbar_arrive(&S.full_a[s]);
-        }
-        cp_async_wait<0>();  // no copy into the ring outlives the item
+        const int bt = tid - 64;
+        tc_build<Cfg>(S, J, tile, nchunks, gk, bt, timeouts);
         // -------------------------------------------------------- epilogue
         const uint32_t c_item = cblk * J.nb * 64;  // first channel of the item
         const uint32_t ncols = 64 * J.nb;
@@ -460,6 +529,170 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
         tc_fence_before();
     }
     gk += nchunks;
+}
+
+// ---------------------------------------------------------------- persistent
+// One CTA per SM over a static sequence of items (item it = blockIdx.x +
+// i * gridDim.x; channel blocks outer, tiles inner). Each role walks the
+// sequence on its own, coupled to the others only through mbarriers: the
+// producer runs ahead into the next item while the MMAs of the current one
+// run, and four epilogue warps (6-9) drain item i's accumulator while the MMAs
+// of item i+1 fill the other one (two TMEM accumulators of 256 columns).
+constexpr int kTcPersistThreads = 320;
+
+struct TcPShared {
+    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], zfill[kTcMaxStages];
+    uint64_t acc_full[2], acc_empty[2];
+    uint32_t tmem;
+    volatile int abort;
+    uint32_t ulo[kTileMaxRings], base[kTileMaxRings + 1];  // the producer's current item
+    float inv_scale[2][kTcMaxN];                           // the epilogue's items (by parity)
+    float4 ring_w[kTcRing * kTcBuilders];
+    uint32_t ring_slot[kTcRing * kTcBuilders];
+};
+
+// Epilogue warps (128 threads, index eb), one item from accumulator `a`:
+// normalise and store straight from registers (16-byte stores along channels
+// for [pixel][channel] cubes; along pixels for [channel][pixel] cubes).
+__device__ __forceinline__ void tc_epilogue_direct(TcPShared &S, const TcJob &J, uint64_t tile, uint32_t cblk,
+                                                   uint32_t nchunks, uint32_t il, int eb,
+                                                   unsigned long long *timeouts) {
+    using namespace sm100;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t a = il & 1;
+    const TileArgs &T = J.T;
+    const GroupArgs &G = J.g;
+    const uint32_t c_item = cblk * J.nb * 64;
+    const uint32_t ncols = 64 * J.nb;
+    for (uint32_t c = eb; c < ncols; c += kTcBuilders)
+        S.inv_scale[a][c] = c_item + c < J.nchan ? J.inv_scale[c_item + c] : 0.f;
+    const bool ok = mbar_wait(&S.acc_full[a], (il >> 1) & 1, kTcWaitNs);
+    if (!ok) tc_give_up(S, timeouts);
+    tc_fence_after();
+    const bool store = !named_barrier_or(3, kTcBuilders, !ok || S.abort);  // scales staged, same decision
+    const uint32_t q4 = warp & 3;  // TMEM lane quarter this warp may access
+    const uint32_t m = q4 * 32 + lane;
+    const uint32_t xx = (uint32_t)(tile % T.ntx) * kTileX + (m & (kTileX - 1));
+    const uint32_t yy = (uint32_t)(tile / T.ntx) * kTileY + m / kTileX;
+    const bool valid = xx < G.nx && yy < G.ny;
+    const uint64_t P = (uint64_t)G.nx * G.ny;
+    const uint64_t p = (uint64_t)yy * G.nx + xx;
+    const double ws = valid ? J.wsum[p] : 0.0;
+    const float inv = (float)(1.0 / ws);
+    if (store && valid && cblk == 0 && J.wout) J.wout[p] = (float)ws;
+    const float *sc = S.inv_scale[a];
+    for (uint32_t cb = 0; cb < 2 * J.nb; ++cb) {
+        uint32_t r[32];
+        if (nchunks > 0) {
+            tmem_ld_32x32b_x32(S.tmem + a * 256u + ((q4 * 32u) << 16) + cb * 32u, r);
+            tmem_wait_ld();
+        } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) r[i] = 0u;
+        }
+        if (!store || !valid) continue;
+        const uint32_t c0 = c_item + cb * 32;
+        float v[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = (__uint_as_float(r[i]) * sc[cb * 32 + i]) * inv;
+        if (J.ostride == 0) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                if (c0 + i < J.nchan) J.out[(uint64_t)(c0 + i) * P + p] = v[i];
+        } else {
+            float *dst = J.out + p * J.ostride + c0;
+            if ((J.ostride & 3) == 0 && c0 + 32 <= J.nchan && (((uintptr_t)J.out) & 15) == 0) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    reinterpret_cast<float4 *>(dst)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (c0 + i < J.nchan) dst[i] = v[i];
+            }
+        }
+    }
+    tc_fence_before();
+    mbar_arrive(&S.acc_empty[a]);  // the accumulator may be overwritten
+}
+
+template <class Cfg>
+__device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_t nitems, uint64_t ntiles,
+                                           const void *zero_page, unsigned long long *timeouts,
+                                           unsigned long long *macs) {
+    using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
+    static_assert(Cfg::kTmemCols <= 256, "two accumulators fit the 512 TMEM columns");
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (uint32_t s = 0; s < ST; ++s) {
+            mbar_init(&S.full_a[s], kTcBuilders);
+            mbar_init(&S.full_b[s], 1);
+            mbar_init(&S.empty[s], 1);
+            mbar_init(&S.zfill[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&S.acc_full[a], 1);
+            mbar_init(&S.acc_empty[a], kTcBuilders);
+        }
+        S.abort = 0;
+        mbar_fence_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&S.tmem, 512);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t gk = 0, il = 0;
+    for (uint64_t it = blockIdx.x; it < nitems; it += gridDim.x, ++il) {
+        const uint64_t tile = J.T.t0 + it % ntiles;
+        const uint32_t cblk = (uint32_t)(it / ntiles);
+        const uint32_t U = J.T.U[tile];
+        const uint32_t nchunks = (U + KC - 1) / KC;
+        if (warp == 0) {
+            // the item's ring table, loaded by the whole producer warp
+            __syncwarp();
+            const int nrt = J.T.nr[tile];
+            for (int j = lane; j < nrt; j += 32) S.ulo[j] = J.T.ulo[tile * kTileMaxRings + j];
+            for (int j = lane; j <= nrt; j += 32) S.base[j] = J.T.base[tile * (kTileMaxRings + 1) + j];
+            __syncwarp();
+            tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
+        } else if (warp == 1) {
+            if (lane == 0) {
+                const uint32_t a = il & 1;
+                if (il >= 2 && !mbar_wait(&S.acc_empty[a], ((il >> 1) - 1) & 1, kTcWaitNs)) tc_give_up(S, timeouts);
+                tc_fence_after();
+                tc_mma<Cfg>(S, J, nchunks, gk, S.tmem + a * 256u, timeouts, macs);
+                if (nchunks == 0)
+                    mbar_arrive(&S.acc_full[a]);
+                else
+                    mma_commit(&S.acc_full[a]);
+            }
+        } else if (warp < 6) {
+            tc_build<Cfg>(S, J, tile, nchunks, gk, tid - 64, timeouts);
+        } else {
+            tc_epilogue_direct(S, J, tile, cblk, nchunks, il, tid - 192, timeouts);
+        }
+        gk += nchunks;
+    }
+    // the copies of the last chunks land before the shared memory is given back
+    if (tid == 0) {
+        for (uint32_t g = gk > ST ? gk - ST : 0; g < gk; ++g) {
+            const uint32_t s = g % ST, ph = (g / ST) & 1;
+            if (!mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
+                tc_give_up(S, timeouts);
+                break;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(S.tmem, 512);
+    }
 }
 
 }  // namespace

@@ -130,12 +130,15 @@ hcg_status hcg_field_split_spectra(hcg_field *field, int engine, int keep_fp32);
  *   1: 128 channels per item, 64-sample chunks, 3 stages
  *   2:  64 channels per item, 64-sample chunks, 4 stages
  *   3: 256 channels per item, 32-sample chunks, 4 stages
+ *   4: shape 0 in a persistent kernel (one CTA per SM; the epilogue of a
+ *      tile overlaps the next tile's MMAs)
+ *   5: shape 3 in the persistent kernel
  * Channel classes: 64-channel blocks 1, 2, 3-4, 5-8, 9-16, ... -> 0, 1, 2, 3, 4, ...
  * hcg_tc_set_config sets the shape of one class (-1: every class); config -1
  * restores the default (the widest item the channels fill).
  * hcg_autotune grids (field, target) with each shape `reps` times (device
  * scratch output), keeps the fastest for the field's channel class and
- * returns it and the best time of each shape (ms[4], may be NULL). The field
+ * returns it and the best time of each shape (ms[6], may be NULL). The field
  * must hold split spectra. No reference counterpart. */
 hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config);
 hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, int *best,

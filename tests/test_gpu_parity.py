@@ -158,6 +158,30 @@ def test_entry_budget_chunks_give_identical_cube(ctx):
     np.testing.assert_array_equal(w1, w2)
 
 
+@pytest.mark.parametrize("nchan", [1, 64])
+def test_ring_pixel_tables_match_binary_searches(ctx, monkeypatch, nchan):
+    """The per-ring pixel tables give the windows the binary searches over the
+    sorted keys give: same candidates, same pairs, bit-identical cube."""
+    job = synth.config2(n=150_000, nchan=nchan, nx=120, size_deg=2.0, build_values=True)
+    prepare(ctx, job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    t = ctx.target_from_header(job.header)
+    out = []
+    for cap in ("0", None):
+        if cap is None:
+            monkeypatch.delenv("HCG_RING_TABLE_MAX", raising=False)
+        else:
+            monkeypatch.setenv("HCG_RING_TABLE_MAX", cap)
+        f = ctx.field(job.lon, job.lat)
+        f.set_spectra(job.values)
+        cube, w = ctx.grid(f, t)
+        st = ctx.stats()
+        out.append((cube, w, st.pairs_candidate, st.pairs_within))
+        f.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert out[0][2:] == out[1][2:]
+
+
 def test_invalid_inputs_are_rejected(ctx):
     prepare(ctx, 0.02, 0.06, 0.01)
     lon = np.array([10.0, 10.1, 10.2])

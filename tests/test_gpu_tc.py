@@ -180,7 +180,7 @@ def test_pipeline_shapes_and_autotune(ctx, small):
     f.split_spectra(api.ENGINE_TC_F16)
     outs = []
     try:
-        for cfg in range(4):
+        for cfg in range(6):
             ctx.tc_set_config(cfg)
             c, w = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
             np.testing.assert_array_equal(w, w32)
@@ -191,9 +191,9 @@ def test_pipeline_shapes_and_autotune(ctx, small):
         ctx.tc_set_config(-1)
         best, ms = ctx.autotune(f, t, reps=1)
         print("autotune", best, ms)
-        assert best in (0, 1, 2, 3) and all(m > 0 for m in ms)
+        assert best in range(6) and all(m > 0 for m in ms)
         with pytest.raises(RuntimeError, match="HCG_EINVAL"):
-            ctx.tc_set_config(5)
+            ctx.tc_set_config(6)
     finally:
         ctx.tc_set_config(-1)
 
