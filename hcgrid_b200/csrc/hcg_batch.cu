@@ -5,19 +5,25 @@
 // channel-slice pairs) from a device-side queue (an atomic head per phase)
 // and look the item's job up in a device job table. Launch shapes do not
 // depend on the batch, and all per-batch state (job table, queue heads,
-// totals, scratch pointers) lives in device memory, so the whole pass is
-// captured once into a CUDA graph and replayed for every batch; the host
-// only uploads the job table before the replay.
+// totals, scratch pointers) lives in device memory, so the phases are
+// captured once into two CUDA graphs and replayed for every batch:
+//   geometry: pixel setup, tile ring tables and candidate counts, offsets,
+//             per-job entry totals;
+//   sums:     FP64 weights -> entries, channel sums (FP32 or tensor cores),
+//             single-channel pixels.
+// Between the two the host reads the entry totals, sizes the shared entry
+// pool for them and routes to the single-job path (hcg_grid, which runs in
+// budget-sized passes) the jobs whose entries do not fit the context's entry
+// budget and those whose tiles span more rings than the tile table holds;
+// routed jobs are skipped by the second graph.
 //
 // Items run the same device functions as the single-job launches
-// (hcg_kernels.cuh), so each job's cube is identical to hcg_grid's. Entries
-// of all jobs share one pool; if a batch needs more than the pool holds, the
-// geometry phase skips the groups that do not fit, flags it, and the host
-// grows the pool and replays. A job whose tiles span more rings than the
-// tile table holds is re-run through hcg_grid.
+// (hcg_kernels.cuh), so each job's cube is identical to hcg_grid's.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "hcg_internal.h"
@@ -44,6 +50,7 @@ struct JobDesc {
     // first item of this job in each phase's item space
     unsigned long long pix_base, grp_base, tile_base, acc_base, c1_base, tc_base;
     TcJob tc;  // tensor-core engine arguments (jobs whose field holds split spectra)
+    uint32_t skip;  // routed to the single-job path: no entries, no sums here
 };
 
 enum { Q_TILE = 0, Q_COUNT, Q_GEOM, Q_ACC, Q_C1, Q_TC, Q_N };
@@ -122,6 +129,7 @@ __global__ void __launch_bounds__(256, 3) kb_group(BatchHdr *H, const JobDesc *_
         const JobDesc &J = jobs[j];
         uint64_t grp = it - J.grp_base;
         if (!COUNT) {
+            if (J.skip) continue;
             // the pool must hold this group's entries; otherwise skip and report
             // (no entries recorded: the pass is replayed once the pool has grown)
             unsigned long long end = J.off[grp] + J.cap[grp];
@@ -152,6 +160,14 @@ __global__ void __launch_bounds__(kScanThreads) kb_scan_apply(BatchHdr *H) {
     scan_apply_item(H->cap_all, H->tot_grp, kBatchScanParts, H->scan_part, H->off_all, blockIdx.x);
 }
 
+// Entries of each job: the difference of the offsets at its group range ends.
+__global__ void __launch_bounds__(256) kb_job_entries(const BatchHdr *__restrict__ H,
+                                                      const JobDesc *__restrict__ jobs,
+                                                      unsigned long long *__restrict__ jent) {
+    for (uint32_t j = threadIdx.x; j < H->njobs; j += blockDim.x)
+        jent[j] = H->off_all[jobs[j].grp_base + jobs[j].g.ngroups] - H->off_all[jobs[j].grp_base];
+}
+
 __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobDesc *__restrict__ jobs) {
     if (H->pool_overflow) return;  // entries incomplete: this pass is replayed after the pool grows
     for (;;) {
@@ -159,6 +175,7 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
         if (it >= H->tot_acc) return;
         int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.acc_base; });
         const JobDesc &J = jobs[j];
+        if (J.skip) continue;
         unsigned long long local = it - J.acc_base;
         uint64_t tile = local / J.nslices;
         uint32_t c0 = (uint32_t)(local % J.nslices) * kSlice;
@@ -170,7 +187,6 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
 // Tensor-core channel sums: one CTA per SM takes (job, channel block, tile)
 // items from the queue; barrier phases and TMEM persist across items.
 using KbTcCfg = TcCfgN4K32;  // the batch kernel's pipeline shape
-constexpr int kKbTcConfig = 0;
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     kb_tc(BatchHdr *H, const JobDesc *__restrict__ jobs, const void *zero_page, unsigned long long *timeouts,
@@ -185,6 +201,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const unsigned long long it = S.item;
         if (it >= H->tot_tc) break;
         const int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.tc_base; });
+        if (jobs[j].skip) {
+            __syncthreads();  // every thread has read S.item
+            continue;
+        }
         const TcJob &J = jobs[j].tc;
         const unsigned long long local = it - jobs[j].tc_base;
         const uint64_t ntiles = (uint64_t)J.T.ntx * J.T.nty;
@@ -212,6 +232,16 @@ __global__ void __launch_bounds__(256) kb_1chan(BatchHdr *H, const JobDesc *__re
 
 static bool batch_uses_tc(const hcg_field *f) { return auto_engine(f) != HCG_ENGINE_FP32; }
 
+// HCG_BATCH_TRACE=1 prints one line per batch pass on stderr (sizes, entry
+// pool, fallbacks, device time).
+bool batch_trace() {
+    static const bool on = [] {
+        const char *v = getenv("HCG_BATCH_TRACE");
+        return v && *v && *v != '0';
+    }();
+    return on;
+}
+
 // Batch state kept by a context: device header + job table, scratch and the
 // captured graph.
 struct BatchState {
@@ -220,12 +250,13 @@ struct BatchState {
     JobDesc *d_jobs = nullptr;
     JobDesc *h_jobs = nullptr;  // pinned
     uint32_t job_cap = 0;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec_geom = nullptr, exec_sums = nullptr;
     int nsm = 0;
     void *scratch[11] = {};
     size_t scratch_size[11] = {};
     CUtensorMap *d_maps = nullptr, *h_maps = nullptr;  // two per job: spectra (hi and lo halves), cube
     unsigned long long *d_jovf = nullptr, *h_jovf = nullptr;  // per job: tiles beyond the ring table
+    unsigned long long *d_jent = nullptr, *h_jent = nullptr;  // per job: entries
     uint32_t map_cap = 0;
     void *zero_page = nullptr;  // the tensor-core engine's zero page
     unsigned long long entry_cap = 0;
@@ -253,33 +284,41 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     cudaError_t e = cudaFuncSetAttribute(kb_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     if ((e = tc_set_smem((const void *)kb_tc, KbTcCfg::kSmem)) != cudaSuccess) return e;
-    cudaGraph_t graph;
-    if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-    cudaMemsetAsync(&B.d_hdr->head[0], 0, sizeof(B.d_hdr->head), s);
-    cudaMemsetAsync(&B.d_hdr->pool_overflow, 0, sizeof(unsigned long long), s);
     const int n = B.nsm;
-    kb_prep<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs, ctx->d_stats);
-    kb_tile_rings<<<n * 4, 256, 0, s>>>(B.d_hdr, B.d_jobs);
-    kb_group<true><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
-    kb_scan_sums<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
-    kb_scan_psum<<<1, kScanThreads, 0, s>>>(B.d_hdr);
-    kb_scan_apply<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
-    kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
-    kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
-    kb_tc<<<n, kTcThreads, KbTcCfg::kSmem, s>>>(B.d_hdr, B.d_jobs, B.zero_page, &ctx->d_stats->timeouts,
-                                          &ctx->d_stats->tc_macs);
-    kb_1chan<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
-    cudaError_t ce = cudaStreamEndCapture(s, &graph);
-    if (ce != cudaSuccess) return ce;
-    e = cudaGraphInstantiate(&B.exec, graph, 0);
-    cudaGraphDestroy(graph);
-    return e;
+    for (int part = 0; part < 2; ++part) {
+        cudaGraph_t graph;
+        if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+        cudaMemsetAsync(&B.d_hdr->head[0], 0, sizeof(B.d_hdr->head), s);
+        cudaMemsetAsync(&B.d_hdr->pool_overflow, 0, sizeof(unsigned long long), s);
+        if (part == 0) {
+            kb_prep<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs, ctx->d_stats);
+            kb_tile_rings<<<n * 4, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+            kb_group<true><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+            kb_scan_sums<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
+            kb_scan_psum<<<1, kScanThreads, 0, s>>>(B.d_hdr);
+            kb_scan_apply<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
+            kb_job_entries<<<1, 256, 0, s>>>(B.d_hdr, B.d_jobs, B.d_jent);
+        } else {
+            kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+            kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
+            kb_tc<<<n, kTcThreads, KbTcCfg::kSmem, s>>>(B.d_hdr, B.d_jobs, B.zero_page, &ctx->d_stats->timeouts,
+                                                  &ctx->d_stats->tc_macs);
+            kb_1chan<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
+        }
+        cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        if (ce != cudaSuccess) return ce;
+        e = cudaGraphInstantiate(part == 0 ? &B.exec_geom : &B.exec_sums, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t batch_release(hcg_context *ctx) {
     BatchState *B = (BatchState *)ctx->batch;
     if (!B) return cudaSuccess;
-    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->exec_geom) cudaGraphExecDestroy(B->exec_geom);
+    if (B->exec_sums) cudaGraphExecDestroy(B->exec_sums);
     for (auto &p : B->scratch)
         if (p) cudaFreeAsync(p, ctx->stream);
     if (B->d_hdr) cudaFreeAsync(B->d_hdr, ctx->stream);
@@ -289,6 +328,8 @@ cudaError_t batch_release(hcg_context *ctx) {
     if (B->h_maps) cudaFreeHost(B->h_maps);
     if (B->d_jovf) cudaFreeAsync(B->d_jovf, ctx->stream);
     if (B->h_jovf) cudaFreeHost(B->h_jovf);
+    if (B->d_jent) cudaFreeAsync(B->d_jent, ctx->stream);
+    if (B->h_jent) cudaFreeHost(B->h_jent);
     if (B->h_hdr) cudaFreeHost(B->h_hdr);
     if (B->h_jobs) cudaFreeHost(B->h_jobs);
     delete B;
@@ -323,11 +364,15 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if (B.h_jobs) cudaFreeHost(B.h_jobs);
         if (B.d_jovf) cudaFreeAsync(B.d_jovf, s);
         if (B.h_jovf) cudaFreeHost(B.h_jovf);
+        if (B.d_jent) cudaFreeAsync(B.d_jent, s);
+        if (B.h_jent) cudaFreeHost(B.h_jent);
         B.job_cap = std::max<uint32_t>(njobs, 64);
         if ((e = cudaMallocAsync(&B.d_jobs, B.job_cap * sizeof(JobDesc), s)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jobs, B.job_cap * sizeof(JobDesc))) != cudaSuccess) return e;
         if ((e = cudaMallocAsync(&B.d_jovf, B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jovf, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
+        if ((e = cudaMallocAsync(&B.d_jent, B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&B.h_jent, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
     }
     if (2 * njobs > B.map_cap) {
         if (B.d_maps) cudaFreeAsync(B.d_maps, s);
@@ -388,26 +433,36 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         (e = grow(B, 8, (tile + 1) * kTileMaxSpan * sizeof(uint16_t), s, &p_ridx)) != cudaSuccess ||
         (e = grow(B, 9, (kBatchScanParts + 1) * sizeof(unsigned long long), s, &p_scan)) != cudaSuccess)
         return e;
-    // per-group windows kept by the tile pass for the weight pass (up to 4 GiB of them)
+    // Per-group windows kept by the tile pass for the weight pass: up to
+    // 4 GiB of them, given to the jobs in order while they fit.
+    const size_t win_tile = (size_t)kWinSpan * kTileGroups * 2 * sizeof(uint4);
+    const size_t wbytes = std::min<size_t>((size_t)(tile + 1) * win_tile, 4ull << 30);
     void *p_win = nullptr;
-    const size_t wbytes = (size_t)(tile + 1) * kWinSpan * kTileGroups * 2 * sizeof(uint4);
-    if (wbytes <= (4ull << 30) && grow(B, 10, wbytes, s, &p_win) != cudaSuccess) {
+    if (grow(B, 10, wbytes, s, &p_win) != cudaSuccess) {
         cudaGetLastError();
         p_win = nullptr;
     }
-    if (B.entry_cap == 0) B.entry_cap = 1ULL << 24;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        void *p_eidx, *p_ew;
-        if ((e = grow(B, 6, (B.entry_cap + 1) * sizeof(uint32_t), s, &p_eidx)) != cudaSuccess ||
-            (e = grow(B, 7, (B.entry_cap + 1) * sizeof(float4), s, &p_ew)) != cudaSuccess) {
-            why = "entry pool of " + std::to_string(B.entry_cap) + " entries";
-            return e;
+    const unsigned long long win_tiles = p_win ? wbytes / win_tile : 0;
+    if (B.entry_cap == 0) B.entry_cap = 1ULL << 20;
+    void *p_eidx = nullptr, *p_ew = nullptr;
+    auto pool = [&](unsigned long long cap) -> cudaError_t {
+        cudaError_t pe;
+        if ((pe = grow(B, 6, (cap + 1) * sizeof(uint32_t), s, &p_eidx)) != cudaSuccess ||
+            (pe = grow(B, 7, (cap + 1) * sizeof(float4), s, &p_ew)) != cudaSuccess) {
+            why = "entry pool of " + std::to_string(cap) + " entries";
+            return pe;
         }
-        int *t_r0 = (int *)p_tiles;
-        int *t_nr = t_r0 + (tile + 1);
-        uint32_t *t_U = (uint32_t *)(t_nr + (tile + 1));
-        uint32_t *t_ulo = t_U + (tile + 1);
-        uint32_t *t_base = t_ulo + (tile + 1) * kTileMaxRings;
+        B.entry_cap = cap;
+        return cudaSuccess;
+    };
+    if ((e = pool(B.entry_cap)) != cudaSuccess) return e;
+    int *t_r0 = (int *)p_tiles;
+    int *t_nr = t_r0 + (tile + 1);
+    uint32_t *t_U = (uint32_t *)(t_nr + (tile + 1));
+    uint32_t *t_ulo = t_U + (tile + 1);
+    uint32_t *t_base = t_ulo + (tile + 1) * kTileMaxRings;
+    // job table and header, with the current entry pool
+    auto fill = [&]() {
         for (uint32_t i = 0; i < njobs; ++i) {
             const hcg_field *f = jobs[i].field;
             const hcg_target *t = jobs[i].target;
@@ -426,7 +481,10 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             d.T.base = t_base + d.tile_base * (kTileMaxRings + 1);
             d.T.ring_idx = (uint16_t *)p_ridx + d.tile_base * kTileMaxSpan;
             d.T.cap = d.cap;  // the tile pass counts each group's candidates
-            d.T.win = p_win ? (uint4 *)p_win + d.tile_base * kWinSpan * kTileGroups * 2 : nullptr;
+            const uint64_t ntiles = (f->nchan > 1) ? (uint64_t)d.T.ntx * d.T.nty : 0;
+            d.T.win = (p_win && d.tile_base + ntiles <= win_tiles)
+                          ? (uint4 *)p_win + d.tile_base * kWinSpan * kTileGroups * 2
+                          : nullptr;
             d.T.overflow = B.d_jovf + i;
             d.X = t->d_x;
             d.Y = t->d_y;
@@ -473,86 +531,103 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         h.off_all = (unsigned long long *)p_off;
         h.cap_all = (uint32_t *)p_cap;
         h.scan_part = (unsigned long long *)p_scan;
-        if ((e = cudaMemcpyAsync(B.d_jobs, B.h_jobs, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, s)) !=
-                cudaSuccess ||
-            (e = cudaMemcpyAsync(B.d_hdr, B.h_hdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(&ctx->d_stats->overflow, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(B.d_jovf, 0, njobs * sizeof(unsigned long long), s)) != cudaSuccess)
-            return e;
-        if (tcn && (e = cudaMemcpyAsync(B.d_maps, B.h_maps, 2 * njobs * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
-                                        s)) != cudaSuccess)
-            return e;
-        if (!B.exec && (e = capture(ctx, B)) != cudaSuccess) return e;
-        cudaEventRecord(ctx->ev0, s);
-        for (auto &ev : ctx->evp) cudaEventRecord(ev, s);  // one graph: phases are not separated
-        if ((e = cudaGraphLaunch(B.exec, s)) != cudaSuccess) return e;
-        cudaEventRecord(ctx->ev1, s);
-        if ((e = cudaMemcpyAsync(B.h_hdr, B.d_hdr, sizeof(BatchHdr), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-            return e;
-        unsigned long long timeouts = 0;
-        if ((e = cudaMemcpyAsync(&timeouts, &ctx->d_stats->timeouts, sizeof timeouts, cudaMemcpyDeviceToHost,
-                                 s)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(B.h_jovf, B.d_jovf, njobs * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                 s)) != cudaSuccess)
-            return e;
-        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-        if (timeouts) {
-            why = std::to_string(timeouts) + " tensor-core pipeline waits ran out";
-            return cudaErrorTimeout;
+    };
+    fill();
+    if ((e = cudaMemcpyAsync(B.d_jobs, B.h_jobs, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(B.d_hdr, B.h_hdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(&ctx->d_stats->overflow, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(B.d_jovf, 0, njobs * sizeof(unsigned long long), s)) != cudaSuccess)
+        return e;
+    if (tcn && (e = cudaMemcpyAsync(B.d_maps, B.h_maps, 2 * njobs * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                                    s)) != cudaSuccess)
+        return e;
+    if (!B.exec_geom && (e = capture(ctx, B)) != cudaSuccess) return e;
+    // geometry graph, then the entry totals of every job
+    cudaEventRecord(ctx->ev0, s);
+    if ((e = cudaGraphLaunch(B.exec_geom, s)) != cudaSuccess) return e;
+    cudaEventRecord(ctx->evp[0], s);
+    if ((e = cudaMemcpyAsync(B.h_jent, B.d_jent, njobs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(B.h_jovf, B.d_jovf, njobs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess)
+        return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    // Routing: jobs whose tiles overflowed the ring table, then the jobs with
+    // the most entries until the rest fit the context's entry budget.
+    fallback.assign(njobs, 0);
+    unsigned long long total = 0;
+    uint32_t nrouted = 0;
+    for (uint32_t i = 0; i < njobs; ++i) {
+        if (B.h_jovf[i] && jobs[i].field->nchan > 1) {
+            fallback[i] = 1;
+            ++nrouted;
+        } else {
+            total += B.h_jent[i];
         }
-        // a job with a tile spanning more rings than its table wrote sample
-        // indices for that tile's groups: it is re-run on its own
-        fallback.assign(njobs, 0);
-        for (uint32_t i = 0; i < njobs; ++i)
-            if (B.h_jovf[i] && jobs[i].field->nchan > 1) fallback[i] = 1;
-        if (B.h_hdr->pool_overflow == 0) return cudaSuccess;
-        const unsigned long long need = B.h_hdr->entries_needed + (B.h_hdr->entries_needed >> 3) + 1024;
-        const unsigned long long max_pool = ctx->entry_budget / (sizeof(uint32_t) + sizeof(float4));
-        if (need <= max_pool) {
-            B.entry_cap = need;  // grow and replay once
-            continue;
-        }
-        // The batch's entries exceed the context's entry budget: the jobs with
-        // the most entries go to the single-job path (which runs them in
-        // budget-sized passes) and the others are batched again.
-        std::vector<unsigned long long> lo(njobs), hi(njobs);
-        for (uint32_t i = 0; i < njobs; ++i) {
-            const unsigned long long *o = (const unsigned long long *)p_off;
-            if ((e = cudaMemcpyAsync(&lo[i], o + J[i].grp_base, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                     s)) != cudaSuccess ||
-                (e = cudaMemcpyAsync(&hi[i], o + J[i].grp_base + J[i].g.ngroups, sizeof(unsigned long long),
-                                     cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-                return e;
-        }
-        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-        std::vector<uint32_t> order(njobs);
-        for (uint32_t i = 0; i < njobs; ++i) order[i] = i;
-        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return hi[a] - lo[a] > hi[b] - lo[b]; });
-        unsigned long long total = B.h_hdr->entries_needed;
-        std::vector<char> out(njobs, 0);
-        for (uint32_t k = 0; k < njobs && total + (total >> 3) + 1024 > max_pool; ++k) {
-            out[order[k]] = 1;
-            total -= hi[order[k]] - lo[order[k]];
-        }
-        std::vector<hcg_job> rest;
-        std::vector<uint32_t> rest_idx;
-        for (uint32_t i = 0; i < njobs; ++i)
-            if (!out[i]) {
-                rest.push_back(jobs[i]);
-                rest_idx.push_back(i);
-            }
-        std::vector<char> sub_fallback;
-        if (!rest.empty()) {
-            B.entry_cap = total + (total >> 3) + 1024;
-            if ((e = grid_batch(ctx, (uint32_t)rest.size(), rest.data(), sub_fallback, why)) != cudaSuccess) return e;
-        }
-        fallback = out;
-        for (size_t k = 0; k < rest_idx.size(); ++k)
-            if (sub_fallback[k]) fallback[rest_idx[k]] = 1;
-        return cudaSuccess;
     }
-    why = "entry pool still too small after growing";
-    return cudaErrorMemoryAllocation;
+    const unsigned long long max_pool = ctx->entry_budget / (sizeof(uint32_t) + sizeof(float4));
+    auto with_slack = [](unsigned long long x) { return x + (x >> 4) + 1024; };
+    if (with_slack(total) > max_pool) {
+        std::vector<uint32_t> order;
+        for (uint32_t i = 0; i < njobs; ++i)
+            if (!fallback[i]) order.push_back(i);
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return B.h_jent[a] > B.h_jent[b]; });
+        for (uint32_t k = 0; k < order.size() && with_slack(total) > max_pool; ++k) {
+            fallback[order[k]] = 1;
+            total -= B.h_jent[order[k]];
+            ++nrouted;
+        }
+    }
+    if (with_slack(total) > B.entry_cap && (e = pool(with_slack(total))) != cudaSuccess) return e;
+    for (uint32_t i = 0; i < njobs; ++i) J[i].skip = fallback[i];
+    fill();
+    if (nrouted) {
+        // routed jobs hold no entries: their offsets are taken out of the scan
+        for (uint32_t i = 0; i < njobs; ++i)
+            if (fallback[i] && J[i].g.ngroups &&
+                (e = cudaMemsetAsync(J[i].cap, 0, J[i].g.ngroups * sizeof(uint32_t), s)) != cudaSuccess)
+                return e;
+    }
+    if ((e = cudaMemcpyAsync(B.d_jobs, B.h_jobs, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(B.d_hdr, B.h_hdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return e;
+    if (nrouted) {
+        kb_scan_sums<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
+        kb_scan_psum<<<1, kScanThreads, 0, s>>>(B.d_hdr);
+        kb_scan_apply<<<kBatchScanParts, kScanThreads, 0, s>>>(B.d_hdr);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    cudaEventRecord(ctx->evp[1], s);
+    cudaEventRecord(ctx->evp[2], s);
+    if ((e = cudaGraphLaunch(B.exec_sums, s)) != cudaSuccess) return e;
+    cudaEventRecord(ctx->ev1, s);
+    if ((e = cudaMemcpyAsync(B.h_hdr, B.d_hdr, sizeof(BatchHdr), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return e;
+    unsigned long long timeouts = 0;
+    if ((e = cudaMemcpyAsync(&timeouts, &ctx->d_stats->timeouts, sizeof timeouts, cudaMemcpyDeviceToHost, s)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    if (batch_trace()) {
+        float mg = 0.f, ms = 0.f;
+        cudaEventElapsedTime(&mg, ctx->ev0, ctx->evp[0]);
+        cudaEventElapsedTime(&ms, ctx->evp[2], ctx->ev1);
+        fprintf(stderr,
+                "[hcg batch] jobs %u pixels %llu tiles %llu (windows kept for %llu) tc-items %llu entries %llu "
+                "pool %llu routed %u geometry %.3f ms sums %.3f ms\n",
+                njobs, pix, tile, win_tiles, tcn, total, B.entry_cap, nrouted, mg, ms);
+    }
+    if (timeouts) {
+        why = std::to_string(timeouts) + " tensor-core pipeline waits ran out";
+        return cudaErrorTimeout;
+    }
+    if (B.h_hdr->pool_overflow) {  // the pool was sized from the same counts: not expected
+        why = "entry pool smaller than the counted entries";
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace hcg

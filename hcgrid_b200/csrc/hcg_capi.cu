@@ -615,6 +615,12 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
         e = grid_field(ctx, jobs[i].field, jobs[i].target, jobs[i].cube, jobs[i].layout, jobs[i].weights,
                        auto_engine(jobs[i].field), why);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch fallback", why);
+        if (batch_trace()) {
+            float ms = 0.f;
+            cudaStreamSynchronize(ctx->stream);
+            cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            fprintf(stderr, "[hcg batch] job %u on its own: %.3f ms\n", i, ms);
+        }
     }
     CK(ctx, cudaStreamSynchronize(ctx->stream), "grid batch");
     return HCG_OK;

@@ -229,6 +229,9 @@ __global__ void k_ring_table(HpxParams h, uint64_t firstring, uint64_t usedrings
         R.t2 = ddiv(dmul(ns, s), dsqrt(ddiv(dadd(1., za), 3.)));
     R.lut_lo = lut[k];
     R.lut_hi = lut[k + 1];
+    R.phi0 = phi;
+    R.dphi = 0.0;  // set by k_ring_phi
+    R.cbmin = 1.0;
     // pixel range of the ring's samples; the table offsets are set on the host
     R.pmin = 0;
     R.span = 0;
@@ -238,6 +241,40 @@ __global__ void k_ring_table(HpxParams h, uint64_t firstring, uint64_t usedrings
         R.span = (uint32_t)(keys[R.lut_hi - 1] - keys[R.lut_lo] + 1);
     }
     rings[k] = R;
+}
+
+// Per ring: the largest |phi| distance of a sample from its pixel centre and
+// the smallest cos(lat) of its samples (block per ring).
+__global__ void __launch_bounds__(256) k_ring_phi(HpxParams h, RingRec *__restrict__ rings,
+                                                  const uint64_t *__restrict__ keys, const double *__restrict__ l2,
+                                                  const double *__restrict__ cb2) {
+    __shared__ double s_d[8], s_c[8];
+    const uint32_t lo = rings[blockIdx.x].lut_lo, hi = rings[blockIdx.x].lut_hi;
+    double dmax = 0.0, cmin = 1.0;
+    for (uint32_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        double z, phi, sth;
+        bool have;
+        pix2loc(h, keys[j], z, phi, sth, have);
+        dmax = fmax(dmax, fabs(remainder(l2[j] - phi, 2.0 * kPi)));
+        cmin = fmin(cmin, cb2[j]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+        cmin = fmin(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_d[threadIdx.x >> 5] = dmax;
+        s_c[threadIdx.x >> 5] = cmin;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            dmax = fmax(dmax, s_d[w]);
+            cmin = fmin(cmin, s_c[w]);
+        }
+        rings[blockIdx.x].dphi = dmax;
+        rings[blockIdx.x].cbmin = cmin;
+    }
 }
 
 // Per-ring pixel tables: entry q of ring k is the first sorted sample of the
@@ -410,6 +447,8 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
     TRY(cudaMallocAsync(&f->d_w, n * sizeof(double), s));
     k_permute_geometry<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, f->d_perm, d_lon, d_lat, d_w, f->d_l2, f->d_b2,
                                                                    f->d_cb2, f->d_w, f->d_half);
+    TRY(cudaGetLastError());
+    k_ring_phi<<<(unsigned)f->usedrings, 256, 0, s>>>(f->hpx, f->d_rings, f->d_keys, f->d_l2, f->d_cb2);
     TRY(cudaGetLastError());
 fail:
     if (k0) cudaFreeAsync(k0, s);

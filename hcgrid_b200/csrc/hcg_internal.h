@@ -42,6 +42,12 @@ struct RingRec {
     uint32_t pmin;
     uint32_t span;
     uint64_t tbl;
+    // Polar windows of the multi-channel path: phi of the first pixel centre,
+    // the largest |phi| distance of a sample of the ring from its pixel
+    // centre, and the smallest cos(lat) of the ring's samples.
+    double phi0;
+    double dphi;
+    double cbmin;
 };
 
 // One target pixel: its coordinates and the phi half of loc2pix for the two
@@ -157,6 +163,7 @@ int sin_target_coords(const char *header, size_t len, uint32_t &nx, uint32_t &ny
 cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, std::vector<char> &fallback,
                        std::string &why);
 cudaError_t batch_release(hcg_context *ctx);
+bool batch_trace();
 struct SinWcs;
 int parse_sin_header(const char *header, size_t len, uint32_t &nx, uint32_t &ny, SinWcs &w, std::string &why);
 cudaError_t sin_coords_device(const SinWcs &w, uint32_t nx, uint32_t ny, double *d_x, double *d_y, cudaStream_t s);

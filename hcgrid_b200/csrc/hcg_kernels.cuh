@@ -96,6 +96,23 @@ __device__ __forceinline__ uint64_t edge_pix(const HpxParams &h, const RingRec &
     return R.zpos ? 2 * ir * (ir - 1) + ip : h.npix - 2 * ir * (ir + 1) + ip;
 }
 
+// Samples [lo, hi) of ring R whose pixels lie in [lpix, rpix].
+__device__ __forceinline__ void pixel_window(const RingRec &R, uint64_t lpix, uint64_t rpix,
+                                             const uint64_t *__restrict__ keys, const uint32_t *__restrict__ ptab,
+                                             uint32_t &lo, uint32_t &hi) {
+    if (R.span) {
+        // the ring's pixel table gives the same bounds as the searches below
+        const int64_t q0 = (int64_t)(lpix - R.startpix) - (int64_t)R.pmin;
+        lo = q0 <= 0 ? R.lut_lo : (q0 >= (int64_t)R.span ? R.lut_hi : __ldg(ptab + R.tbl + q0));
+        const int64_t q1 = (int64_t)(rpix - R.startpix) - (int64_t)R.pmin + 1;  // first pixel > rpix
+        const uint32_t h1 = q1 <= 0 ? R.lut_lo : (q1 >= (int64_t)R.span ? R.lut_hi : __ldg(ptab + R.tbl + q1));
+        hi = h1 > lo ? h1 : lo;
+        return;
+    }
+    lo = lower_bound_u64(keys, R.lut_lo, R.lut_hi, lpix);
+    hi = upper_bound_u64(keys, lo, R.lut_hi, rpix);
+}
+
 // Candidate interval [lo, hi) of one ring for one pixel
 // (gridding.cu:329-367). Returns false where the reference would spin.
 __device__ __forceinline__ bool ring_window(const HpxParams &h, const RingRec &R, const PixPrep &P,
@@ -107,17 +124,7 @@ __device__ __forceinline__ bool ring_window(const HpxParams &h, const RingRec &R
     uint64_t rpix = P.polar ? R.startpix + R.npr - 1 : edge_pix(h, R, P, 1);
     if (!(rpix >= R.startpix && rpix < R.startpix + R.npr)) return false;
     if (R.lut_lo == 0) return true;  // first used ring: the reference's search returns "none"
-    if (R.span) {
-        // the ring's pixel table gives the same bounds as the searches below
-        const int64_t q0 = (int64_t)(lpix - R.startpix) - (int64_t)R.pmin;
-        lo = q0 <= 0 ? R.lut_lo : (q0 >= (int64_t)R.span ? R.lut_hi : __ldg(ptab + R.tbl + q0));
-        const int64_t q1 = (int64_t)(rpix - R.startpix) - (int64_t)R.pmin + 1;  // first pixel > rpix
-        const uint32_t h1 = q1 <= 0 ? R.lut_lo : (q1 >= (int64_t)R.span ? R.lut_hi : __ldg(ptab + R.tbl + q1));
-        hi = h1 > lo ? h1 : lo;
-        return true;
-    }
-    lo = lower_bound_u64(keys, R.lut_lo, R.lut_hi, lpix);
-    hi = upper_bound_u64(keys, lo, R.lut_hi, rpix);
+    pixel_window(R, lpix, rpix, keys, ptab, lo, hi);
     return true;
 }
 
@@ -181,6 +188,7 @@ struct GridArgs {
     const uint32_t *ptab; // per-ring pixel tables (RingRec::tbl)
     double hlo, hhi;      // haversine thresholds bracketing sphere_radius (see pair_weight)
     int series;           // d^2 from the arcsine-squared series (small sphere_radius)
+    double hpolar;        // haversine bound of every accepted pair (polar windows)
 };
 
 // Host: GridArgs of a field. The cutoff d < r (d = 2 asin(sqrt(h)) in degrees,
@@ -196,7 +204,41 @@ inline GridArgs grid_args(const hcg_field *f, const PixPrep *prep, DevStats *sta
     a.hlo = hstar * (1.0 - 1e-9);
     a.hhi = hstar * (1.0 + 1e-9);
     a.series = hstar < 1e-3;
+    a.hpolar = hstar * (1.0 + 1e-6);
     return a;
+}
+
+// Candidate interval of the multi-channel path. Where the reference takes a
+// whole ring (pixels within 20 deg of a pole, gridding.cu:340-354) the
+// interval holds the ring's pixels whose centres lie within W in phi of the
+// pixel, which contain every sample of the ring within the radius: an
+// accepted pair has hav(d) < hpolar, so hav(dphi) < hpolar / (cos b_s cos b_p)
+// with cos b_s >= the ring's smallest cos(lat), and a sample lies within
+// R.dphi of its pixel centre. The accepted pairs are the whole ring's; only
+// candidates beyond the radius are left out. Wrapping windows keep the whole ring.
+__device__ __forceinline__ bool ring_window_mc(const GridArgs &a, const RingRec &R, const PixPrep &P, uint32_t &lo,
+                                               uint32_t &hi) {
+    if (!P.polar || R.lut_lo == 0) return ring_window(a.h, R, P, a.keys, a.ptab, lo, hi);
+    uint64_t lpix = R.startpix, rpix = R.startpix + R.npr - 1;
+    const double H = a.hpolar / (R.cbmin * P.cb1);
+    if (H < 1.0) {
+        const double W = 2.0 * asin(sqrt(H)) * (1.0 + 1e-9) + R.dphi + 1e-9;
+        const double dp = 2.0 * kPi / (double)R.npr;
+        const double lp = P.l1 - 2.0 * kPi * floor(P.l1 / (2.0 * kPi));
+        const double jl = floor((lp - W - R.phi0) / dp), jh = ceil((lp + W - R.phi0) / dp);
+        if (jl >= 0.0 && jh < (double)R.npr && jh - jl + 1.0 < (double)R.npr) {
+            lpix = R.startpix + (uint64_t)jl;
+            rpix = R.startpix + (uint64_t)jh;
+        }
+    }
+    pixel_window(R, lpix, rpix, a.keys, a.ptab, lo, hi);
+    return true;
+}
+
+// Candidates the reference visits on ring R for a pixel of the multi-channel
+// path that ring_window_mc narrowed (whole polar rings), beyond [lo, hi).
+__device__ __forceinline__ uint32_t polar_extra(const RingRec &R, uint32_t lo, uint32_t hi) {
+    return R.lut_lo == 0 ? 0u : (R.lut_hi - R.lut_lo) - (hi - lo);
 }
 
 // 32-byte read-only load (no double4 overload of __ldg)
@@ -223,6 +265,7 @@ __device__ __forceinline__ PixHalf pix_half(const PixPrep &P) {
 // pairs from asin^2(x) = sum_n (2x)^(2n) / (2 n^2 C(2n, n)) at x = sqrt(h)
 // (five terms; used when h* < 1e-3, truncation below 1e-16 relative), else
 // from asin itself. Pairs inside the threshold band take the full formula.
+template <bool F32EXP = false>
 __device__ __forceinline__ double pair_weight_s(const GridArgs &a, const PixPrep &P, const PixHalf &q,
                                                 const double4 &s, double cb2, double win, uint32_t idx) {
     const double sb = q.sb * s.w - q.cb * s.z;  // sin((b1 - b2) / 2)
@@ -243,6 +286,11 @@ __device__ __forceinline__ double pair_weight_s(const GridArgs &a, const PixPrep
         if (!(d < a.sphere_radius)) return 0.0;
         d2 = d * d;
     }
+    // Multi-channel entries hold FP32 weights: the Gaussian is evaluated in
+    // FP32 there, from the FP64 argument x = d^2 p0 rounded once (expf within
+    // 2 ulp: relative error below 2.4e-7 + 6e-8 x, 5e-7 at d = 3 sigma);
+    // distance and cutoff stay FP64.
+    if (F32EXP) return win * (double)expf((float)(-d2 * a.p0));
     return win * exp(-d2 * a.p0);
 }
 
@@ -380,11 +428,13 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
     }
     __syncwarp();
     int R0 = 1 << 30, R1 = -1;
+    bool polar = false;  // a pixel whose windows ring_window_mc narrowed
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         if (valid[q] && s_prep[q].nr > 0) {
             R0 = min(R0, s_prep[q].ur);
             R1 = max(R1, s_prep[q].ur + s_prep[q].nr - 1);
+            polar |= s_prep[q].polar != 0;
         }
     }
     unsigned lt = (1u << lane) - 1u;
@@ -436,7 +486,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
             for (int q = 0; q < 4; ++q) {
                 const PixPrep &P = s_prep[q];
                 if (valid[q] && k >= P.ur && k < P.ur + P.nr) {
-                    if (!ring_window(a.h, R, P, a.keys, a.ptab, lo[q], hi[q])) {
+                    if (!ring_window_mc(a, R, P, lo[q], hi[q])) {
                         ++skips;
                     } else if (hi[q] > lo[q]) {
                         glo = min(glo, lo[q]);
@@ -449,6 +499,14 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
         if (COUNT) {
             count += len;
             continue;
+        }
+        if (!COUNT && polar && k <= R1) {  // candidate statistic: the whole rings the reference visits
+            const RingRec &R = a.rings[k];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const PixPrep &P = s_prep[q];
+                if (valid[q] && P.polar && k >= P.ur && k < P.ur + P.nr) cand += polar_extra(R, lo[q], hi[q]);
+            }
         }
         uint32_t incl = len;
 #pragma unroll
@@ -479,7 +537,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if (idx >= s_lo[q] && idx < s_hi[q]) {
-                        const double wt = pair_weight_s(a, s_prep[q], s_half[q], hs, cb2, win, idx);
+                        const double wt = pair_weight_s<true>(a, s_prep[q], s_half[q], hs, cb2, win, idx);
                         ++cand;
                         if (wt > 0.0) {
                             ws[q] += wt;
@@ -749,7 +807,7 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
             const PixPrep &P = s_prep[p];
             if (P.nr > 0 && k >= P.ur && k < P.ur + P.nr) {
                 uint32_t lo, hi;
-                if (!ring_window(a.h, R, P, a.keys, a.ptab, lo, hi)) {
+                if (!ring_window_mc(a, R, P, lo, hi)) {
                     wlo[q] = 1;  // lo > hi: the reference would spin on this ring
                 } else {
                     wlo[q] = lo;
