@@ -18,6 +18,7 @@ GAUSS1D, GAUSS2D, TAPERED_SINC = 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
 SAMPLE_MAJOR, CHANNEL_MAJOR = 0, 1
 ENGINE_AUTO, ENGINE_FP32, ENGINE_TC_BF16, ENGINE_TC_F16 = 0, 1, 2, 3
+TC_WEIGHTS_AUTO, TC_WEIGHTS_ENTRIES, TC_WEIGHTS_DIRECT = 0, 1, 2
 
 STATUS = {0: "HCG_OK", 1: "HCG_EINVAL", 2: "HCG_ENOMEM", 3: "HCG_ETIMEOUT", 4: "HCG_EDEVICE", 5: "HCG_EIO",
           6: "HCG_EUNSUPPORTED", 7: "HCG_ESTATE"}
@@ -58,6 +59,7 @@ EXPORTS = {
     "hcg_field_set_spectra": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_field_split_spectra": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_tc_set_config": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_tc_set_weights": ([C.c_void_p, C.c_int], C.c_int),
     "hcg_autotune": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_sorted": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_destroy": ([C.c_void_p], C.c_int),
@@ -268,6 +270,12 @@ class Context:
 
     def tc_set_config(self, config: int, channel_class: int = -1):
         self._check(self.L.hcg_tc_set_config(self.h, channel_class, config))
+
+    def tc_set_weights(self, mode: int):
+        """How the tensor-core engines build weight operands: TC_WEIGHTS_AUTO,
+        TC_WEIGHTS_ENTRIES (FP64 weight pass) or TC_WEIGHTS_DIRECT (evaluated in
+        the kernel)."""
+        self._check(self.L.hcg_tc_set_weights(self.h, mode))
 
     def autotune(self, field: "Field", target: "Target", reps: int = 2):
         """Time each tensor-core pipeline shape on (field, target); keeps and

@@ -257,6 +257,7 @@ struct BatchState {
     CUtensorMap *d_maps = nullptr, *h_maps = nullptr;  // two per job: spectra (hi and lo halves), cube
     unsigned long long *d_jovf = nullptr, *h_jovf = nullptr;  // per job: tiles beyond the ring table
     unsigned long long *d_jent = nullptr, *h_jent = nullptr;  // per job: entries
+    unsigned long long *d_jusum = nullptr, *h_jusum = nullptr;  // per job: staged slots of its tiles (sum, largest)
     uint32_t map_cap = 0;
     void *zero_page = nullptr;  // the tensor-core engine's zero page
     unsigned long long entry_cap = 0;
@@ -330,6 +331,8 @@ cudaError_t batch_release(hcg_context *ctx) {
     if (B->h_jovf) cudaFreeHost(B->h_jovf);
     if (B->d_jent) cudaFreeAsync(B->d_jent, ctx->stream);
     if (B->h_jent) cudaFreeHost(B->h_jent);
+    if (B->d_jusum) cudaFreeAsync(B->d_jusum, ctx->stream);
+    if (B->h_jusum) cudaFreeHost(B->h_jusum);
     if (B->h_hdr) cudaFreeHost(B->h_hdr);
     if (B->h_jobs) cudaFreeHost(B->h_jobs);
     delete B;
@@ -366,6 +369,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if (B.h_jovf) cudaFreeHost(B.h_jovf);
         if (B.d_jent) cudaFreeAsync(B.d_jent, s);
         if (B.h_jent) cudaFreeHost(B.h_jent);
+        if (B.d_jusum) cudaFreeAsync(B.d_jusum, s);
+        if (B.h_jusum) cudaFreeHost(B.h_jusum);
         B.job_cap = std::max<uint32_t>(njobs, 64);
         if ((e = cudaMallocAsync(&B.d_jobs, B.job_cap * sizeof(JobDesc), s)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jobs, B.job_cap * sizeof(JobDesc))) != cudaSuccess) return e;
@@ -373,6 +378,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if ((e = cudaMallocHost(&B.h_jovf, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
         if ((e = cudaMallocAsync(&B.d_jent, B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jent, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
+        if ((e = cudaMallocAsync(&B.d_jusum, 2 * B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&B.h_jusum, 2 * B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
     }
     if (2 * njobs > B.map_cap) {
         if (B.d_maps) cudaFreeAsync(B.d_maps, s);
@@ -486,6 +493,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
                           ? (uint4 *)p_win + d.tile_base * kWinSpan * kTileGroups * 2
                           : nullptr;
             d.T.overflow = B.d_jovf + i;
+            d.T.ustat = B.d_jusum + 2 * i;
             d.X = t->d_x;
             d.Y = t->d_y;
             d.firstring = f->firstring;
@@ -537,7 +545,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
             cudaSuccess ||
         (e = cudaMemcpyAsync(B.d_hdr, B.h_hdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
         (e = cudaMemsetAsync(&ctx->d_stats->overflow, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess ||
-        (e = cudaMemsetAsync(B.d_jovf, 0, njobs * sizeof(unsigned long long), s)) != cudaSuccess)
+        (e = cudaMemsetAsync(B.d_jovf, 0, njobs * sizeof(unsigned long long), s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(B.d_jusum, 0, 2 * njobs * sizeof(unsigned long long), s)) != cudaSuccess)
         return e;
     if (tcn && (e = cudaMemcpyAsync(B.d_maps, B.h_maps, 2 * njobs * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
                                     s)) != cudaSuccess)
@@ -550,16 +559,23 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
     if ((e = cudaMemcpyAsync(B.h_jent, B.d_jent, njobs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) !=
             cudaSuccess ||
         (e = cudaMemcpyAsync(B.h_jovf, B.d_jovf, njobs * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s)) !=
-            cudaSuccess)
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(B.h_jusum, B.d_jusum, 2 * njobs * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             s)) != cudaSuccess)
         return e;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-    // Routing: jobs whose tiles overflowed the ring table, then the jobs with
-    // the most entries until the rest fit the context's entry budget.
+    // Routing: jobs whose tiles overflowed the ring table, tensor-core jobs
+    // with dense tiles (the single-job kernel evaluates their weights itself)
+    // or with tiles longer than one accumulation segment (the single-job
+    // kernels accumulate in segments), then the jobs with the most entries
+    // until the rest fit the context's entry budget.
     fallback.assign(njobs, 0);
     unsigned long long total = 0;
     uint32_t nrouted = 0;
     for (uint32_t i = 0; i < njobs; ++i) {
-        if (B.h_jovf[i] && jobs[i].field->nchan > 1) {
+        if ((B.h_jovf[i] && jobs[i].field->nchan > 1) ||
+            (J[i].tc.nb && (tc_use_weights(ctx, B.h_jusum[2 * i], B.h_jent[i]) ||
+                            B.h_jusum[2 * i + 1] > kTcOneSegmentSlots))) {
             fallback[i] = 1;
             ++nrouted;
         } else {

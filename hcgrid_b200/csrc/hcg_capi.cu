@@ -540,6 +540,15 @@ hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config) {
     return HCG_OK;
 }
 
+hcg_status hcg_tc_set_weights(hcg_context *ctx, int mode) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    if (mode < HCG_TC_WEIGHTS_AUTO || mode > HCG_TC_WEIGHTS_DIRECT)
+        return fail(ctx, HCG_EINVAL, "unknown tensor-core weight mode");
+    ctx->tc_weights = mode;
+    return HCG_OK;
+}
+
 hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, int *best,
                         float *ms) {
     if (!ctx || !field || !target || reps < 1) return HCG_EINVAL;

@@ -188,7 +188,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         T.base = (uint32_t *)ctx->scratch.get(12, ntiles * (kTileMaxRings + 1) * sizeof(uint32_t), s, e);
         T.ring_idx = (uint16_t *)ctx->scratch.get(14, ntiles * kTileMaxSpan * sizeof(uint16_t), s, e);
         unsigned long long *rowoff =
-            (unsigned long long *)ctx->scratch.get(13, (T.nty + 2) * sizeof(unsigned long long), s, e);
+            (unsigned long long *)ctx->scratch.get(13, (T.nty + 4) * sizeof(unsigned long long), s, e);
         const uint32_t parts = (uint32_t)std::min<uint64_t>(1024, (g.ngroups + 4095) / 4096 + 1);
         unsigned long long *psum =
             (unsigned long long *)ctx->scratch.get(15, (parts + 1) * sizeof(unsigned long long), s, e);
@@ -205,8 +205,10 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         }
         T.overflow = &ctx->d_stats->overflow;
         T.pad = tc ? 8 : 1;  // the tensor-core engine loads ring runs as boxes of 8 samples
+        T.ustat = ctx->d_stats->ustat;
         if (e != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(T.overflow, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(T.ustat, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
         k_tile_rings<<<(unsigned)ntiles, 256, 0, s>>>(a, g, T);
         TileArgs none{};
         // groups of tiles whose ring span exceeds the table (cap unknown) are counted here
@@ -219,10 +221,12 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         const uint64_t groups_per_row = (uint64_t)(kTileY / 2) * g.gx;
         k_row_offsets<<<(T.nty + 1 + 255) / 256, 256, 0, s>>>(off, g.ngroups, groups_per_row, T.nty, rowoff);
         if ((e = cudaMemcpyAsync(rowoff + T.nty + 1, T.overflow, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
-                                 s)) != cudaSuccess)
+                                 s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(rowoff + T.nty + 2, T.ustat, 2 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
             return e;
         cudaEventRecord(ctx->evp[1], s);
-        std::vector<unsigned long long> ro(T.nty + 2);
+        std::vector<unsigned long long> ro(T.nty + 4);
         if ((e = cudaMemcpyAsync(ro.data(), rowoff, ro.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                  s)) != cudaSuccess)
             return e;
@@ -232,6 +236,14 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             why = "a tile spans more than " + std::to_string(kTileMaxSpan) + " rings or holds samples in more than " +
                   std::to_string(kTileMaxRings) + ": the FP32 fallback needs the FP32 spectra";
             return cudaErrorInvalidValue;
+        }
+        const uint32_t ostride = layout == HCG_LAYOUT_CHANNEL_MAJOR ? 0 : f->nchan;  // 0: [channel][pixel]
+        if (tc && tiled && tc_use_weights(ctx, ro[T.nty + 2], ro[T.nty])) {
+            // dense tiles: the tensor-core kernel evaluates the weights itself (no entries)
+            cudaEventRecord(ctx->evp[2], s);
+            if ((e = tc_weights(ctx, f, a, g, T, ntiles, d_cube, ostride, d_wts, why)) != cudaSuccess) return e;
+            cudaEventRecord(ctx->ev1, s);
+            return cudaGetLastError();
         }
         const unsigned long long budget = ctx->entry_budget / (sizeof(uint32_t) + sizeof(float4));
         std::vector<std::pair<uint32_t, uint32_t>> chunks;
@@ -251,7 +263,6 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             return e;
         }
         float *dst = d_cube;
-        const uint32_t ostride = layout == HCG_LAYOUT_CHANNEL_MAJOR ? 0 : f->nchan;  // 0: [channel][pixel]
         const int smem = kStageSlots * kSlice * (int)sizeof(float);
         static bool attr_set = false;
         if (tiled && !attr_set) {
@@ -275,7 +286,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
                 TileArgs Tc = T;
                 Tc.t0 = (uint64_t)ch.first * T.ntx;
                 e = tc_accum(ctx, f, gc, Tc, (uint64_t)(ch.second - ch.first) * T.ntx, off, cnt, e_idx, e_w, wsum, dst,
-                             ostride, d_wts, why);
+                             ostride, d_wts, ro[T.nty + 3], why);
                 if (e != cudaSuccess) return e;
             } else if (tiled) {
                 TileArgs Tc = T;

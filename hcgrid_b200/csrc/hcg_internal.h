@@ -24,6 +24,7 @@ struct DevStats {
     unsigned long long overflow;
     unsigned long long timeouts;  // bounded device waits that ran out (tensor-core engine)
     unsigned long long tc_macs;   // tensor-core multiply-adds issued (tensor-core engine)
+    unsigned long long ustat[2];  // staged slots of all tiles and of the largest (tile pass)
 };
 
 // One HEALPix ring that holds samples, with the ring half of loc2pix
@@ -96,6 +97,7 @@ struct hcg_context {
     float last_ms = 0.f;
     unsigned long long entry_budget = 4ULL << 30;  // bytes of (sample, weights) entries per launch run
     int tc_config[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // tensor-core pipeline shape per channel class (-1: default)
+    int tc_weights = 0;  // tensor-core weight operands: 0 automatic, 1 from entries, 2 evaluated in the kernel
     void *batch = nullptr;                          // batch engine state (hcg_batch.cu)
 };
 
@@ -149,6 +151,16 @@ inline int tc_class_of(uint32_t cpad) {
 // (multi-channel fields with finite spectra), else the FP32 engine.
 inline int auto_engine(const hcg_field *f) {
     return (f->xfmt && f->nchan > 1 && f->xnonfinite == 0) ? f->xfmt : HCG_ENGINE_FP32;
+}
+// Tensor-core weight operand: evaluated in the kernel (HCG_TC_WEIGHTS_DIRECT)
+// or written as entries by the FP64 weight pass. Automatic mode takes the
+// entries: the kernel-side evaluation (four builder warps per SM) runs below
+// the weight pass's rate even on the densest tiles measured (usum: staged
+// slots of all tiles, cap_total: union candidates of all 2x2 groups).
+inline bool tc_use_weights(const hcg_context *ctx, unsigned long long usum, unsigned long long cap_total) {
+    (void)usum;
+    (void)cap_total;
+    return ctx->tc_weights == HCG_TC_WEIGHTS_DIRECT;
 }
 cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, const double *d_lat,
                         const double *d_w, std::string &why);

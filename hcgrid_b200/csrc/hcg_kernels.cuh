@@ -176,6 +176,9 @@ __device__ __forceinline__ void store_cube4(float *__restrict__ out, uint32_t os
     }
 }
 
+}  // namespace
+
+// Geometry arguments of the gathering kernels (shared by several translation units).
 struct GridArgs {
     HpxParams h;
     const RingRec *rings;
@@ -190,6 +193,8 @@ struct GridArgs {
     int series;           // d^2 from the arcsine-squared series (small sphere_radius)
     double hpolar;        // haversine bound of every accepted pair (polar windows)
 };
+
+namespace {
 
 // Host: GridArgs of a field. The cutoff d < r (d = 2 asin(sqrt(h)) in degrees,
 // helpers.cu:128-130) is decided from the haversine h alone when h is outside
@@ -387,13 +392,20 @@ struct TileArgs {
     uint4 *win;                // [tile][kWinSpan][kTileGroups][2]: the group's 4 pixel windows per ring (or null)
     unsigned long long *overflow;
     uint32_t pad;  // ring runs take a multiple of `pad` slots (> 1: the tensor-core engine's 8-row boxes)
+    unsigned long long *ustat;  // [0]: sum, [1]: largest of the tiles' staged slots U (or null)
 };
 
 // hcg_tc.cu: tensor-core accumulation of `ntiles` tiles from T.t0, after
 // k_group emitted the entries (slot mode) and the weight sums.
 cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, const TileArgs &T, uint64_t ntiles,
                      const unsigned long long *off, const uint32_t *cnt, const uint32_t *e_slot, const float4 *e_w,
-                     const double *wsum, float *out, uint32_t ostride, float *wout, std::string &why);
+                     const double *wsum, float *out, uint32_t ostride, float *wout, unsigned long long umax,
+                     std::string &why);
+// hcg_tc.cu: tensor-core accumulation of `ntiles` tiles whose weights the
+// kernel evaluates itself (dense tiles; no entries).
+cudaError_t tc_weights(hcg_context *ctx, const hcg_field *f, const GridArgs &a, const GroupArgs &g,
+                       const TileArgs &T, uint64_t ntiles, float *out, uint32_t ostride, float *wout,
+                       std::string &why);
 
 namespace {
 
@@ -865,6 +877,10 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
                 T.r0[tile] = r0;
                 T.nr[tile] = (int)count;
                 T.U[tile] = run;
+                if (T.ustat) {
+                    atomicAdd(T.ustat, (unsigned long long)run);
+                    atomicMax(T.ustat + 1, (unsigned long long)run);
+                }
             }
         }
     }
@@ -887,6 +903,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool va
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
     unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>

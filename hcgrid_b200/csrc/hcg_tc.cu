@@ -45,6 +45,17 @@ __global__ void __launch_bounds__(kTcPersistThreads, 1)
     tc_persist<Cfg>(S, J, nitems, ntiles, zero_page, timeouts, macs);
 }
 
+template <class Cfg>
+__global__ void __launch_bounds__(kTcPersistThreads, 1)
+    k_tile_tc_weights(const __grid_constant__ CUtensorMap tm, TcJob J, uint64_t nitems, uint64_t ntiles,
+                      unsigned long long *timeouts, unsigned long long *macs) {
+    __shared__ TcDShared S;
+    J.map = &tm;
+    J.out_map = nullptr;
+    if (threadIdx.x == 0) sm100::prefetch_tensormap(&tm);
+    tc_persist_weights<Cfg>(S, J, nitems, ntiles, timeouts, macs);
+}
+
 // ------------------------------------------------------------ spectra split
 // Per-channel largest magnitude and the count of non-finite values.
 __global__ void k_split_amax(const float *__restrict__ spec, uint64_t n, uint32_t nchan, uint32_t cstride,
@@ -310,9 +321,53 @@ cudaError_t launch_tc(hcg_context *ctx, const hcg_field *f, TcJob &J, const Tile
 }
 }  // namespace
 
+namespace {
+template <class Cfg>
+cudaError_t launch_tc_weights(hcg_context *ctx, const hcg_field *f, TcJob &J, const TileArgs &T, uint64_t ntiles,
+                              std::string &why) {
+    cudaStream_t s = ctx->stream;
+    CUtensorMap tm;
+    if (!tc_prepare_job(f, Cfg::kNb, &tm, J)) {
+        why = "cuTensorMapEncodeTiled";
+        return cudaErrorInvalidValue;
+    }
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set) {
+        cudaError_t e = tc_set_smem((const void *)k_tile_tc_weights<Cfg>, Cfg::kSmem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    J.T = T;
+    const uint64_t nitems = ntiles * J.ncb;
+    const unsigned grid = (unsigned)std::min<uint64_t>(nitems, (uint64_t)(nsm > 0 ? nsm : 148));
+    if (grid == 0) return cudaSuccess;
+    k_tile_tc_weights<Cfg><<<grid, kTcPersistThreads, Cfg::kSmem, s>>>(tm, J, nitems, ntiles,
+                                                                      &ctx->d_stats->timeouts, &ctx->d_stats->tc_macs);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t tc_weights(hcg_context *ctx, const hcg_field *f, const GridArgs &a, const GroupArgs &g,
+                       const TileArgs &T, uint64_t ntiles, float *out, uint32_t ostride, float *wout,
+                       std::string &why) {
+    TcJob J{};
+    J.a = a;
+    J.g = g;
+    J.out = out;
+    J.ostride = ostride;
+    J.wout = wout;
+    const uint32_t b = f->xcpad / 64;
+    if (b >= 4) return launch_tc_weights<TcCfgN4S2>(ctx, f, J, T, ntiles, why);
+    if (b >= 2) return launch_tc_weights<TcCfgN2S3>(ctx, f, J, T, ntiles, why);
+    return launch_tc_weights<TcCfgN1S4>(ctx, f, J, T, ntiles, why);
+}
+
 cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, const TileArgs &T, uint64_t ntiles,
                      const unsigned long long *off, const uint32_t *cnt, const uint32_t *e_slot, const float4 *e_w,
-                     const double *wsum, float *out, uint32_t ostride, float *wout, std::string &why) {
+                     const double *wsum, float *out, uint32_t ostride, float *wout, unsigned long long umax,
+                     std::string &why) {
     cudaStream_t s = ctx->stream;
     TcJob J{};
     cudaError_t e = cudaSuccess;
@@ -328,7 +383,11 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
     J.out = out;
     J.ostride = ostride;
     J.wout = wout;
-    switch (tc_pick(ctx, f)) {
+    int cfg = tc_pick(ctx, f);
+    // tiles longer than one accumulation segment take the persistent kernel,
+    // which accumulates in segments (the one-item kernel does not)
+    if (cfg < 4 && umax > kTcOneSegmentSlots) cfg = cfg == 3 ? 5 : 4;
+    switch (cfg) {
         case 0: return launch_tc<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
         case 1: return launch_tc<TcCfgN2S3>(ctx, f, J, T, ntiles, zero, why);
         case 2: return launch_tc<TcCfgN1S4>(ctx, f, J, T, ntiles, zero, why);

@@ -116,6 +116,7 @@ struct TcJob {
     uint32_t ostride;   // 0: [channel][pixel]; else [pixel][ostride]
     float *wout;
     const CUtensorMap *out_map;  // 3-D map of the cube (null: direct stores); box = one item
+    GridArgs a;                  // geometry of the direct-weight builders (tc_build_weights)
 };
 
 constexpr int kTcRing = 8;  // entries in flight per builder thread
@@ -322,6 +323,78 @@ __device__ __forceinline__ bool tc_mma(SH &S, const TcJob &J, uint32_t nchunks, 
     }
     if (acc) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)KC * nchunks);
     return ok;
+}
+
+// Accumulation segments of the persistent kernels: the tensor cores' FP32
+// accumulation drops low bits of the products it adds (the sums come out low
+// by up to ~2^-24 of the running sum per MMA), so long K loops drift. An
+// item's chunks are accumulated in segments of kTcSegChunks chunks (the last
+// one also takes a remainder of up to kTcSegChunks / 2 chunks), each in a
+// fresh accumulator (the two TMEM halves in turn), and the epilogue adds the
+// segments with round-to-nearest FP32 adds (in the cube buffer) before it
+// normalises them.
+constexpr uint32_t kTcSegChunks = 16;
+// The one-item kernels (k_tile_tc, the batch kernel) accumulate an item in one
+// segment: they take tiles of at most this many staged slots (longer ones go to
+// the persistent kernels).
+constexpr uint32_t kTcOneSegmentSlots = 1536;
+
+__host__ __device__ constexpr uint32_t tc_segments(uint32_t nchunks) {
+    return nchunks > kTcSegChunks + kTcSegChunks / 2 ? (nchunks + kTcSegChunks / 2 - 1) / kTcSegChunks : 1;
+}
+
+// MMA issue (one thread) of one item in segments; `gs` counts the CTA's
+// segments (accumulator gs & 1, barriers acc_full / acc_empty by parity).
+template <class Cfg, class SH>
+__device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchunks, uint32_t gk, uint32_t &gs,
+                                           unsigned long long *timeouts, unsigned long long *macs) {
+    using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
+    const TcStage<Cfg> st{tc_smem_base()};
+    const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
+    const uint32_t nseg = tc_segments(nchunks);
+    bool ok = true;
+    uint32_t k = 0, issued = 0;
+    for (uint32_t q = 0; q < nseg; ++q, ++gs) {
+        const uint32_t a = gs & 1;
+        if (ok && gs >= 2 && !mbar_wait(&S.acc_empty[a], ((gs >> 1) - 1) & 1, kTcWaitNs)) {
+            tc_give_up(S, timeouts);
+            ok = false;
+        }
+        tc_fence_after();
+        const uint32_t d_tmem = S.tmem + a * 256u;
+        const uint32_t kend = q + 1 == nseg ? nchunks : (q + 1) * kTcSegChunks;
+        uint32_t acc = 0;
+        for (; k < kend && ok && !S.abort; ++k) {
+            const uint32_t g = gk + k, s = g % ST, ph = (g / ST) & 1;
+            if (!mbar_wait(&S.full_a[s], ph, kTcWaitNs) || !mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
+                tc_give_up(S, timeouts);
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t ah = smem_u32(st.A_hi(s)), al = smem_u32(st.A_lo(s));
+            const uint32_t bh = smem_u32(st.B(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
+#pragma unroll
+            for (int kk = 0; kk < (int)(KC / 16); ++kk) {
+                const uint64_t adh = smem_desc(ah + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
+                const uint64_t adl = smem_desc(al + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
+                const uint64_t bdh = smem_desc(bh + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
+                const uint64_t bdl = smem_desc(bl + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
+                mma_f16_ss(d_tmem, adh, bdh, idesc, acc);
+                mma_f16_ss(d_tmem, adh, bdl, idesc, 1);
+                mma_f16_ss(d_tmem, adl, bdh, idesc, 1);
+                acc = 1;
+            }
+            mma_commit(&S.empty[s]);
+            ++issued;
+        }
+        if (acc)
+            mma_commit(&S.acc_full[a]);  // fires once this segment's MMAs have completed
+        else
+            mbar_arrive(&S.acc_full[a]);
+    }
+    if (issued) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)KC * issued);
 }
 
 // Builders (kTcBuilders threads, index bt), one item: the weights of the
@@ -554,22 +627,19 @@ struct TcPShared {
 // Epilogue warps (128 threads, index eb), one item from accumulator `a`:
 // normalise and store straight from registers (16-byte stores along channels
 // for [pixel][channel] cubes; along pixels for [channel][pixel] cubes).
-__device__ __forceinline__ void tc_epilogue_direct(TcPShared &S, const TcJob &J, uint64_t tile, uint32_t cblk,
-                                                   uint32_t nchunks, uint32_t il, int eb,
+template <class SH, bool WSMEM = false>
+__device__ __forceinline__ void tc_epilogue_direct(SH &S, const TcJob &J, uint64_t tile, uint32_t cblk,
+                                                   uint32_t nchunks, uint32_t il, uint32_t &gse, int eb,
                                                    unsigned long long *timeouts) {
     using namespace sm100;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t a = il & 1;
+    const uint32_t ia = il & 1;  // the item's scale buffer
     const TileArgs &T = J.T;
     const GroupArgs &G = J.g;
     const uint32_t c_item = cblk * J.nb * 64;
     const uint32_t ncols = 64 * J.nb;
     for (uint32_t c = eb; c < ncols; c += kTcBuilders)
-        S.inv_scale[a][c] = c_item + c < J.nchan ? J.inv_scale[c_item + c] : 0.f;
-    const bool ok = mbar_wait(&S.acc_full[a], (il >> 1) & 1, kTcWaitNs);
-    if (!ok) tc_give_up(S, timeouts);
-    tc_fence_after();
-    const bool store = !named_barrier_or(3, kTcBuilders, !ok || S.abort);  // scales staged, same decision
+        S.inv_scale[ia][c] = c_item + c < J.nchan ? J.inv_scale[c_item + c] : 0.f;
     const uint32_t q4 = warp & 3;  // TMEM lane quarter this warp may access
     const uint32_t m = q4 * 32 + lane;
     const uint32_t xx = (uint32_t)(tile % T.ntx) * kTileX + (m & (kTileX - 1));
@@ -577,43 +647,85 @@ __device__ __forceinline__ void tc_epilogue_direct(TcPShared &S, const TcJob &J,
     const bool valid = xx < G.nx && yy < G.ny;
     const uint64_t P = (uint64_t)G.nx * G.ny;
     const uint64_t p = (uint64_t)yy * G.nx + xx;
-    const double ws = valid ? J.wsum[p] : 0.0;
-    const float inv = (float)(1.0 / ws);
-    if (store && valid && cblk == 0 && J.wout) J.wout[p] = (float)ws;
-    const float *sc = S.inv_scale[a];
-    for (uint32_t cb = 0; cb < 2 * J.nb; ++cb) {
-        uint32_t r[32];
-        if (nchunks > 0) {
-            tmem_ld_32x32b_x32(S.tmem + a * 256u + ((q4 * 32u) << 16) + cb * 32u, r);
-            tmem_wait_ld();
-        } else {
-#pragma unroll
-            for (int i = 0; i < 32; ++i) r[i] = 0u;
+    const float *sc = S.inv_scale[ia];
+    const uint32_t nseg = tc_segments(nchunks);
+    bool store = false;
+    float inv = 0.f;
+    for (uint32_t q = 0; q < nseg; ++q, ++gse) {
+        const uint32_t a = gse & 1;
+        const bool ok = mbar_wait(&S.acc_full[a], (gse >> 1) & 1, kTcWaitNs);
+        if (!ok) tc_give_up(S, timeouts);
+        tc_fence_after();
+        if (q == 0) store = !named_barrier_or(3, kTcBuilders, !ok || S.abort);  // scales staged, same decision
+        // Segments before the last are added up unnormalised; the last one
+        // brings the weight sum (the builders' sums are complete once every
+        // chunk has been accumulated) and the sum is normalised.
+        const bool last = q + 1 == nseg;
+        if (last) {
+            double ws = 0.0;
+            if constexpr (WSMEM) {
+                // the builders' FP64 weight sums of this item (shared memory, by item parity)
+                if (!mbar_wait(&S.ws_full[ia], (il >> 1) & 1, kTcWaitNs)) tc_give_up(S, timeouts);
+                ws = S.wsum[ia][m];
+                mbar_arrive(&S.ws_empty[ia]);
+            } else {
+                ws = valid ? J.wsum[p] : 0.0;
+            }
+            inv = (float)(1.0 / ws);
+            if (store && valid && cblk == 0 && J.wout) J.wout[p] = (float)ws;
         }
-        if (!store || !valid) continue;
-        const uint32_t c0 = c_item + cb * 32;
-        float v[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) v[i] = (__uint_as_float(r[i]) * sc[cb * 32 + i]) * inv;
-        if (J.ostride == 0) {
-#pragma unroll
-            for (int i = 0; i < 32; ++i)
-                if (c0 + i < J.nchan) J.out[(uint64_t)(c0 + i) * P + p] = v[i];
-        } else {
-            float *dst = J.out + p * J.ostride + c0;
-            if ((J.ostride & 3) == 0 && c0 + 32 <= J.nchan && (((uintptr_t)J.out) & 15) == 0) {
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    reinterpret_cast<float4 *>(dst)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        for (uint32_t cb = 0; cb < 2 * J.nb; ++cb) {
+            uint32_t r[32];
+            if (nchunks > 0) {
+                tmem_ld_32x32b_x32(S.tmem + a * 256u + ((q4 * 32u) << 16) + cb * 32u, r);
+                tmem_wait_ld();
             } else {
 #pragma unroll
+                for (int i = 0; i < 32; ++i) r[i] = 0u;
+            }
+            if (!store || !valid) continue;
+            const uint32_t c0 = c_item + cb * 32;
+            const float f = last ? inv : 1.f;
+            float v[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]) * sc[cb * 32 + i];
+            if (J.ostride == 0) {
+#pragma unroll
                 for (int i = 0; i < 32; ++i)
-                    if (c0 + i < J.nchan) dst[i] = v[i];
+                    if (c0 + i < J.nchan) {
+                        float *d = J.out + (uint64_t)(c0 + i) * P + p;
+                        *d = (q ? *d + v[i] : v[i]) * f;
+                    }
+            } else {
+                float *dst = J.out + p * J.ostride + c0;
+                if ((J.ostride & 3) == 0 && c0 + 32 <= J.nchan && (((uintptr_t)J.out) & 15) == 0) {
+                    float4 *d4 = reinterpret_cast<float4 *>(dst);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        float4 o = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                        if (q) {
+                            const float4 b = d4[i];
+                            o.x += b.x;
+                            o.y += b.y;
+                            o.z += b.z;
+                            o.w += b.w;
+                        }
+                        o.x *= f;
+                        o.y *= f;
+                        o.z *= f;
+                        o.w *= f;
+                        d4[i] = o;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (c0 + i < J.nchan) dst[i] = (q ? dst[i] + v[i] : v[i]) * f;
+                }
             }
         }
+        tc_fence_before();
+        mbar_arrive(&S.acc_empty[a]);  // the accumulator may be overwritten
     }
-    tc_fence_before();
-    mbar_arrive(&S.acc_empty[a]);  // the accumulator may be overwritten
 }
 
 template <class Cfg>
@@ -645,7 +757,7 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    uint32_t gk = 0, il = 0;
+    uint32_t gk = 0, il = 0, gs = 0, gse = 0;  // chunks, items, MMA and epilogue segments
     for (uint64_t it = blockIdx.x; it < nitems; it += gridDim.x, ++il) {
         const uint64_t tile = J.T.t0 + it % ntiles;
         const uint32_t cblk = (uint32_t)(it / ntiles);
@@ -660,24 +772,307 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
             __syncwarp();
             tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
         } else if (warp == 1) {
-            if (lane == 0) {
-                const uint32_t a = il & 1;
-                if (il >= 2 && !mbar_wait(&S.acc_empty[a], ((il >> 1) - 1) & 1, kTcWaitNs)) tc_give_up(S, timeouts);
-                tc_fence_after();
-                tc_mma<Cfg>(S, J, nchunks, gk, S.tmem + a * 256u, timeouts, macs);
-                if (nchunks == 0)
-                    mbar_arrive(&S.acc_full[a]);
-                else
-                    mma_commit(&S.acc_full[a]);
-            }
+            if (lane == 0) tc_mma_seg<Cfg>(S, J, nchunks, gk, gs, timeouts, macs);
         } else if (warp < 6) {
             tc_build<Cfg>(S, J, tile, nchunks, gk, tid - 64, timeouts);
         } else {
-            tc_epilogue_direct(S, J, tile, cblk, nchunks, il, tid - 192, timeouts);
+            tc_epilogue_direct(S, J, tile, cblk, nchunks, il, gse, tid - 192, timeouts);
         }
         gk += nchunks;
     }
     // the copies of the last chunks land before the shared memory is given back
+    if (tid == 0) {
+        for (uint32_t g = gk > ST ? gk - ST : 0; g < gk; ++g) {
+            const uint32_t s = g % ST, ph = (g / ST) & 1;
+            if (!mbar_wait(&S.full_b[s], ph, kTcWaitNs)) {
+                tc_give_up(S, timeouts);
+                break;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(S.tmem, 512);
+    }
+}
+
+// ----------------------------------------------------------- direct weights
+// Dense tiles (most staged samples lie within the radius of most of the
+// tile's pixels, e.g. beams many pixels wide): the builders evaluate the
+// weights of the chunk's slots for their own pixel from the samples'
+// geometry, so no entries are written or read and no FP64 weight pass runs
+// before. Builder thread bt owns operand row m = bt (pixel (m % 16, m / 16)
+// of the tile) and, per chunk: loads the geometry of 64 slots into shared
+// memory (cp.async, one chunk ahead), then for each slot whose sample lies in
+// its pixel's window of the slot's ring (ring_window_mc, the windows the
+// tile pass unioned) evaluates the FP64 distance, cutoff and FP32 Gaussian
+// (pair_weight_s, the entry path's weight), accumulates the FP64 weight sum
+// and writes the hi/lo row of the K-major operand in 16-byte pieces. The
+// epilogue takes the weight sums from shared memory.
+constexpr int kTcGeo = 64;  // slots per chunk of the direct builders
+
+struct TcDShared {
+    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], zfill[kTcMaxStages];
+    uint64_t acc_full[2], acc_empty[2], ws_full[2], ws_empty[2];
+    uint32_t tmem;
+    volatile int abort;
+    uint32_t ulo[kTileMaxRings], base[kTileMaxRings + 1];    // the producer's current item
+    uint32_t bulo[kTileMaxRings], bbase[kTileMaxRings + 1];  // the builders' current item
+    float inv_scale[2][kTcMaxN];
+    double wsum[2][kTcM];
+    double4 g_half[2][kTcGeo];
+    double g_cb[2][kTcGeo], g_w[2][kTcGeo];
+};
+
+template <class Cfg>
+__device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, uint64_t tile, uint32_t cblk,
+                                                 uint32_t U, uint32_t nchunks, uint32_t gk, uint32_t il, int bt,
+                                                 unsigned long long *timeouts) {
+    using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
+    static_assert(KC == kTcGeo, "direct builders take 64-slot chunks");
+    const TcStage<Cfg> st{tc_smem_base()};
+    const TileArgs &T = J.T;
+    const GridArgs &a = J.a;
+    const uint32_t a2 = il & 1;
+    // the builders' copy of the tile's ring table (after every builder is done with the last one)
+    named_barrier(4, kTcBuilders);
+    const int nrt = T.nr[tile];
+    for (int j = bt; j < nrt; j += kTcBuilders) S.bulo[j] = T.ulo[tile * kTileMaxRings + j];
+    for (int j = bt; j <= nrt; j += kTcBuilders) S.bbase[j] = T.base[tile * (kTileMaxRings + 1) + j];
+    named_barrier(4, kTcBuilders);
+    // this thread's pixel
+    const uint32_t m = (uint32_t)bt;
+    const uint32_t xx = (uint32_t)(tile % T.ntx) * kTileX + (m & (kTileX - 1));
+    const uint32_t yy = (uint32_t)(tile / T.ntx) * kTileY + m / kTileX;
+    const bool valid = xx < J.g.nx && yy < J.g.ny;
+    PixPrep P{};
+    if (valid) P = a.prep[(uint64_t)yy * J.g.nx + xx];
+    const PixHalf ph = pix_half(P);
+    const int r0 = T.r0[tile];
+    const uint32_t nrows = J.nrows;
+    // geometry of chunk kk into buffer kk & 1 (threads 0..63, one slot each)
+    auto load = [&](uint32_t kk) {
+        if (bt < kTcGeo && kk < nchunks) {
+            const uint32_t slot = kk * KC + bt;
+            uint32_t idx = nrows - 1;
+            if (slot < U) {
+                int lo = 0, hi = nrt;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (S.bbase[mid] <= slot) lo = mid; else hi = mid;
+                }
+                idx = min(S.bulo[lo] + (slot - S.bbase[lo]), nrows - 1);
+            }
+            const uint32_t b = kk & 1;
+            cp_async16(&S.g_half[b][bt], a.half + idx, true);
+            cp_async16(reinterpret_cast<uint8_t *>(&S.g_half[b][bt]) + 16,
+                       reinterpret_cast<const uint8_t *>(a.half + idx) + 16, true);
+            cp_async8(&S.g_cb[b][bt], a.cb2 + idx);
+            cp_async8(&S.g_w[b][bt], a.w + idx);
+        }
+        cp_async_commit();
+    };
+    load(0);
+    // ring cursor: compacted ring c of the current slot, its span index j and this pixel's window there
+    int c = -1, j = -1;
+    uint32_t cbase = 0, cnext = 0, culo = 0, wlo = 0, whi = 0;
+    double wsum = 0.0;
+    unsigned long long within = 0;
+    bool failed = false;
+    for (uint32_t k = 0; k < nchunks; ++k) {
+        const uint32_t g = gk + k, s = g % ST;
+        named_barrier(4, kTcBuilders);  // every builder is done with chunk k - 1's geometry
+        load(k + 1);
+        cp_async_wait<1>();  // this thread's copies of chunk k have landed
+        bool bad = S.abort;
+        if (!bad && g >= ST && !mbar_wait(&S.empty[s], ((g / ST) - 1) & 1, kTcWaitNs)) {
+            tc_give_up(S, timeouts);
+            bad = true;
+        }
+        if (named_barrier_or(4, kTcBuilders, bad)) {  // chunk k's geometry visible; the same exit in every builder
+            failed = true;
+            break;
+        }
+        const uint32_t b = k & 1;
+        uint8_t *ah = st.A_hi(s), *al = st.A_lo(s);
+        for (uint32_t s8 = 0; s8 < KC / 8; ++s8) {
+            // ring runs take multiples of 8 slots: one ring per 8-slot piece
+            const uint32_t slot0 = k * KC + s8 * 8;
+            if (slot0 < U && (slot0 >= cnext || c < 0)) {
+                // next occupied ring (uniform across the builders) and this pixel's window there
+                while (c + 1 < nrt && S.bbase[c + 1] <= slot0) ++c;
+                cbase = S.bbase[c];
+                cnext = S.bbase[c + 1];
+                culo = S.bulo[c];
+                do {
+                    ++j;
+                } while (j < kTileMaxSpan && T.ring_idx[tile * kTileMaxSpan + j] != (uint16_t)c);
+                wlo = whi = 0;
+                const int kr = r0 + j;
+                if (P.nr > 0 && kr >= P.ur && kr < P.ur + P.nr) {
+                    uint32_t lo, hi;
+                    if (ring_window_mc(a, a.rings[kr], P, lo, hi)) {
+                        wlo = lo;
+                        whi = hi;
+                    }
+                }
+            }
+            // The 8 slots' pair tests as straight-line code (independent FP64
+            // chains the scheduler can interleave): haversines, then the weights
+            // of the pairs below the threshold band, the same arithmetic as
+            // pair_weight_s; pairs inside the band take pair_weight_s itself.
+            double hh[8];
+            bool inw[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const uint32_t q = s8 * 8 + e;
+                const uint32_t idx = culo + (slot0 + e - cbase);
+                inw[e] = slot0 + e < U && idx >= wlo && idx < whi;
+                const double4 gq = S.g_half[b][q];
+                const double sb = ph.sb * gq.w - ph.cb * gq.z;  // sin((b1 - b2) / 2)
+                const double sl = ph.sl * gq.y - ph.cl * gq.x;  // sin((l1 - l2) / 2)
+                hh[e] = sb * sb + P.cb1 * S.g_cb[b][q] * (sl * sl);
+            }
+            float wv[8];
+            bool band = false;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const double h = hh[e];
+                double d2;
+                if (a.series) {
+                    const double t =
+                        h * (1.0 + h * (1.0 / 3.0 + h * (8.0 / 45.0 + h * (4.0 / 35.0 + h * (128.0 / 1575.0)))));
+                    d2 = 4.0 * t * (kRad2Deg * kRad2Deg);
+                } else {
+                    const double d = 2.0 * asin(sqrt(h)) * kRad2Deg;
+                    d2 = d * d;
+                }
+                const bool acc = inw[e] && h < a.hlo;
+                band |= inw[e] && h >= a.hlo && h <= a.hhi;
+                const double wt = acc ? S.g_w[b][s8 * 8 + e] * (double)expf((float)(-d2 * a.p0)) : 0.0;
+                wv[e] = 0.f;
+                if (wt > 0.0) {
+                    wsum += wt;
+                    ++within;
+                    wv[e] = (float)wt;
+                }
+            }
+            if (band) {
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    if (!(inw[e] && hh[e] >= a.hlo && hh[e] <= a.hhi)) continue;
+                    const uint32_t q = s8 * 8 + e;
+                    const double wt = pair_weight_s<true>(a, P, ph, S.g_half[b][q], S.g_cb[b][q], S.g_w[b][q],
+                                                          culo + (slot0 + e - cbase));
+                    if (wt > 0.0) {
+                        wsum += wt;
+                        ++within;
+                        wv[e] = (float)wt;
+                    }
+                }
+            }
+            uint32_t hv[4], lv[4];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const float ws = wv[e] * J.wscale;
+                const uint16_t h = tc_to16(ws, J.fmt);
+                const uint16_t l = tc_to16(ws - tc_from16(h, J.fmt), J.fmt);
+                if (e & 1) {
+                    hv[e >> 1] |= (uint32_t)h << 16;
+                    lv[e >> 1] |= (uint32_t)l << 16;
+                } else {
+                    hv[e >> 1] = h;
+                    lv[e >> 1] = l;
+                }
+            }
+            const uint32_t o = tc_a_offset<KC>(m, s8 * 8);
+            *reinterpret_cast<uint4 *>(ah + o) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+            *reinterpret_cast<uint4 *>(al + o) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(&S.full_a[s]);
+    }
+    cp_async_wait<0>();  // no geometry copy outlives the item
+    // the pixel's FP64 weight sum for the epilogue (after it has read the sum two items back)
+    if (!failed && il >= 2 && !mbar_wait(&S.ws_empty[a2], ((il >> 1) - 1) & 1, kTcWaitNs)) tc_give_up(S, timeouts);
+    S.wsum[a2][m] = valid ? wsum : 0.0;
+    mbar_arrive(&S.ws_full[a2]);
+    if (cblk == 0 && valid) {
+        // statistics: the pixel's pairs and the candidates the reference visits on its rings
+        unsigned long long cand = 0, skips = 0;
+        for (int kr = P.ur; kr < P.ur + P.nr; ++kr) {
+            const RingRec &R = a.rings[kr];
+            uint32_t lo, hi;
+            if (!ring_window_mc(a, R, P, lo, hi)) {
+                ++skips;
+            } else {
+                cand += hi - lo;
+                if (P.polar) cand += polar_extra(R, lo, hi);
+            }
+        }
+        if (cand) atomicAdd(&a.stats->pairs_candidate, cand);
+        if (within) atomicAdd(&a.stats->pairs_within, within);
+        if (skips) atomicAdd(&a.stats->ring_skips, skips);
+    }
+}
+
+// Persistent direct-weight kernel body: roles as in tc_persist, the builders
+// being tc_build_weights and the epilogue reading their weight sums.
+template <class Cfg>
+__device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J, uint64_t nitems, uint64_t ntiles,
+                                                   unsigned long long *timeouts, unsigned long long *macs) {
+    using namespace sm100;
+    constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
+    static_assert(Cfg::kTmemCols <= 256, "two accumulators fit the 512 TMEM columns");
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (uint32_t s = 0; s < ST; ++s) {
+            mbar_init(&S.full_a[s], kTcBuilders);
+            mbar_init(&S.full_b[s], 1);
+            mbar_init(&S.empty[s], 1);
+            mbar_init(&S.zfill[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&S.acc_full[a], 1);
+            mbar_init(&S.acc_empty[a], kTcBuilders);
+            mbar_init(&S.ws_full[a], kTcBuilders);
+            mbar_init(&S.ws_empty[a], kTcBuilders);
+        }
+        S.abort = 0;
+        mbar_fence_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&S.tmem, 512);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t gk = 0, il = 0, gs = 0, gse = 0;  // chunks, items, MMA and epilogue segments
+    for (uint64_t it = blockIdx.x; it < nitems; it += gridDim.x, ++il) {
+        const uint64_t tile = J.T.t0 + it % ntiles;
+        const uint32_t cblk = (uint32_t)(it / ntiles);
+        const uint32_t U = J.T.U[tile];
+        const uint32_t nchunks = (U + KC - 1) / KC;
+        if (warp == 0) {
+            __syncwarp();
+            const int nrt = J.T.nr[tile];
+            for (int j = lane; j < nrt; j += 32) S.ulo[j] = J.T.ulo[tile * kTileMaxRings + j];
+            for (int j = lane; j <= nrt; j += 32) S.base[j] = J.T.base[tile * (kTileMaxRings + 1) + j];
+            __syncwarp();
+            tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
+        } else if (warp == 1) {
+            if (lane == 0) tc_mma_seg<Cfg>(S, J, nchunks, gk, gs, timeouts, macs);
+        } else if (warp < 6) {
+            tc_build_weights<Cfg>(S, J, tile, cblk, U, nchunks, gk, il, tid - 64, timeouts);
+        } else {
+            tc_epilogue_direct<TcDShared, true>(S, J, tile, cblk, nchunks, il, gse, tid - 192, timeouts);
+        }
+        gk += nchunks;
+    }
     if (tid == 0) {
         for (uint32_t g = gk > ST ? gk - ST : 0; g < gk; ++g) {
             const uint32_t s = g % ST, ph = (g / ST) & 1;

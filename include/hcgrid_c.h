@@ -141,6 +141,21 @@ hcg_status hcg_field_split_spectra(hcg_field *field, int engine, int keep_fp32);
  * returns it and the best time of each shape (ms[6], may be NULL). The field
  * must hold split spectra. No reference counterpart. */
 hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config);
+
+/* How the tensor-core engines build the weight operand of a tile:
+ *   HCG_TC_WEIGHTS_AUTO    (0): the library's choice (currently entries: the
+ *                              faster of the two on every workload measured);
+ *   HCG_TC_WEIGHTS_ENTRIES (1): an FP64 weight pass writes entries (pixel-group,
+ *                              sample, 4 weights) that the kernel scatters;
+ *   HCG_TC_WEIGHTS_DIRECT  (2): the kernel's builder warps evaluate the FP64
+ *                              distance, cutoff and Gaussian of every staged
+ *                              sample for every pixel of the tile.
+ * The accepted pairs and weights are the same; the FP64 weight sums can differ
+ * in the last bits (summation order). No reference counterpart. */
+#define HCG_TC_WEIGHTS_AUTO 0
+#define HCG_TC_WEIGHTS_ENTRIES 1
+#define HCG_TC_WEIGHTS_DIRECT 2
+hcg_status hcg_tc_set_weights(hcg_context *ctx, int mode);
 hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, int *best,
                         float *ms);
 /* Sorted keys (n+1 with the npix sentinel), permutation (n) and ring LUT

@@ -183,8 +183,10 @@ def test_ring_pixel_tables_match_binary_searches(ctx, monkeypatch, nchan):
 
 
 @pytest.mark.parametrize("ra", [120.0, 0.4])
-@pytest.mark.parametrize("engine", [api.ENGINE_FP32, api.ENGINE_TC_F16])
-def test_polar_multichannel_vs_oracle(ctx, ra, engine):
+@pytest.mark.parametrize("engine,weights", [(api.ENGINE_FP32, api.TC_WEIGHTS_AUTO),
+                                            (api.ENGINE_TC_F16, api.TC_WEIGHTS_ENTRIES),
+                                            (api.ENGINE_TC_F16, api.TC_WEIGHTS_DIRECT)])
+def test_polar_multichannel_vs_oracle(ctx, ra, engine, weights):
     """Pixels within 20 deg of the pole, where the reference takes whole
     rings. The multi-channel path narrows each ring to the pixels that can
     hold a sample within the radius: the accepted pairs, the candidate count
@@ -200,7 +202,11 @@ def test_polar_multichannel_vs_oracle(ctx, ra, engine):
         f.split_spectra(engine)
     t = ctx.target_from_header(job.header)
     xw, yw = t.coords()
-    cube, w = ctx.grid(f, t, engine=engine)
+    ctx.tc_set_weights(weights)
+    try:
+        cube, w = ctx.grid(f, t, engine=engine)
+    finally:
+        ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
     st = ctx.stats()
     g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
     ps = O.presort(g.hpx, job.lon, job.lat)

@@ -46,6 +46,15 @@ def plane_errors(cube, ref):
     return worst
 
 
+@pytest.fixture
+def entries_mode(ctx):
+    """Weight operands from the FP64 weight pass's entries: the weight sums
+    are then bit-identical to the FP32 engine's."""
+    ctx.tc_set_weights(api.TC_WEIGHTS_ENTRIES)
+    yield
+    ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
+
+
 @pytest.fixture(scope="module")
 def small(ctx):
     """Config-2 generator, 150k samples over 2 deg, 100 channels (not a
@@ -68,7 +77,7 @@ def small(ctx):
 
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("layout", [api.SAMPLE_MAJOR, api.CHANNEL_MAJOR])
-def test_tc_matches_oracle(ctx, small, engine, layout):
+def test_tc_matches_oracle(ctx, small, entries_mode, engine, layout):
     job, f, t, ref, c32, w32 = small
     prepare(ctx, job)
     f.split_spectra(engine)
@@ -95,7 +104,7 @@ def test_auto_engine_uses_the_split(ctx, small):
 
 
 @pytest.mark.parametrize("nchan", [64, 98, 300])
-def test_tc_channel_blocks(ctx, nchan):
+def test_tc_channel_blocks(ctx, entries_mode, nchan):
     """64 channels (one 64-channel block), 98 (rows not a multiple of 16
     bytes: direct stores instead of the TMA store) and 300 (two CTAs per
     tile, the second partly past the last channel)."""
@@ -113,7 +122,7 @@ def test_tc_channel_blocks(ctx, nchan):
 
 
 @pytest.mark.parametrize("layout", [api.SAMPLE_MAJOR, api.CHANNEL_MAJOR])
-def test_tc_empty_tiles_and_padding(ctx, layout):
+def test_tc_empty_tiles_and_padding(ctx, entries_mode, layout):
     """A 97x97 map larger than the field: partial edge tiles (the TMA store
     clips them; channel-major rows of 97 floats take direct stores) and
     whole tiles without samples, which come out NaN with zero weight exactly
@@ -133,6 +142,103 @@ def test_tc_empty_tiles_and_padding(ctx, layout):
     np.testing.assert_array_equal(np.isnan(ct), np.isnan(c32))
     np.testing.assert_array_equal(wt, w32)
     assert plane_errors(ct, c32.astype(np.float64)) <= 5e-5
+
+
+@pytest.fixture(scope="module")
+def dense(ctx):
+    """A beam 27 pixels wide over 2.8k samples per pixel disc (20k samples on
+    0.3 deg, 64x64 map, FWHM 180"): tiles whose staged samples mostly lie within
+    the radius of their pixels, where the kernel evaluates the weights itself.
+    100 channels: two 64-channel blocks, the second partly past the last."""
+    shape = dict(block=0, n=20_000, size_deg=0.3, ra=150.0, dec=20.0, grid=64, nchan=100, fwhm=180.0, seed=5)
+    job = synth.block_job(shape)
+    prepare(ctx, job)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(job.values)
+    t = ctx.target_from_header(job.header)
+    xw, yw = t.coords()
+    g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    ps = O.presort(g.hpx, job.lon, job.lat)
+    oc, ow, ost = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], job.values[ps.perm].astype(np.float64), xw, yw)
+    yield job, f, t, oc / ow[:, None], ow, ost
+    f.close()
+    t.close()
+
+
+@pytest.mark.parametrize("mode", [api.TC_WEIGHTS_DIRECT, api.TC_WEIGHTS_ENTRIES])
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("layout", [api.SAMPLE_MAJOR, api.CHANNEL_MAJOR])
+def test_tc_weight_modes_match_oracle(ctx, dense, mode, engine, layout):
+    """Both weight-operand modes give the reference's pairs (accepted and
+    candidate counts equal to the oracle's), its weight sums within 1e-6 and
+    its cube within the split's tolerance."""
+    job, f, t, ref, ow, ost = dense
+    prepare(ctx, job)
+    f.split_spectra(engine)
+    ctx.tc_set_weights(mode)
+    try:
+        cube, w = ctx.grid(f, t, layout=layout, engine=engine)
+        st = ctx.stats()
+    finally:
+        ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
+    if layout == api.CHANNEL_MAJOR:
+        cube = cube.T
+    assert st.pairs_within == ost.pairs_within
+    assert st.pairs_candidate == ost.pairs_visited
+    ok = ow > 0
+    assert np.abs(w[ok] - ow[ok]).max() / ow.max() <= 1e-6
+    err = plane_errors(cube, ref)
+    print(f"mode {mode} engine {engine} layout {layout}: max plane-relative error {err:.3e}")
+    assert err <= TOL[engine]
+
+
+def test_tc_weight_modes_deterministic_and_checked(ctx, dense):
+    """Each mode gives the same bits on every call; the automatic mode is one
+    of the two; unknown modes are refused."""
+    job, f, t, ref, ow, ost = dense
+    prepare(ctx, job)
+    f.split_spectra(api.ENGINE_TC_F16)
+    out = {}
+    for mode in (api.TC_WEIGHTS_AUTO, api.TC_WEIGHTS_ENTRIES, api.TC_WEIGHTS_DIRECT):
+        ctx.tc_set_weights(mode)
+        try:
+            a, wa = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+            b, wb = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+        finally:
+            ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
+        np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(wa, wb)
+        out[mode] = (a, wa)
+    auto = out[api.TC_WEIGHTS_AUTO][0]
+    assert any(np.array_equal(auto, out[m][0], equal_nan=True)
+               for m in (api.TC_WEIGHTS_ENTRIES, api.TC_WEIGHTS_DIRECT))
+    with pytest.raises(RuntimeError, match="HCG_EINVAL"):
+        ctx.tc_set_weights(3)
+
+
+@pytest.mark.parametrize("nchan", [64, 300])
+def test_tc_direct_weights_channel_blocks(ctx, nchan):
+    """Direct weights with one 64-channel block (64-channel items) and with
+    300 channels (256-channel items, the second partly past the last channel),
+    against the FP32 engine."""
+    shape = dict(block=0, n=20_000, size_deg=0.3, ra=150.0, dec=20.0, grid=64, nchan=nchan, fwhm=180.0, seed=6)
+    job = synth.block_job(shape)
+    prepare(ctx, job)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(job.values)
+    t = ctx.target_from_header(job.header)
+    c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+    f.split_spectra(api.ENGINE_TC_F16)
+    ctx.tc_set_weights(api.TC_WEIGHTS_DIRECT)
+    try:
+        ct, wt = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
+    finally:
+        ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
+    ok = w32 > 0
+    assert np.abs(wt[ok] - w32[ok]).max() / w32.max() <= 1e-6
+    assert plane_errors(ct, c32.astype(np.float64)) <= 1e-5
+    f.close()
+    t.close()
 
 
 def test_tc_state_and_input_checks(ctx):
