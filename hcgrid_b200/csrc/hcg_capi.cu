@@ -114,6 +114,67 @@ void hcg::Scratch::release(cudaStream_t s) {
     size.clear();
 }
 
+uint64_t hcg::job_pixels(const hcg_job &job) {
+    return job.target ? (uint64_t)job.target->nx * job.target->ny : 0;
+}
+
+// hcg_grid after its argument checks; the caller holds the context lock.
+static hcg_status grid_checked(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube,
+                               int layout, float *weights_out, int mem, int engine) {
+    if (field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
+    if (!field->d_spec && !field->xfmt) return fail(ctx, HCG_ESTATE, "field has no spectra (hcg_field_set_spectra)");
+    if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
+        return fail(ctx, HCG_EINVAL, "unknown layout");
+    if (engine < HCG_ENGINE_AUTO || engine > HCG_ENGINE_TC_F16) return fail(ctx, HCG_EINVAL, "unknown engine");
+    if (engine == HCG_ENGINE_AUTO) engine = auto_engine(field);
+    const bool tc = engine != HCG_ENGINE_FP32 && field->nchan > 1;
+    if (tc && field->xfmt != engine)
+        return fail(ctx, HCG_ESTATE, "the tensor-core engine needs hcg_field_split_spectra with the same engine");
+    if (tc && field->xnonfinite)
+        return fail(ctx, HCG_EINVAL,
+                    std::to_string(field->xnonfinite) + " non-finite spectrum values: grid with HCG_ENGINE_FP32");
+    if (!tc && !field->d_spec)
+        return fail(ctx, HCG_ESTATE, "the FP32 spectra were dropped by hcg_field_split_spectra");
+    cudaStream_t s = ctx->stream;
+    const size_t P = (size_t)target->nx * target->ny;
+    const size_t cube_bytes = P * field->nchan * sizeof(float);
+    float *dc = cube, *dw = weights_out;
+    if (mem == HCG_MEM_HOST) {
+        cudaError_t e = cudaSuccess;
+        dc = (float *)ctx->scratch.get(16, cube_bytes, s, e);
+        if (weights_out) dw = (float *)ctx->scratch.get(17, P * sizeof(float), s, e);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "output buffers");
+    }
+    CK(ctx, cudaMemsetAsync(ctx->d_stats, 0, offsetof(DevStats, invalid_input), s), "stats reset");
+    std::string why;
+    cudaError_t e = grid_field(ctx, field, target, dc, layout, dw, engine, why);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "grid", why);
+    if (tc) {
+        unsigned long long to = 0;
+        CK(ctx, cudaMemcpyAsync(&to, &ctx->d_stats->timeouts, sizeof(to), cudaMemcpyDeviceToHost, s), "timeouts");
+        CK(ctx, cudaStreamSynchronize(s), "grid");
+        if (to) return fail(ctx, HCG_ETIMEOUT, std::to_string(to) + " tensor-core pipeline waits ran out");
+    }
+    if (mem == HCG_MEM_HOST) {
+        CK(ctx, cudaMemcpyAsync(cube, dc, cube_bytes, cudaMemcpyDeviceToHost, s), "cube download");
+        if (weights_out)
+            CK(ctx, cudaMemcpyAsync(weights_out, dw, P * sizeof(float), cudaMemcpyDeviceToHost, s), "weights download");
+        CK(ctx, cudaStreamSynchronize(s), "grid");
+    }
+    return HCG_OK;
+}
+
+// One server job on a lane's context (the field carries its kernel
+// parameters; lane contexts are not prepared themselves).
+hcg_status hcg::grid_job(hcg_context *ctx, const hcg_job &job) {
+    if (!ctx || !job.field || !job.target || !job.cube) return HCG_EINVAL;
+    Guard g(ctx);
+    if (job.field->ctx->device != ctx->device || job.target->ctx->device != ctx->device)
+        return fail(ctx, HCG_EINVAL, "job lives on another device");
+    return grid_checked(ctx, job.field, job.target, job.cube, job.layout, job.weights, HCG_MEM_DEVICE,
+                        HCG_ENGINE_AUTO);
+}
+
 extern "C" {
 
 const char *hcg_status_string(hcg_status s) {
@@ -487,47 +548,7 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
     if (!ctx || !field || !target || !cube) return HCG_EINVAL;
     Guard g(ctx);
     if (!ctx->prepared) return fail(ctx, HCG_ESTATE, "hcg_prepare_grid_kernel must come first");
-    if (field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
-    if (!field->d_spec && !field->xfmt) return fail(ctx, HCG_ESTATE, "field has no spectra (hcg_field_set_spectra)");
-    if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
-        return fail(ctx, HCG_EINVAL, "unknown layout");
-    if (engine < HCG_ENGINE_AUTO || engine > HCG_ENGINE_TC_F16) return fail(ctx, HCG_EINVAL, "unknown engine");
-    if (engine == HCG_ENGINE_AUTO) engine = auto_engine(field);
-    const bool tc = engine != HCG_ENGINE_FP32 && field->nchan > 1;
-    if (tc && field->xfmt != engine)
-        return fail(ctx, HCG_ESTATE, "the tensor-core engine needs hcg_field_split_spectra with the same engine");
-    if (tc && field->xnonfinite)
-        return fail(ctx, HCG_EINVAL,
-                    std::to_string(field->xnonfinite) + " non-finite spectrum values: grid with HCG_ENGINE_FP32");
-    if (!tc && !field->d_spec)
-        return fail(ctx, HCG_ESTATE, "the FP32 spectra were dropped by hcg_field_split_spectra");
-    cudaStream_t s = ctx->stream;
-    const size_t P = (size_t)target->nx * target->ny;
-    const size_t cube_bytes = P * field->nchan * sizeof(float);
-    float *dc = cube, *dw = weights_out;
-    if (mem == HCG_MEM_HOST) {
-        cudaError_t e = cudaSuccess;
-        dc = (float *)ctx->scratch.get(16, cube_bytes, s, e);
-        if (weights_out) dw = (float *)ctx->scratch.get(17, P * sizeof(float), s, e);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "output buffers");
-    }
-    CK(ctx, cudaMemsetAsync(ctx->d_stats, 0, offsetof(DevStats, invalid_input), s), "stats reset");
-    std::string why;
-    cudaError_t e = grid_field(ctx, field, target, dc, layout, dw, engine, why);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "grid", why);
-    if (tc) {
-        unsigned long long to = 0;
-        CK(ctx, cudaMemcpyAsync(&to, &ctx->d_stats->timeouts, sizeof(to), cudaMemcpyDeviceToHost, s), "timeouts");
-        CK(ctx, cudaStreamSynchronize(s), "grid");
-        if (to) return fail(ctx, HCG_ETIMEOUT, std::to_string(to) + " tensor-core pipeline waits ran out");
-    }
-    if (mem == HCG_MEM_HOST) {
-        CK(ctx, cudaMemcpyAsync(cube, dc, cube_bytes, cudaMemcpyDeviceToHost, s), "cube download");
-        if (weights_out)
-            CK(ctx, cudaMemcpyAsync(weights_out, dw, P * sizeof(float), cudaMemcpyDeviceToHost, s), "weights download");
-        CK(ctx, cudaStreamSynchronize(s), "grid");
-    }
-    return HCG_OK;
+    return grid_checked(ctx, field, target, cube, layout, weights_out, mem, engine);
 }
 
 hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config) {

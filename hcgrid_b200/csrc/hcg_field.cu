@@ -232,6 +232,8 @@ __global__ void k_ring_table(HpxParams h, uint64_t firstring, uint64_t usedrings
     R.phi0 = phi;
     R.dphi = 0.0;  // set by k_ring_phi
     R.cbmin = 1.0;
+    R.bmin = 0.0;
+    R.bmax = 0.0;
     // pixel range of the ring's samples; the table offsets are set on the host
     R.pmin = 0;
     R.span = 0;
@@ -243,37 +245,47 @@ __global__ void k_ring_table(HpxParams h, uint64_t firstring, uint64_t usedrings
     rings[k] = R;
 }
 
-// Per ring: the largest |phi| distance of a sample from its pixel centre and
-// the smallest cos(lat) of its samples (block per ring).
+// Per ring: the largest |phi| distance of a sample from its pixel centre,
+// the smallest cos(lat) and the latitude range of its samples (block per ring).
 __global__ void __launch_bounds__(256) k_ring_phi(HpxParams h, RingRec *__restrict__ rings,
                                                   const uint64_t *__restrict__ keys, const double *__restrict__ l2,
-                                                  const double *__restrict__ cb2) {
-    __shared__ double s_d[8], s_c[8];
+                                                  const double *__restrict__ b2, const double *__restrict__ cb2) {
+    __shared__ double s_d[8], s_c[8], s_lo[8], s_hi[8];
     const uint32_t lo = rings[blockIdx.x].lut_lo, hi = rings[blockIdx.x].lut_hi;
-    double dmax = 0.0, cmin = 1.0;
+    double dmax = 0.0, cmin = 1.0, bl = 1e300, bh = -1e300;
     for (uint32_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
         double z, phi, sth;
         bool have;
         pix2loc(h, keys[j], z, phi, sth, have);
         dmax = fmax(dmax, fabs(remainder(l2[j] - phi, 2.0 * kPi)));
         cmin = fmin(cmin, cb2[j]);
+        bl = fmin(bl, b2[j]);
+        bh = fmax(bh, b2[j]);
     }
     for (int o = 16; o > 0; o >>= 1) {
         dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
         cmin = fmin(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+        bl = fmin(bl, __shfl_xor_sync(0xffffffffu, bl, o));
+        bh = fmax(bh, __shfl_xor_sync(0xffffffffu, bh, o));
     }
     if ((threadIdx.x & 31) == 0) {
         s_d[threadIdx.x >> 5] = dmax;
         s_c[threadIdx.x >> 5] = cmin;
+        s_lo[threadIdx.x >> 5] = bl;
+        s_hi[threadIdx.x >> 5] = bh;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
             dmax = fmax(dmax, s_d[w]);
             cmin = fmin(cmin, s_c[w]);
+            bl = fmin(bl, s_lo[w]);
+            bh = fmax(bh, s_hi[w]);
         }
         rings[blockIdx.x].dphi = dmax;
         rings[blockIdx.x].cbmin = cmin;
+        rings[blockIdx.x].bmin = hi > lo ? bl : 0.0;
+        rings[blockIdx.x].bmax = hi > lo ? bh : 0.0;
     }
 }
 
@@ -448,7 +460,7 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
     k_permute_geometry<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, f->d_perm, d_lon, d_lat, d_w, f->d_l2, f->d_b2,
                                                                    f->d_cb2, f->d_w, f->d_half);
     TRY(cudaGetLastError());
-    k_ring_phi<<<(unsigned)f->usedrings, 256, 0, s>>>(f->hpx, f->d_rings, f->d_keys, f->d_l2, f->d_cb2);
+    k_ring_phi<<<(unsigned)f->usedrings, 256, 0, s>>>(f->hpx, f->d_rings, f->d_keys, f->d_l2, f->d_b2, f->d_cb2);
     TRY(cudaGetLastError());
 fail:
     if (k0) cudaFreeAsync(k0, s);

@@ -43,12 +43,14 @@ struct RingRec {
     uint32_t pmin;
     uint32_t span;
     uint64_t tbl;
-    // Polar windows of the multi-channel path: phi of the first pixel centre,
+    // Chord windows of the multi-channel path: phi of the first pixel centre,
     // the largest |phi| distance of a sample of the ring from its pixel
-    // centre, and the smallest cos(lat) of the ring's samples.
+    // centre, the smallest cos(lat) and the latitude range (radians) of the
+    // ring's samples.
     double phi0;
     double dphi;
     double cbmin;
+    double bmin, bmax;
 };
 
 // One target pixel: its coordinates and the phi half of loc2pix for the two
@@ -176,6 +178,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
                        std::string &why);
 cudaError_t batch_release(hcg_context *ctx);
 bool batch_trace();
+uint64_t job_pixels(const hcg_job &job);  // the target's pixel count (the server's job classes)
+hcg_status grid_job(hcg_context *ctx, const hcg_job &job);  // one server job, device buffers, automatic engine
 struct SinWcs;
 int parse_sin_header(const char *header, size_t len, uint32_t &nx, uint32_t &ny, SinWcs &w, std::string &why);
 cudaError_t sin_coords_device(const SinWcs &w, uint32_t nx, uint32_t ny, double *d_x, double *d_y, cudaStream_t s);

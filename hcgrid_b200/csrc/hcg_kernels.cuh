@@ -213,37 +213,42 @@ inline GridArgs grid_args(const hcg_field *f, const PixPrep *prep, DevStats *sta
     return a;
 }
 
-// Candidate interval of the multi-channel path. Where the reference takes a
-// whole ring (pixels within 20 deg of a pole, gridding.cu:340-354) the
-// interval holds the ring's pixels whose centres lie within W in phi of the
-// pixel, which contain every sample of the ring within the radius: an
-// accepted pair has hav(d) < hpolar, so hav(dphi) < hpolar / (cos b_s cos b_p)
-// with cos b_s >= the ring's smallest cos(lat), and a sample lies within
-// R.dphi of its pixel centre. The accepted pairs are the whole ring's; only
-// candidates beyond the radius are left out. Wrapping windows keep the whole ring.
+// Candidate interval of the multi-channel path: the reference's window
+// (gridding.cu:329-367; whole rings within 20 deg of a pole, 340-354)
+// intersected with the pixels whose centres can hold a sample of the ring
+// within the radius. An accepted pair has hav(d) < hpolar, and hav(d) =
+// hav(db) + cos b_p cos b_s hav(dphi) with |db| >= the distance of b_p from
+// the ring's latitude range and cos b_s >= the ring's smallest cos(lat), which
+// bounds |dphi|; a sample lies within R.dphi of its pixel centre. The accepted
+// pairs are the reference window's; only candidates beyond the radius are
+// left out. Windows whose phi range wraps keep the reference's. `ref_len` is
+// the reference window's length (its candidate count).
 __device__ __forceinline__ bool ring_window_mc(const GridArgs &a, const RingRec &R, const PixPrep &P, uint32_t &lo,
-                                               uint32_t &hi) {
-    if (!P.polar || R.lut_lo == 0) return ring_window(a.h, R, P, a.keys, a.ptab, lo, hi);
-    uint64_t lpix = R.startpix, rpix = R.startpix + R.npr - 1;
-    const double H = a.hpolar / (R.cbmin * P.cb1);
-    if (H < 1.0) {
-        const double W = 2.0 * asin(sqrt(H)) * (1.0 + 1e-9) + R.dphi + 1e-9;
-        const double dp = 2.0 * kPi / (double)R.npr;
-        const double lp = P.l1 - 2.0 * kPi * floor(P.l1 / (2.0 * kPi));
-        const double jl = floor((lp - W - R.phi0) / dp), jh = ceil((lp + W - R.phi0) / dp);
-        if (jl >= 0.0 && jh < (double)R.npr && jh - jl + 1.0 < (double)R.npr) {
-            lpix = R.startpix + (uint64_t)jl;
-            rpix = R.startpix + (uint64_t)jh;
-        }
+                                               uint32_t &hi, uint32_t &ref_len) {
+    ref_len = 0;
+    if (!ring_window(a.h, R, P, a.keys, a.ptab, lo, hi)) return false;
+    ref_len = hi > lo ? hi - lo : 0;
+    if (R.lut_lo == 0 || hi <= lo) return true;
+    // hav(db) >= y^2 (1 - y^2 / 3) with y = db / 2 (sin y >= y - y^3 / 6)
+    const double y = 0.5 * fmax(0.0, fmax(R.bmin - P.b1, P.b1 - R.bmax));
+    const double hb = y < 1.0 ? y * y * (1.0 - y * y * (1.0 / 3.0)) : 0.0;
+    if (!(hb < a.hpolar)) {  // no sample of the ring within the radius
+        hi = lo;
+        return true;
     }
-    pixel_window(R, lpix, rpix, a.keys, a.ptab, lo, hi);
+    const double H = (a.hpolar - hb) / (R.cbmin * P.cb1);
+    if (!(H < 0.25)) return true;
+    // |dphi| <= 2 asin(sqrt(H)) <= 2 sqrt(H / (1 - H)) (asin x = atan(x / sqrt(1 - x^2)) <= x / sqrt(1 - x^2))
+    const double W = 2.0 * sqrt(H / (1.0 - H)) * (1.0 + 1e-9) + R.dphi + 1e-9;
+    const double dp = 2.0 * kPi / (double)R.npr;
+    const double lp = P.l1 - 2.0 * kPi * floor(P.l1 / (2.0 * kPi));
+    const double jl = floor((lp - W - R.phi0) / dp), jh = ceil((lp + W - R.phi0) / dp);
+    if (!(jl >= 0.0 && jh < (double)R.npr && jh - jl + 1.0 < (double)R.npr)) return true;
+    uint32_t clo, chi;
+    pixel_window(R, R.startpix + (uint64_t)jl, R.startpix + (uint64_t)jh, a.keys, a.ptab, clo, chi);
+    lo = max(lo, clo);
+    hi = max(lo, min(hi, chi));
     return true;
-}
-
-// Candidates the reference visits on ring R for a pixel of the multi-channel
-// path that ring_window_mc narrowed (whole polar rings), beyond [lo, hi).
-__device__ __forceinline__ uint32_t polar_extra(const RingRec &R, uint32_t lo, uint32_t hi) {
-    return R.lut_lo == 0 ? 0u : (R.lut_hi - R.lut_lo) - (hi - lo);
 }
 
 // 32-byte read-only load (no double4 overload of __ldg)
@@ -440,17 +445,15 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
     }
     __syncwarp();
     int R0 = 1 << 30, R1 = -1;
-    bool polar = false;  // a pixel whose windows ring_window_mc narrowed
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         if (valid[q] && s_prep[q].nr > 0) {
             R0 = min(R0, s_prep[q].ur);
             R1 = max(R1, s_prep[q].ur + s_prep[q].nr - 1);
-            polar |= s_prep[q].polar != 0;
         }
     }
     unsigned lt = (1u << lane) - 1u;
-    unsigned long long count = 0, cand = 0, within = 0, skips = 0;
+    unsigned long long count = 0, within = 0;
     uint32_t base = 0;
     double ws[4] = {0.0, 0.0, 0.0, 0.0};
     const unsigned long long eoff = COUNT ? 0 : off[grp] - g.ebase;
@@ -481,9 +484,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
             const uint32_t kl[4] = {w0.x, w0.z, w1.x, w1.z}, kh[4] = {w0.y, w0.w, w1.y, w1.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                if (kl[q] > kh[q]) {
-                    ++skips;
-                } else {
+                if (kl[q] <= kh[q]) {  // lo > hi: a ring the reference would spin on
                     lo[q] = kl[q];
                     hi[q] = kh[q];
                     if (hi[q] > lo[q]) {
@@ -498,9 +499,8 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
             for (int q = 0; q < 4; ++q) {
                 const PixPrep &P = s_prep[q];
                 if (valid[q] && k >= P.ur && k < P.ur + P.nr) {
-                    if (!ring_window_mc(a, R, P, lo[q], hi[q])) {
-                        ++skips;
-                    } else if (hi[q] > lo[q]) {
+                    uint32_t rl;
+                    if (ring_window_mc(a, R, P, lo[q], hi[q], rl) && hi[q] > lo[q]) {
                         glo = min(glo, lo[q]);
                         ghi = max(ghi, hi[q]);
                     }
@@ -511,14 +511,6 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
         if (COUNT) {
             count += len;
             continue;
-        }
-        if (!COUNT && polar && k <= R1) {  // candidate statistic: the whole rings the reference visits
-            const RingRec &R = a.rings[k];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const PixPrep &P = s_prep[q];
-                if (valid[q] && P.polar && k >= P.ur && k < P.ur + P.nr) cand += polar_extra(R, lo[q], hi[q]);
-            }
         }
         uint32_t incl = len;
 #pragma unroll
@@ -550,7 +542,6 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
                 for (int q = 0; q < 4; ++q) {
                     if (idx >= s_lo[q] && idx < s_hi[q]) {
                         const double wt = pair_weight_s<true>(a, s_prep[q], s_half[q], hs, cb2, win, idx);
-                        ++cand;
                         if (wt > 0.0) {
                             ws[q] += wt;
                             wq[q] = (float)wt;
@@ -570,9 +561,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
         }
     }
     count = warp_sum_u64(count);
-    cand = warp_sum_u64(cand);
     within = warp_sum_u64(within);
-    skips = warp_sum_u64(skips);
     if (COUNT) {
         if (lane == 0) cap[grp] = (uint32_t)count;
         return;
@@ -584,9 +573,7 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (valid[q]) wsum[pix[q]] = ws[q];
-        if (cand) atomicAdd(&a.stats->pairs_candidate, cand);
         if (within) atomicAdd(&a.stats->pairs_within, within);
-        if (skips) atomicAdd(&a.stats->ring_skips, skips);
     }
 }
 
@@ -793,6 +780,16 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
         const uint64_t grp = (uint64_t)gyi * g.gx + gxi;
         if (gxi < g.gx && grp < g.ngroups) T.cap[grp] = known ? s_cnt[tid] : kCapUnknown;
     };
+    // the candidate statistic: the reference windows' lengths (the pairs the
+    // reference visits) of every (pixel, ring) of the tile, and the rings the
+    // reference would spin on
+    unsigned long long cand = 0, skips = 0;
+    auto add_cand = [&]() {
+        cand = warp_sum_u64(cand);
+        skips = warp_sum_u64(skips);
+        if ((tid & 31) == 0 && cand) atomicAdd(&a.stats->pairs_candidate, cand);
+        if ((tid & 31) == 0 && skips) atomicAdd(&a.stats->ring_skips, skips);
+    };
     if (nrt <= 0 || nrt > kTileMaxSpan) {
         if (tid == 0) {
             T.r0[tile] = 0;
@@ -801,6 +798,17 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
             if (nrt > kTileMaxSpan) atomicAdd(T.overflow, 1ULL);
         }
         write_caps(nrt <= 0);  // no samples: nothing to count
+        if (nrt > 0 && tid < kTileX * kTileY) {
+            const PixPrep &P = s_prep[tid];
+            for (int k = P.ur; k < P.ur + P.nr; ++k) {
+                uint32_t lo, hi, rl;
+                if (ring_window_mc(a, a.rings[k], P, lo, hi, rl))
+                    cand += rl;
+                else
+                    ++skips;
+            }
+        }
+        add_cand();
         return;
     }
     for (int j = tid; j < nrt; j += blockDim.x) { s_lo[j] = 0xffffffffu; s_hi[j] = 0; }
@@ -818,10 +826,12 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
             const int p = (2 * (gq / (kTileX / 2)) + (q >> 1)) * kTileX + 2 * (gq % (kTileX / 2)) + (q & 1);
             const PixPrep &P = s_prep[p];
             if (P.nr > 0 && k >= P.ur && k < P.ur + P.nr) {
-                uint32_t lo, hi;
-                if (!ring_window_mc(a, R, P, lo, hi)) {
+                uint32_t lo, hi, rl;
+                if (!ring_window_mc(a, R, P, lo, hi, rl)) {
                     wlo[q] = 1;  // lo > hi: the reference would spin on this ring
+                    ++skips;
                 } else {
+                    cand += rl;
                     wlo[q] = lo;
                     whi[q] = hi;
                     if (hi > lo) {
@@ -842,6 +852,7 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
             atomicMax(&s_hi[j], ghi);
         }
     }
+    add_cand();
     __syncthreads();
     write_caps(true);
     if (tid < 32) {  // one warp: compaction of the occupied rings and prefix sums of their lengths

@@ -2,14 +2,17 @@
 //
 // Clients submit jobs (a resident field, a target and device output
 // buffers) as they arrive. A dispatcher thread admits pending jobs in
-// arrival order while their HBM footprint fits the budget, forms a batch of
-// at most `max_batch` jobs and hands it to one of `lanes` worker lanes; each
-// lane owns its own context (stream + captured batch graph) on the same
-// device, so a batch that arrives while another is on the GPU is launched
-// right away and the two overlap on the device. When a batch finishes, its
-// footprint is released and the dispatcher admits more jobs. Every job
-// records submit, start and finish times (host steady clock), from which the
-// latency percentiles are taken.
+// arrival order while their HBM footprint fits the budget and hands them to
+// one of `lanes` worker lanes: a job whose target has at least
+// kSingleJobPixels pixels alone, with the GPU to itself (its kernels fill the
+// GPU by themselves; it runs through hcg_grid), else a batch of consecutive
+// smaller jobs (at most `max_batch`, through hcg_grid_batch's persistent
+// kernels). Each lane owns its own context (stream + captured batch graphs)
+// on the same device, so a batch that arrives while another batch is on the
+// GPU is launched right away and the two overlap on the device. When a lane finishes, its footprint is
+// released and the dispatcher admits more jobs. Every job records submit,
+// start and finish times (host steady clock), from which the latency
+// percentiles are taken.
 #include <stdint.h>
 #include <string.h>
 
@@ -25,9 +28,15 @@
 
 #include "hcgrid_c.h"
 
+namespace hcg {  // hcg_capi.cu
+uint64_t job_pixels(const hcg_job &job);                    // the target's pixel count
+hcg_status grid_job(hcg_context *ctx, const hcg_job &job);  // hcg_grid of one job on a lane's context
+}
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
+constexpr uint64_t kSingleJobPixels = 1ull << 20;
 
 struct Pending {
     uint64_t ticket;
@@ -58,7 +67,9 @@ struct hcg_server {
     std::vector<std::thread> workers;
     std::thread dispatcher;
     std::vector<std::vector<Pending>> lane_batch;
-    bool stop = false;
+    std::vector<char> lane_single;  // the lane's work is one large job (hcg_grid)
+    bool stop = false;          // no more submissions; the dispatcher leaves once the queue is empty
+    bool workers_stop = false;  // set after the dispatcher has left: lanes finish their work and leave
     uint64_t next_ticket = 1;
     uint32_t batches = 0;
     Clock::time_point t0 = Clock::now();
@@ -69,16 +80,22 @@ struct hcg_server {
     void worker(size_t li) {
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
-            cv_work.wait(lk, [&] { return stop || !lane_batch[li].empty(); });
-            if (lane_batch[li].empty() && stop) return;
+            cv_work.wait(lk, [&] { return workers_stop || !lane_batch[li].empty(); });
+            if (lane_batch[li].empty() && workers_stop) return;
             std::vector<Pending> b;
             b.swap(lane_batch[li]);
+            const bool single = lane_single[li];
             uint32_t bid = ++batches;
             lk.unlock();
             double ts = now();
-            std::vector<hcg_job> jobs(b.size());
-            for (size_t i = 0; i < b.size(); ++i) jobs[i] = b[i].job;
-            hcg_status st = hcg_grid_batch(lanes[li], (uint32_t)jobs.size(), jobs.data());
+            hcg_status st;
+            if (single) {
+                st = hcg::grid_job(lanes[li], b[0].job);
+            } else {
+                std::vector<hcg_job> jobs(b.size());
+                for (size_t i = 0; i < b.size(); ++i) jobs[i] = b[i].job;
+                st = hcg_grid_batch(lanes[li], (uint32_t)jobs.size(), jobs.data());
+            }
             double td = now();
             lk.lock();
             for (auto &p : b) {
@@ -100,12 +117,20 @@ struct hcg_server {
     void dispatch() {
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
+            // A large job runs with the GPU to itself (its persistent kernels
+            // assign work statically: CTAs that start late behind another
+            // lane's kernels stretch the whole launch); batches of small jobs
+            // overlap each other.
             cv_work.wait(lk, [&] {
                 if (stop && queue.empty()) return true;
                 if (queue.empty()) return false;
-                for (size_t i = 0; i < lanes.size(); ++i)
-                    if (!lane_busy[i]) return true;
-                return false;
+                size_t busy = 0;
+                for (size_t i = 0; i < lanes.size(); ++i) {
+                    if (lane_busy[i] && lane_single[i]) return false;
+                    busy += lane_busy[i] ? 1 : 0;
+                }
+                if (hcg::job_pixels(queue.front().job) >= kSingleJobPixels) return busy == 0;
+                return busy < lanes.size();
             });
             if (stop && queue.empty()) {
                 cv_work.notify_all();
@@ -117,8 +142,10 @@ struct hcg_server {
             // admit in arrival order while the footprint fits (a job larger
             // than the whole budget runs alone once nothing else is resident)
             std::vector<Pending> b;
-            while (!queue.empty() && b.size() < max_batch) {
+            const bool single = hcg::job_pixels(queue.front().job) >= kSingleJobPixels;
+            while (!queue.empty() && b.size() < (single ? 1u : max_batch)) {
                 const Pending &p = queue.front();
+                if (!b.empty() && hcg::job_pixels(p.job) >= kSingleJobPixels) break;  // large jobs run alone
                 if (in_use + p.bytes > budget && !(in_use == 0 && b.empty())) break;
                 in_use += p.bytes;
                 b.push_back(p);
@@ -129,6 +156,7 @@ struct hcg_server {
                 continue;
             }
             lane_busy[li] = true;
+            lane_single[li] = single;
             lane_batch[li] = std::move(b);
             cv_work.notify_all();
         }
@@ -157,6 +185,7 @@ hcg_status hcg_server_create(hcg_context *ctx, int device, uint32_t lanes, uint6
     }
     s->lane_busy.assign(lanes, false);
     s->lane_batch.resize(lanes);
+    s->lane_single.assign(lanes, 0);
     for (uint32_t i = 0; i < lanes; ++i) s->workers.emplace_back([s, i] { s->worker(i); });
     s->dispatcher = std::thread([s] { s->dispatch(); });
     *out = s;
@@ -229,6 +258,7 @@ hcg_status hcg_server_destroy(hcg_server *s) {
     s->dispatcher.join();
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        s->workers_stop = true;
         s->cv_work.notify_all();
     }
     for (auto &w : s->workers) w.join();

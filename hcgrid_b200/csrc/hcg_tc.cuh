@@ -402,6 +402,8 @@ __device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchun
 template <class Cfg, class SH>
 __device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, uint32_t nchunks, uint32_t gk, int bt,
                                          unsigned long long *timeouts) {
+    const float wscale = J.wscale;  // kernel-parameter scalars held in registers for the loops below
+    const uint32_t fmt = J.fmt;
     using namespace sm100;
     constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
     const TcStage<Cfg> st{tc_smem_base()};
@@ -476,9 +478,9 @@ __device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, u
             const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const float w = wv[q] * J.wscale;
-                const uint16_t h = tc_to16(w, J.fmt);
-                const uint16_t l = tc_to16(w - tc_from16(h, J.fmt), J.fmt);
+                const float w = wv[q] * wscale;
+                const uint16_t h = tc_to16(w, fmt);
+                const uint16_t l = tc_to16(w - tc_from16(h, fmt), fmt);
                 const uint32_t o = tc_a_offset<KC>(mrow[q], col);
                 *(uint16_t *)(ah + o) = h;
                 *(uint16_t *)(al + o) = l;
@@ -853,6 +855,11 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     const PixHalf ph = pix_half(P);
     const int r0 = T.r0[tile];
     const uint32_t nrows = J.nrows;
+    // kernel-parameter scalars held in registers for the slot loop
+    const double hlo = a.hlo, hhi = a.hhi, p0 = a.p0, cb1 = P.cb1;
+    const bool series = a.series != 0;
+    const float wscale = J.wscale;
+    const uint32_t fmt = J.fmt;
     // geometry of chunk kk into buffer kk & 1 (threads 0..63, one slot each)
     auto load = [&](uint32_t kk) {
         if (bt < kTcGeo && kk < nchunks) {
@@ -913,8 +920,8 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                 wlo = whi = 0;
                 const int kr = r0 + j;
                 if (P.nr > 0 && kr >= P.ur && kr < P.ur + P.nr) {
-                    uint32_t lo, hi;
-                    if (ring_window_mc(a, a.rings[kr], P, lo, hi)) {
+                    uint32_t lo, hi, rl;
+                    if (ring_window_mc(a, a.rings[kr], P, lo, hi, rl)) {
                         wlo = lo;
                         whi = hi;
                     }
@@ -934,7 +941,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                 const double4 gq = S.g_half[b][q];
                 const double sb = ph.sb * gq.w - ph.cb * gq.z;  // sin((b1 - b2) / 2)
                 const double sl = ph.sl * gq.y - ph.cl * gq.x;  // sin((l1 - l2) / 2)
-                hh[e] = sb * sb + P.cb1 * S.g_cb[b][q] * (sl * sl);
+                hh[e] = sb * sb + cb1 * S.g_cb[b][q] * (sl * sl);
             }
             float wv[8];
             bool band = false;
@@ -942,7 +949,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
             for (int e = 0; e < 8; ++e) {
                 const double h = hh[e];
                 double d2;
-                if (a.series) {
+                if (series) {
                     const double t =
                         h * (1.0 + h * (1.0 / 3.0 + h * (8.0 / 45.0 + h * (4.0 / 35.0 + h * (128.0 / 1575.0)))));
                     d2 = 4.0 * t * (kRad2Deg * kRad2Deg);
@@ -950,9 +957,9 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                     const double d = 2.0 * asin(sqrt(h)) * kRad2Deg;
                     d2 = d * d;
                 }
-                const bool acc = inw[e] && h < a.hlo;
-                band |= inw[e] && h >= a.hlo && h <= a.hhi;
-                const double wt = acc ? S.g_w[b][s8 * 8 + e] * (double)expf((float)(-d2 * a.p0)) : 0.0;
+                const bool acc = inw[e] && h < hlo;
+                band |= inw[e] && h >= hlo && h <= hhi;
+                const double wt = acc ? S.g_w[b][s8 * 8 + e] * (double)expf((float)(-d2 * p0)) : 0.0;
                 wv[e] = 0.f;
                 if (wt > 0.0) {
                     wsum += wt;
@@ -963,7 +970,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
             if (band) {
 #pragma unroll
                 for (int e = 0; e < 8; ++e) {
-                    if (!(inw[e] && hh[e] >= a.hlo && hh[e] <= a.hhi)) continue;
+                    if (!(inw[e] && hh[e] >= hlo && hh[e] <= hhi)) continue;
                     const uint32_t q = s8 * 8 + e;
                     const double wt = pair_weight_s<true>(a, P, ph, S.g_half[b][q], S.g_cb[b][q], S.g_w[b][q],
                                                           culo + (slot0 + e - cbase));
@@ -977,9 +984,9 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
             uint32_t hv[4], lv[4];
 #pragma unroll
             for (int e = 0; e < 8; ++e) {
-                const float ws = wv[e] * J.wscale;
-                const uint16_t h = tc_to16(ws, J.fmt);
-                const uint16_t l = tc_to16(ws - tc_from16(h, J.fmt), J.fmt);
+                const float ws = wv[e] * wscale;
+                const uint16_t h = tc_to16(ws, fmt);
+                const uint16_t l = tc_to16(ws - tc_from16(h, fmt), fmt);
                 if (e & 1) {
                     hv[e >> 1] |= (uint32_t)h << 16;
                     lv[e >> 1] |= (uint32_t)l << 16;
@@ -1000,23 +1007,8 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     if (!failed && il >= 2 && !mbar_wait(&S.ws_empty[a2], ((il >> 1) - 1) & 1, kTcWaitNs)) tc_give_up(S, timeouts);
     S.wsum[a2][m] = valid ? wsum : 0.0;
     mbar_arrive(&S.ws_full[a2]);
-    if (cblk == 0 && valid) {
-        // statistics: the pixel's pairs and the candidates the reference visits on its rings
-        unsigned long long cand = 0, skips = 0;
-        for (int kr = P.ur; kr < P.ur + P.nr; ++kr) {
-            const RingRec &R = a.rings[kr];
-            uint32_t lo, hi;
-            if (!ring_window_mc(a, R, P, lo, hi)) {
-                ++skips;
-            } else {
-                cand += hi - lo;
-                if (P.polar) cand += polar_extra(R, lo, hi);
-            }
-        }
-        if (cand) atomicAdd(&a.stats->pairs_candidate, cand);
-        if (within) atomicAdd(&a.stats->pairs_within, within);
-        if (skips) atomicAdd(&a.stats->ring_skips, skips);
-    }
+    // the pixel's accepted pairs (candidates and skipped rings are counted by the tile pass)
+    if (cblk == 0 && within) atomicAdd(&a.stats->pairs_within, within);
 }
 
 // Persistent direct-weight kernel body: roles as in tc_persist, the builders

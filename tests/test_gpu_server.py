@@ -74,3 +74,41 @@ def test_served_tensor_core_jobs_equal_single_calls(ctx):
         ref_cube, ref_w = ctx.grid(f, t)
         np.testing.assert_array_equal(cube.cpu().numpy(), ref_cube.reshape(-1))
         np.testing.assert_array_equal(w.cpu().numpy(), ref_w)
+
+
+def test_large_jobs_run_alone_and_errors_do_not_stall_the_server(ctx):
+    """A job whose target has at least 2^20 pixels runs alone on a lane
+    (hcg_grid path, on a lane context that was never prepared) beside batches
+    of small jobs; its cube equals the single call's. A failing job reports
+    its error, and closing the server with jobs still queued returns once
+    they are done."""
+    big = dict(block=9, n=40_000, size_deg=1.0, ra=80.0, dec=10.0, grid=1024, nchan=4, fwhm=180.0, seed=29)
+    jobs = [make(ctx, s) for s in [big] + SHAPES]
+    ctx.synchronize()
+    bad_field = ctx.field(jobs[1][0].lon, jobs[1][0].lat)  # no spectra
+    srv = api.Server(ctx, lanes=2, hbm_budget=1 << 32, max_batch=4)
+    try:
+        outs, tickets = [], []
+        for job, f, t in jobs:
+            P = t.nx * t.ny
+            cube = torch.full((P * job.nchan,), float("inf"), device="cuda")
+            w = torch.full((P,), float("inf"), device="cuda")
+            tickets.append(srv.submit(f, t, cube, w, footprint=4 * P * (job.nchan + 1)))
+            outs.append((job, f, t, cube, w))
+        for tk in tickets:
+            srv.wait(tk)
+        P1 = jobs[1][2].nx * jobs[1][2].ny
+        bad = srv.submit(bad_field, jobs[1][2], torch.empty(P1, device="cuda"), None, footprint=4 * P1)
+        with pytest.raises(RuntimeError):
+            srv.wait(bad)
+        # queued work at close: the lanes finish it before the server goes
+        for job, f, t in jobs[1:]:
+            P = t.nx * t.ny
+            srv.submit(f, t, torch.empty(P * job.nchan, device="cuda"), None, footprint=4 * P)
+    finally:
+        srv.close()
+    bad_field.close()
+    for job, f, t, cube, w in outs:
+        ref_cube, ref_w = ctx.grid(f, t)
+        np.testing.assert_array_equal(cube.cpu().numpy(), ref_cube.reshape(-1))
+        np.testing.assert_array_equal(w.cpu().numpy(), ref_w)

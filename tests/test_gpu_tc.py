@@ -220,23 +220,26 @@ def test_tc_weight_modes_deterministic_and_checked(ctx, dense):
 def test_tc_direct_weights_channel_blocks(ctx, nchan):
     """Direct weights with one 64-channel block (64-channel items) and with
     300 channels (256-channel items, the second partly past the last channel),
-    against the FP32 engine."""
+    against the FP64 oracle."""
     shape = dict(block=0, n=20_000, size_deg=0.3, ra=150.0, dec=20.0, grid=64, nchan=nchan, fwhm=180.0, seed=6)
     job = synth.block_job(shape)
     prepare(ctx, job)
     f = ctx.field(job.lon, job.lat)
     f.set_spectra(job.values)
     t = ctx.target_from_header(job.header)
-    c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+    xw, yw = t.coords()
     f.split_spectra(api.ENGINE_TC_F16)
     ctx.tc_set_weights(api.TC_WEIGHTS_DIRECT)
     try:
         ct, wt = ctx.grid(f, t, engine=api.ENGINE_TC_F16)
     finally:
         ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
-    ok = w32 > 0
-    assert np.abs(wt[ok] - w32[ok]).max() / w32.max() <= 1e-6
-    assert plane_errors(ct, c32.astype(np.float64)) <= 1e-5
+    g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    ps = O.presort(g.hpx, job.lon, job.lat)
+    oc, ow, _ = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], job.values[ps.perm].astype(np.float64), xw, yw)
+    ok = ow > 0
+    assert np.abs(wt[ok] - ow[ok]).max() / ow.max() <= 1e-6
+    assert plane_errors(ct, oc / ow[:, None]) <= TOL[api.ENGINE_TC_F16]
     f.close()
     t.close()
 
