@@ -574,8 +574,9 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
     uint32_t nrouted = 0;
     for (uint32_t i = 0; i < njobs; ++i) {
         if ((B.h_jovf[i] && jobs[i].field->nchan > 1) ||
-            (J[i].tc.nb && (tc_use_weights(ctx, B.h_jusum[2 * i], B.h_jent[i]) ||
-                            B.h_jusum[2 * i + 1] > kTcOneSegmentSlots))) {
+            (J[i].tc.nb &&
+             (tc_use_weights(ctx, B.h_jusum[2 * i], B.h_jent[i], (unsigned long long)J[i].T.ntx * J[i].T.nty) ||
+              B.h_jusum[2 * i + 1] > kTcOneSegmentSlots))) {
             fallback[i] = 1;
             ++nrouted;
         } else {

@@ -238,7 +238,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             return cudaErrorInvalidValue;
         }
         const uint32_t ostride = layout == HCG_LAYOUT_CHANNEL_MAJOR ? 0 : f->nchan;  // 0: [channel][pixel]
-        if (tc && tiled && tc_use_weights(ctx, ro[T.nty + 2], ro[T.nty])) {
+        if (tc && tiled && tc_use_weights(ctx, ro[T.nty + 2], ro[T.nty], ntiles)) {
             // dense tiles: the tensor-core kernel evaluates the weights itself (no entries)
             cudaEventRecord(ctx->evp[2], s);
             if ((e = tc_weights(ctx, f, a, g, T, ntiles, d_cube, ostride, d_wts, why)) != cudaSuccess) return e;

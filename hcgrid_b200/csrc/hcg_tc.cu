@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(kTcPersistThreads, 1)
 }
 
 template <class Cfg>
-__global__ void __launch_bounds__(kTcPersistThreads, 1)
+__global__ void __launch_bounds__(kTcDThreads, 1)
     k_tile_tc_weights(const __grid_constant__ CUtensorMap tm, TcJob J, uint64_t nitems, uint64_t ntiles,
                       unsigned long long *timeouts, unsigned long long *macs) {
     __shared__ TcDShared S;
@@ -343,7 +343,7 @@ cudaError_t launch_tc_weights(hcg_context *ctx, const hcg_field *f, TcJob &J, co
     const uint64_t nitems = ntiles * J.ncb;
     const unsigned grid = (unsigned)std::min<uint64_t>(nitems, (uint64_t)(nsm > 0 ? nsm : 148));
     if (grid == 0) return cudaSuccess;
-    k_tile_tc_weights<Cfg><<<grid, kTcPersistThreads, Cfg::kSmem, s>>>(tm, J, nitems, ntiles,
+    k_tile_tc_weights<Cfg><<<grid, kTcDThreads, Cfg::kSmem, s>>>(tm, J, nitems, ntiles,
                                                                       &ctx->d_stats->timeouts, &ctx->d_stats->tc_macs);
     return cudaGetLastError();
 }

@@ -668,7 +668,7 @@ __device__ __forceinline__ void tc_epilogue_direct(SH &S, const TcJob &J, uint64
             if constexpr (WSMEM) {
                 // the builders' FP64 weight sums of this item (shared memory, by item parity)
                 if (!mbar_wait(&S.ws_full[ia], (il >> 1) & 1, kTcWaitNs)) tc_give_up(S, timeouts);
-                ws = S.wsum[ia][m];
+                ws = (S.wsum[ia][0][m] + S.wsum[ia][1][m]) + S.wsum[ia][2][m];
                 mbar_arrive(&S.ws_empty[ia]);
             } else {
                 ws = valid ? J.wsum[p] : 0.0;
@@ -805,15 +805,20 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
 // tile's pixels, e.g. beams many pixels wide): the builders evaluate the
 // weights of the chunk's slots for their own pixel from the samples'
 // geometry, so no entries are written or read and no FP64 weight pass runs
-// before. Builder thread bt owns operand row m = bt (pixel (m % 16, m / 16)
-// of the tile) and, per chunk: loads the geometry of 64 slots into shared
-// memory (cp.async, one chunk ahead), then for each slot whose sample lies in
-// its pixel's window of the slot's ring (ring_window_mc, the windows the
-// tile pass unioned) evaluates the FP64 distance, cutoff and FP32 Gaussian
-// (pair_weight_s, the entry path's weight), accumulates the FP64 weight sum
-// and writes the hi/lo row of the K-major operand in 16-byte pieces. The
-// epilogue takes the weight sums from shared memory.
-constexpr int kTcGeo = 64;  // slots per chunk of the direct builders
+// before. Twelve builder warps (latency hiding for the FP64 chains): thread
+// bt owns operand row m = bt % 128 (pixel (m % 16, m / 16) of the tile) and
+// the 8-slot pieces p = bt / 128 (mod 3) of each 64-slot chunk. Per chunk
+// the first 64 builders load the chunk's sample geometry into shared memory
+// (cp.async, one chunk ahead); then, for each slot whose sample lies in its
+// pixel's window of the slot's ring (ring_window_mc, the windows the tile pass
+// unioned), a builder evaluates the FP64 distance, cutoff and FP32 Gaussian
+// (pair_weight_s's arithmetic), accumulates the FP64 weight sum and writes its
+// hi/lo pieces of the K-major operand row (16-byte stores). The epilogue adds
+// the three partial weight sums of a row from shared memory.
+constexpr int kTcGeo = 64;          // slots per chunk of the direct builders
+constexpr int kTcDRow = 3;          // direct builders per operand row
+constexpr int kTcDBuilders = kTcDRow * kTcM;
+constexpr int kTcDThreads = 64 + kTcDBuilders + kTcBuilders;  // producer, MMA, builders, epilogue
 
 struct TcDShared {
     uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], zfill[kTcMaxStages];
@@ -823,7 +828,7 @@ struct TcDShared {
     uint32_t ulo[kTileMaxRings], base[kTileMaxRings + 1];    // the producer's current item
     uint32_t bulo[kTileMaxRings], bbase[kTileMaxRings + 1];  // the builders' current item
     float inv_scale[2][kTcMaxN];
-    double wsum[2][kTcM];
+    double wsum[2][kTcDRow][kTcM];  // by item parity: the builders' partial sums of each row
     double4 g_half[2][kTcGeo];
     double g_cb[2][kTcGeo], g_w[2][kTcGeo];
 };
@@ -840,13 +845,13 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     const GridArgs &a = J.a;
     const uint32_t a2 = il & 1;
     // the builders' copy of the tile's ring table (after every builder is done with the last one)
-    named_barrier(4, kTcBuilders);
+    named_barrier(4, kTcDBuilders);
     const int nrt = T.nr[tile];
-    for (int j = bt; j < nrt; j += kTcBuilders) S.bulo[j] = T.ulo[tile * kTileMaxRings + j];
-    for (int j = bt; j <= nrt; j += kTcBuilders) S.bbase[j] = T.base[tile * (kTileMaxRings + 1) + j];
-    named_barrier(4, kTcBuilders);
-    // this thread's pixel
-    const uint32_t m = (uint32_t)bt;
+    for (int j = bt; j < nrt; j += kTcDBuilders) S.bulo[j] = T.ulo[tile * kTileMaxRings + j];
+    for (int j = bt; j <= nrt; j += kTcDBuilders) S.bbase[j] = T.base[tile * (kTileMaxRings + 1) + j];
+    named_barrier(4, kTcDBuilders);
+    // this thread's pixel and pieces
+    const uint32_t m = (uint32_t)bt & (kTcM - 1), qb = (uint32_t)bt / kTcM;
     const uint32_t xx = (uint32_t)(tile % T.ntx) * kTileX + (m & (kTileX - 1));
     const uint32_t yy = (uint32_t)(tile / T.ntx) * kTileY + m / kTileX;
     const bool valid = xx < J.g.nx && yy < J.g.ny;
@@ -891,7 +896,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     bool failed = false;
     for (uint32_t k = 0; k < nchunks; ++k) {
         const uint32_t g = gk + k, s = g % ST;
-        named_barrier(4, kTcBuilders);  // every builder is done with chunk k - 1's geometry
+        named_barrier(4, kTcDBuilders);  // every builder is done with chunk k - 1's geometry
         load(k + 1);
         cp_async_wait<1>();  // this thread's copies of chunk k have landed
         bool bad = S.abort;
@@ -899,17 +904,17 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
             tc_give_up(S, timeouts);
             bad = true;
         }
-        if (named_barrier_or(4, kTcBuilders, bad)) {  // chunk k's geometry visible; the same exit in every builder
+        if (named_barrier_or(4, kTcDBuilders, bad)) {  // chunk k's geometry visible; the same exit in every builder
             failed = true;
             break;
         }
         const uint32_t b = k & 1;
         uint8_t *ah = st.A_hi(s), *al = st.A_lo(s);
-        for (uint32_t s8 = 0; s8 < KC / 8; ++s8) {
+        for (uint32_t s8 = qb; s8 < KC / 8; s8 += kTcDRow) {
             // ring runs take multiples of 8 slots: one ring per 8-slot piece
             const uint32_t slot0 = k * KC + s8 * 8;
             if (slot0 < U && (slot0 >= cnext || c < 0)) {
-                // next occupied ring (uniform across the builders) and this pixel's window there
+                // next occupied ring (the same in the builders of a piece) and this pixel's window there
                 while (c + 1 < nrt && S.bbase[c + 1] <= slot0) ++c;
                 cbase = S.bbase[c];
                 cnext = S.bbase[c + 1];
@@ -927,72 +932,72 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                     }
                 }
             }
-            // The 8 slots' pair tests as straight-line code (independent FP64
-            // chains the scheduler can interleave): haversines, then the weights
-            // of the pairs below the threshold band, the same arithmetic as
-            // pair_weight_s; pairs inside the band take pair_weight_s itself.
-            double hh[8];
-            bool inw[8];
+            // The piece's pair tests in two halves of 4 slots as straight-line
+            // code (independent FP64 chains the scheduler can interleave):
+            // haversines, then the weights of the pairs below the threshold
+            // band, the same arithmetic as pair_weight_s; pairs inside the band
+            // take pair_weight_s itself.
+            uint32_t hv[4], lv[4];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const uint32_t q = s8 * 8 + e;
-                const uint32_t idx = culo + (slot0 + e - cbase);
-                inw[e] = slot0 + e < U && idx >= wlo && idx < whi;
-                const double4 gq = S.g_half[b][q];
-                const double sb = ph.sb * gq.w - ph.cb * gq.z;  // sin((b1 - b2) / 2)
-                const double sl = ph.sl * gq.y - ph.cl * gq.x;  // sin((l1 - l2) / 2)
-                hh[e] = sb * sb + cb1 * S.g_cb[b][q] * (sl * sl);
-            }
-            float wv[8];
-            bool band = false;
+            for (int half = 0; half < 2; ++half) {
+                double hh[4];
+                bool inw[4];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const double h = hh[e];
-                double d2;
-                if (series) {
-                    const double t =
-                        h * (1.0 + h * (1.0 / 3.0 + h * (8.0 / 45.0 + h * (4.0 / 35.0 + h * (128.0 / 1575.0)))));
-                    d2 = 4.0 * t * (kRad2Deg * kRad2Deg);
-                } else {
-                    const double d = 2.0 * asin(sqrt(h)) * kRad2Deg;
-                    d2 = d * d;
+                for (int e = 0; e < 4; ++e) {
+                    const uint32_t q = s8 * 8 + half * 4 + e;
+                    const uint32_t idx = culo + (slot0 + half * 4 + e - cbase);
+                    inw[e] = slot0 + half * 4 + e < U && idx >= wlo && idx < whi;
+                    const double4 gq = S.g_half[b][q];
+                    const double sb = ph.sb * gq.w - ph.cb * gq.z;  // sin((b1 - b2) / 2)
+                    const double sl = ph.sl * gq.y - ph.cl * gq.x;  // sin((l1 - l2) / 2)
+                    hh[e] = sb * sb + cb1 * S.g_cb[b][q] * (sl * sl);
                 }
-                const bool acc = inw[e] && h < hlo;
-                band |= inw[e] && h >= hlo && h <= hhi;
-                const double wt = acc ? S.g_w[b][s8 * 8 + e] * (double)expf((float)(-d2 * p0)) : 0.0;
-                wv[e] = 0.f;
-                if (wt > 0.0) {
-                    wsum += wt;
-                    ++within;
-                    wv[e] = (float)wt;
-                }
-            }
-            if (band) {
+                float wv[4];
+                bool band = false;
 #pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    if (!(inw[e] && hh[e] >= hlo && hh[e] <= hhi)) continue;
-                    const uint32_t q = s8 * 8 + e;
-                    const double wt = pair_weight_s<true>(a, P, ph, S.g_half[b][q], S.g_cb[b][q], S.g_w[b][q],
-                                                          culo + (slot0 + e - cbase));
+                for (int e = 0; e < 4; ++e) {
+                    const double h = hh[e];
+                    double d2;
+                    if (series) {
+                        const double t =
+                            h * (1.0 + h * (1.0 / 3.0 + h * (8.0 / 45.0 + h * (4.0 / 35.0 + h * (128.0 / 1575.0)))));
+                        d2 = 4.0 * t * (kRad2Deg * kRad2Deg);
+                    } else {
+                        const double d = 2.0 * asin(sqrt(h)) * kRad2Deg;
+                        d2 = d * d;
+                    }
+                    const bool acc = inw[e] && h < hlo;
+                    band |= inw[e] && h >= hlo && h <= hhi;
+                    const double wt = acc ? S.g_w[b][s8 * 8 + half * 4 + e] * (double)gauss_f32(d2 * p0) : 0.0;
+                    wv[e] = 0.f;
                     if (wt > 0.0) {
                         wsum += wt;
                         ++within;
                         wv[e] = (float)wt;
                     }
                 }
-            }
-            uint32_t hv[4], lv[4];
+                if (band) {
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const float ws = wv[e] * wscale;
-                const uint16_t h = tc_to16(ws, fmt);
-                const uint16_t l = tc_to16(ws - tc_from16(h, fmt), fmt);
-                if (e & 1) {
-                    hv[e >> 1] |= (uint32_t)h << 16;
-                    lv[e >> 1] |= (uint32_t)l << 16;
-                } else {
-                    hv[e >> 1] = h;
-                    lv[e >> 1] = l;
+                    for (int e = 0; e < 4; ++e) {
+                        if (!(inw[e] && hh[e] >= hlo && hh[e] <= hhi)) continue;
+                        const uint32_t q = s8 * 8 + half * 4 + e;
+                        const double wt = pair_weight_s<true>(a, P, ph, S.g_half[b][q], S.g_cb[b][q], S.g_w[b][q],
+                                                              culo + (slot0 + half * 4 + e - cbase));
+                        if (wt > 0.0) {
+                            wsum += wt;
+                            ++within;
+                            wv[e] = (float)wt;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 4; e += 2) {
+                    const float w0 = wv[e] * wscale, w1 = wv[e + 1] * wscale;
+                    const uint16_t h0 = tc_to16(w0, fmt), h1 = tc_to16(w1, fmt);
+                    const uint16_t l0 = tc_to16(w0 - tc_from16(h0, fmt), fmt);
+                    const uint16_t l1 = tc_to16(w1 - tc_from16(h1, fmt), fmt);
+                    hv[half * 2 + e / 2] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+                    lv[half * 2 + e / 2] = (uint32_t)l0 | ((uint32_t)l1 << 16);
                 }
             }
             const uint32_t o = tc_a_offset<KC>(m, s8 * 8);
@@ -1005,10 +1010,11 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     cp_async_wait<0>();  // no geometry copy outlives the item
     // the pixel's FP64 weight sum for the epilogue (after it has read the sum two items back)
     if (!failed && il >= 2 && !mbar_wait(&S.ws_empty[a2], ((il >> 1) - 1) & 1, kTcWaitNs)) tc_give_up(S, timeouts);
-    S.wsum[a2][m] = valid ? wsum : 0.0;
+    S.wsum[a2][qb][m] = valid ? wsum : 0.0;
     mbar_arrive(&S.ws_full[a2]);
-    // the pixel's accepted pairs (candidates and skipped rings are counted by the tile pass)
-    if (cblk == 0 && within) atomicAdd(&a.stats->pairs_within, within);
+    // the accepted pairs (candidates and skipped rings are counted by the tile pass)
+    within = warp_sum_u64(within);
+    if (cblk == 0 && (bt & 31) == 0 && within) atomicAdd(&a.stats->pairs_within, within);
 }
 
 // Persistent direct-weight kernel body: roles as in tc_persist, the builders
@@ -1022,7 +1028,7 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         for (uint32_t s = 0; s < ST; ++s) {
-            mbar_init(&S.full_a[s], kTcBuilders);
+            mbar_init(&S.full_a[s], kTcDBuilders);
             mbar_init(&S.full_b[s], 1);
             mbar_init(&S.empty[s], 1);
             mbar_init(&S.zfill[s], 1);
@@ -1030,7 +1036,7 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
         for (int a = 0; a < 2; ++a) {
             mbar_init(&S.acc_full[a], 1);
             mbar_init(&S.acc_empty[a], kTcBuilders);
-            mbar_init(&S.ws_full[a], kTcBuilders);
+            mbar_init(&S.ws_full[a], kTcDBuilders);
             mbar_init(&S.ws_empty[a], kTcBuilders);
         }
         S.abort = 0;
@@ -1058,10 +1064,11 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
             tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
         } else if (warp == 1) {
             if (lane == 0) tc_mma_seg<Cfg>(S, J, nchunks, gk, gs, timeouts, macs);
-        } else if (warp < 6) {
+        } else if (tid < 64 + kTcDBuilders) {
             tc_build_weights<Cfg>(S, J, tile, cblk, U, nchunks, gk, il, tid - 64, timeouts);
         } else {
-            tc_epilogue_direct<TcDShared, true>(S, J, tile, cblk, nchunks, il, gse, tid - 192, timeouts);
+            tc_epilogue_direct<TcDShared, true>(S, J, tile, cblk, nchunks, il, gse, tid - (64 + kTcDBuilders),
+                                                timeouts);
         }
         gk += nchunks;
     }

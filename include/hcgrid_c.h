@@ -143,8 +143,10 @@ hcg_status hcg_field_split_spectra(hcg_field *field, int engine, int keep_fp32);
 hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config);
 
 /* How the tensor-core engines build the weight operand of a tile:
- *   HCG_TC_WEIGHTS_AUTO    (0): the library's choice (currently entries: the
- *                              faster of the two on every workload measured);
+ *   HCG_TC_WEIGHTS_AUTO    (0): per call, from the tile pass's counts: evaluated in
+ *                              the kernel for very dense tiles (at least 4096 staged
+ *                              samples per tile, dense evaluation at most 2.5x the
+ *                              weight pass's pairs), else entries;
  *   HCG_TC_WEIGHTS_ENTRIES (1): an FP64 weight pass writes entries (pixel-group,
  *                              sample, 4 weights) that the kernel scatters;
  *   HCG_TC_WEIGHTS_DIRECT  (2): the kernel's builder warps evaluate the FP64
