@@ -816,6 +816,7 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
 // hi/lo pieces of the K-major operand row (16-byte stores). The epilogue adds
 // the three partial weight sums of a row from shared memory.
 constexpr int kTcGeo = 64;          // slots per chunk of the direct builders
+constexpr int kTcGeoBufs = 2;       // geometry buffers: loads run one chunk ahead
 constexpr int kTcDRow = 3;          // direct builders per operand row
 constexpr int kTcDBuilders = kTcDRow * kTcM;
 constexpr int kTcDThreads = 64 + kTcDBuilders + kTcBuilders;  // producer, MMA, builders, epilogue
@@ -829,8 +830,8 @@ struct TcDShared {
     uint32_t bulo[kTileMaxRings], bbase[kTileMaxRings + 1];  // the builders' current item
     float inv_scale[2][kTcMaxN];
     double wsum[2][kTcDRow][kTcM];  // by item parity: the builders' partial sums of each row
-    double4 g_half[2][kTcGeo];
-    double g_cb[2][kTcGeo], g_w[2][kTcGeo];
+    double4 g_half[kTcGeoBufs][kTcGeo];  // sample geometry of the chunks in flight
+    double g_cb[kTcGeoBufs][kTcGeo], g_w[kTcGeoBufs][kTcGeo];
 };
 
 template <class Cfg>
@@ -850,8 +851,10 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     for (int j = bt; j < nrt; j += kTcDBuilders) S.bulo[j] = T.ulo[tile * kTileMaxRings + j];
     for (int j = bt; j <= nrt; j += kTcDBuilders) S.bbase[j] = T.base[tile * (kTileMaxRings + 1) + j];
     named_barrier(4, kTcDBuilders);
-    // this thread's pixel and pieces
+    // this thread's pixel and pieces; its 2x2 group and place there (the tile pass's kept windows)
     const uint32_t m = (uint32_t)bt & (kTcM - 1), qb = (uint32_t)bt / kTcM;
+    const uint32_t wgq = (m >> 5) * (kTileX / 2) + ((m & (kTileX - 1)) >> 1);
+    const uint32_t wq = (((m >> 4) & 1) << 1) | (m & 1);
     const uint32_t xx = (uint32_t)(tile % T.ntx) * kTileX + (m & (kTileX - 1));
     const uint32_t yy = (uint32_t)(tile / T.ntx) * kTileY + m / kTileX;
     const bool valid = xx < J.g.nx && yy < J.g.ny;
@@ -865,7 +868,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     const bool series = a.series != 0;
     const float wscale = J.wscale;
     const uint32_t fmt = J.fmt;
-    // geometry of chunk kk into buffer kk & 1 (threads 0..63, one slot each)
+    // geometry of chunk kk into buffer kk % kTcGeoBufs (threads 0..63, one slot each)
     auto load = [&](uint32_t kk) {
         if (bt < kTcGeo && kk < nchunks) {
             const uint32_t slot = kk * KC + bt;
@@ -878,7 +881,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                 }
                 idx = min(S.bulo[lo] + (slot - S.bbase[lo]), nrows - 1);
             }
-            const uint32_t b = kk & 1;
+            const uint32_t b = kk % kTcGeoBufs;
             cp_async16(&S.g_half[b][bt], a.half + idx, true);
             cp_async16(reinterpret_cast<uint8_t *>(&S.g_half[b][bt]) + 16,
                        reinterpret_cast<const uint8_t *>(a.half + idx) + 16, true);
@@ -908,7 +911,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
             failed = true;
             break;
         }
-        const uint32_t b = k & 1;
+        const uint32_t b = k % kTcGeoBufs;
         uint8_t *ah = st.A_hi(s), *al = st.A_lo(s);
         for (uint32_t s8 = qb; s8 < KC / 8; s8 += kTcDRow) {
             // ring runs take multiples of 8 slots: one ring per 8-slot piece
@@ -924,7 +927,16 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                 } while (j < kTileMaxSpan && T.ring_idx[tile * kTileMaxSpan + j] != (uint16_t)c);
                 wlo = whi = 0;
                 const int kr = r0 + j;
-                if (P.nr > 0 && kr >= P.ur && kr < P.ur + P.nr) {
+                if (T.win && j < kWinSpan) {
+                    // the window the tile pass kept for this pixel and ring (lo > hi: none)
+                    const uint32_t *w = reinterpret_cast<const uint32_t *>(
+                        T.win + ((tile * kWinSpan + (uint64_t)j) * kTileGroups + wgq) * 2);
+                    const uint32_t lo = __ldg(w + 2 * wq), hi = __ldg(w + 2 * wq + 1);
+                    if (lo <= hi) {
+                        wlo = lo;
+                        whi = hi;
+                    }
+                } else if (P.nr > 0 && kr >= P.ur && kr < P.ur + P.nr) {
                     uint32_t lo, hi, rl;
                     if (ring_window_mc(a, a.rings[kr], P, lo, hi, rl)) {
                         wlo = lo;
