@@ -156,16 +156,16 @@ inline int auto_engine(const hcg_field *f) {
 }
 // Tensor-core weight operand: evaluated in the kernel (HCG_TC_WEIGHTS_DIRECT)
 // or written as entries by the FP64 weight pass. Automatic mode evaluates in
-// the kernel for very dense tiles: at least 4096 staged samples per tile on
-// average (beams many pixels wide over dense sampling), where the kernel's
-// 128 x U pair tests are at most 2.5x the weight pass's (usum: staged slots of
-// all `ntiles` tiles; cap_total: union candidates of all 2x2 groups, each for
-// up to 4 pixels). Measured on B200, the entries are faster below that.
+// the kernel for dense tiles: at least 1024 staged samples per tile on average
+// (beams many pixels wide over dense sampling), where the kernel's 128 x U pair
+// tests are at most 2.5x the weight pass's (usum: staged slots of all `ntiles`
+// tiles; cap_total: union candidates of all 2x2 groups, each for up to 4
+// pixels). Measured on B200, the entries are faster below that.
 inline bool tc_use_weights(const hcg_context *ctx, unsigned long long usum, unsigned long long cap_total,
                            unsigned long long ntiles) {
     if (ctx->tc_weights == HCG_TC_WEIGHTS_ENTRIES) return false;
     if (ctx->tc_weights == HCG_TC_WEIGHTS_DIRECT) return true;
-    return usum >= 4096ull * ntiles && 128.0 * (double)usum <= 2.5 * 4.0 * (double)cap_total;
+    return usum >= 1024ull * ntiles && 128.0 * (double)usum <= 2.5 * 4.0 * (double)cap_total;
 }
 cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, const double *d_lat,
                         const double *d_w, std::string &why);

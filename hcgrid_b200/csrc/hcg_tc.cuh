@@ -866,6 +866,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     // kernel-parameter scalars held in registers for the slot loop
     const double hlo = a.hlo, hhi = a.hhi, p0 = a.p0, cb1 = P.cb1;
     const bool series = a.series != 0;
+    const float x2scale = a.x2scale;
     const float wscale = J.wscale;
     const uint32_t fmt = J.fmt;
     // geometry of chunk kk into buffer kk % kTcGeoBufs (threads 0..63, one slot each)
@@ -895,7 +896,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     int c = -1, j = -1;
     uint32_t cbase = 0, cnext = 0, culo = 0, wlo = 0, whi = 0;
     double wsum = 0.0;
-    unsigned long long within = 0;
+    uint32_t within = 0;
     bool failed = false;
     for (uint32_t k = 0; k < nchunks; ++k) {
         const uint32_t g = gk + k, s = g % ST;
@@ -969,18 +970,17 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const double h = hh[e];
-                    double d2;
+                    // the Gaussian of an accepted pair, as pair_weight_s evaluates it
+                    float ex;
                     if (series) {
-                        const double t =
-                            h * (1.0 + h * (1.0 / 3.0 + h * (8.0 / 45.0 + h * (4.0 / 35.0 + h * (128.0 / 1575.0)))));
-                        d2 = 4.0 * t * (kRad2Deg * kRad2Deg);
+                        ex = gauss_series_f32(h, x2scale);
                     } else {
                         const double d = 2.0 * asin(sqrt(h)) * kRad2Deg;
-                        d2 = d * d;
+                        ex = gauss_f32(d * d * p0);
                     }
                     const bool acc = inw[e] && h < hlo;
                     band |= inw[e] && h >= hlo && h <= hhi;
-                    const double wt = acc ? S.g_w[b][s8 * 8 + half * 4 + e] * (double)gauss_f32(d2 * p0) : 0.0;
+                    const double wt = acc ? S.g_w[b][s8 * 8 + half * 4 + e] * (double)ex : 0.0;
                     wv[e] = 0.f;
                     if (wt > 0.0) {
                         wsum += wt;
@@ -1025,8 +1025,8 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
     S.wsum[a2][qb][m] = valid ? wsum : 0.0;
     mbar_arrive(&S.ws_full[a2]);
     // the accepted pairs (candidates and skipped rings are counted by the tile pass)
-    within = warp_sum_u64(within);
-    if (cblk == 0 && (bt & 31) == 0 && within) atomicAdd(&a.stats->pairs_within, within);
+    const unsigned long long wsum_pairs = warp_sum_u64(within);
+    if (cblk == 0 && (bt & 31) == 0 && wsum_pairs) atomicAdd(&a.stats->pairs_within, wsum_pairs);
 }
 
 // Persistent direct-weight kernel body: roles as in tc_persist, the builders

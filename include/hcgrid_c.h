@@ -144,7 +144,7 @@ hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config);
 
 /* How the tensor-core engines build the weight operand of a tile:
  *   HCG_TC_WEIGHTS_AUTO    (0): per call, from the tile pass's counts: evaluated in
- *                              the kernel for very dense tiles (at least 4096 staged
+ *                              the kernel for dense tiles (at least 1024 staged
  *                              samples per tile, dense evaluation at most 2.5x the
  *                              weight pass's pairs), else entries;
  *   HCG_TC_WEIGHTS_ENTRIES (1): an FP64 weight pass writes entries (pixel-group,
