@@ -2,7 +2,7 @@
 """Benchmark of the B200 gridder on the reference's headline workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload config2|config1]
+                    [--workload config2|config1|config5] [--served-jobs J]
 
 A step is one gridding pass (hcg_grid: pixel setup, candidate selection,
 FP64 weights, channel sums, normalisation) over the resident field of the
@@ -12,6 +12,11 @@ hcgrid_b200/synth.py). `value` is gridded sample-channels/s with inputs
 resident in HBM; `e2e` repeats the metric through the C ABI from host
 buffers (field creation with the on-device sort, spectra upload, gridding,
 cube download). Inputs are larger than L2 (16 GB of spectra), so no flush.
+
+At N=1 the config-2 line also carries `served_config5`: the served form
+(config 5, a stream of J gridding requests through hcg_server, timed against
+the plain FP32 engine and the tensor-core engine per call on the same
+requests; `--workload config5` prints its full record).
 
 Multi-GPU (torchrun): every rank grids its own copy of the job (weak
 scaling, no collective on the data path); timings are the max over ranks.
@@ -53,6 +58,9 @@ def parse():
     ap.add_argument("--jobs", type=int, default=200, help="config5: requests in the stream (the full form has 2000)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
     ap.add_argument("--detail", default=None, help="config5: write per-request times of the per-call arms here")
+    ap.add_argument("--served-jobs", type=int, default=200,
+                    help="config2 at N=1: also run the served form (config5) on this many requests and report it "
+                         "under 'served_config5' (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--engine", default="tc-f16", choices=list(ENGINES),
@@ -324,6 +332,10 @@ def device_block_spectra(lon_d, lat_d, shape, nchan, seed, torch, dev):
 
 
 def served_main(args):
+    print(json.dumps(served_run(args)))
+
+
+def served_run(args):
     """Config 5: a stream of gridding requests with config-4 shapes (seed 3),
     30% of them re-gridding an earlier request's field with new spectra.
     Fields (sorted samples, ring LUT) and targets stay resident; each request
@@ -498,11 +510,11 @@ def served_main(args):
     if args.detail:
         with open(args.detail, "w") as fh:
             json.dump(detail, fh)
-    print(json.dumps(out))
     for f, t, _, _ in base.values():
         f.close()
         t.close()
     ctx.close()
+    return out
 
 
 def main():
@@ -516,6 +528,22 @@ def main():
     world, rank, local = dist_setup(args)
     job = job_for(args)
     P = job.nx * job.ny
+    served = None
+    if args.impl == "ours" and world == 1 and args.workload == "config2" and args.served_jobs > 0:
+        # the served form (config 5) before the config-2 field takes its memory
+        import torch
+        sargs = argparse.Namespace(**vars(args))
+        sargs.jobs, sargs.detail = args.served_jobs, None
+        try:
+            s = served_run(sargs)
+            served = {"value": s["value"], "unit": UNIT, "requests": s["steps"],
+                      "served_over_plain": s["served_over_plain"], "plain_per_call": s["plain"]["value"],
+                      "tc_per_call": s["tc_per_call"]["value"], "p50_s": s["served"]["p50_s"],
+                      "p99_s": s["served"]["p99_s"], "load": "Poisson arrivals at 80% of closed-loop capacity",
+                      "workload": s["config"]["workload"]}
+        except Exception as ex:  # reported, not fatal
+            served = {"value": None, "error": repr(ex)}
+        torch.cuda.empty_cache()
     if args.impl == "reference":
         if rank == 0:
             vals = []
@@ -669,12 +697,20 @@ def main():
     if tc and dom == 3:
         tpk, tkind = tensor_peak()
         tflops = 2.0 * st.tc_macs / (avg[3] * 1e-3) / 1e12
-        roofline["tensor"] = {"achieved": round(tflops, 1), "peak": tpk, "unit": "TFLOP/s",
-                              "frac": round(tflops / tpk, 4), "issued_macs": int(st.tc_macs),
-                              "useful_macs": int(st.pairs_within) * job.nchan,
-                              "peak_source": tkind + " (MEASURED_PEAKS.json bf16_tflops, burst)"}
+        useful = int(st.pairs_within) * job.nchan
+        tensor = {"achieved": round(tflops, 1), "peak": tpk, "unit": "TFLOP/s", "frac": round(tflops / tpk, 4),
+                  "issued_macs": int(st.tc_macs), "useful_macs": useful,
+                  "useful_tflops_x3": round(2.0 * 3 * useful / (avg[3] * 1e-3) / 1e12, 1),
+                  "peak_source": tkind + " (MEASURED_PEAKS.json bf16_tflops, burst)",
+                  "counts": "issued: the dense tile products the pipe executes (3 per MAC of the compensated "
+                            "split); useful: accepted pairs x channels"}
         if tflops / tpk > roofline["frac"]:
-            roofline["bound"] = "tensor"
+            # the tensor pipe is the binding resource: its figures lead, HBM's are kept beside
+            hbm = {k: roofline.pop(k) for k in ("achieved", "peak", "unit", "frac", "peak_source")}
+            roofline.pop("bound")
+            roofline = {"bound": "tensor", "kernel": roofline.pop("kernel"), **tensor, "hbm": hbm, **roofline}
+        else:
+            roofline["tensor"] = tensor
 
     # end to end through the C ABI from host buffers
     e2e = None
@@ -729,7 +765,8 @@ def main():
                           "tc_pipeline": tune},
                "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,
                "e2e": e2e, "cpu_baseline": cpu, "plain_fp32": plain,
-               "over_plain_fp32": round(value / plain["value"], 3) if plain else None}
+               "over_plain_fp32": round(value / plain["value"], 3) if plain else None,
+               "served_config5": served}
         print(json.dumps(out))
     field.close()
     target.close()
