@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--jobs", type=int, default=200, help="config5: requests in the stream (the full form has 2000)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
     ap.add_argument("--detail", default=None, help="config5: write per-request times of the per-call arms here")
+    ap.add_argument("--tc-weights", default="auto", choices=["auto", "entries", "direct"],
+                    help="tensor-core weight operands (hcg_tc_set_weights)")
     ap.add_argument("--served-jobs", type=int, default=200,
                     help="config2 at N=1: also run the served form (config5) on this many requests and report it "
                          "under 'served_config5' (0: skip)")
@@ -605,6 +607,8 @@ def main():
 
     tune = None
     if engine != api.ENGINE_FP32 and job.nchan > 1:
+        ctx.tc_set_weights({"auto": api.TC_WEIGHTS_AUTO, "entries": api.TC_WEIGHTS_ENTRIES,
+                            "direct": api.TC_WEIGHTS_DIRECT}[args.tc_weights])
         if args.tc_config is not None:
             ctx.tc_set_config(args.tc_config)
             tune = {"config": args.tc_config, "how": "fixed by --tc-config"}
@@ -762,7 +766,7 @@ def main():
                           "parallelism": "replica per GPU" if world > 1 else "single GPU",
                           "l2": "inputs larger than L2 (spectra %.1f GB), no flush" % (4 * job.n * job.nchan / 1e9),
                           "engine": ENGINE_TEXT[args.engine] if job.nchan > 1 else ENGINE_TEXT["fp32"],
-                          "tc_pipeline": tune},
+                          "tc_pipeline": tune, "tc_weights": args.tc_weights},
                "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,
                "e2e": e2e, "cpu_baseline": cpu, "plain_fp32": plain,
                "over_plain_fp32": round(value / plain["value"], 3) if plain else None,

@@ -151,6 +151,25 @@ __device__ __forceinline__ float tc_from16(uint16_t b, uint32_t fmt) {
     return fmt ? __bfloat162float(__ushort_as_bfloat16(b)) : __half2float(__ushort_as_half(b));
 }
 
+// hi/lo split of two weights at once (paired conversions): `hi` and `lo` hold
+// the 16-bit values of a (low half) and b (high half), the same values as
+// tc_to16 of each and of its remainder.
+__device__ __forceinline__ void tc_split2(float a, float b, uint32_t fmt, uint32_t &hi, uint32_t &lo) {
+    if (fmt) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        const float2 f = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(a - f.x, b - f.y);
+        hi = *reinterpret_cast<const uint32_t *>(&h);
+        lo = *reinterpret_cast<const uint32_t *>(&l);
+    } else {
+        const __half2 h = __floats2half2_rn(a, b);
+        const float2 f = __half22float2(h);
+        const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
+        hi = *reinterpret_cast<const uint32_t *>(&h);
+        lo = *reinterpret_cast<const uint32_t *>(&l);
+    }
+}
+
 // byte offset of element (row m, column k) of a K-major 128-row x KC-column
 // 16-bit operand in swizzled 8-row atoms (the 16-byte chunk index is XORed
 // with address bits 7-9 for the 128-byte swizzle, 7-8 for the 64-byte one)
@@ -1003,14 +1022,8 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                     }
                 }
 #pragma unroll
-                for (int e = 0; e < 4; e += 2) {
-                    const float w0 = wv[e] * wscale, w1 = wv[e + 1] * wscale;
-                    const uint16_t h0 = tc_to16(w0, fmt), h1 = tc_to16(w1, fmt);
-                    const uint16_t l0 = tc_to16(w0 - tc_from16(h0, fmt), fmt);
-                    const uint16_t l1 = tc_to16(w1 - tc_from16(h1, fmt), fmt);
-                    hv[half * 2 + e / 2] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-                    lv[half * 2 + e / 2] = (uint32_t)l0 | ((uint32_t)l1 << 16);
-                }
+                for (int e = 0; e < 4; e += 2)
+                    tc_split2(wv[e] * wscale, wv[e + 1] * wscale, fmt, hv[half * 2 + e / 2], lv[half * 2 + e / 2]);
             }
             const uint32_t o = tc_a_offset<KC>(m, s8 * 8);
             *reinterpret_cast<uint4 *>(ah + o) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
