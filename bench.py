@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config5"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config3", "config5"])
     ap.add_argument("--jobs", type=int, default=200, help="config5: requests in the stream (the full form has 2000)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
     ap.add_argument("--detail", default=None, help="config5: write per-request times of the per-call arms here")
@@ -65,8 +65,9 @@ def parse():
                          "under 'served_config5' (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--engine", default="tc-f16", choices=list(ENGINES),
-                    help="channel-sum engine: tensor cores with a 16-bit hi/lo split, or FP32 CUDA cores")
+    ap.add_argument("--engine", default=None, choices=list(ENGINES),
+                    help="channel-sum engine: tensor cores with a 16-bit hi/lo split, or FP32 CUDA cores "
+                         "(default: tc-bf16 for config3, tc-f16 otherwise)")
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="also time this many steps of the plain FP32 engine on the same field (0: skip)")
     ap.add_argument("--tc-config", type=int, default=None,
@@ -78,7 +79,12 @@ def parse():
     ap.add_argument("--channels", type=int, default=None)
     ap.add_argument("--pixels-x", type=int, default=None)
     ap.add_argument("--field-deg", type=float, default=None)
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.engine is None:
+        args.engine = "tc-bf16" if args.workload == "config3" else "tc-f16"
+    if args.workload == "config3" and "--e2e-steps" not in sys.argv:
+        args.e2e_steps = 0  # 65 GB of host spectra: the e2e leg is the config-2 line's
+    return args
 
 
 ENGINES = {"fp32": 1, "tc-f16": 3, "tc-bf16": 2}
@@ -120,11 +126,16 @@ def job_for(args):
         kw["nx"] = args.pixels_x
     if args.workload == "config1":
         return synth.config1(**kw)
+    if args.workload == "config3":
+        kw["nchan"] = 4096  # the precision form: config-2 geometry, 4,096 channels
     if args.channels:
         kw["nchan"] = args.channels
     if args.field_deg:
         kw["size_deg"] = args.field_deg
-    return synth.config2(**kw)
+    job = synth.config2(**kw)
+    if args.workload == "config3":
+        job.name = "config3"
+    return job
 
 
 def algorithmic_bytes(n, c, p):
@@ -589,16 +600,18 @@ def main():
     engine = ENGINES[args.engine]
     field = ctx.field(lon_d, lat_d)
     field.set_spectra(S)
-    plain_steps = args.plain_steps if (engine != api.ENGINE_FP32 and job.nchan > 1) else 0
-    if engine != api.ENGINE_FP32 and job.nchan > 1:
-        field.split_spectra(engine, keep_fp32=plain_steps > 0)
-    target = ctx.target_from_header(job.header)
     ctx.synchronize()
     S_host = None
     if args.e2e_steps > 0:
         S_host = torch.empty((job.n, job.nchan), dtype=torch.float32, pin_memory=True)
         S_host.copy_(S)
-    del S
+    del S  # the field holds its own (sorted) copy
+    torch.cuda.empty_cache()
+    plain_steps = args.plain_steps if (engine != api.ENGINE_FP32 and job.nchan > 1) else 0
+    if engine != api.ENGINE_FP32 and job.nchan > 1:
+        field.split_spectra(engine, keep_fp32=plain_steps > 0)
+    target = ctx.target_from_header(job.header)
+    ctx.synchronize()
     torch.cuda.empty_cache()
     cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
     wts = torch.empty(P, dtype=torch.float32, device=dev)

@@ -323,3 +323,56 @@ def test_coarse_pixels_many_rings(ctx):
     ct, wt = ctx.grid(f, t)
     np.testing.assert_array_equal(wt, w32)
     assert plane_errors(ct, c32.astype(np.float64)) <= 1e-5
+
+
+def test_config3_precision_subcube(ctx):
+    """The precision form (config 3) at reduced size: the config-2 generator
+    (same sample density, 60" pixels) with 4,096 channels, BF16 hi/lo
+    spectra with per-channel scales; the relative error of a 256 x 256 x 64
+    sub-cube (central pixels, 64 channels across the band) against the FP64
+    oracle stays within the BF16 tolerance, and the FP16 split within 1e-5."""
+    torch = pytest.importorskip("torch")
+    job = synth.config2(n=600_000, nchan=4096, nx=464, size_deg=7.75)
+    prepare(ctx, job)
+    G, L, noise = job.factors
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(job.seed)
+    S = torch.empty((job.n, job.nchan), dtype=torch.float32, device=dev)
+    Ld = torch.from_numpy(L).to(dev)
+    for i in range(0, job.n, 1 << 17):
+        Gd = torch.from_numpy(G[i:i + (1 << 17)]).to(dev)
+        torch.matmul(Gd, Ld, out=S[i:i + (1 << 17)])
+        S[i:i + (1 << 17)].add_(torch.randn((Gd.shape[0], job.nchan), generator=gen, device=dev), alpha=noise)
+    chans = np.linspace(0, job.nchan - 1, 64).round().astype(np.int64)
+    vals = S[:, torch.from_numpy(chans).to(dev)].double().cpu().numpy()
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(S)
+    del S
+    t = ctx.target_from_header(job.header)
+    xw, yw = t.coords()
+    y0 = x0 = (464 - 256) // 2
+    sub = (np.arange(256)[:, None] + y0) * 464 + (np.arange(256)[None, :] + x0)
+    sub = sub.reshape(-1)
+    g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    ps = O.presort(g.hpx, job.lon, job.lat)
+    oc, ow, _ = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm], xw[sub], yw[sub])
+    ref = oc / ow[:, None]
+    P = 464 * 464
+    errs = {}
+    for engine in (api.ENGINE_TC_BF16, api.ENGINE_TC_F16):
+        f.split_spectra(engine)
+        cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
+        w = torch.empty(P, dtype=torch.float32, device=dev)
+        ctx.grid(f, t, cube, w, engine=engine)
+        got = cube[torch.from_numpy(sub).to(dev)][:, torch.from_numpy(chans).to(dev)].cpu().numpy()
+        errs[engine] = plane_errors(got, ref)
+        ok = ow > 0
+        assert np.abs(w[torch.from_numpy(sub).to(dev)].cpu().numpy()[ok] - ow[ok]).max() / ow.max() <= 1e-6
+        del cube
+    print("config-3 sub-cube max plane-relative error: bf16 %.3e, f16 %.3e"
+          % (errs[api.ENGINE_TC_BF16], errs[api.ENGINE_TC_F16]))
+    assert errs[api.ENGINE_TC_BF16] <= TOL[api.ENGINE_TC_BF16]
+    assert errs[api.ENGINE_TC_F16] <= TOL[api.ENGINE_TC_F16]
+    f.close()
+    t.close()
