@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
 using KbTcCfg = TcCfgN4K32;  // the batch kernel's pipeline shape
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    kb_tc(BatchHdr *H, const JobDesc *__restrict__ jobs, const void *zero_page, unsigned long long *timeouts,
+    kb_tc(BatchHdr *H, const JobDesc *__restrict__ jobs, unsigned long long *timeouts,
           unsigned long long *macs) {
     __shared__ TcShared S;
     if (H->pool_overflow) return;  // entries incomplete: this pass is replayed after the pool grows
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint64_t tile = local % ntiles;  // tiles fastest: neighbours share staged samples in L2
         tc_load_rings(S, J.T, tile);
         __syncthreads();
-        tc_item<KbTcCfg>(S, J, tile, (uint32_t)(local / ntiles), gk, itn, zero_page, timeouts, macs);
+        tc_item<KbTcCfg>(S, J, tile, (uint32_t)(local / ntiles), gk, itn, timeouts, macs);
         ++itn;
         __syncthreads();  // every role is done with the item's ring table and accumulator
     }
@@ -259,7 +259,6 @@ struct BatchState {
     unsigned long long *d_jent = nullptr, *h_jent = nullptr;  // per job: entries
     unsigned long long *d_jusum = nullptr, *h_jusum = nullptr;  // per job: staged slots of its tiles (sum, largest)
     uint32_t map_cap = 0;
-    void *zero_page = nullptr;  // the tensor-core engine's zero page
     unsigned long long entry_cap = 0;
 };
 
@@ -302,7 +301,7 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
         } else {
             kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
             kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
-            kb_tc<<<n, kTcThreads, KbTcCfg::kSmem, s>>>(B.d_hdr, B.d_jobs, B.zero_page, &ctx->d_stats->timeouts,
+            kb_tc<<<n, kTcThreads, KbTcCfg::kSmem, s>>>(B.d_hdr, B.d_jobs, &ctx->d_stats->timeouts,
                                                   &ctx->d_stats->tc_macs);
             kb_1chan<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
         }
@@ -325,7 +324,6 @@ cudaError_t batch_release(hcg_context *ctx) {
     if (B->d_hdr) cudaFreeAsync(B->d_hdr, ctx->stream);
     if (B->d_jobs) cudaFreeAsync(B->d_jobs, ctx->stream);
     if (B->d_maps) cudaFreeAsync(B->d_maps, ctx->stream);
-    if (B->zero_page) cudaFreeAsync(B->zero_page, ctx->stream);
     if (B->h_maps) cudaFreeHost(B->h_maps);
     if (B->d_jovf) cudaFreeAsync(B->d_jovf, ctx->stream);
     if (B->h_jovf) cudaFreeHost(B->h_jovf);
@@ -350,12 +348,9 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         BatchState *B = new BatchState();
         cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
         if ((e = cudaMallocAsync(&B->d_hdr, sizeof(BatchHdr), s)) != cudaSuccess ||
-            (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess ||
-            (e = cudaMallocAsync(&B->zero_page, (size_t)kTcZeroWindows * kTcMaxA, s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(B->zero_page, 0, (size_t)kTcZeroWindows * kTcMaxA, s)) != cudaSuccess) {
+            (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess) {
             if (B->d_hdr) cudaFreeAsync(B->d_hdr, s);
             if (B->h_hdr) cudaFreeHost(B->h_hdr);
-            if (B->zero_page) cudaFreeAsync(B->zero_page, s);
             delete B;
             return e;
         }

@@ -586,18 +586,19 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
     }
     count = warp_sum_u64(count);
     within = warp_sum_u64(within);
-    if (COUNT) {
+    if constexpr (COUNT) {
         if (lane == 0) cap[grp] = (uint32_t)count;
         return;
-    }
+    } else {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) ws[q] = warp_sum(ws[q]);
-    if (lane == 0) {
-        cnt[grp] = base;
+        for (int q = 0; q < 4; ++q) ws[q] = warp_sum(ws[q]);
+        if (lane == 0) {
+            cnt[grp] = base;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (valid[q]) wsum[pix[q]] = ws[q];
-        if (within) atomicAdd(&a.stats->pairs_within, within);
+            for (int q = 0; q < 4; ++q)
+                if (valid[q]) wsum[pix[q]] = ws[q];
+            if (within) atomicAdd(&a.stats->pairs_within, within);
+        }
     }
 }
 

@@ -21,7 +21,7 @@ namespace {
 template <class Cfg>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tile_tc(const __grid_constant__ CUtensorMap tm, const __grid_constant__ CUtensorMap tm_out, int has_out, TcJob J,
-              const void *zero_page, unsigned long long *timeouts, unsigned long long *macs) {
+              unsigned long long *timeouts, unsigned long long *macs) {
     __shared__ TcShared S;
     J.map = &tm;
     J.out_map = has_out ? &tm_out : nullptr;
@@ -30,19 +30,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_setup<Cfg>(S);  // ends with a CTA barrier
     if (threadIdx.x == 0) sm100::prefetch_tensormap(&tm);
     uint32_t gk = 0;
-    tc_item<Cfg>(S, J, tile, blockIdx.y, gk, 0, zero_page, timeouts, macs);
+    tc_item<Cfg>(S, J, tile, blockIdx.y, gk, 0, timeouts, macs);
     tc_teardown<Cfg>(S, gk, timeouts);
 }
 
 template <class Cfg>
 __global__ void __launch_bounds__(kTcPersistThreads, 1)
     k_tile_tc_persist(const __grid_constant__ CUtensorMap tm, TcJob J, uint64_t nitems, uint64_t ntiles,
-                      const void *zero_page, unsigned long long *timeouts, unsigned long long *macs) {
+                      unsigned long long *timeouts, unsigned long long *macs) {
     __shared__ TcPShared S;
     J.map = &tm;
     J.out_map = nullptr;
     if (threadIdx.x == 0) sm100::prefetch_tensormap(&tm);
-    tc_persist<Cfg>(S, J, nitems, ntiles, zero_page, timeouts, macs);
+    tc_persist<Cfg>(S, J, nitems, ntiles, timeouts, macs);
 }
 
 template <class Cfg>
@@ -269,7 +269,7 @@ int tc_pick(const hcg_context *ctx, const hcg_field *f) {
 namespace {
 template <class Cfg>
 cudaError_t launch_tc_persist(hcg_context *ctx, const hcg_field *f, TcJob &J, const TileArgs &T, uint64_t ntiles,
-                              const void *zero, std::string &why) {
+                              std::string &why) {
     cudaStream_t s = ctx->stream;
     CUtensorMap tm;
     if (!tc_prepare_job(f, Cfg::kNb, &tm, J)) {
@@ -288,14 +288,14 @@ cudaError_t launch_tc_persist(hcg_context *ctx, const hcg_field *f, TcJob &J, co
     const uint64_t nitems = ntiles * J.ncb;
     const unsigned grid = (unsigned)std::min<uint64_t>(nitems, (uint64_t)(nsm > 0 ? nsm : 148));
     if (grid == 0) return cudaSuccess;
-    k_tile_tc_persist<Cfg><<<grid, kTcPersistThreads, Cfg::kSmem, s>>>(tm, J, nitems, ntiles, zero,
+    k_tile_tc_persist<Cfg><<<grid, kTcPersistThreads, Cfg::kSmem, s>>>(tm, J, nitems, ntiles,
                                                                       &ctx->d_stats->timeouts, &ctx->d_stats->tc_macs);
     return cudaGetLastError();
 }
 
 template <class Cfg>
 cudaError_t launch_tc(hcg_context *ctx, const hcg_field *f, TcJob &J, const TileArgs &T, uint64_t ntiles,
-                      const void *zero, std::string &why) {
+                      std::string &why) {
     cudaStream_t s = ctx->stream;
     CUtensorMap tm, tm_out;
     if (!tc_prepare_job(f, Cfg::kNb, &tm, J)) {
@@ -314,7 +314,7 @@ cudaError_t launch_tc(hcg_context *ctx, const hcg_field *f, TcJob &J, const Tile
         J.T = T;
         J.T.t0 = T.t0 + t0;
         dim3 grid((unsigned)std::min<uint64_t>(ntiles - t0, 0x7fffffffull), J.ncb);
-        k_tile_tc<Cfg><<<grid, kTcThreads, Cfg::kSmem, s>>>(tm, tm_out, has_out, J, zero, &ctx->d_stats->timeouts,
+        k_tile_tc<Cfg><<<grid, kTcThreads, Cfg::kSmem, s>>>(tm, tm_out, has_out, J, &ctx->d_stats->timeouts,
                                                             &ctx->d_stats->tc_macs);
     }
     return cudaGetLastError();
@@ -368,12 +368,7 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
                      const unsigned long long *off, const uint32_t *cnt, const uint32_t *e_slot, const float4 *e_w,
                      const double *wsum, float *out, uint32_t ostride, float *wout, unsigned long long umax,
                      std::string &why) {
-    cudaStream_t s = ctx->stream;
     TcJob J{};
-    cudaError_t e = cudaSuccess;
-    void *zero = ctx->scratch.get(20, (size_t)kTcZeroWindows * kTcMaxA, s, e);
-    if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(zero, 0, (size_t)kTcZeroWindows * kTcMaxA, s)) != cudaSuccess) return e;
     J.g = g;
     J.off = off;
     J.cnt = cnt;
@@ -388,12 +383,12 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
     // which accumulates in segments (the one-item kernel does not)
     if (cfg < 4 && umax > kTcOneSegmentSlots) cfg = cfg == 3 ? 5 : 4;
     switch (cfg) {
-        case 0: return launch_tc<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
-        case 1: return launch_tc<TcCfgN2S3>(ctx, f, J, T, ntiles, zero, why);
-        case 2: return launch_tc<TcCfgN1S4>(ctx, f, J, T, ntiles, zero, why);
-        case 3: return launch_tc<TcCfgN4K32>(ctx, f, J, T, ntiles, zero, why);
-        case 4: return launch_tc_persist<TcCfgN4S2>(ctx, f, J, T, ntiles, zero, why);
-        default: return launch_tc_persist<TcCfgN4K32>(ctx, f, J, T, ntiles, zero, why);
+        case 0: return launch_tc<TcCfgN4S2>(ctx, f, J, T, ntiles, why);
+        case 1: return launch_tc<TcCfgN2S3>(ctx, f, J, T, ntiles, why);
+        case 2: return launch_tc<TcCfgN1S4>(ctx, f, J, T, ntiles, why);
+        case 3: return launch_tc<TcCfgN4K32>(ctx, f, J, T, ntiles, why);
+        case 4: return launch_tc_persist<TcCfgN4S2>(ctx, f, J, T, ntiles, why);
+        default: return launch_tc_persist<TcCfgN4K32>(ctx, f, J, T, ntiles, why);
     }
 }
 

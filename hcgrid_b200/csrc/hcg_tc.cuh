@@ -20,14 +20,13 @@
 //
 // One work item = one tile x up to 256 channels (nb 64-channel blocks).
 // Warp roles in a 192-thread CTA:
-//   warp 0    producer: per K chunk (64 or 32 slots), one bulk copy of a
-//             zero page over the chunk's weight operand, then the spectra:
-//             runs of 8 sorted samples, each one 4-D TMA box (64 channels x 8
-//             rows x nb channel blocks x hi/lo, 128-byte swizzle: the
-//             MN-major B atoms);
+//   warp 0    producer: per K chunk (64 or 32 slots), the spectra: runs of 8
+//             sorted samples, each one 4-D TMA box (64 channels x 8 rows x nb
+//             channel blocks x hi/lo, 128-byte swizzle: the MN-major B atoms);
 //   warp 1    TMEM allocation and MMA issue (one thread);
-//   warps 2-5 write the weights of the chunk's entries into the zeroed
-//             K-major operand (swizzled), then run the epilogue: tcgen05.ld
+//   warps 2-5 zero their operand rows and write the weights of the chunk's
+//             entries into the K-major operand (swizzled), then run the
+//             epilogue: tcgen05.ld
 //             of the accumulator, multiplication by the inverse channel
 //             scales and by 1 / (FP64 weight sum) into a shared-memory tile
 //             laid out as the cube's box, written by one TMA bulk tensor
@@ -58,9 +57,7 @@ namespace hcg {
 constexpr int kTcM = kTileX * kTileY;  // 128 pixels: the MMA's M
 constexpr int kTcThreads = 192;
 constexpr int kTcBuilders = 128;
-constexpr uint32_t kTcMaxA = kTcM * 64 * 2 * 2;  // largest weight operand (hi + lo) of a chunk: 32 KB
 constexpr uint64_t kTcWaitNs = 1000000000ull;
-constexpr uint32_t kTcZeroWindows = 160;  // zero region: kTcZeroWindows x 32 KB (5 MB)
 constexpr uint32_t kTcMaxN = 256;         // channels per item (the MMA's largest N)
 static_assert(kTcM == 128, "a tile is one M=128 MMA");
 
@@ -85,7 +82,6 @@ struct TcCfg {
     static constexpr uint32_t kTmemCols = NB * 64 <= 64 ? 64 : (NB * 64 <= 128 ? 128 : 256);
     static_assert(KC == 64 || KC == 32, "chunks of 64 or 32 slots");
     static_assert(ST * kStageBytes <= 192 * 1024, "operand buffers fit shared memory");
-    static_assert(2 * kAHalf <= kTcMaxA, "zero page covers the weight operand");
 };
 using TcCfgN4S2 = TcCfg<4, 2, 64>;  // 256 channels per item, 64-slot chunks, 2 stages
 using TcCfgN2S3 = TcCfg<2, 3, 64>;  // 128 channels, 64-slot chunks, 3 stages
@@ -123,7 +119,7 @@ constexpr int kTcRing = 8;  // entries in flight per builder thread
 constexpr int kTcMaxStages = 4;
 
 struct TcShared {
-    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], zfill[kTcMaxStages], acc_full;
+    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], acc_full;
     uint32_t tmem;
     volatile int abort;
     unsigned long long item;
@@ -194,7 +190,6 @@ __device__ __forceinline__ void tc_setup(TcShared &S) {
             mbar_init(&S.full_a[s], kTcBuilders);
             mbar_init(&S.full_b[s], 1);
             mbar_init(&S.empty[s], 1);
-            mbar_init(&S.zfill[s], 1);
         }
         mbar_init(&S.acc_full, 1);
         S.abort = 0;
@@ -517,7 +512,7 @@ __device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, u
 // `itn` its items; both advance identically in every thread.
 template <class Cfg>
 __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t tile, uint32_t cblk, uint32_t &gk,
-                                        uint32_t itn, const void *zero_page, unsigned long long *timeouts,
+                                        uint32_t itn, unsigned long long *timeouts,
                                         unsigned long long *macs) {
     using namespace sm100;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -635,7 +630,7 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
 constexpr int kTcPersistThreads = 320;
 
 struct TcPShared {
-    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], zfill[kTcMaxStages];
+    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages];
     uint64_t acc_full[2], acc_empty[2];
     uint32_t tmem;
     volatile int abort;
@@ -751,8 +746,7 @@ __device__ __forceinline__ void tc_epilogue_direct(SH &S, const TcJob &J, uint64
 
 template <class Cfg>
 __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_t nitems, uint64_t ntiles,
-                                           const void *zero_page, unsigned long long *timeouts,
-                                           unsigned long long *macs) {
+                                           unsigned long long *timeouts, unsigned long long *macs) {
     using namespace sm100;
     constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
     static_assert(Cfg::kTmemCols <= 256, "two accumulators fit the 512 TMEM columns");
@@ -762,7 +756,6 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
             mbar_init(&S.full_a[s], kTcBuilders);
             mbar_init(&S.full_b[s], 1);
             mbar_init(&S.empty[s], 1);
-            mbar_init(&S.zfill[s], 1);
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&S.acc_full[a], 1);
@@ -841,7 +834,7 @@ constexpr int kTcDBuilders = kTcDRow * kTcM;
 constexpr int kTcDThreads = 64 + kTcDBuilders + kTcBuilders;  // producer, MMA, builders, epilogue
 
 struct TcDShared {
-    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages], zfill[kTcMaxStages];
+    uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages];
     uint64_t acc_full[2], acc_empty[2], ws_full[2], ws_empty[2];
     uint32_t tmem;
     volatile int abort;
@@ -1056,7 +1049,6 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
             mbar_init(&S.full_a[s], kTcDBuilders);
             mbar_init(&S.full_b[s], 1);
             mbar_init(&S.empty[s], 1);
-            mbar_init(&S.zfill[s], 1);
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&S.acc_full[a], 1);
