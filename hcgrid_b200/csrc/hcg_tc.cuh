@@ -1,14 +1,15 @@
 // Tensor-core channel accumulation (tcgen05, sm_100a): the per-tile device
-// code shared by the single-job kernel (hcg_tc.cu) and the persistent batch
-// kernel (hcg_batch.cu).
+// code of the single-job kernels (hcg_tc.cu: one item per CTA, persistent,
+// and persistent with in-kernel weights) and of the persistent batch kernel
+// (hcg_batch.cu).
 //
 // For one 16x8-pixel tile the gridded cube is a dense product
 //     cube[pixel][channel] = sum_slot W[pixel][slot] * X[slot][channel]
 // where the slots are the tile's staged samples (the union of the ring
 // windows of its pixels, one contiguous run of sorted samples per HEALPix
-// ring, padded to a multiple of 8) and W holds the FP64-evaluated GAUSS1D
-// weights of the pairs inside sphere_radius (zero elsewhere): the weights the
-// FP32 engine sums. The product runs on the 5th-generation tensor cores as a
+// ring, padded to a multiple of 8) and W holds the GAUSS1D weights of the
+// pairs inside sphere_radius (FP64 distance and cutoff, FP32 Gaussian; zero
+// elsewhere): the weights the FP32 engine sums. The product runs on the 5th-generation tensor cores as a
 // compensated 16-bit split, W = Wh + Wl and X = Xh + Xl with
 // hi = round(x), lo = round(x - hi):
 //     W X ~= Wh Xh + Wh Xl + Wl Xh
@@ -19,7 +20,8 @@
 // (per-term error ~3 * 2^-22). Scales are powers of two: exact.
 //
 // One work item = one tile x up to 256 channels (nb 64-channel blocks).
-// Warp roles in a 192-thread CTA:
+// Warp roles in the one-item 192-thread CTA (the persistent kernels below
+// add epilogue warps and, with in-kernel weights, more builders):
 //   warp 0    producer: per K chunk (64 or 32 slots), the spectra: runs of 8
 //             sorted samples, each one 4-D TMA box (64 channels x 8 rows x nb
 //             channel blocks x hi/lo, 128-byte swizzle: the MN-major B atoms);
