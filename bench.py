@@ -303,9 +303,12 @@ def dist_setup(args):
 
 
 def reduce_max(torch, dist, v):
+    """The largest of the ranks' values (every rank calls it; the timing
+    convention: a multi-GPU step takes as long as its slowest rank)."""
     if dist is None:
         return v
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
