@@ -181,6 +181,10 @@ void orc_pix2ang(const orc_healpix *h, uint64_t pix, double *theta, double *phi)
 int orc_prepare_grid_kernel(orc_gmaps *g, uint32_t kernel_type, double *params, double sphere_radius,
                             double hpx_max_res) {
     static double last_r = -1, last_res = -1;
+    const int taper_fix = (kernel_type & ORC_TAPER_FIX) != 0;
+    kernel_type &= ~ORC_TAPER_FIX;
+    if (taper_fix && kernel_type != ORC_TAPERED_SINC) return -1;
+    g->taper_fix = taper_fix;
     if (kernel_type == ORC_GAUSS1D) {
         params[0] = 0.5 / pow(params[0], 2.);
         g->bearing_needed = 0;
@@ -273,9 +277,34 @@ static double true_angular_distance(double l1, double b1, double l2, double b2) 
     return 2 * asin(sqrt(pow(sin((b1 - b2) / 2.), 2) + cos(b1) * cos(b2) * pow(sin((l1 - l2) / 2.), 2)));
 }
 
-/* gridding.cu:238-241 (GAUSS1D). GAUSS2D / TAPERED_SINC are outside the
- * path this restatement covers. */
-static double kernel_gauss1d(double distance, double p0) { return exp(-distance * distance * p0); }
+/* helpers.cu:133-137: great-circle bearing of (l2, b2) seen from (l1, b1),
+ * radians. */
+static double great_circle_bearing(double l1, double b1, double l2, double b2) {
+    double l_diff = l2 - l1;
+    double cos_b2 = cos(b2);
+    return atan2(cos_b2 * sin(l_diff), cos(b1) * sin(b2) - sin(b1) * cos_b2 * cos(l_diff));
+}
+
+/* gridding.cu:229-235 */
+static double sinc(double x) { return fabs(x) < 1.e-10 ? 1. : sin(x) / x; }
+
+/* gridding.cu:237-257: the grid kernel at `distance` degrees and `bearing`
+ * radians. GAUSS1D takes the transformed 0.5 / sigma^2; GAUSS2D
+ * (sigma_maj, sigma_min, PA) and TAPERED_SINC (sigma, a, b) take their
+ * parameters as given. The reference's taper is exp(pow(-(arg / a), 2)) =
+ * exp(+(arg / a)^2); taper_fix takes exp(-(arg / a)^2). */
+static double kernel_func(const orc_gmaps *g, double distance, double bearing) {
+    const double *p = g->params;
+    if (g->kernel_type == ORC_GAUSS1D) return exp(-distance * distance * p[0]);
+    if (g->kernel_type == ORC_GAUSS2D) {
+        double ellarg = pow(p[0], 2.0) * pow(sin(bearing - p[2]), 2.0) + pow(p[1], 2.0) * pow(cos(bearing - p[2]), 2.0);
+        double Earg = pow(distance / p[0] / p[1], 2.0) / 2. * ellarg;
+        return exp(-Earg);
+    }
+    double arg = PI * distance / p[0];
+    double t = pow(-(arg / p[1]), 2.0);
+    return sinc(arg / p[2]) * exp(g->taper_fix ? -t : t);
+}
 
 typedef struct {
     uint64_t uring, dring;
@@ -356,13 +385,20 @@ void orc_grid(const orc_gmaps *g, long n, const uint64_t *sorted_keys, const uin
               uint64_t usedrings, const double *lons, const double *lats, const double *weights, const double *data,
               long nchan, long npix_map, const double *xwcs, const double *ywcs, int mode, double *cube_out,
               double *wts_out, orc_stats *stats) {
+    orc_grid_ex(g, n, sorted_keys, lut, firstring, usedrings, lons, lats, weights, data, nchan, npix_map, xwcs, ywcs,
+                mode, cube_out, wts_out, NULL, stats);
+}
+
+void orc_grid_ex(const orc_gmaps *g, long n, const uint64_t *sorted_keys, const uint32_t *lut, uint64_t firstring,
+                 uint64_t usedrings, const double *lons, const double *lats, const double *weights,
+                 const double *data, long nchan, long npix_map, const double *xwcs, const double *ywcs, int mode,
+                 double *cube_out, double *wts_out, double *wabs_out, orc_stats *stats) {
     const orc_healpix *h = &g->hpx;
-    const double p0 = g->params[0];
     long long visited = 0, within = 0, a3 = 0;
 #pragma omp parallel for schedule(dynamic, 16) reduction(+ : visited, within, a3)
     for (long p = 0; p < npix_map; ++p) {
         double *acc = cube_out + p * nchan;
-        double wsum = 0.0;
+        double wsum = 0.0, wabs = 0.0;
         for (long c = 0; c < nchan; ++c) acc[c] = 0.0;
         pixel_setup ps;
         setup_pixel(g, firstring, usedrings, xwcs[p], ywcs[p], &ps);
@@ -374,12 +410,14 @@ void orc_grid(const orc_gmaps *g, long n, const uint64_t *sorted_keys, const uin
                     double l2 = lons[i] * DEG2RAD;
                     double b2 = lats[i] * DEG2RAD;
                     double sdist = true_angular_distance(ps.l1, ps.b1, l2, b2) * RAD2DEG;
+                    double sbear = g->bearing_needed ? great_circle_bearing(ps.l1, ps.b1, l2, b2) : 0.;
                     ++visited;
                     if (sdist < g->sphere_radius) {
-                        double tweight = weights[i] * kernel_gauss1d(sdist, p0);
+                        double tweight = weights[i] * kernel_func(g, sdist, sbear);
                         const double *x = data + (long)i * nchan;
                         for (long c = 0; c < nchan; ++c) acc[c] += x[c] * tweight;
                         wsum += tweight;
+                        wabs += fabs(tweight);
                         ++within;
                     }
                 }
@@ -406,18 +444,21 @@ void orc_grid(const orc_gmaps *g, long n, const uint64_t *sorted_keys, const uin
                     double b2 = lats[i] * DEG2RAD;
                     if (limit < 1.0 && hav(ps.l1 - l2) > limit) continue;
                     double sdist = true_angular_distance(ps.l1, ps.b1, l2, b2) * RAD2DEG;
+                    double sbear = g->bearing_needed ? great_circle_bearing(ps.l1, ps.b1, l2, b2) : 0.;
                     ++visited;
                     if (sdist < g->sphere_radius) {
-                        double tweight = weights[i] * kernel_gauss1d(sdist, p0);
+                        double tweight = weights[i] * kernel_func(g, sdist, sbear);
                         const double *x = data + (long)i * nchan;
                         for (long c = 0; c < nchan; ++c) acc[c] += x[c] * tweight;
                         wsum += tweight;
+                        wabs += fabs(tweight);
                         ++within;
                     }
                 }
             }
         }
         wts_out[p] = wsum;
+        if (wabs_out) wabs_out[p] = wabs;
     }
     if (stats) {
         stats->pairs_visited = visited;

@@ -21,6 +21,9 @@ extern "C" {
 #define ORC_GAUSS1D 1
 #define ORC_GAUSS2D 2
 #define ORC_TAPERED_SINC 3
+/* OR'd into the kernel type: TAPERED_SINC with the taper exp(-(arg/p1)^2)
+ * instead of the reference's exp(+(arg/p1)^2) (gridding.cu:255). */
+#define ORC_TAPER_FIX 0x100u
 
 typedef struct {
     uint64_t nside, order, nrings, npface, ncap, npix;
@@ -34,6 +37,7 @@ typedef struct {
     double sphere_radius;  /* degrees */
     double disc_size;      /* radians */
     int bearing_needed;
+    int taper_fix;         /* ORC_TAPER_FIX was given */
 } orc_gmaps;
 
 typedef struct {
@@ -79,6 +83,12 @@ void orc_grid(const orc_gmaps *g, long n, const uint64_t *sorted_keys, const uin
               uint64_t usedrings, const double *lons, const double *lats, const double *weights, const double *data,
               long nchan, long npix_map, const double *xwcs, const double *ywcs, int mode, double *cube_out,
               double *wts_out, orc_stats *stats);
+/* orc_grid, and when wabs_out is not NULL also sum |weight| per pixel (the
+ * conditioning of the normalisation for kernels with negative lobes). */
+void orc_grid_ex(const orc_gmaps *g, long n, const uint64_t *sorted_keys, const uint32_t *lut, uint64_t firstring,
+                 uint64_t usedrings, const double *lons, const double *lats, const double *weights,
+                 const double *data, long nchan, long npix_map, const double *xwcs, const double *ywcs, int mode,
+                 double *cube_out, double *wts_out, double *wabs_out, orc_stats *stats);
 
 /* gmap.cpp:306-312: datacube / weights (0/0 gives NaN). */
 void orc_normalize(long npix_map, long nchan, const double *cube, const double *wts, double *out);

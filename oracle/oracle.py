@@ -24,7 +24,8 @@ LIB_ORACLE = os.path.join(HERE, "lib", "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libhcgrid_ref.so")
 REF_CLI = os.path.join(HERE, "_ref", "HCGrid")
 
-GAUSS1D = 1
+GAUSS1D, GAUSS2D, TAPERED_SINC = 1, 2, 3
+TAPER_FIX = 0x100  # OR'd into TAPERED_SINC: taper exp(-(arg/a)^2) instead of the reference's exp(+(arg/a)^2)
 MAX_Y = 1 << 30
 
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
@@ -53,6 +54,7 @@ class GMaps(C.Structure):
         ("sphere_radius", C.c_double),
         ("disc_size", C.c_double),
         ("bearing_needed", C.c_int),
+        ("taper_fix", C.c_int),
     ]
 
 
@@ -86,6 +88,9 @@ def lib():
         L.orc_grid.argtypes = [C.POINTER(GMaps), C.c_long, _u64p, _u32p, C.c_uint64, C.c_uint64, _f64p, _f64p,
                                _f64p, _f64p, C.c_long, C.c_long, _f64p, _f64p, C.c_int, _f64p, _f64p,
                                C.POINTER(Stats)]
+        L.orc_grid_ex.argtypes = [C.POINTER(GMaps), C.c_long, _u64p, _u32p, C.c_uint64, C.c_uint64, _f64p, _f64p,
+                                  _f64p, _f64p, C.c_long, C.c_long, _f64p, _f64p, C.c_int, _f64p, _f64p, _f64p,
+                                  C.POINTER(Stats)]
         L.orc_pixel_windows.argtypes = [C.POINTER(GMaps), C.c_long, _u64p, _u32p, C.c_uint64, C.c_uint64,
                                         C.c_double, C.c_double, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                         _u32p, _u32p, C.c_long, C.POINTER(C.c_long)]
@@ -104,10 +109,13 @@ def healpix(nside: int) -> Healpix:
     return h
 
 
-def prepare_grid_kernel(sigma_deg: float, sphere_radius: float, hpx_max_res: float) -> GMaps:
+def prepare_grid_kernel(sigma_deg: float, sphere_radius: float, hpx_max_res: float, kernel_type: int = GAUSS1D,
+                        params=None) -> GMaps:
+    """gmap.cpp:64-99. GAUSS1D takes sigma_deg; GAUSS2D and TAPERED_SINC take
+    `params` (three values, used as given)."""
     g = GMaps()
-    p = np.array([sigma_deg, 0.0, 0.0])
-    rc = lib().orc_prepare_grid_kernel(C.byref(g), GAUSS1D, p, sphere_radius, hpx_max_res)
+    p = np.array([sigma_deg, 0.0, 0.0]) if params is None else np.array(params, np.float64).copy()
+    rc = lib().orc_prepare_grid_kernel(C.byref(g), kernel_type, p, sphere_radius, hpx_max_res)
     assert rc == 0
     return g
 
@@ -173,9 +181,10 @@ def presort(h: Healpix, lons: np.ndarray, lats: np.ndarray) -> Presorted:
     return Presorted(sk, perm, fr.value, ur.value, lut[:m].copy())
 
 
-def grid(g: GMaps, ps: Presorted, lons, lats, data, xwcs, ywcs, weights=None, mode=0):
+def grid(g: GMaps, ps: Presorted, lons, lats, data, xwcs, ywcs, weights=None, mode=0, want_abs=False):
     """FP64 gridding of sorted inputs. data: [n] or [n, C] in SORTED order.
-    Returns (cube[npix, C], weights[npix], stats) unnormalised."""
+    Returns (cube[npix, C], weights[npix], stats) unnormalised, and with
+    want_abs the per-pixel sum of |weight| as a fourth item."""
     n = len(lons)
     data = np.asarray(data, np.float64)
     squeeze = data.ndim == 1
@@ -186,13 +195,15 @@ def grid(g: GMaps, ps: Presorted, lons, lats, data, xwcs, ywcs, weights=None, mo
     npix = len(xwcs)
     cube = np.empty((npix, nchan))
     wts = np.empty(npix)
+    wabs = np.empty(npix)
     st = Stats()
-    lib().orc_grid(C.byref(g), n, ps.keys, ps.lut, ps.firstring, ps.usedrings,
-                   np.ascontiguousarray(lons, np.float64), np.ascontiguousarray(lats, np.float64),
-                   np.ascontiguousarray(weights, np.float64), data2, nchan, npix,
-                   np.ascontiguousarray(xwcs, np.float64), np.ascontiguousarray(ywcs, np.float64), mode,
-                   cube, wts, C.byref(st))
-    return (cube[:, 0] if squeeze else cube), wts, st
+    lib().orc_grid_ex(C.byref(g), n, ps.keys, ps.lut, ps.firstring, ps.usedrings,
+                      np.ascontiguousarray(lons, np.float64), np.ascontiguousarray(lats, np.float64),
+                      np.ascontiguousarray(weights, np.float64), data2, nchan, npix,
+                      np.ascontiguousarray(xwcs, np.float64), np.ascontiguousarray(ywcs, np.float64), mode,
+                      cube, wts, wabs, C.byref(st))
+    out = (cube[:, 0] if squeeze else cube), wts, st
+    return out + (wabs,) if want_abs else out
 
 
 def pixel_windows(g: GMaps, ps: Presorted, xw: float, yw: float, cap: int = 4096):
@@ -244,15 +255,16 @@ def ref():
     return _ref
 
 
-def ref_prepare(sigma_deg: float, sphere_radius: float, hpx_max_res: float):
+def ref_prepare(sigma_deg: float, sphere_radius: float, hpx_max_res: float, kernel_type: int = GAUSS1D,
+                params=None):
     """HCGrid.cpp:137-151 sequence: _Healpix_init(1, RING), then
     _prepare_grid_kernel. Returns (params_after, disc_size, healpix_state)."""
     R = ref()
     R.ref_healpix_init(1)
     out = np.zeros(3)
     ds, sr = C.c_double(), C.c_double()
-    R.ref_prepare_grid_kernel(1, np.array([sigma_deg, 0.0, 0.0]), sphere_radius, hpx_max_res, out,
-                              C.byref(ds), C.byref(sr))
+    p = np.array([sigma_deg, 0.0, 0.0]) if params is None else np.array(params, np.float64).copy()
+    R.ref_prepare_grid_kernel(kernel_type, p, sphere_radius, hpx_max_res, out, C.byref(ds), C.byref(sr))
     return out, ds.value, ref_state()
 
 

@@ -12,7 +12,11 @@ the reference's functions return: HEALPix pixel/ring values
 set_WCS through wcslib (HCGrid/gmap.cpp:183-250), and the FP64 datacube and
 weight map of the `hcgrid` kernel body (HCGrid/gridding.cu:277-403).
 Multi-channel cases run the reference kernel once per channel, as HCGrid+
-does (HCGrid+/gridding-omp.cu:616-626).
+does (HCGrid+/gridding-omp.cu:616-626). kernels.npz holds the same kernel
+body with the GAUSS2D and TAPERED_SINC grid kernels (HCGrid/gridding.cu:
+237-257, parameters as _prepare_grid_kernel leaves them, gmap.cpp:73-80).
+
+`python tests/golden/make_golden.py kernels` writes kernels.npz alone.
 """
 from __future__ import annotations
 
@@ -152,8 +156,55 @@ def synth_case(name, n, ra, dec, size, nx, pix_arcsec, fwhm, nchan, seed):
     save(case)
 
 
+# (name, kernel type, parameters in units of sigma except the angle PA in
+# radians): GAUSS2D (sigma_maj, sigma_min, PA), TAPERED_SINC (sigma, a, b)
+KERNEL_CASES = [
+    ("gauss2d_pa04", O.GAUSS2D, (1.3, 0.8, 0.4)),
+    ("gauss2d_pa_neg", O.GAUSS2D, (0.7, 1.1, -1.2)),
+    ("sinc", O.TAPERED_SINC, (1.0, 9.0, 1.55)),
+]
+
+
+def kernel_cases():
+    rng = np.random.default_rng(15)
+    ra, dec, size = 30.0, 40.0, 0.6
+    lon, lat = synth.raster_scan(6000, ra, dec, size, 2.0, rng)
+    vals = np.stack([rng.normal(1.0, 0.3, len(lon)), rng.normal(0.0, 1.0, len(lon))], axis=1)
+    hdr = synth.sin_header(24, 24, ra, dec, 60.0 / 3600.0)
+    nx, ny, nz, xw, yw = target_coords(hdr)
+    sigma = 180.0 / 3600.0 * synth.FWHM_TO_SIGMA
+    r, res = 3 * sigma, sigma / 2
+    out = dict(lon=lon, lat=lat, values=vals, sigma=sigma, sphere_radius=r, hpx_max_res=res, nx=nx, ny=ny,
+               xwcs=xw, ywcs=yw, header=np.array(hdr), names=np.array([c[0] for c in KERNEL_CASES]))
+    for name, kt, p in KERNEL_CASES:
+        params = np.array([p[0] * sigma, p[1] * sigma if kt == O.GAUSS2D else p[1], p[2]])
+        pr, disc, st = O.ref_prepare(sigma, r, res, kt, params)
+        assert np.array_equal(pr, params)  # GAUSS2D / TAPERED_SINC parameters are not transformed
+        keys, slon, slat, sdat, fr, ur, lut = O.ref_presort(lon, lat, vals[:, 0], 2)
+        theta = np.pi / 2 - (np.pi / 180.0) * lat
+        phi = (np.pi / 180.0) * lon
+        k0 = np.empty(len(lon), np.uint64)
+        O.ref().ref_ang2pix(len(lon), np.ascontiguousarray(theta), np.ascontiguousarray(phi), k0)
+        perm = np.argsort(k0, kind="stable").astype(np.uint32)
+        cubes, wts = [], None
+        for c in range(vals.shape[1]):
+            cube, w = O.ref_grid(keys, slon, slat, np.ascontiguousarray(vals[perm, c]), lut, fr, ur, nx, ny, xw, yw)
+            cubes.append(cube)
+            assert wts is None or np.array_equal(wts, w)
+            wts = w
+        out[name + "_type"] = np.uint32(kt)
+        out[name + "_params"] = params
+        out[name + "_cube"] = np.stack(cubes, axis=1)
+        out[name + "_wts"] = wts
+    np.savez_compressed(os.path.join(OUT, "kernels.npz"), **out)
+    print("wrote kernels", ", ".join(c[0] for c in KERNEL_CASES))
+
+
 def main():
     O.build(with_ref=True)
+    if sys.argv[1:] == ["kernels"]:
+        kernel_cases()
+        return
     healpix_vectors()
     input1_case()
     synth_case("synth_dec40", 20000, 30.0, 40.0, 1.2, 48, 60.0, 180.0, 4, 10)
@@ -161,6 +212,7 @@ def main():
     synth_case("synth_wrap", 16000, 0.3, 10.0, 1.2, 40, 90.0, 180.0, 1, 12)
     synth_case("synth_south", 16000, 250.0, -25.0, 1.0, 40, 72.0, 300.0, 2, 13)
     synth_case("synth_fwhm60", 12000, 80.0, 55.0, 0.3, 32, 20.0, 60.0, 1, 14)
+    kernel_cases()
 
 
 if __name__ == "__main__":

@@ -1,5 +1,6 @@
 """The CPU restatement (oracle/) against the reference's golden vectors and,
 where the reference build is present, against the reference itself."""
+import ctypes
 import os
 
 import numpy as np
@@ -117,3 +118,93 @@ def test_config1_reduced_vs_reference():
     cube, wts, s = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm], xw, yw)
     np.testing.assert_array_equal(wts, wts_r)
     np.testing.assert_array_equal(cube, cube_r)
+
+
+# ---------------------------------------------------------------------------
+# GAUSS2D and TAPERED_SINC grid kernels (HCGrid/gridding.cu:237-257)
+
+@pytest.fixture(scope="module")
+def kernels_golden():
+    z = np.load(os.path.join(GOLDEN, "kernels.npz"))
+    return {k: z[k] for k in z.files}
+
+
+def _kernel_grid(z, kt, params, weights=None, want_abs=False):
+    g = O.prepare_grid_kernel(float(z["sigma"]), float(z["sphere_radius"]), float(z["hpx_max_res"]), kt, params)
+    ps = O.presort(g.hpx, z["lon"], z["lat"])
+    w = None if weights is None else weights[ps.perm]
+    return O.grid(g, ps, z["lon"][ps.perm], z["lat"][ps.perm], z["values"][ps.perm], z["xwcs"], z["ywcs"],
+                  weights=w, want_abs=want_abs)
+
+
+@pytest.mark.parametrize("name", ["gauss2d_pa04", "gauss2d_pa_neg", "sinc"])
+def test_kernel_types_match_reference_bitexact(kernels_golden, name):
+    z = kernels_golden
+    cube, wts, st = _kernel_grid(z, int(z[name + "_type"]), z[name + "_params"])
+    assert st.a3_events == 0 and st.pairs_within > 0
+    np.testing.assert_array_equal(wts, z[name + "_wts"])
+    np.testing.assert_array_equal(cube, z[name + "_cube"])
+
+
+def test_kernel_types_match_reference_build(kernels_golden):
+    """Fresh parameters against the reference's own kernel body (host build)."""
+    if not O.have_ref():
+        pytest.skip("reference host build not present")
+    z = kernels_golden
+    rng = np.random.default_rng(3)
+    s = float(z["sigma"])
+    cases = [(O.GAUSS2D, [s * rng.uniform(0.5, 2), s * rng.uniform(0.5, 2), rng.uniform(-3, 3)]) for _ in range(2)]
+    cases += [(O.TAPERED_SINC, [s * rng.uniform(0.7, 1.5), rng.uniform(2, 12), rng.uniform(1, 3)]) for _ in range(2)]
+    for kt, params in cases:
+        cube, wts, _ = _kernel_grid(z, kt, params)
+        O.ref_prepare(s, float(z["sphere_radius"]), float(z["hpx_max_res"]), kt, params)
+        keys, slon, slat, sdat, fr, ur, lut = O.ref_presort(z["lon"], z["lat"], z["values"][:, 0], 2)
+        rc, rw = O.ref_grid(keys, slon, slat, sdat, lut, fr, ur, int(z["nx"]), int(z["ny"]), z["xwcs"], z["ywcs"])
+        np.testing.assert_array_equal(wts, rw)
+        np.testing.assert_array_equal(cube[:, 0], rc)
+
+
+def _hav_deg(l1, b1, l2, b2):
+    l1, b1, l2, b2 = map(np.deg2rad, (l1, b1, l2, b2))
+    return np.rad2deg(2 * np.arcsin(np.sqrt(np.sin((b1 - b2) / 2) ** 2 + np.cos(b1) * np.cos(b2) *
+                                            np.sin((l1 - l2) / 2) ** 2)))
+
+
+def test_kernel_formulas_single_pairs():
+    """One sample, one pixel: the weight map is the kernel itself. GAUSS2D
+    with its bearing, TAPERED_SINC in the reference's form exp(+(arg/a)^2)
+    and, with TAPER_FIX, exp(-(arg/a)^2)."""
+    sigma = 0.02
+    r = 3 * sigma
+    lon0, lat0 = 50.0, 20.0
+    ang = np.linspace(0, 2 * np.pi, 13)[:-1]
+    dist = np.linspace(0.002, 0.055, 12)
+    lon = lon0 + dist * np.sin(ang) / np.cos(np.deg2rad(lat0))
+    lat = lat0 + dist * np.cos(ang)
+    for kt, params in [(O.GAUSS2D, [0.03, 0.015, 0.7]), (O.TAPERED_SINC, [0.02, 2.52, 1.55]),
+                       (O.TAPERED_SINC | O.TAPER_FIX, [0.02, 2.52, 1.55])]:
+        for i in range(len(lon)):
+            g = O.prepare_grid_kernel(sigma, r, sigma / 2, kt, params)
+            ps = O.presort(g.hpx, np.array([lon[i]]), np.array([lat[i]]))
+            _, w, st = O.grid(g, ps, np.array([lon[i]]), np.array([lat[i]]), np.ones(1), np.array([lon0]),
+                              np.array([lat0]))
+            d = _hav_deg(lon0, lat0, lon[i], lat[i])
+            if kt == O.GAUSS2D:
+                l1, b1, l2, b2 = map(np.deg2rad, (lon0, lat0, lon[i], lat[i]))
+                bear = np.arctan2(np.cos(b2) * np.sin(l2 - l1),
+                                  np.cos(b1) * np.sin(b2) - np.sin(b1) * np.cos(b2) * np.cos(l2 - l1))
+                p0, p1, pa = params
+                ell = p0 ** 2 * np.sin(bear - pa) ** 2 + p1 ** 2 * np.cos(bear - pa) ** 2
+                want = np.exp(-((d / p0 / p1) ** 2) / 2 * ell)
+            else:
+                arg = np.pi * d / params[0]
+                x = arg / params[2]
+                t = (arg / params[1]) ** 2
+                want = np.sin(x) / x * np.exp(-t if kt & O.TAPER_FIX else t)
+            if st.pairs_within == 0:
+                assert w[0] == 0.0  # the reference's window missed the sample (quirk A1)
+                continue
+            np.testing.assert_allclose(w[0], want, rtol=1e-12)
+    # the flag is TAPERED_SINC's only
+    g = O.GMaps()
+    assert O.lib().orc_prepare_grid_kernel(ctypes.byref(g), O.GAUSS2D | O.TAPER_FIX, np.zeros(3), r, sigma / 2) == -1
