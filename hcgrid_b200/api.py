@@ -15,6 +15,7 @@ import numpy as np
 from . import build as _build
 
 GAUSS1D, GAUSS2D, TAPERED_SINC = 1, 2, 3
+TAPER_FIX = 0x100  # OR'd into TAPERED_SINC: taper exp(-(arg/a)^2) instead of the reference's exp(+(arg/a)^2)
 MEM_HOST, MEM_DEVICE = 0, 1
 SAMPLE_MAJOR, CHANNEL_MAJOR = 0, 1
 ENGINE_AUTO, ENGINE_FP32, ENGINE_TC_BF16, ENGINE_TC_F16 = 0, 1, 2, 3

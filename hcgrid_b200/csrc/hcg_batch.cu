@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256) kb_1chan(BatchHdr *H, const JobDesc *__re
         if (it >= H->tot_c1) return;
         int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.c1_base; });
         const JobDesc &J = jobs[j];
-        grid1_item(J.a, J.spec, J.cstride, J.out, J.wout, it - J.c1_base);
+        grid1_item<false>(J.a, J.spec, J.cstride, J.out, J.wout, it - J.c1_base);  // GAUSS1D jobs only
     }
 }
 
@@ -570,7 +570,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
     for (uint32_t i = 0; i < njobs; ++i) {
         if ((B.h_jovf[i] && jobs[i].field->nchan > 1) ||
             (J[i].tc.nb &&
-             (tc_use_weights(ctx, B.h_jusum[2 * i], B.h_jent[i], (unsigned long long)J[i].T.ntx * J[i].T.nty) ||
+             (tc_use_weights(ctx, jobs[i].field, B.h_jusum[2 * i], B.h_jent[i], (unsigned long long)J[i].T.ntx * J[i].T.nty) ||
               B.h_jusum[2 * i + 1] > kTcOneSegmentSlots))) {
             fallback[i] = 1;
             ++nrouted;

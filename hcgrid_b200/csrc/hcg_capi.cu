@@ -121,11 +121,15 @@ uint64_t hcg::job_pixels(const hcg_job &job) {
 // hcg_grid after its argument checks; the caller holds the context lock.
 static hcg_status grid_checked(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube,
                                int layout, float *weights_out, int mem, int engine) {
-    if (field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
     if (!field->d_spec && !field->xfmt) return fail(ctx, HCG_ESTATE, "field has no spectra (hcg_field_set_spectra)");
     if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
         return fail(ctx, HCG_EINVAL, "unknown layout");
     if (engine < HCG_ENGINE_AUTO || engine > HCG_ENGINE_TC_F16) return fail(ctx, HCG_EINVAL, "unknown engine");
+    if (!fp32_weights_fit(field))
+        return fail(ctx, HCG_EINVAL,
+                    "weights up to " + std::to_string(field->wbound) +
+                        " (sample weights times the kernel's bound) exceed the FP32 weights of the multi-channel "
+                        "engines");
     if (engine == HCG_ENGINE_AUTO) engine = auto_engine(field);
     const bool tc = engine != HCG_ENGINE_FP32 && field->nchan > 1;
     if (tc && field->xfmt != engine)
@@ -133,6 +137,11 @@ static hcg_status grid_checked(hcg_context *ctx, const hcg_field *field, const h
     if (tc && field->xnonfinite)
         return fail(ctx, HCG_EINVAL,
                     std::to_string(field->xnonfinite) + " non-finite spectrum values: grid with HCG_ENGINE_FP32");
+    if (tc && !tc_weights_fit(field))
+        return fail(ctx, HCG_EINVAL,
+                    "weights up to " + std::to_string(field->wbound) +
+                        " (sample weights times the kernel's bound) exceed the tensor-core range: grid with "
+                        "HCG_ENGINE_FP32");
     if (!tc && !field->d_spec)
         return fail(ctx, HCG_ESTATE, "the FP32 spectra were dropped by hcg_field_split_spectra");
     cudaStream_t s = ctx->stream;
@@ -264,7 +273,10 @@ hcg_status hcg_prepare_grid_kernel(hcg_context *ctx, uint32_t kernel_type, doubl
     Guard g(ctx);
     if (!kernel_params) return fail(ctx, HCG_EINVAL, "kernel_params is NULL");
     if (!(sphere_radius > 0) || !(hpx_max_res > 0)) return fail(ctx, HCG_EINVAL, "sphere_radius and hpx_max_res must be > 0");
-    // gmap.cpp:69-80
+    // gmap.cpp:69-80; HCG_TAPER_FIX is TAPERED_SINC's only flag
+    const bool taper_fix = (kernel_type & HCG_TAPER_FIX) != 0;
+    kernel_type &= ~HCG_TAPER_FIX;
+    if (taper_fix && kernel_type != HCG_TAPERED_SINC) return fail(ctx, HCG_EINVAL, "HCG_TAPER_FIX needs TAPERED_SINC");
     if (kernel_type == HCG_GAUSS1D) {
         kernel_params[0] = 0.5 / pow(kernel_params[0], 2.);
         ctx->bearing = false;
@@ -276,6 +288,7 @@ hcg_status hcg_prepare_grid_kernel(hcg_context *ctx, uint32_t kernel_type, doubl
         return fail(ctx, HCG_EINVAL, "unknown kernel type");
     }
     ctx->kernel_type = kernel_type;
+    ctx->taper_fix = taper_fix;
     memcpy(ctx->kparams, kernel_params, 3 * sizeof(double));
     // gmap.cpp:89-95: rebuild HEALPix only when the sphere moved by > 3e-5
     if (!ctx->prepared || fabs(ctx->last_r - sphere_radius) > 3e-5 || fabs(ctx->last_res - hpx_max_res) > 3e-5) {
@@ -320,8 +333,10 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
     f->hpx = ctx->hpx;
     f->sphere_radius = ctx->sphere_radius;
     f->kparam0 = ctx->kparams[0];
+    memcpy(f->kparams, ctx->kparams, sizeof f->kparams);
     f->disc_size = ctx->disc_size;
     f->kernel_type = ctx->kernel_type;
+    f->taper_fix = ctx->taper_fix;
     f->geom_refs = new (std::nothrow) int(1);
     if (!f->geom_refs) { delete f; return fail(ctx, HCG_ENOMEM, "host allocation"); }
     const double *dl = lon, *db = lat, *dw = weights;
@@ -340,6 +355,14 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
     std::string why;
     cudaError_t e = build_field(ctx, f, dl, db, dw, why);
     if (tmp) cudaFreeAsync(tmp, s);
+    // |kernel| <= 1 except for the reference's TAPERED_SINC taper, whose
+    // exp(+(pi d / (sigma a))^2) grows to its value at d = sphere_radius
+    double kbound = 1.0;
+    if (f->kernel_type == HCG_TAPERED_SINC && !f->taper_fix) {
+        const double t = 3.1415926535897932384626433832 * f->sphere_radius / (f->kparams[0] * f->kparams[1]);
+        kbound = exp(t * t);
+    }
+    f->wbound = f->wmax * kbound;
     if (e != cudaSuccess) {
         hcg_status st = cuda_fail(ctx, e, "field build", why);
         cudaStreamSynchronize(s);
@@ -630,18 +653,33 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
             return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " lives on another device");
         if (!j.field->d_spec && auto_engine(j.field) == HCG_ENGINE_FP32)
             return fail(ctx, HCG_ESTATE, "job " + std::to_string(i) + ": field has no spectra for its engine");
-        if (j.field->kernel_type != HCG_GAUSS1D) return fail(ctx, HCG_EUNSUPPORTED, "only GAUSS1D is gridded");
+        if (!fp32_weights_fit(j.field))
+            return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + ": weights exceed the FP32 weights of the "
+                                         "multi-channel engines");
         if (j.layout != HCG_LAYOUT_SAMPLE_MAJOR && j.layout != HCG_LAYOUT_CHANNEL_MAJOR)
             return fail(ctx, HCG_EINVAL, "unknown layout");
     }
     CK(ctx, cudaMemsetAsync(ctx->d_stats, 0, offsetof(DevStats, invalid_input), ctx->stream), "stats reset");
+    // The batch kernels evaluate GAUSS1D; jobs with the other kernels run on
+    // their own after the batch, as do the jobs the batch routes out.
+    std::vector<hcg_job> shared;
+    std::vector<uint32_t> index;  // shared job -> caller's job
+    for (uint32_t i = 0; i < njobs; ++i) {
+        if (jobs[i].field->kernel_type != HCG_GAUSS1D) continue;
+        shared.push_back(jobs[i]);
+        index.push_back(i);
+    }
     std::vector<char> fallback;
     std::string why;
-    cudaError_t e = grid_batch(ctx, njobs, jobs, fallback, why);
+    cudaError_t e = cudaSuccess;
+    if (!shared.empty()) e = grid_batch(ctx, (uint32_t)shared.size(), shared.data(), fallback, why);
     if (e == cudaErrorTimeout) return fail(ctx, HCG_ETIMEOUT, why);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch", why);
+    std::vector<char> alone(njobs, 0);
+    for (uint32_t k = 0; k < shared.size(); ++k) alone[index[k]] = fallback[k];
+    for (uint32_t i = 0; i < njobs; ++i) alone[i] |= jobs[i].field->kernel_type != HCG_GAUSS1D;
     for (uint32_t i = 0; i < njobs; ++i) {
-        if (!fallback[i]) continue;
+        if (!alone[i]) continue;
         e = grid_field(ctx, jobs[i].field, jobs[i].target, jobs[i].cube, jobs[i].layout, jobs[i].weights,
                        auto_engine(jobs[i].field), why);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch fallback", why);

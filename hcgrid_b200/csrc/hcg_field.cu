@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "hcg_internal.h"
@@ -299,23 +300,35 @@ __global__ void __launch_bounds__(256) k_ring_ptab(const RingRec *__restrict__ r
         ptab[R.tbl + q] = lower_bound_u64(keys, R.lut_lo, R.lut_hi, p0 + q);
 }
 
+// Also the largest |w| of the per-sample weights (when given) into *wbits as
+// the bits of a non-negative double, whose order as integers is the order of
+// the values; NaN sorts above infinity.
 __global__ void k_permute_geometry(uint64_t n, const uint32_t *__restrict__ perm, const double *__restrict__ lon,
                                    const double *__restrict__ lat, const double *__restrict__ w,
                                    double *__restrict__ l2, double *__restrict__ b2, double *__restrict__ cb2,
-                                   double *__restrict__ wout, double4 *__restrict__ half) {
+                                   double *__restrict__ wout, double4 *__restrict__ half,
+                                   unsigned long long *__restrict__ wbits) {
     uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    uint32_t i = perm[j];
-    double b = dmul(lat[i], kDeg2Rad);
-    double l = dmul(lon[i], kDeg2Rad);
-    l2[j] = l;
-    b2[j] = b;
-    cb2[j] = cos(b);
-    wout[j] = w ? w[i] : 1.0;
-    double4 q;
-    sincos(l * 0.5, &q.x, &q.y);
-    sincos(b * 0.5, &q.z, &q.w);
-    half[j] = q;
+    unsigned long long wb = 0;
+    if (j < n) {
+        uint32_t i = perm[j];
+        double b = dmul(lat[i], kDeg2Rad);
+        double l = dmul(lon[i], kDeg2Rad);
+        l2[j] = l;
+        b2[j] = b;
+        cb2[j] = cos(b);
+        const double wi = w ? w[i] : 1.0;
+        wout[j] = wi;
+        wb = (unsigned long long)__double_as_longlong(fabs(wi));
+        double4 q;
+        sincos(l * 0.5, &q.x, &q.y);
+        sincos(b * 0.5, &q.z, &q.w);
+        half[j] = q;
+    }
+    if (!w) return;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) wb = max(wb, __shfl_xor_sync(0xffffffffu, wb, o));
+    if ((threadIdx.x & 31) == 0 && wb) atomicMax(wbits, wb);
 }
 
 // out[j][0..cstride) = in[perm[j]][0..nchan), zero padded; one warp per row.
@@ -365,6 +378,7 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
     uint32_t *v0 = nullptr, *v1 = nullptr, *hist = nullptr;
     KeyRange *range = nullptr;
     RingSpan *span = nullptr;
+    unsigned long long *wbits = nullptr;
     uint32_t nblocks = (uint32_t)((n + kSortTile - 1) / kSortTile);
 #define TRY(x)                         \
     do {                               \
@@ -457,12 +471,22 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
     TRY(cudaMallocAsync(&f->d_cb2, n * sizeof(double), s));
     TRY(cudaMallocAsync(&f->d_half, n * sizeof(double4), s));
     TRY(cudaMallocAsync(&f->d_w, n * sizeof(double), s));
+    TRY(cudaMallocAsync(&wbits, sizeof(unsigned long long), s));
+    TRY(cudaMemsetAsync(wbits, 0, sizeof(unsigned long long), s));
     k_permute_geometry<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, f->d_perm, d_lon, d_lat, d_w, f->d_l2, f->d_b2,
-                                                                   f->d_cb2, f->d_w, f->d_half);
+                                                                   f->d_cb2, f->d_w, f->d_half, wbits);
     TRY(cudaGetLastError());
     k_ring_phi<<<(unsigned)f->usedrings, 256, 0, s>>>(f->hpx, f->d_rings, f->d_keys, f->d_l2, f->d_b2, f->d_cb2);
     TRY(cudaGetLastError());
+    f->wmax = 1.0;
+    if (d_w) {
+        unsigned long long hb = 0;
+        TRY(cudaMemcpyAsync(&hb, wbits, sizeof hb, cudaMemcpyDeviceToHost, s));
+        TRY(cudaStreamSynchronize(s));
+        memcpy(&f->wmax, &hb, sizeof hb);
+    }
 fail:
+    if (wbits) cudaFreeAsync(wbits, s);
     if (k0) cudaFreeAsync(k0, s);
     if (k1) cudaFreeAsync(k1, s);
     if (v0) cudaFreeAsync(v0, s);

@@ -45,14 +45,16 @@ __global__ void k_pixel_prep(HpxParams h, uint64_t firstring, uint64_t usedrings
     if (p < npixmap) prep_item(h, firstring, usedrings, disc, X, Y, out, stats, p);
 }
 
+// GEN: fields whose kernel is not GAUSS1D
+template <bool GEN>
 __global__ void __launch_bounds__(256) k_grid_1chan(GridArgs a, uint64_t npixmap, const float *__restrict__ data,
                                                     uint32_t cstride, float *__restrict__ out,
                                                     float *__restrict__ wout) {
     uint64_t p = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    if (p < npixmap) grid1_item(a, data, cstride, out, wout, p);
+    if (p < npixmap) grid1_item<GEN>(a, data, cstride, out, wout, p);
 }
 
-template <bool COUNT>
+template <bool COUNT, bool GEN = false>  // GEN: fields whose kernel is not GAUSS1D
 __global__ void __launch_bounds__(256, 3) k_group(GridArgs a, GroupArgs g, uint32_t *__restrict__ cap,
                                                const unsigned long long *__restrict__ off,
                                                uint32_t *__restrict__ e_idx, float4 *__restrict__ e_w,
@@ -62,7 +64,8 @@ __global__ void __launch_bounds__(256, 3) k_group(GridArgs a, GroupArgs g, uint3
     __shared__ PixHalf s_half[8][4];
     int warp = threadIdx.x >> 5;
     uint64_t grp = g.g0 + blockIdx.x * 8ull + warp;
-    if (grp < g.g1) group_item<COUNT>(a, g, cap, off, e_idx, e_w, cnt, wsum, tiles, grp, s_prep[warp], s_half[warp]);
+    if (grp < g.g1)
+        group_item<COUNT, GEN>(a, g, cap, off, e_idx, e_w, cnt, wsum, tiles, grp, s_prep[warp], s_half[warp]);
 }
 
 __global__ void __launch_bounds__(256) k_group_accum(GroupArgs g, const unsigned long long *__restrict__ off,
@@ -157,7 +160,11 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
     if (f->nchan == 1) {
         cudaEventRecord(ctx->evp[1], s);
         cudaEventRecord(ctx->evp[2], s);
-        k_grid_1chan<<<(unsigned)((P * 32 + 255) / 256), 256, 0, s>>>(a, P, f->d_spec, f->cstride, d_cube, d_wts);
+        const unsigned nblk = (unsigned)((P * 32 + 255) / 256);
+        if (f->kernel_type == HCG_GAUSS1D)
+            k_grid_1chan<false><<<nblk, 256, 0, s>>>(a, P, f->d_spec, f->cstride, d_cube, d_wts);
+        else
+            k_grid_1chan<true><<<nblk, 256, 0, s>>>(a, P, f->d_spec, f->cstride, d_cube, d_wts);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
         GroupArgs g;
@@ -238,7 +245,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             return cudaErrorInvalidValue;
         }
         const uint32_t ostride = layout == HCG_LAYOUT_CHANNEL_MAJOR ? 0 : f->nchan;  // 0: [channel][pixel]
-        if (tc && tiled && tc_use_weights(ctx, ro[T.nty + 2], ro[T.nty], ntiles)) {
+        if (tc && tiled && tc_use_weights(ctx, f, ro[T.nty + 2], ro[T.nty], ntiles)) {
             // dense tiles: the tensor-core kernel evaluates the weights itself (no entries)
             cudaEventRecord(ctx->evp[2], s);
             if ((e = tc_weights(ctx, f, a, g, T, ntiles, d_cube, ostride, d_wts, why)) != cudaSuccess) return e;
@@ -279,7 +286,10 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             gc.ebase = ro[ch.first];
             if (gc.g1 <= gc.g0) continue;
             unsigned cb = (unsigned)((gc.g1 - gc.g0 + 7) / 8);
-            k_group<false><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tiled ? T : none);
+            if (f->kernel_type == HCG_GAUSS1D)
+                k_group<false><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tiled ? T : none);
+            else
+                k_group<false, true><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tiled ? T : none);
             if (first) cudaEventRecord(ctx->evp[2], s);  // phase marks are exact for a single chunk
             first = false;
             if (tiled && tc) {

@@ -90,6 +90,7 @@ struct hcg_context {
     double kparams[3] = {0, 0, 0};
     double sphere_radius = 0, disc_size = 0;
     bool bearing = false;
+    bool taper_fix = false;  // HCG_TAPER_FIX
     double last_r = -1, last_res = -1;
     hcg::HpxParams hpx = {};
     hcg::DevStats *d_stats = nullptr;
@@ -108,7 +109,11 @@ struct hcg_field {
     uint64_t n = 0;
     hcg::HpxParams hpx = {};
     double sphere_radius = 0, kparam0 = 0, disc_size = 0;  // kernel setup the field was built with
+    double kparams[3] = {0, 0, 0};
     uint32_t kernel_type = 0;
+    bool taper_fix = false;
+    double wmax = 1.0;    // max |per-sample weight| (inf or NaN when one is not finite)
+    double wbound = 1.0;  // bound of |weight| of an accepted pair: wmax * the kernel's bound
     uint64_t firstring = 0, usedrings = 0;
     uint64_t *d_keys = nullptr;   // n + 1, sorted, sentinel npix
     uint32_t *d_perm = nullptr;   // sorted position -> input index
@@ -151,8 +156,15 @@ inline int tc_class_of(uint32_t cpad) {
 }
 // HCG_ENGINE_AUTO: the tensor-core engine of the field's split spectra
 // (multi-channel fields with finite spectra), else the FP32 engine.
+// The tensor-core weight operand holds |w| * (power-of-two weight scale)
+// below 2^15 (FP16 range); weights above 2^100 or not finite stay on FP32.
+inline bool tc_weights_fit(const hcg_field *f) { return f->wbound <= 0x1p100; }
+// The multi-channel engines keep weights as FP32 entries: a multi-channel
+// field whose weight bound passes 2^120 (the reference's taper with a narrow
+// taper width) is refused; single-channel fields sum in FP64.
+inline bool fp32_weights_fit(const hcg_field *f) { return f->nchan <= 1 || !(f->wbound > 0x1p120); }
 inline int auto_engine(const hcg_field *f) {
-    return (f->xfmt && f->nchan > 1 && f->xnonfinite == 0) ? f->xfmt : HCG_ENGINE_FP32;
+    return (f->xfmt && f->nchan > 1 && f->xnonfinite == 0 && tc_weights_fit(f)) ? f->xfmt : HCG_ENGINE_FP32;
 }
 // Tensor-core weight operand: evaluated in the kernel (HCG_TC_WEIGHTS_DIRECT)
 // or written as entries by the FP64 weight pass. Automatic mode evaluates in
@@ -161,9 +173,10 @@ inline int auto_engine(const hcg_field *f) {
 // tests are at most 2.5x the weight pass's (usum: staged slots of all `ntiles`
 // tiles; cap_total: union candidates of all 2x2 groups, each for up to 4
 // pixels). Measured on B200, the entries are faster below that.
-inline bool tc_use_weights(const hcg_context *ctx, unsigned long long usum, unsigned long long cap_total,
-                           unsigned long long ntiles) {
-    if (ctx->tc_weights == HCG_TC_WEIGHTS_ENTRIES) return false;
+// Only GAUSS1D weights are evaluated in the kernel.
+inline bool tc_use_weights(const hcg_context *ctx, const hcg_field *f, unsigned long long usum,
+                           unsigned long long cap_total, unsigned long long ntiles) {
+    if (f->kernel_type != HCG_GAUSS1D || ctx->tc_weights == HCG_TC_WEIGHTS_ENTRIES) return false;
     if (ctx->tc_weights == HCG_TC_WEIGHTS_DIRECT) return true;
     return usum >= 1024ull * ntiles && 128.0 * (double)usum <= 2.5 * 4.0 * (double)cap_total;
 }

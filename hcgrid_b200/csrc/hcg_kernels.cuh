@@ -193,6 +193,10 @@ struct GridArgs {
     int series;           // d^2 from the arcsine-squared series (small sphere_radius)
     double hpolar;        // haversine bound of every accepted pair (chord windows)
     float x2scale;        // 4 R2D^2 p0 log2(e): the FP32 Gaussian's exponent per unit of the series
+    int series32;         // series && GAUSS1D: accepted pairs below the band take gauss_series_f32
+    uint32_t ktype;       // HCG_GAUSS1D, HCG_GAUSS2D or HCG_TAPERED_SINC
+    int ktaper;           // TAPERED_SINC with HCG_TAPER_FIX
+    double kp1, kp2;      // second and third kernel parameters (p0 is the first)
 };
 
 namespace {
@@ -212,6 +216,11 @@ inline GridArgs grid_args(const hcg_field *f, const PixPrep *prep, DevStats *sta
     a.series = hstar < 1e-3;
     a.hpolar = hstar * (1.0 + 1e-6);
     a.x2scale = (float)(4.0 * kRad2Deg * kRad2Deg * f->kparam0 * 1.4426950408889634);
+    a.ktype = f->kernel_type;
+    a.series32 = a.series && f->kernel_type == HCG_GAUSS1D;
+    a.ktaper = f->taper_fix;
+    a.kp1 = f->kparams[1];
+    a.kp2 = f->kparams[2];
     return a;
 }
 
@@ -294,20 +303,50 @@ __device__ __forceinline__ float gauss_series_f32(double h, float x2scale) {
     return r;
 }
 
+// The grid kernels other than GAUSS1D (gridding.cu:242-256), FP64, for an
+// accepted pair at d degrees: GAUSS2D (sigma_maj, sigma_min, PA) at the
+// great-circle bearing of the sample seen from the pixel (helpers.cu:133-137),
+// TAPERED_SINC (sigma, a, b) with sinc(x) = 1 for |x| < 1e-10
+// (gridding.cu:229-235) and the taper exp(+(arg/a)^2) of the reference, or
+// exp(-(arg/a)^2) with HCG_TAPER_FIX. Kept out of line: the GAUSS1D loops
+// that inline pair_weight_s only branch to it.
+__device__ __noinline__ double kernel_other(const GridArgs &a, const PixPrep &P, double d, double cb2,
+                                            uint32_t idx) {
+    const double p0 = a.p0, p1 = a.kp1, p2 = a.kp2;
+    if (a.ktype == HCG_GAUSS2D) {
+        double sdl, cdl;
+        sincos(__ldg(a.l2 + idx) - P.l1, &sdl, &cdl);
+        const double sb2 = sin(__ldg(a.b2 + idx)), sb1 = sin(P.b1);
+        const double bear = atan2(cb2 * sdl, P.cb1 * sb2 - sb1 * cb2 * cdl);
+        double sa, ca;
+        sincos(bear - p2, &sa, &ca);
+        const double ell = (p0 * p0) * (sa * sa) + (p1 * p1) * (ca * ca);
+        const double q = d / p0 / p1;
+        return exp(-((q * q) / 2. * ell));
+    }
+    const double arg = kPi * d / p0;
+    const double x = arg / p2;
+    const double s = fabs(x) < 1.e-10 ? 1. : sin(x) / x;
+    const double t = (arg / p1) * (arg / p1);
+    return s * exp(a.ktaper ? -t : t);
+}
+
 // Weight of sample idx for the pixel (0 outside sphere_radius): the
 // haversine h = sin^2(db/2) + cos b1 cos b2 sin^2(dl/2) with the half-angle
 // differences expanded from precomputed sines and cosines; d^2 for accepted
 // pairs from asin^2(x) = sum_n (2x)^(2n) / (2 n^2 C(2n, n)) at x = sqrt(h)
 // (five terms; used when h* < 1e-3, truncation below 1e-16 relative), else
 // from asin itself. Pairs inside the threshold band take the full formula.
-template <bool F32EXP = false>
+// GEN: the field's kernel may be other than GAUSS1D (kernel_other); without
+// it the code is GAUSS1D's alone.
+template <bool F32EXP = false, bool GEN = true>
 __device__ __forceinline__ double pair_weight_s(const GridArgs &a, const PixPrep &P, const PixHalf &q,
                                                 const double4 &s, double cb2, double win, uint32_t idx) {
     const double sb = q.sb * s.w - q.cb * s.z;  // sin((b1 - b2) / 2)
     const double sl = q.sl * s.y - q.cl * s.x;  // sin((l1 - l2) / 2)
     const double h = sb * sb + P.cb1 * cb2 * (sl * sl);
     if (h > a.hhi) return 0.0;
-    if (F32EXP && h < a.hlo && a.series) return win * (double)gauss_series_f32(h, a.x2scale);
+    if (F32EXP && h < a.hlo && a.series32) return win * (double)gauss_series_f32(h, a.x2scale);
     double d2;
     if (h < a.hlo) {
         if (a.series) {
@@ -322,18 +361,24 @@ __device__ __forceinline__ double pair_weight_s(const GridArgs &a, const PixPrep
         if (!(d < a.sphere_radius)) return 0.0;
         d2 = d * d;
     }
+    if (GEN && a.ktype != HCG_GAUSS1D) {
+        const double k = kernel_other(a, P, sqrt(d2), cb2, idx);
+        return win * (F32EXP ? (double)(float)k : k);
+    }
     // Multi-channel entries hold FP32 weights: the Gaussian is evaluated in
     // FP32 there (gauss_f32); distance and cutoff stay FP64.
     if (F32EXP) return win * (double)gauss_f32(d2 * a.p0);
     return win * exp(-d2 * a.p0);
 }
 
+template <bool GEN>
 __device__ __forceinline__ double pair_weight(const GridArgs &a, const PixPrep &P, const PixHalf &q, uint32_t idx) {
-    return pair_weight_s(a, P, q, ldg4(a.half + idx), __ldg(a.cb2 + idx), __ldg(a.w + idx), idx);
+    return pair_weight_s<false, GEN>(a, P, q, ldg4(a.half + idx), __ldg(a.cb2 + idx), __ldg(a.w + idx), idx);
 }
 
 // Single channel: one warp per pixel, FP64 throughout.
-// Warp-collective: every lane passes the same pixel p.
+// Warp-collective: every lane passes the same pixel p. GEN as pair_weight_s.
+template <bool GEN>
 __device__ __forceinline__ void grid1_item(const GridArgs &a, const float *__restrict__ data, uint32_t cstride,
                                            float *__restrict__ out, float *__restrict__ wout, uint64_t p) {
     int lane = threadIdx.x & 31;
@@ -363,9 +408,9 @@ __device__ __forceinline__ void grid1_item(const GridArgs &a, const float *__res
             uint32_t s_len = __shfl_sync(0xffffffffu, len, src);
             if (t < total) {
                 uint32_t idx = s_lo + (t - (s_incl - s_len));
-                const double wt = pair_weight(a, P, ph, idx);
+                const double wt = pair_weight<GEN>(a, P, ph, idx);
                 ++cand;
-                if (wt > 0.0) {
+                if (wt != 0.0) {
                     acc += (double)__ldg(data + (uint64_t)idx * cstride) * wt;
                     ws += wt;
                     ++within;
@@ -445,7 +490,7 @@ namespace {
 // its tile's staged list instead of the sample index.
 // Warp-collective: every lane passes the same group; s_prep is this warp's
 // 4-entry shared-memory slot.
-template <bool COUNT>
+template <bool COUNT, bool GEN = false>  // GEN as pair_weight_s
 __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g, uint32_t *__restrict__ cap,
                                            const unsigned long long *__restrict__ off,
                                            uint32_t *__restrict__ e_idx, float4 *__restrict__ e_w,
@@ -565,8 +610,8 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if (idx >= s_lo[q] && idx < s_hi[q]) {
-                        const double wt = pair_weight_s<true>(a, s_prep[q], s_half[q], hs, cb2, win, idx);
-                        if (wt > 0.0) {
+                        const double wt = pair_weight_s<true, GEN>(a, s_prep[q], s_half[q], hs, cb2, win, idx);
+                        if (wt != 0.0) {
                             ws[q] += wt;
                             wq[q] = (float)wt;
                             any = true;

@@ -43,11 +43,12 @@ __global__ void k_noalloc_prep(HpxParams h, uint64_t firstring, uint64_t usedrin
     if (p < npix) prep_item(h, firstring, usedrings, disc, X, Y, prep, stats, p);
 }
 
+template <bool GEN>  // fields whose kernel is not GAUSS1D
 __global__ void __launch_bounds__(256) k_noalloc_grid(GridArgs a, uint64_t npix, const float *__restrict__ data,
                                                       uint32_t cstride, float *__restrict__ out,
                                                       float *__restrict__ wout) {
     uint64_t p = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    if (p < npix) grid1_item(a, data, cstride, out, wout, p);
+    if (p < npix) grid1_item<GEN>(a, data, cstride, out, wout, p);
 }
 
 constexpr int kMaxDevices = 64;
@@ -76,10 +77,6 @@ extern "C" hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field,
     if (!field->d_spec || field->nchan != 1) {
         ctx->err = "hcg_grid_noalloc grids single-channel fields that have spectra";
         return field->d_spec ? HCG_EINVAL : HCG_ESTATE;
-    }
-    if (field->kernel_type != HCG_GAUSS1D) {
-        ctx->err = "only GAUSS1D is gridded";
-        return HCG_EUNSUPPORTED;
     }
     const uint64_t P = (uint64_t)target->nx * target->ny;
     if (P > kNoAllocMaxPixels) {
@@ -117,8 +114,11 @@ extern "C" hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field,
                                                                     prep, ctx->d_stats);
         for (auto &ev : ctx->evp) cudaEventRecord(ev, s);
         const GridArgs a = grid_args(field, prep, ctx->d_stats);
-        k_noalloc_grid<<<(unsigned)((P * 32 + 255) / 256), 256, 0, s>>>(a, P, field->d_spec, field->cstride, cube,
-                                                                        weights_out);
+        const unsigned nblk = (unsigned)((P * 32 + 255) / 256);
+        if (field->kernel_type == HCG_GAUSS1D)
+            k_noalloc_grid<false><<<nblk, 256, 0, s>>>(a, P, field->d_spec, field->cstride, cube, weights_out);
+        else
+            k_noalloc_grid<true><<<nblk, 256, 0, s>>>(a, P, field->d_spec, field->cstride, cube, weights_out);
         cudaEventRecord(ctx->ev1, s);
         e = cudaGetLastError();
     }

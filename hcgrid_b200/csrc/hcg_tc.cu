@@ -157,6 +157,16 @@ void free_split(hcg_field *f, cudaStream_t s) {
     f->xnonfinite = 0;
 }
 
+// Power-of-two scale of the weight operand: BF16 holds any weight as it is;
+// FP16 weights are scaled so that the field's weight bound stays below 2^15
+// (2^15 for |w| <= 1, the kernels' own bound with unit sample weights).
+static float tc_weight_scale(const hcg_field *f, bool bf16) {
+    if (bf16 || !tc_weights_fit(f)) return 1.f;  // the engine refuses fields beyond 2^100
+    int e = 0;
+    if (f->wbound > 1.0) frexp(f->wbound, &e);  // wbound < 2^e
+    return ldexpf(1.f, 15 - e);
+}
+
 cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::string &why) {
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaSuccess;
@@ -181,7 +191,7 @@ cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::s
     lo = hi + (size_t)n * cpad;  // [2][cpad / 64][n][64]: the lo half follows the hi half
     bad = (unsigned long long *)(amax + cpad);  // cpad is a multiple of 64: 8-byte aligned
     cudaMemsetAsync(amax, 0, cpad * sizeof(unsigned int) + sizeof(unsigned long long), s);
-    const float wscale = fmt ? 1.f : 32768.f;
+    const float wscale = tc_weight_scale(f, fmt != 0);
     if (n > 0) {
         const uint32_t rpb = 4096;
         dim3 grid((f->nchan + 255) / 256, (unsigned)((n + rpb - 1) / rpb));
@@ -248,7 +258,7 @@ bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map, TcJob &J) 
     J.nchan = f->nchan;
     J.nrows = (uint32_t)f->n;
     J.fmt = f->xfmt == HCG_ENGINE_TC_BF16 ? 1u : 0u;
-    J.wscale = J.fmt ? 1.f : 32768.f;
+    J.wscale = tc_weight_scale(f, J.fmt != 0);
     J.inv_scale = f->d_xinv;
     return true;
 }

@@ -996,7 +996,7 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                     band |= inw[e] && h >= hlo && h <= hhi;
                     const double wt = acc ? S.g_w[b][s8 * 8 + half * 4 + e] * (double)ex : 0.0;
                     wv[e] = 0.f;
-                    if (wt > 0.0) {
+                    if (wt != 0.0) {
                         wsum += wt;
                         ++within;
                         wv[e] = (float)wt;
@@ -1007,9 +1007,10 @@ __device__ __forceinline__ void tc_build_weights(TcDShared &S, const TcJob &J, u
                     for (int e = 0; e < 4; ++e) {
                         if (!(inw[e] && hh[e] >= hlo && hh[e] <= hhi)) continue;
                         const uint32_t q = s8 * 8 + half * 4 + e;
-                        const double wt = pair_weight_s<true>(a, P, ph, S.g_half[b][q], S.g_cb[b][q], S.g_w[b][q],
-                                                              culo + (slot0 + half * 4 + e - cbase));
-                        if (wt > 0.0) {
+                        const double wt =
+                            pair_weight_s<true, false>(a, P, ph, S.g_half[b][q], S.g_cb[b][q], S.g_w[b][q],
+                                                       culo + (slot0 + half * 4 + e - cbase));
+                        if (wt != 0.0) {
                             wsum += wt;
                             ++within;
                             wv[e] = (float)wt;

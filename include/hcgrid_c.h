@@ -42,10 +42,23 @@ typedef enum {
     HCG_ESTATE = 7        /* call out of order (e.g. grid before prepare) */
 } hcg_status;
 
-/* Kernel types (HCGrid/constants.h:66-69). Only GAUSS1D is gridded. */
+/* Kernel types (HCGrid/constants.h:66-69) and their weights at distance d
+ * (degrees) inside sphere_radius (HCGrid/gridding.cu:237-257):
+ *   GAUSS1D      params (sigma): exp(-d^2 p0), p0 = 0.5 / sigma^2;
+ *   GAUSS2D      params (sigma_maj, sigma_min, PA), PA in radians:
+ *                exp(-(d / (smaj smin))^2 / 2 * (smaj^2 sin^2(bear - PA) +
+ *                smin^2 cos^2(bear - PA))), bear the great-circle bearing of
+ *                the sample seen from the pixel (helpers.cu:133-137);
+ *   TAPERED_SINC params (sigma, a, b): arg = pi d / sigma,
+ *                sinc(arg / b) * exp(+(arg / a)^2), the reference's taper
+ *                (exp(pow(-(arg/a), 2)), gridding.cu:255);
+ *   HCG_TAPERED_SINC | HCG_TAPER_FIX: the same with exp(-(arg / a)^2).
+ * GAUSS1D's weights come from its FP32 exponential on the multi-channel
+ * engines; the other kernels are evaluated in FP64. */
 #define HCG_GAUSS1D 1
 #define HCG_GAUSS2D 2
 #define HCG_TAPERED_SINC 3
+#define HCG_TAPER_FIX 0x100u
 
 /* Where a buffer lives. */
 #define HCG_MEM_HOST 0
@@ -99,7 +112,8 @@ hcg_status hcg_context_destroy(hcg_context *ctx);
 const char *hcg_last_error(const hcg_context *ctx);
 
 /* _prepare_grid_kernel: GAUSS1D params[0] = sigma (deg) is replaced in place
- * by 0.5/sigma^2, as the reference does; nside follows from hpx_max_res
+ * by 0.5/sigma^2, as the reference does (GAUSS2D and TAPERED_SINC take their
+ * three parameters as given); nside follows from hpx_max_res
  * (deg); HEALPix is rebuilt only if sphere_radius or hpx_max_res moved by
  * more than 3e-5 since the previous call on this context. */
 hcg_status hcg_prepare_grid_kernel(hcg_context *ctx, uint32_t kernel_type, double *kernel_params,
@@ -151,7 +165,8 @@ hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config);
  *                              sample, 4 weights) that the kernel scatters;
  *   HCG_TC_WEIGHTS_DIRECT  (2): the kernel's builder warps evaluate the FP64
  *                              distance, cutoff and Gaussian of every staged
- *                              sample for every pixel of the tile.
+ *                              sample for every pixel of the tile (GAUSS1D
+ *                              fields; the other kernels always use entries).
  * The accepted pairs and weights are the same; the FP64 weight sums can differ
  * in the last bits (summation order). No reference counterpart. */
 #define HCG_TC_WEIGHTS_AUTO 0

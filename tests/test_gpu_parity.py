@@ -234,15 +234,26 @@ def test_invalid_inputs_are_rejected(ctx):
     with pytest.raises(api.HcgError) as e:
         ctx.grid(f, t)  # no spectra yet
     assert e.value.status == 7
-    # a field grids with the kernel set up when it was created: GAUSS2D is
-    # accepted by the setup (as in the reference) but not gridded
-    kp = np.array([0.02, 0.02, 0.0])
-    ctx.prepare_grid_kernel(api.GAUSS2D, kp, 0.06, 0.01)
-    f2 = ctx.field(lon, np.array([10.0, 10.05, 10.1]))
+    # a field grids with the kernel set up when it was created
+    lat = np.array([10.0, 10.05, 10.1])
+    ctx.prepare_grid_kernel(api.GAUSS2D, np.array([0.02, 0.01, 0.3]), 0.06, 0.01)
+    f2 = ctx.field(lon, lat)
     f2.set_spectra(np.ones(3, np.float32))
-    with pytest.raises(api.HcgError) as e:
-        ctx.grid(f2, t)
-    assert e.value.status == 6
+    prepare(ctx, 0.02, 0.06, 0.01)
+    f1 = ctx.field(lon, lat)
+    f1.set_spectra(np.ones(3, np.float32))
+    xw, yw = t.coords()
+    for f, kt, params in ((f2, O.GAUSS2D, [0.02, 0.01, 0.3]), (f1, O.GAUSS1D, None)):
+        _, w = ctx.grid(f, t)
+        g = O.prepare_grid_kernel(0.02, 0.06, 0.01, kt, params)
+        ps = O.presort(g.hpx, lon, lat)
+        _, ow, _ = O.grid(g, ps, lon[ps.perm], lat[ps.perm], np.ones(3), xw, yw)
+        np.testing.assert_allclose(w, ow, rtol=1e-6)
+    # HCG_TAPER_FIX is TAPERED_SINC's flag; unknown kernel types are refused
+    for kt in (api.GAUSS2D | api.TAPER_FIX, 7):
+        with pytest.raises(api.HcgError) as e:
+            ctx.prepare_grid_kernel(kt, np.array([0.02, 0.01, 0.3]), 0.06, 0.01)
+        assert e.value.status == 1
 
 
 def test_empty_pixels_are_nan_and_single_sample_weight(ctx):
