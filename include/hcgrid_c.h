@@ -219,8 +219,9 @@ typedef struct {
  * launch over all jobs' work items fed by a device-side queue, and the pass
  * is a CUDA graph replayed per batch. Jobs may differ in sample count, map
  * size, channel count and kernel (each field grids with the kernel setup it
- * was created under). Returns when all cubes are written; each cube equals
- * what hcg_grid writes for that job. */
+ * was created under; the batch pass takes GAUSS1D jobs, GAUSS2D and
+ * TAPERED_SINC jobs run after it one at a time). Returns when all cubes are
+ * written; each cube equals what hcg_grid writes for that job. */
 hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs);
 
 /* Serving loop with continuous batching. `lanes` contexts on `device` (the
