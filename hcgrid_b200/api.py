@@ -63,6 +63,8 @@ EXPORTS = {
     "hcg_tc_set_weights": ([C.c_void_p, C.c_int], C.c_int),
     "hcg_autotune": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_sorted": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "hcg_field_band_samples": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p],
+                               C.c_int),
     "hcg_field_destroy": ([C.c_void_p], C.c_int),
     "hcg_field_share": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
     "hcg_target_create": ([C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int,
@@ -393,6 +395,14 @@ class Field:
         lut = np.empty(inf.usedrings + 1, np.uint32)
         self.ctx._check(self.ctx.L.hcg_field_sorted(self.h, keys.ctypes.data, perm.ctypes.data, lut.ctypes.data))
         return keys, perm, lut, inf.firstring, inf.usedrings
+
+    def band_samples(self, target: "Target", y0: int, y1: int):
+        """Sorted positions [s0, s1) whose samples alone grid target rows
+        [y0, y1) as this field does (hcg_field_band_samples)."""
+        s0, s1 = C.c_uint64(), C.c_uint64()
+        self.ctx._check(self.ctx.L.hcg_field_band_samples(self.ctx.h, self.h, target.h, y0, y1, C.byref(s0),
+                                                          C.byref(s1)))
+        return s0.value, s1.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -21,7 +21,8 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libhcgrid_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["hcg_field.cu", "hcg_grid.cu", "hcg_batch.cu", "hcg_noalloc.cu", "hcg_tc.cu", "hcg_capi.cu"]
+CU_SOURCES = ["hcg_field.cu", "hcg_grid.cu", "hcg_batch.cu", "hcg_noalloc.cu", "hcg_tc.cu", "hcg_capi.cu",
+              "hcg_shard.cu"]
 CXX_SOURCES = ["hcg_wcs.cpp", "hcg_fits.cpp", "hcg_compat.cpp", "hcg_server.cpp"]
 CLI = os.path.join(PKG, "bin", "HCGrid")
 

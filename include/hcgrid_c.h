@@ -178,6 +178,17 @@ hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_targ
 /* Sorted keys (n+1 with the npix sentinel), permutation (n) and ring LUT
  * (usedrings+1); any pointer may be NULL. Host memory. */
 hcg_status hcg_field_sorted(const hcg_field *field, uint64_t *keys, uint32_t *perm, uint32_t *lut);
+
+/* Dec-band sharding (no reference counterpart). For the target rows
+ * [y0, y1): the sorted positions [*s0, *s1) (positions in hcg_field_sorted's
+ * order; perm maps them to input samples) such that a field made of those
+ * samples alone, in that order, grids the rows as this field does: the
+ * complete rings their pixels visit (HCGrid/gridding.cu:306-323) and one
+ * sample in front, whose ring takes the place of the first used ring that
+ * the reference never grids (gridding.cu:326,363-367). *s0 == *s1 when the
+ * rows see no samples (their pixels are empty: NaN, weight 0). */
+hcg_status hcg_field_band_samples(hcg_context *ctx, const hcg_field *field, const hcg_target *target,
+                                  uint32_t y0, uint32_t y1, uint64_t *s0, uint64_t *s1);
 hcg_status hcg_field_destroy(hcg_field *field);
 /* A second handle on the same resident geometry (sorted samples, LUT, ring
  * table) without spectra: new spectra on known sample positions skip the
