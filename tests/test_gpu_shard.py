@@ -1,9 +1,12 @@
 """Dec-band sharding on one GPU: the bands of a job gridded one after
 another from the sample ranges hcg_field_band_samples gives, assembled, equal
 the whole map gridded at once (each band's pixels meet the same candidates in
-the same order; differences are bounded by the FP32 cube's rounding). A map
-taller than the data has bands that see no sample: NaN rows, weight 0, as
-the whole map has them."""
+the same order). On the FP32 engines that leaves the FP32 cube's rounding;
+a band's FP16 tensor-core split takes its power-of-two channel scales from
+the band's own spectra, so there the two results are each within the FP16
+engine's 1e-5 of the FP64 cube, and within 2e-5 of each other. A map taller
+than the data has bands that see no sample: NaN rows, weight 0, as the whole
+map has them."""
 import numpy as np
 import pytest
 
@@ -11,7 +14,7 @@ from hcgrid_b200 import api, shard, synth
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-6  # of the plane's largest |value|
+TOL = {"single": 1e-6, api.ENGINE_FP32: 1e-6, api.ENGINE_TC_F16: 2e-5}  # of the plane's largest |value|
 
 
 @pytest.fixture(scope="module")
@@ -21,12 +24,12 @@ def ctx():
     c.close()
 
 
-def close(got, ref, w_got, w_ref):
+def close(got, ref, w_got, w_ref, tol):
     nan = np.isnan(ref)
     assert np.array_equal(np.isnan(got), nan)
     ok = ~nan
     if ok.any():
-        assert np.abs(got[ok] - ref[ok]).max() <= TOL * np.abs(ref[ok]).max()
+        assert np.abs(got[ok] - ref[ok]).max() <= tol * np.abs(ref[ok]).max()
     np.testing.assert_allclose(w_got, w_ref, rtol=1e-6, atol=0)
 
 
@@ -77,7 +80,7 @@ def test_bands_equal_whole_map(ctx, job, engine, kernel):
     f.close()
     cube, w, sizes = sharded(ctx, t, j.lon, j.lat, values, 3, weights=weights, engine=eng)
     assert 0 < max(sizes) < j.n  # each band took part of the samples
-    close(cube, ref.reshape(cube.shape), w, wref)
+    close(cube, ref.reshape(cube.shape), w, wref, TOL[engine])
 
 
 def test_bands_beyond_the_data_are_empty(ctx, job):
@@ -93,6 +96,6 @@ def test_bands_beyond_the_data_are_empty(ctx, job):
     f.close()
     cube, w, sizes = sharded(ctx, t, j.lon, j.lat, values, 6)
     assert sizes[0] == 0 and sizes[-1] == 0 and min(sizes[1:-1]) > 0
-    close(cube, ref, w, wref)
+    close(cube, ref, w, wref, TOL[api.ENGINE_FP32])
     assert np.isnan(cube[:16 * 48]).all() and (w[:16 * 48] == 0).all()
     t.close()
