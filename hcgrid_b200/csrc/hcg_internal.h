@@ -159,10 +159,11 @@ inline int tc_class_of(uint32_t cpad) {
 // The tensor-core weight operand holds |w| * (power-of-two weight scale)
 // below 2^15 (FP16 range); weights above 2^100 or not finite stay on FP32.
 inline bool tc_weights_fit(const hcg_field *f) { return f->wbound <= 0x1p100; }
-// The multi-channel engines keep weights as FP32 entries: a multi-channel
-// field whose weight bound passes 2^120 (the reference's taper with a narrow
-// taper width) is refused; single-channel fields sum in FP64.
-inline bool fp32_weights_fit(const hcg_field *f) { return f->nchan <= 1 || !(f->wbound > 0x1p120); }
+// The FP32 engine keeps weights as FP32 entries and sums w x in FP32: a
+// multi-channel field whose weight bound passes 2^100 (the reference's taper
+// with a narrow taper width) is refused, which leaves 2^28 for the sample
+// count times |x| below FP32's range; single-channel fields sum in FP64.
+inline bool fp32_weights_fit(const hcg_field *f) { return f->nchan <= 1 || !(f->wbound > 0x1p100); }
 inline int auto_engine(const hcg_field *f) {
     return (f->xfmt && f->nchan > 1 && f->xnonfinite == 0 && tc_weights_fit(f)) ? f->xfmt : HCG_ENGINE_FP32;
 }

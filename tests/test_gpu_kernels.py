@@ -213,49 +213,45 @@ def test_direct_weight_mode_takes_entries_for_other_kernels(ctx, multi):
 
 def test_weight_range_limits(ctx, multi):
     """The reference's taper with a narrow width a grows to
-    exp((pi r / (sigma a))^2) at the radius. a = 1.08 (about 1e33, above
-    2^100): the tensor cores refuse the field and AUTO grids it on the FP32
-    engine. a = 0.5 (about 1e154, above 2^120): the multi-channel engines
-    refuse it; a single channel grids in FP64 (its weight map overflows
-    FP32 to inf)."""
+    exp((pi r / (sigma a))^2) at the radius: a = 1.08 about 1e33, a = 0.5
+    about 1e154, both above the multi-channel engines' 2^100 (the tensor
+    cores and the FP32 engine refuse such a field, AUTO included). A single
+    channel still grids in FP64; at a = 0.5 its FP32 weight map overflows to
+    inf."""
     job, t, xw, yw = multi
     s, r, res = job.sigma_deg, job.sphere_radius, job.hpx_max_res
-    params = [s, 1.08, 1.55]
-    ctx.prepare_grid_kernel(api.TAPERED_SINC, np.array(params), r, res)
-    f = ctx.field(job.lon, job.lat)
-    f.set_spectra(job.values)
-    f.split_spectra(api.ENGINE_TC_F16)
-    with pytest.raises(api.HcgError) as e:
-        ctx.grid(f, t, engine=api.ENGINE_TC_F16)
-    assert e.value.status == 1
-    cube, w = ctx.grid(f, t)
-    oc, ow, wabs = oracle(job.lon, job.lat, job.values, xw, yw, s, r, res, api.TAPERED_SINC, params)
-    check(cube, w, oc, ow, wabs, job.values, TOL[api.ENGINE_FP32])
-    f.close()
-
-    params = [s, 0.5, 1.55]
-    ctx.prepare_grid_kernel(api.TAPERED_SINC, np.array(params), r, res)
-    f = ctx.field(job.lon, job.lat)
-    f.set_spectra(job.values)
-    for engine in (api.ENGINE_AUTO, api.ENGINE_FP32):
-        with pytest.raises(api.HcgError) as e:
-            ctx.grid(f, t, engine=engine)
-        assert e.value.status == 1
-    f.close()
-    f = ctx.field(job.lon, job.lat)
-    f.set_spectra(np.ascontiguousarray(job.values[:, 0]))
-    cube, w = ctx.grid(f, t)
-    v = job.values[:, :1]
-    oc, ow, wabs = oracle(job.lon, job.lat, v, xw, yw, s, r, res, api.TAPERED_SINC, params)
-    ref = oc / ow[:, None]
-    nan = np.isnan(ref)
-    assert np.array_equal(np.isnan(cube), nan) and (~nan).sum() > 0
-    with np.errstate(divide="ignore", invalid="ignore"):
-        kappa = wabs / np.abs(ow)
-    err = np.abs(cube.astype(np.float64) - ref)[~nan]
-    assert np.all(err <= TOL[SINGLE] * kappa[:, None][~nan] * np.abs(v).max())
-    assert np.all(np.isinf(w[ow > 3.4e38]))
-    f.close()
+    for a in (1.08, 0.5):
+        params = [s, a, 1.55]
+        ctx.prepare_grid_kernel(api.TAPERED_SINC, np.array(params), r, res)
+        f = ctx.field(job.lon, job.lat)
+        f.set_spectra(job.values)
+        for engine in (api.ENGINE_AUTO, api.ENGINE_FP32):
+            with pytest.raises(api.HcgError) as e:
+                ctx.grid(f, t, engine=engine)
+            assert e.value.status == 1
+        f.split_spectra(api.ENGINE_TC_F16)
+        for engine in (api.ENGINE_AUTO, api.ENGINE_TC_F16):
+            with pytest.raises(api.HcgError) as e:
+                ctx.grid(f, t, engine=engine)
+            assert e.value.status == 1
+        f.close()
+        f = ctx.field(job.lon, job.lat)
+        f.set_spectra(np.ascontiguousarray(job.values[:, 0]))
+        cube, w = ctx.grid(f, t)
+        f.close()
+        v = job.values[:, :1]
+        oc, ow, wabs = oracle(job.lon, job.lat, v, xw, yw, s, r, res, api.TAPERED_SINC, params)
+        ref = oc / ow[:, None]
+        nan = np.isnan(ref)
+        assert np.array_equal(np.isnan(cube), nan) and (~nan).sum() > 0
+        with np.errstate(divide="ignore", invalid="ignore"):
+            kappa = wabs / np.abs(ow)
+        err = np.abs(cube.astype(np.float64) - ref)[~nan]
+        assert np.all(err <= TOL[SINGLE] * kappa[:, None][~nan] * np.abs(v).max())
+        with np.errstate(over="ignore"):
+            big = np.isinf(ow.astype(np.float32))  # beyond FP32, either sign
+        assert np.array_equal(np.isinf(w), big) and np.all(np.sign(w[big]) == np.sign(ow[big]))
+        assert np.all(np.abs(w[~big].astype(np.float64) - ow[~big]) <= 1e-6 * wabs[~big] + 1e-300)
 
 
 def test_noalloc_grids_other_kernels(ctx, golden):
