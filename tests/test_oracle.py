@@ -208,3 +208,14 @@ def test_kernel_formulas_single_pairs():
     # the flag is TAPERED_SINC's only
     g = O.GMaps()
     assert O.lib().orc_prepare_grid_kernel(ctypes.byref(g), O.GAUSS2D | O.TAPER_FIX, np.zeros(3), r, sigma / 2) == -1
+
+
+def test_sum_abs_weights_is_the_conditioning(kernels_golden):
+    """Sum |w| per pixel: equal to sum w for positive weights (GAUSS1D), at
+    least |sum w| with the sinc's negative lobes."""
+    z = kernels_golden
+    s = float(z["sigma"])
+    _, w1, _, a1 = _kernel_grid(z, O.GAUSS1D, [s, 0.0, 0.0], want_abs=True)
+    np.testing.assert_allclose(a1, w1, rtol=1e-12)
+    _, w2, _, a2 = _kernel_grid(z, O.TAPERED_SINC, [s, 9.0, 1.55], want_abs=True)
+    assert np.all(a2 >= np.abs(w2) * (1 - 1e-12)) and np.any(a2 > np.abs(w2) * 1.01)
