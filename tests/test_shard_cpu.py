@@ -90,3 +90,52 @@ def test_assemble_over_two_gloo_ranks():
         outs.append(json.loads(out.strip().splitlines()[-1]))
     assert outs[0]["ok"] and outs[0]["bands"] == [[0, 16], [16, 40]]
     assert outs[1]["none"]
+
+
+# The band sample range, argued in hcgrid_b200/csrc/hcg_shard.cu, checked with
+# the FP64 oracle on the CPU: complete rings of the band, one sample in front.
+
+def _band_range(g, ps, xw, yw, p0, p1):
+    """hcg_field_band_samples' rule from the oracle's per-pixel ring ranges."""
+    from oracle import oracle as O
+    lo, hi = None, None
+    for p in range(p0, p1):
+        ur, dr, _, _, _ = O.pixel_windows(g, ps, xw[p], yw[p])
+        if dr >= ur:
+            lo = ur if lo is None else min(lo, ur)
+            hi = dr if hi is None else max(hi, dr)
+    if lo is None:
+        return 0, 0
+    rlo, rend = lo - ps.firstring, hi - ps.firstring + 1
+    a, b = int(ps.lut[rlo]), int(ps.lut[rend])
+    if b <= a:
+        return 0, 0
+    return (a - 1 if a > 0 else 0), b
+
+
+@pytest.mark.parametrize("case", ["synth_dec40", "synth_polar", "synth_wrap"])
+def test_band_sample_ranges_grid_bands_exactly(case):
+    from conftest import load_case
+    from oracle import oracle as O
+    c = load_case(case)
+    g = O.prepare_grid_kernel(float(c["sigma"]), float(c["sphere_radius"]), float(c["hpx_max_res"]))
+    lon, lat = c["lon"], c["lat"]
+    vals = np.asarray(c["values"], np.float64).reshape(len(lon), -1)[:, 0]
+    ps = O.presort(g.hpx, lon, lat)
+    xw, yw = c["xwcs"], c["ywcs"]
+    nx, ny = int(c["nx"]), int(c["ny"])
+    whole, ww, _ = O.grid(g, ps, lon[ps.perm], lat[ps.perm], vals[ps.perm], xw, yw)
+    for y0, y1 in shard.plan(ny, 3):
+        p0, p1 = y0 * nx, y1 * nx
+        s0, s1 = _band_range(g, ps, xw, yw, p0, p1)
+        if s1 == s0:
+            assert np.all(ww[p0:p1] == 0)
+            continue
+        assert s1 - s0 < len(lon)  # a part of the samples
+        idx = ps.perm[s0:s1]
+        gb = O.prepare_grid_kernel(float(c["sigma"]), float(c["sphere_radius"]), float(c["hpx_max_res"]))
+        pb = O.presort(gb.hpx, lon[idx], lat[idx])
+        cb, wb, _ = O.grid(gb, pb, lon[idx][pb.perm], lat[idx][pb.perm], vals[idx][pb.perm], xw[p0:p1], yw[p0:p1])
+        np.testing.assert_array_equal(wb, ww[p0:p1])
+        np.testing.assert_array_equal(cb, whole[p0:p1])
+
