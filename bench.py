@@ -246,11 +246,15 @@ class CStdoutToStderr:
         os.close(self.saved)
 
 
-def cpu_baseline(job, budget_s=20.0):
+def cpu_baseline(job, budget_s=12.0):
     """Reference CPU path on a bounded sample: full pre-sort of all samples
-    plus the kernel body for one channel on a central square of the target;
-    extrapolated to the whole job as HCGrid+ runs it (geometry repeated per
-    channel): T = T_sort + C * T_kernel(1 channel, all pixels)."""
+    plus the kernel body for one channel on central squares of the target,
+    100x100 and then doubling while the sample stays within about `budget_s`
+    (up to the whole map); extrapolated to the whole job as HCGrid+ runs it
+    (geometry repeated per channel): T = T_sort + C * T_kernel, with T_kernel
+    the whole map's time for one channel, measured when the whole map was
+    sampled, else from a + b * pixels fitted to the two largest squares (a:
+    the per-call setup, b: the per-pixel body)."""
     from hcgrid_b200 import api
     from oracle import oracle as O
     nx, ny, xw, yw = api.header_coords(job.header)
@@ -259,10 +263,13 @@ def cpu_baseline(job, budget_s=20.0):
     vals = np.asarray(vals, np.float64).reshape(job.n, -1)[:, 0].copy()
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    side = min(nx, 400 if job.n > 1_000_000 else nx)
-    x0 = (nx - side) // 2
-    sel = (np.arange(side)[:, None] + x0) * nx + (np.arange(side)[None, :] + x0)
-    sx, sy = np.ascontiguousarray(xw[sel.ravel()]), np.ascontiguousarray(yw[sel.ravel()])
+    ny = nx  # square targets (the reference's own assumption, HCGrid/gridding.cu:289)
+
+    def square(side):
+        x0, y0 = (nx - side) // 2, (ny - side) // 2
+        sel = (np.arange(side)[:, None] + y0) * nx + (np.arange(side)[None, :] + x0)
+        return np.ascontiguousarray(xw[sel.ravel()]), np.ascontiguousarray(yw[sel.ravel()])
+
     with CStdoutToStderr():
         if O.have_ref():
             kind = "reference"
@@ -270,9 +277,12 @@ def cpu_baseline(job, budget_s=20.0):
             t0 = time.perf_counter()
             keys, slon, slat, sdat, fr, ur, lut = O.ref_presort(job.lon, job.lat, vals, 2)
             t_sort = time.perf_counter() - t0
-            t0 = time.perf_counter()
-            O.ref_grid(keys, slon, slat, sdat, lut, fr, ur, side, side, sx, sy)
-            t_sub = time.perf_counter() - t0
+
+            def body(side):
+                sx, sy = square(side)
+                t0 = time.perf_counter()
+                O.ref_grid(keys, slon, slat, sdat, lut, fr, ur, side, side, sx, sy)
+                return time.perf_counter() - t0
         else:
             kind = "port"
             g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
@@ -280,17 +290,41 @@ def cpu_baseline(job, budget_s=20.0):
             ps = O.presort(g.hpx, job.lon, job.lat)
             t_sort = time.perf_counter() - t0
             sl, sb, sd = job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm]
-            t0 = time.perf_counter()
-            O.grid(g, ps, sl, sb, sd, sx, sy)
-            t_sub = time.perf_counter() - t0
-    t_kernel = t_sub * P / (side * side)
+
+            def body(side):
+                sx, sy = square(side)
+                t0 = time.perf_counter()
+                O.grid(g, ps, sl, sb, sd, sx, sy)
+                return time.perf_counter() - t0
+        pts = [(min(nx, 100), None)]
+        pts[0] = (pts[0][0], body(pts[0][0]))
+        spent = t_sort + pts[0][1]
+        while pts[-1][0] < nx:
+            s = min(nx, 2 * pts[-1][0])
+            if spent + pts[-1][1] * (s / pts[-1][0]) ** 2 > budget_s:
+                break
+            pts.append((s, body(s)))
+            spent += pts[-1][1]
+    side, t_sub = pts[-1]
+    if side >= nx:
+        t_kernel, how = t_sub, "the whole map measured"
+    else:
+        b, a = t_sub / side ** 2, 0.0
+        if len(pts) >= 2:
+            (s1, t1), (s2, t2) = pts[-2], pts[-1]
+            if t2 > t1:
+                b = (t2 - t1) / (s2 ** 2 - s1 ** 2)
+                a = max(0.0, t1 - b * s1 ** 2)
+        t_kernel = a + b * P
+        how = "extrapolated to %d pixels by a + b * pixels (a = %.3f s, b = %.3g s)" % (P, a, b)
     t_job = t_sort + job.nchan * t_kernel
     value = job.n * job.nchan / t_job
-    sample = ("pre-sort of all %d samples (%.2f s) + kernel body for 1 channel on the central %dx%d pixels "
-              "(%.2f s), extrapolated to %d pixels x %d channels (T = %.1f s)"
-              % (job.n, t_sort, side, side, t_sub, P, job.nchan, t_job))
+    sample = ("pre-sort of all %d samples (%.2f s) + kernel body for 1 channel on central squares of %s pixels "
+              "(%s s); one channel %.2f s (%s), times %d channels (T = %.1f s)"
+              % (job.n, t_sort, ", ".join("%d^2" % s for s, _ in pts), ", ".join("%.2f" % t for _, t in pts),
+                 t_kernel, how, job.nchan, t_job))
     return {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
-            "seconds_measured": t_sort + t_sub}
+            "seconds_measured": round(spent, 2)}
 
 
 # ---------------------------------------------------------------------------
