@@ -65,6 +65,8 @@ def parse():
                          "under 'served_config5' (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the check of the timed cube against the FP64 oracle and the FP32 engine")
     ap.add_argument("--engine", default=None, choices=list(ENGINES),
                     help="channel-sum engine: tensor cores with a 16-bit hi/lo split, or FP32 CUDA cores "
                          "(default: tc-bf16 for config3, tc-f16 otherwise)")
@@ -136,6 +138,12 @@ def job_for(args):
     if args.workload == "config3":
         job.name = "config3"
     return job
+
+
+def workload_text(job):
+    """The workload string both arms report (the same config, the same words)."""
+    return ("%s: %d samples x %d channels -> %dx%d RA---SIN/DEC--SIN, GAUSS1D FWHM %g\", sphere_radius 3 sigma"
+            % (job.name, job.n, job.nchan, job.nx, job.ny, job.fwhm_arcsec))
 
 
 def algorithmic_bytes(n, c, p):
@@ -246,6 +254,19 @@ class CStdoutToStderr:
         os.close(self.saved)
 
 
+def reference_coords(job):
+    """Target pixel centres of the workload's header as the reference computes
+    them (its own read_output_map + set_WCS through oracle/_ref), else, where
+    that build is absent, the library's host SIN projection."""
+    from oracle import oracle as O
+    if O.have_ref():
+        nx, ny, xw, yw = O.ref_header_coords(job.header)
+        return nx, ny, xw, yw, "reference set_WCS (wcslib)"
+    from hcgrid_b200 import api
+    nx, ny, xw, yw = api.header_coords(job.header)
+    return nx, ny, xw, yw, "hcg_header_coords (reference build absent)"
+
+
 def cpu_baseline(job, budget_s=12.0):
     """Reference CPU path on a bounded sample: full pre-sort of all samples
     plus the kernel body for one channel on central squares of the target,
@@ -254,16 +275,16 @@ def cpu_baseline(job, budget_s=12.0):
     (geometry repeated per channel): T = T_sort + C * T_kernel, with T_kernel
     the whole map's time for one channel, measured when the whole map was
     sampled, else from a + b * pixels fitted to the two largest squares (a:
-    the per-call setup, b: the per-pixel body)."""
-    from hcgrid_b200 import api
+    the per-call setup, b: the per-pixel body). Target pixel centres come
+    from the reference's own set_WCS."""
     from oracle import oracle as O
-    nx, ny, xw, yw = api.header_coords(job.header)
+    nx, ny, xw, yw, coords_from = reference_coords(job)
     P = nx * ny
     vals = job.values if job.values is not None else (job.factors[0] @ job.factors[1][:, :1])[:, 0]
     vals = np.asarray(vals, np.float64).reshape(job.n, -1)[:, 0].copy()
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    ny = nx  # square targets (the reference's own assumption, HCGrid/gridding.cu:289)
+    full = min(nx, ny)  # the reference grids square maps (HCGrid/gridding.cu:289)
 
     def square(side):
         x0, y0 = (nx - side) // 2, (ny - side) // 2
@@ -296,17 +317,17 @@ def cpu_baseline(job, budget_s=12.0):
                 t0 = time.perf_counter()
                 O.grid(g, ps, sl, sb, sd, sx, sy)
                 return time.perf_counter() - t0
-        pts = [(min(nx, 100), None)]
+        pts = [(min(full, 100), None)]
         pts[0] = (pts[0][0], body(pts[0][0]))
         spent = t_sort + pts[0][1]
-        while pts[-1][0] < nx:
-            s = min(nx, 2 * pts[-1][0])
+        while pts[-1][0] < full:
+            s = min(full, 2 * pts[-1][0])
             if spent + pts[-1][1] * (s / pts[-1][0]) ** 2 > budget_s:
                 break
             pts.append((s, body(s)))
             spent += pts[-1][1]
     side, t_sub = pts[-1]
-    if side >= nx:
+    if side * side >= P:
         t_kernel, how = t_sub, "the whole map measured"
     else:
         b, a = t_sub / side ** 2, 0.0
@@ -320,11 +341,82 @@ def cpu_baseline(job, budget_s=12.0):
     t_job = t_sort + job.nchan * t_kernel
     value = job.n * job.nchan / t_job
     sample = ("pre-sort of all %d samples (%.2f s) + kernel body for 1 channel on central squares of %s pixels "
-              "(%s s); one channel %.2f s (%s), times %d channels (T = %.1f s)"
+              "(%s s); one channel %.2f s (%s), times %d channels (T = %.1f s); target pixels from %s"
               % (job.n, t_sort, ", ".join("%d^2" % s for s, _ in pts), ", ".join("%.2f" % t for _, t in pts),
-                 t_kernel, how, job.nchan, t_job))
+                 t_kernel, how, job.nchan, t_job, coords_from))
     return {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
             "seconds_measured": round(spent, 2)}
+
+
+def reference_subcube(job, sub, vals):
+    """The checker of the timed cube (part of the CPU leg, outside every
+    timed region): the FP64 oracle (the C restatement of the reference's
+    gridding, pinned bit-exact to the reference's host build) on the target
+    pixels `sub` for the spectra columns `vals` [n, k] (input order). Returns
+    (cube [len(sub), k] normalised, weights, cond [len(sub), k]) with cond =
+    sum(w |x|) / sum(w): the magnitude of the summed terms, the scale of the
+    rounding errors of any summation order."""
+    from oracle import oracle as O
+    _, _, xw, yw, _ = reference_coords(job)
+    g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    ps = O.presort(g.hpx, job.lon, job.lat)
+    v = np.asarray(vals, np.float64)
+    both = np.concatenate([v, np.abs(v)], axis=1)[ps.perm]
+    oc, ow, _ = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], both, xw[sub], yw[sub])
+    with np.errstate(invalid="ignore", divide="ignore"):
+        k = v.shape[1]
+        return oc[:, :k] / ow[:, None], ow, oc[:, k:] / ow[:, None]
+
+
+def error_measures(got, ref, cond=None):
+    """Relative errors of a gridded (sub-)cube against a reference, per
+    channel plane (columns), over the pixels where the reference is finite:
+      plane: max |got - ref| / max |ref| of the plane (the measure of the
+             parity tests);
+      elem:  max |got - ref| / |ref| over elements with |ref| above 1e-3 of
+             their plane's largest |value|;
+      cond:  max |got - ref| / cond, cond = sum(w |x|) / sum(w) per element
+             (relative to the magnitude of the summed terms).
+    The NaN patterns (pixels without samples) must agree."""
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    nan = np.isnan(ref)
+    out = {"nan_pattern_equal": bool(np.array_equal(np.isnan(got), nan))}
+    err = np.where(nan, 0.0, np.abs(got - ref))
+    mag = np.where(nan, 0.0, np.abs(ref))
+    pmax = mag.max(axis=0)
+    out["max_rel_err_plane"] = float((err.max(axis=0) / np.maximum(pmax, 1e-300)).max())
+    big = mag > 1e-3 * pmax[None, :]
+    out["max_rel_err_elem"] = float((err[big] / mag[big]).max()) if big.any() else 0.0
+    if cond is not None:
+        c = np.where(nan, 1.0, np.asarray(cond, np.float64))
+        out["max_rel_err_cond"] = float((err / np.maximum(c, 1e-300)).max())
+    return out
+
+
+def device_cube_errors(torch, got, ref, rows=1 << 17):
+    """error_measures' plane and elem figures of two whole device cubes
+    [pixels][channels] (ref: the FP32 engine's), in row blocks."""
+    P = ref.shape[0]
+    pmax = torch.zeros(ref.shape[1], dtype=torch.float64, device=ref.device)
+    emax = torch.zeros_like(pmax)
+    same_nan = True
+    for i in range(0, P, rows):
+        r, g = ref[i:i + rows].double(), got[i:i + rows].double()
+        nan = torch.isnan(r)
+        same_nan &= bool(torch.equal(nan, torch.isnan(g)))
+        pmax = torch.maximum(pmax, torch.where(nan, 0.0, r.abs()).amax(dim=0))
+        emax = torch.maximum(emax, torch.where(nan, 0.0, (g - r).abs()).amax(dim=0))
+    elem = torch.zeros((), dtype=torch.float64, device=ref.device)
+    for i in range(0, P, rows):
+        r, g = ref[i:i + rows].double(), got[i:i + rows].double()
+        mag = torch.where(torch.isnan(r), 0.0, r.abs())
+        big = mag > 1e-3 * pmax[None, :]
+        rel = torch.where(big, (g - r).abs() / torch.where(big, mag, 1.0), 0.0)
+        elem = torch.maximum(elem, rel.max())
+    return {"nan_pattern_equal": same_nan,
+            "max_rel_err_plane": float((emax / torch.clamp(pmax, min=1e-300)).max()),
+            "max_rel_err_elem": float(elem)}
 
 
 # ---------------------------------------------------------------------------
@@ -607,8 +699,7 @@ def main():
             out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
                    "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                    "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, %s generator)" % job.name,
-                   "config": {"workload": "%s: %d samples x %d channels -> %dx%d SIN, GAUSS1D FWHM %g\""
-                              % (job.name, job.n, job.nchan, job.nx, job.ny, job.fwhm_arcsec)},
+                   "config": {"workload": workload_text(job)},
                    "cpu_baseline": info, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                                                  "d2h_bytes_per_step": 0}}
             print(json.dumps(out))
@@ -638,6 +729,18 @@ def main():
     field = ctx.field(lon_d, lat_d)
     field.set_spectra(S)
     ctx.synchronize()
+    # the checked sub-cube: central side x side pixels x k channels spread over
+    # the band (config 3: 256 x 256 x 64, config 2: 64 x 64 x 16)
+    check = None
+    if rank == 0 and world == 1 and not args.no_check:
+        side = min(256 if job.name == "config3" else 64, job.nx, job.ny)
+        k = min(64 if job.name == "config3" else 16, job.nchan)
+        chans = np.linspace(0, job.nchan - 1, k).round().astype(np.int64)
+        x0, y0 = (job.nx - side) // 2, (job.ny - side) // 2
+        subpix = ((np.arange(side)[:, None] + y0) * job.nx + (np.arange(side)[None, :] + x0)).reshape(-1)
+        vals = S[:, torch.from_numpy(chans).to(dev)].double().cpu().numpy()
+        check = {"side": side, "chans": chans, "sub": subpix, "vals": vals,
+                 "sub_d": torch.from_numpy(subpix).to(dev), "chans_d": torch.from_numpy(chans).to(dev)}
     S_host = None
     if args.e2e_steps > 0:
         S_host = torch.empty((job.n, job.nchan), dtype=torch.float32, pin_memory=True)
@@ -695,7 +798,15 @@ def main():
     ms_per_step = reduce_max(torch, dist, total_ms / args.steps)
     clocks = clk.summary()
     st = ctx.stats()  # counters of the last timed step (before the plain engine runs)
+    timed_sub = None
+    cube_timed = None
+    if check is not None:
+        timed_sub = cube[check["sub_d"]][:, check["chans_d"]].double().cpu().numpy()
+        if plain_steps > 0 and torch.cuda.mem_get_info(dev)[0] > cube.numel() * 4 + (8 << 30):
+            cube_timed = cube.clone()  # the last timed step's cube, against the FP32 engine's below
     plain = None
+    plain_sub = None
+    vs_fp32 = None
     if plain_steps > 0:
         # the plain FP32 CUDA-core engine on the same resident field, same timing rules
         for _ in range(2):
@@ -711,6 +822,13 @@ def main():
         pe1.record(stream)
         torch.cuda.synchronize(dev)
         pms = reduce_max(torch, dist, pe0.elapsed_time(pe1) / plain_steps)
+        if check is not None:
+            plain_sub = cube[check["sub_d"]][:, check["chans_d"]].double().cpu().numpy()
+            if cube_timed is not None:
+                vs_fp32 = device_cube_errors(torch, cube_timed, cube)
+                vs_fp32["what"] = "the whole timed cube against the FP32 engine's cube of the same field"
+                del cube_timed
+                torch.cuda.empty_cache()
         plain = {"engine": ENGINE_TEXT["fp32"], "value": job.n * job.nchan * world / (pms * 1e-3),
                  "ms_per_step": round(pms, 3), "steps": plain_steps, "warmup": 2}
     work = job.n * job.nchan
@@ -828,6 +946,23 @@ def main():
             cpu = cpu_baseline(job)
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "error": repr(ex)}
+    validation = None
+    if check is not None:
+        # the CPU leg's checker, after every timed region
+        try:
+            ref_sub, ref_w, cond = reference_subcube(job, check["sub"], check["vals"])
+            validation = {"reference": "FP64 oracle (C restatement pinned bit-exact to the reference's host build) "
+                                       "on the central %dx%d pixels x %d channels spread over the band"
+                                       % (check["side"], check["side"], len(check["chans"])),
+                          "channels": [int(c) for c in check["chans"]],
+                          "elem_floor": "elements with |ref| > 1e-3 of their plane's max",
+                          "timed_cube_vs_fp64": error_measures(timed_sub, ref_sub, cond)}
+            if plain_sub is not None:
+                validation["fp32_engine_vs_fp64"] = error_measures(plain_sub, ref_sub, cond)
+            if vs_fp32 is not None:
+                validation["timed_cube_vs_fp32_engine"] = vs_fp32
+        except Exception as ex:  # reported, not fatal
+            validation = {"error": repr(ex)}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -835,9 +970,7 @@ def main():
                "scaling": "weak", "vs_baseline": None,
                "dtype": DTYPE_TEXT[args.engine] if job.nchan > 1 else DTYPE_TEXT["fp32"],
                "data": "synthetic (seeded %s generator, hcgrid_b200/synth.py)" % job.name,
-               "config": {"workload": "%s: %d samples x %d channels -> %dx%d RA---SIN/DEC--SIN, GAUSS1D FWHM %g\", "
-                                      "sphere_radius 3 sigma" % (job.name, job.n, job.nchan, job.nx, job.ny,
-                                                                  job.fwhm_arcsec),
+               "config": {"workload": workload_text(job),
                           "samples": job.n, "channels": job.nchan, "pixels": P, "nside": ctx.info(field).nside,
                           "parallelism": "replica per GPU" if world > 1 else "single GPU",
                           "l2": "inputs larger than L2 (spectra %.1f GB), no flush" % (4 * job.n * job.nchan / 1e9),
@@ -846,7 +979,7 @@ def main():
                "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,
                "e2e": e2e, "cpu_baseline": cpu, "plain_fp32": plain,
                "over_plain_fp32": round(value / plain["value"], 3) if plain else None,
-               "served_config5": served}
+               "served_config5": served, "validation": validation}
         print(json.dumps(out))
     field.close()
     target.close()

@@ -79,6 +79,7 @@ EXPORTS = {
     "hcg_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "hcg_synchronize": ([C.c_void_p], C.c_int),
     "hcg_set_entry_budget": ([C.c_void_p, C.c_uint64], C.c_int),
+    "hcg_set_coarsening_factor": ([C.c_void_p, C.c_uint32], C.c_int),
     "hcg_grid_batch": ([C.c_void_p, C.c_uint32, C.c_void_p], C.c_int),
     "hcg_grid_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_server_create": ([C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)], C.c_int),
@@ -299,6 +300,11 @@ class Context:
 
     def set_entry_budget(self, nbytes: int):
         self._check(self.L.hcg_set_entry_budget(self.h, nbytes))
+
+    def set_coarsening_factor(self, factor: int):
+        """HCGrid's coarsening factor (1-3): runs of `factor` pixels along a
+        row take the candidate windows of the run's first pixel."""
+        self._check(self.L.hcg_set_coarsening_factor(self.h, factor))
 
 
 class Server:

@@ -114,6 +114,21 @@ void hcg::Scratch::release(cudaStream_t s) {
     size.clear();
 }
 
+// An output buffer that kernels on `device` may write: its device memory,
+// managed memory, or page-locked host memory mapped into the address space.
+// Pageable host memory and another device's memory are refused before any
+// launch (a kernel writing there would fault).
+static bool writable_on(const void *p, int device) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (at.type == cudaMemoryTypeManaged) return true;
+    if (at.type == cudaMemoryTypeHost) return at.devicePointer != nullptr;
+    return at.type == cudaMemoryTypeDevice && at.device == device;
+}
+
 uint64_t hcg::job_pixels(const hcg_job &job) {
     return job.target ? (uint64_t)job.target->nx * job.target->ny : 0;
 }
@@ -180,6 +195,8 @@ hcg_status hcg::grid_job(hcg_context *ctx, const hcg_job &job) {
     Guard g(ctx);
     if (job.field->ctx->device != ctx->device || job.target->ctx->device != ctx->device)
         return fail(ctx, HCG_EINVAL, "job lives on another device");
+    if (!writable_on(job.cube, ctx->device) || (job.weights && !writable_on(job.weights, ctx->device)))
+        return fail(ctx, HCG_EINVAL, "job outputs are not device memory of the lane's device");
     return grid_checked(ctx, job.field, job.target, job.cube, job.layout, job.weights, HCG_MEM_DEVICE,
                         HCG_ENGINE_AUTO);
 }
@@ -571,6 +588,11 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
     if (!ctx || !field || !target || !cube) return HCG_EINVAL;
     Guard g(ctx);
     if (!ctx->prepared) return fail(ctx, HCG_ESTATE, "hcg_prepare_grid_kernel must come first");
+    if (field->ctx->device != ctx->device || target->ctx->device != ctx->device)
+        return fail(ctx, HCG_EINVAL, "field or target lives on another device than the context");
+    if (mem == HCG_MEM_DEVICE && (!writable_on(cube, ctx->device) || (weights_out && !writable_on(weights_out, ctx->device))))
+        return fail(ctx, HCG_EINVAL, "HCG_MEM_DEVICE outputs must be device memory of the context's device "
+                                     "(or managed or mapped host memory)");
     return grid_checked(ctx, field, target, cube, layout, weights_out, mem, engine);
 }
 
@@ -651,6 +673,9 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
         if (!j.field || !j.target || !j.cube) return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " incomplete");
         if (j.field->ctx->device != ctx->device || j.target->ctx->device != ctx->device)
             return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " lives on another device");
+        if (!writable_on(j.cube, ctx->device) || (j.weights && !writable_on(j.weights, ctx->device)))
+            return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + ": outputs are not device memory of the "
+                                         "context's device");
         if (!j.field->d_spec && auto_engine(j.field) == HCG_ENGINE_FP32)
             return fail(ctx, HCG_ESTATE, "job " + std::to_string(i) + ": field has no spectra for its engine");
         if (!fp32_weights_fit(j.field))
@@ -665,7 +690,8 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
     std::vector<hcg_job> shared;
     std::vector<uint32_t> index;  // shared job -> caller's job
     for (uint32_t i = 0; i < njobs; ++i) {
-        if (jobs[i].field->kernel_type != HCG_GAUSS1D) continue;
+        // coarsened runs grid on the single-job path
+        if (jobs[i].field->kernel_type != HCG_GAUSS1D || ctx->factor > 1) continue;
         shared.push_back(jobs[i]);
         index.push_back(i);
     }
@@ -677,7 +703,7 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
     if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch", why);
     std::vector<char> alone(njobs, 0);
     for (uint32_t k = 0; k < shared.size(); ++k) alone[index[k]] = fallback[k];
-    for (uint32_t i = 0; i < njobs; ++i) alone[i] |= jobs[i].field->kernel_type != HCG_GAUSS1D;
+    for (uint32_t i = 0; i < njobs; ++i) alone[i] |= jobs[i].field->kernel_type != HCG_GAUSS1D || ctx->factor > 1;
     for (uint32_t i = 0; i < njobs; ++i) {
         if (!alone[i]) continue;
         e = grid_field(ctx, jobs[i].field, jobs[i].target, jobs[i].cube, jobs[i].layout, jobs[i].weights,
@@ -728,6 +754,15 @@ hcg_status hcg_set_entry_budget(hcg_context *ctx, uint64_t bytes) {
     if (!ctx || bytes < 4096) return HCG_EINVAL;
     Guard g(ctx);
     ctx->entry_budget = bytes;
+    return HCG_OK;
+}
+
+hcg_status hcg_set_coarsening_factor(hcg_context *ctx, uint32_t factor) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    if (factor < 1 || factor > 3)
+        return fail(ctx, HCG_EINVAL, "coarsening factor must be 1, 2 or 3 (the reference's kernel holds 3 pixels)");
+    ctx->factor = factor;
     return HCG_OK;
 }
 

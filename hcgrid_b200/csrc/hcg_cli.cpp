@@ -7,8 +7,8 @@
 // GAUSS1D with sigma = FWHM / sqrt(8 ln 2) (FWHM = --beam_size arcsec,
 // default 300), sphere_radius = 5 sigma and hpx_max_res = sigma / 2
 // (HCGrid.cpp:141-151). --block_num, --register_num and --sp_num are the
-// reference's launch-shape hints and are accepted; --coarsening_factor is
-// accepted and every pixel keeps its own disc (the reference's factor 1).
+// reference's launch-shape hints and are accepted; --coarsening_factor (1-3)
+// sets h_GMaps.factor, which groups pixels as the reference's kernel does.
 // --sphere_sigmas N changes the 5-sigma radius (e.g. 3 for the README's form).
 #include <getopt.h>
 #include <math.h>
@@ -65,10 +65,15 @@ int main(int argc, char **argv) {
     std::string sorted = sfile ? std::string("!") + path + sfile + num + ".fits" : "";
     double fwhm = (beam ? atoi(beam) : 300) / 3600.;
     double sigma = fwhm / sqrt(8 * log(2));
-    double kp[3] = {sigma, 0.0, 0.0};
+    _Healpix_init(1, 2);
+    // heap-allocated as the reference's driver does: _prepare_grid_kernel
+    // retains it and data_free releases it
+    double *kp = (double *)calloc(3, sizeof(double));
+    if (!kp) return 1;
+    kp[0] = sigma;
     double k = nsig ? atof(nsig) : 5.0;
     _prepare_grid_kernel(HCG_GAUSS1D, kp, k * sigma, sigma / 2.);
-    if (factor && atoi(factor) > 1) fprintf(stderr, "HCGrid: coarsening factor %s accepted; each pixel keeps its own disc\n", factor);
+    h_GMaps.factor = factor ? (uint32_t)atoi(factor) : 1;
     int ord = atoi(order), bd = bdim ? atoi(bdim) : 64;
     printf("order: %s, num: %s, ", order, num);
     solve_gridding(in.c_str(), tar.c_str(), out.c_str(), sfile ? sorted.c_str() : nullptr, ord, bd);

@@ -124,6 +124,27 @@ __global__ void k_row_offsets(const unsigned long long *__restrict__ off, uint64
     out[r] = off[g0];
 }
 
+// Coarsening: pixel p of row-run [lead, lead + factor) takes the ring range,
+// the phi halves of its windows and the polar rule of the run's first pixel
+// (HCGrid/gridding.cu:284-308: the disc of l1[0], b1[0]); its own l1, b1,
+// cb1 stay for distance and weight. Leaders are only read, so in place.
+__global__ void k_coarsen(PixPrep *__restrict__ prep, uint32_t nx, uint64_t npix, uint32_t factor) {
+    const uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    const uint32_t x = (uint32_t)(p % nx), back = x % factor;
+    if (back == 0) return;
+    const PixPrep L = prep[p - back];
+    PixPrep &P = prep[p];
+    for (int e = 0; e < 2; ++e) {
+        P.tt[e] = L.tt[e];
+        P.t1[e] = L.t1[e];
+        P.tp[e] = L.tp[e];
+    }
+    P.ur = L.ur;
+    P.nr = L.nr;
+    P.polar = L.polar;
+}
+
 // Target pixel centres of a SIN header, one thread per pixel.
 __global__ void k_sin_coords(SinWcs w, uint32_t nx, uint64_t npix, double *__restrict__ X, double *__restrict__ Y) {
     uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -135,6 +156,12 @@ __global__ void k_sin_coords(SinWcs w, uint32_t nx, uint64_t npix, double *__res
 }
 
 }  // namespace
+
+cudaError_t coarsen_prep(PixPrep *prep, uint32_t nx, uint64_t npix, uint32_t factor, cudaStream_t s) {
+    if (factor <= 1 || npix == 0) return cudaSuccess;
+    k_coarsen<<<(unsigned)((npix + 255) / 256), 256, 0, s>>>(prep, nx, npix, factor);
+    return cudaGetLastError();
+}
 
 cudaError_t sin_coords_device(const SinWcs &w, uint32_t nx, uint32_t ny, double *d_x, double *d_y, cudaStream_t s) {
     uint64_t n = (uint64_t)nx * ny;
@@ -155,6 +182,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
     cudaEventRecord(ctx->ev0, s);
     k_pixel_prep<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(f->hpx, f->firstring, f->usedrings, f->disc_size, P,
                                                               t->d_x, t->d_y, prep, ctx->d_stats);
+    if ((e = coarsen_prep(prep, t->nx, P, ctx->factor, s)) != cudaSuccess) return e;
     cudaEventRecord(ctx->evp[0], s);
     const GridArgs a = grid_args(f, prep, ctx->d_stats);
     if (f->nchan == 1) {

@@ -101,6 +101,7 @@ struct hcg_context {
     unsigned long long entry_budget = 4ULL << 30;  // bytes of (sample, weights) entries per launch run
     int tc_config[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // tensor-core pipeline shape per channel class (-1: default)
     int tc_weights = 0;  // tensor-core weight operands: 0 automatic, 1 from entries, 2 evaluated in the kernel
+    uint32_t factor = 1;  // coarsening factor (hcg_set_coarsening_factor)
     void *batch = nullptr;                          // batch engine state (hcg_batch.cu)
 };
 
@@ -184,6 +185,9 @@ inline bool tc_use_weights(const hcg_context *ctx, const hcg_field *f, unsigned 
 cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, const double *d_lat,
                         const double *d_w, std::string &why);
 cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, uint32_t nchan, int layout);
+// Coarsening (hcg_set_coarsening_factor): each pixel takes the window fields
+// of the first pixel of its run of `factor` along its row.
+cudaError_t coarsen_prep(PixPrep *prep, uint32_t nx, uint64_t npix, uint32_t factor, cudaStream_t s);
 cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t, float *d_cube, int layout,
                        float *d_wts, int engine, std::string &why);
 // hcg_tc.cu: hi/lo split of a field's spectra; tensor-core accumulation

@@ -1,13 +1,14 @@
 // Single-channel gridding that allocates nothing (hcg_grid_noalloc).
 //
 // Who needs it: callers that cannot allocate device memory at the time they
-// grid. A real-time pipeline that reserves its device memory when it starts
-// and must not meet an allocation failure (or the stall of a device-wide
-// allocation) in the middle of an observation, and code that grids while a
-// stream capture is open, where cudaMalloc is not permitted, are the usual
-// cases. hcg_grid takes its per-pixel scratch from the context's pool, which
-// may have to grow; this entry point takes it from a fixed array compiled
-// into the library instead.
+// grid. A real-time pipeline (a telescope backend gridding each scan as it
+// lands) reserves its device memory when it starts and must not meet an
+// allocation failure, or the device-wide stall of cudaMalloc/cudaFree, in the
+// middle of an observation; a host application whose own allocator already
+// holds the GPU's memory lends the library only the inputs and outputs.
+// hcg_grid takes its per-pixel scratch from the context's pool, which may
+// have to grow; this entry point takes it from a fixed array compiled into
+// the library instead.
 //
 // The scratch is the per-pixel setup (ring range and the phi half of the
 // window arithmetic, 96 bytes a pixel) in a file-scope __device__ array of
@@ -55,13 +56,15 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 PixPrep *g_prep_addr[kMaxDevices] = {};
 
-bool is_device_memory(const void *p) {
+// Device (or managed) memory that kernels on `device` may write.
+bool is_device_memory(const void *p, int device) {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    if (at.type == cudaMemoryTypeManaged) return true;
+    return at.type == cudaMemoryTypeDevice && at.device == device;
 }
 
 }  // namespace
@@ -84,11 +87,18 @@ extern "C" hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field,
                    std::to_string(kNoAllocMaxPixels) + " (use hcg_grid)";
         return HCG_EINVAL;
     }
-    if (!is_device_memory(cube) || (weights_out && !is_device_memory(weights_out))) {
-        ctx->err = "hcg_grid_noalloc writes device buffers only";
+    if (field->ctx->device != ctx->device || target->ctx->device != ctx->device) {
+        ctx->err = "hcg_grid_noalloc: field or target lives on another device than the context";
         return HCG_EINVAL;
     }
-    if (ctx->device < 0 || ctx->device >= kMaxDevices) return HCG_EINVAL;
+    if (!is_device_memory(cube, ctx->device) || (weights_out && !is_device_memory(weights_out, ctx->device))) {
+        ctx->err = "hcg_grid_noalloc writes device buffers of the context's device only";
+        return HCG_EINVAL;
+    }
+    if (ctx->device < 0 || ctx->device >= kMaxDevices) {
+        ctx->err = "hcg_grid_noalloc supports device ordinals below " + std::to_string(kMaxDevices);
+        return HCG_EINVAL;
+    }
     PixPrep *prep;
     {
         std::lock_guard<std::mutex> g(g_setup_mu);
@@ -106,12 +116,16 @@ extern "C" hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field,
         prep = g_prep_addr[ctx->device];
     }
     cudaStream_t s = ctx->stream;
+    // every counter hcg_get_stats reports starts at zero, as in hcg_grid
     cudaError_t e = cudaMemsetAsync(ctx->d_stats, 0, offsetof(DevStats, invalid_input), s);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(&ctx->d_stats->timeouts, 0, 2 * sizeof(unsigned long long), s);
     if (e == cudaSuccess) {
         cudaEventRecord(ctx->ev0, s);
         k_noalloc_prep<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(field->hpx, field->firstring, field->usedrings,
                                                                     field->disc_size, P, target->d_x, target->d_y,
                                                                     prep, ctx->d_stats);
+        e = coarsen_prep(prep, target->nx, P, ctx->factor, s);
         for (auto &ev : ctx->evp) cudaEventRecord(ev, s);
         const GridArgs a = grid_args(field, prep, ctx->d_stats);
         const unsigned nblk = (unsigned)((P * 32 + 255) / 256);
@@ -120,7 +134,7 @@ extern "C" hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field,
         else
             k_noalloc_grid<true><<<nblk, 256, 0, s>>>(a, P, field->d_spec, field->cstride, cube, weights_out);
         cudaEventRecord(ctx->ev1, s);
-        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGetLastError();
     }
     if (e != cudaSuccess) {
         cudaGetLastError();

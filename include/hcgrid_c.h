@@ -257,21 +257,36 @@ hcg_status hcg_server_destroy(hcg_server *server);
  * (default 4 GiB). */
 hcg_status hcg_set_entry_budget(hcg_context *ctx, uint64_t bytes);
 
+/* HCGrid's coarsening factor (h_GMaps.factor, HCGrid/gridding.cu:284-308):
+ * the pixels of each target row are taken in runs of `factor` (1-3) from
+ * x = 0; every pixel of a run takes the ring range, the HEALPix pixel
+ * windows of each ring and the polar rule from the disc of the run's first
+ * pixel, and keeps its own distance, cutoff and weight. 1 (the default):
+ * every pixel its own disc. Applies to hcg_grid and hcg_grid_noalloc on
+ * this context; hcg_grid_batch on a context with factor > 1 grids each job
+ * on its own. */
+hcg_status hcg_set_coarsening_factor(hcg_context *ctx, uint32_t factor);
+
 /* Wait for all work queued on the context's stream. */
 hcg_status hcg_synchronize(hcg_context *ctx);
 
-/* hcg_grid for single-channel fields without any allocation, for callers
- * that cannot allocate device memory when they grid (a pipeline that fixed
- * its device memory at start-up, or code running inside an open stream
- * capture, where cudaMalloc is not allowed). No counterpart in the
- * reference. Its per-pixel scratch is a fixed array inside the library of
+/* hcg_grid for single-channel fields without any allocation. No counterpart
+ * in the reference. For callers that cannot allocate device memory at the
+ * time they grid: a real-time pipeline (a telescope backend gridding each
+ * scan as it lands) that reserves all its device memory when it starts, so
+ * that an observation never meets an allocation failure or the device-wide
+ * stall of cudaMalloc/cudaFree; or a host application whose own allocator
+ * already holds the GPU's memory and lends the library only the inputs and
+ * outputs. Its per-pixel scratch is a fixed array inside the library of
  * 131072 pixels (12 MiB, held on every GPU that loads the library until the
  * process exits): larger targets are rejected with HCG_EINVAL. cube and
- * weights_out (optional) are device buffers of nx*ny floats. The first call
- * on a device looks up the array's device address; make it before any stream
- * capture. Calls share the array, so calls whose work overlaps on the GPU
- * race: issue them one after another. Asynchronous on the context's stream,
- * like hcg_grid with device buffers. */
+ * weights_out (optional) are device buffers of nx*ny floats on the
+ * context's device, and field and target must belong to a context on that
+ * device (HCG_EINVAL otherwise, before anything is launched). The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture. Calls share the array, so calls whose work overlaps on the
+ * GPU race: issue them one after another. Asynchronous on the context's
+ * stream, like hcg_grid with device buffers. */
 hcg_status hcg_grid_noalloc(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube,
                             float *weights_out);
 

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import re
 import subprocess
 
 import numpy as np
@@ -34,10 +35,32 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 
-def build(with_ref: bool = True) -> None:
-    """Compile the restatement (and the reference build when its tree exists)."""
-    targets = ["oracle"] + (["ref"] if with_ref else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+def reference_root() -> str:
+    """Where the reference tree lies: $HCG_REFERENCE, else the REF default
+    that oracle/Makefile's recipe reads it from (one place holds that path)."""
+    env = os.environ.get("HCG_REFERENCE")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as fh:
+        for line in fh:
+            m = re.match(r"\s*REF\s*\?=\s*(\S+)", line)
+            if m:
+                return m.group(1)
+    return ""
+
+
+def reference_data() -> str:
+    """The reference's test fixtures (input1.fits, target1.fits)."""
+    return os.path.join(reference_root(), "test_data")
+
+
+def build(with_ref: bool = True, dropin: bool = False) -> None:
+    """Compile the restatement (and the reference build when its tree
+    exists); `dropin` also links the reference's own driver, unchanged,
+    against the B200 library (the relink check of the C++ boundary)."""
+    targets = ["oracle"] + (["ref"] if with_ref else []) + (["dropin"] if dropin and with_ref else [])
+    env = dict(os.environ, REF=reference_root())
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True, env=env)
 
 
 class Healpix(C.Structure):
@@ -289,7 +312,9 @@ def ref_presort(lons, lats, data, order_arg=2):
     return keys, lo, la, da, fr.value, ur.value, lut[: ur.value + 1].copy()
 
 
-def ref_grid(keys, lons, lats, data, lut, firstring, usedrings, nx, ny, xwcs, ywcs, weights=None):
+def ref_grid(keys, lons, lats, data, lut, firstring, usedrings, nx, ny, xwcs, ywcs, weights=None, factor=1):
+    """The reference's kernel body on the host (one channel, square maps);
+    `factor` is its coarsening factor h_GMaps.factor (1-3)."""
     n = len(lons)
     if weights is None:
         weights = np.ones(n)
@@ -299,7 +324,7 @@ def ref_grid(keys, lons, lats, data, lut, firstring, usedrings, nx, ny, xwcs, yw
     ref().ref_grid(n, keys, np.ascontiguousarray(lons, np.float64), np.ascontiguousarray(lats, np.float64),
                    np.ascontiguousarray(data, np.float64), np.ascontiguousarray(weights, np.float64), lut,
                    firstring, usedrings, nx, ny, np.ascontiguousarray(xwcs, np.float64),
-                   np.ascontiguousarray(ywcs, np.float64), 1, cube, wts)
+                   np.ascontiguousarray(ywcs, np.float64), factor, cube, wts)
     return cube, wts
 
 
@@ -311,3 +336,27 @@ def ref_target_wcs(path: str, cap: int = 1 << 24):
     assert ok == 1
     num = nx.value * ny.value
     return nx.value, ny.value, nz.value, xw[:num].copy(), yw[:num].copy()
+
+
+def ref_header_coords(header: str):
+    """Target pixel centres of a FITS header through the reference's own
+    read_output_map + set_WCS (wcslib's wcsp2s, HCGrid/gmap.cpp:151-250):
+    the header is written as a header-only FITS file and read back by the
+    reference's host build. Returns (nx, ny, xwcs, ywcs) in degrees."""
+    import tempfile
+    assert len(header) % 80 == 0
+    cards = [header[i:i + 80] for i in range(0, len(header), 80)]
+    kv = {c[:8].strip(): c[10:].split("/")[0].strip() for c in cards if c[8:10] == "= "}
+    n = 1
+    for i in range(1, int(kv["NAXIS"]) + 1):
+        n *= int(kv["NAXIS%d" % i])
+    nb = n * abs(int(kv["BITPIX"])) // 8
+    h = header.encode("ascii")
+    h += b" " * ((-len(h)) % 2880)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "target.fits")
+        with open(p, "wb") as fh:
+            fh.write(h)
+            fh.write(b"\0" * (nb + (-nb) % 2880))
+        nx, ny, _, xw, yw = ref_target_wcs(p, cap=max(1 << 20, n))
+    return nx, ny, xw, yw

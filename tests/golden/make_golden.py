@@ -35,7 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 import fitsutil as F  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REF_DATA = "/root/reference/test_data"
+REF_DATA = O.reference_data()
 
 
 def target_coords(header: str):

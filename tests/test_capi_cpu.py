@@ -69,7 +69,7 @@ WCS_CASES = [(30, 40, 300, 60 / 3600), (0.3, 10, 40, 90 / 3600), (120, 76, 40, 7
 def test_header_coords_match_wcslib(case):
     import fitsutil
     if case == "target1":
-        hdr = _reference_header("/root/reference/test_data/target1.fits")
+        hdr = _reference_header(os.path.join(O.reference_data(), "target1.fits"))
     else:
         ra, dec, nx, pix = case
         hdr = synth.sin_header(nx, nx, ra, dec, pix)

@@ -7,9 +7,10 @@ import pytest
 
 from conftest import load_case
 from hcgrid_b200 import api, synth
+from oracle import oracle as O
 import fitsutil
 
-REF_DATA = "/root/reference/test_data"
+REF_DATA = O.reference_data()
 
 
 def test_read_input_map_matches_golden():

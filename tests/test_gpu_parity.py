@@ -254,6 +254,14 @@ def test_invalid_inputs_are_rejected(ctx):
         with pytest.raises(api.HcgError) as e:
             ctx.prepare_grid_kernel(kt, np.array([0.02, 0.01, 0.3]), 0.06, 0.01)
         assert e.value.status == 1
+    # outputs declared as device memory must be writable by the context's
+    # device: pageable host memory is refused before anything is launched
+    import ctypes as C
+    host = np.zeros(4, np.float32)
+    st = ctx.L.hcg_grid(ctx.h, f1.h, t.h, host.ctypes.data_as(C.c_void_p), api.SAMPLE_MAJOR, None,
+                        api.MEM_DEVICE, api.ENGINE_AUTO)
+    assert st == 1 and b"device memory" in ctx.L.hcg_last_error(ctx.h)
+    assert np.all(host == 0)
 
 
 def test_empty_pixels_are_nan_and_single_sample_weight(ctx):

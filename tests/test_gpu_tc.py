@@ -2,10 +2,13 @@
 the FP64 oracle and the FP32 engine, through the C ABI.
 
 Tolerances, relative to the largest |value| of each channel plane (the
-measure of the FP32 parity tests):
-  * FP16 hi/lo: 1e-5 (per-term error of the three-product split ~3 * 2^-22,
-    plus FP32 accumulation);
-  * BF16 hi/lo: 5e-5 (per-term bound 3 * 2^-16 = 4.6e-5).
+measure of the FP32 parity tests), 1e-5 for both splits, the bound the
+north-star workload states:
+  * FP16 hi/lo: per-term error of the three-product split ~3 * 2^-22, plus
+    FP32 accumulation (measured up to 7.3e-6 on the densest field);
+  * BF16 hi/lo: per-term bound 3 * 2^-16 = 4.6e-5, but the errors of the
+    many terms of a pixel are independent and partly cancel: measured up to
+    5.9e-6 on every field here.
 Weights are the FP64 sums of the same entries the FP32 engine uses, so the
 weight map is bit-identical to the FP32 engine's, as is the NaN pattern of
 empty pixels."""
@@ -17,7 +20,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-TOL = {api.ENGINE_TC_F16: 1e-5, api.ENGINE_TC_BF16: 5e-5}
+TOL = {api.ENGINE_TC_F16: 1e-5, api.ENGINE_TC_BF16: 1e-5}
 ENGINES = [api.ENGINE_TC_F16, api.ENGINE_TC_BF16]
 
 
@@ -374,5 +377,59 @@ def test_config3_precision_subcube(ctx):
           % (errs[api.ENGINE_TC_BF16], errs[api.ENGINE_TC_F16]))
     assert errs[api.ENGINE_TC_BF16] <= TOL[api.ENGINE_TC_BF16]
     assert errs[api.ENGINE_TC_F16] <= TOL[api.ENGINE_TC_F16]
+    f.close()
+    t.close()
+
+
+def test_config2_full_size_subcube(ctx):
+    """The headline workload at its full size (config 2: 4,000,000 samples x
+    1,024 channels onto 1200 x 1200 pixels): the tensor-core cube (FP16
+    hi/lo, the pipeline shape the engine picks for this size, accumulation
+    segments, entry runs) and the FP32 engine's cube on the central 64 x 64
+    pixels x 16 channels spread over the band, against the FP64 oracle."""
+    torch = pytest.importorskip("torch")
+    job = synth.config2()
+    assert (job.n, job.nchan, job.nx, job.ny) == (4_000_000, 1024, 1200, 1200)
+    prepare(ctx, job)
+    G, L, noise = job.factors
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(job.seed)
+    S = torch.empty((job.n, job.nchan), dtype=torch.float32, device=dev)
+    Ld = torch.from_numpy(L).to(dev)
+    for i in range(0, job.n, 1 << 18):
+        Gd = torch.from_numpy(G[i:i + (1 << 18)]).to(dev)
+        torch.matmul(Gd, Ld, out=S[i:i + (1 << 18)])
+        S[i:i + (1 << 18)].add_(torch.randn((Gd.shape[0], job.nchan), generator=gen, device=dev), alpha=noise)
+    chans = np.linspace(0, job.nchan - 1, 16).round().astype(np.int64)
+    vals = S[:, torch.from_numpy(chans).to(dev)].double().cpu().numpy()
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(S)
+    del S
+    t = ctx.target_from_header(job.header)
+    xw, yw = t.coords()
+    y0 = x0 = (1200 - 64) // 2
+    sub = ((np.arange(64)[:, None] + y0) * 1200 + (np.arange(64)[None, :] + x0)).reshape(-1)
+    g = O.prepare_grid_kernel(job.sigma_deg, job.sphere_radius, job.hpx_max_res)
+    ps = O.presort(g.hpx, job.lon, job.lat)
+    oc, ow, _ = O.grid(g, ps, job.lon[ps.perm], job.lat[ps.perm], vals[ps.perm], xw[sub], yw[sub])
+    ref = oc / ow[:, None]
+    P = 1200 * 1200
+    sub_d, chans_d = torch.from_numpy(sub).to(dev), torch.from_numpy(chans).to(dev)
+    errs = {}
+    f.split_spectra(api.ENGINE_TC_F16)
+    for engine in (api.ENGINE_TC_F16, api.ENGINE_FP32):
+        cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
+        w = torch.empty(P, dtype=torch.float32, device=dev)
+        ctx.grid(f, t, cube, w, engine=engine)
+        got = cube[sub_d][:, chans_d].cpu().numpy()
+        errs[engine] = plane_errors(got, ref)
+        ok = ow > 0
+        assert np.abs(w[sub_d].cpu().numpy()[ok] - ow[ok]).max() / ow.max() <= 1e-6
+        del cube
+    print("config-2 full size, 64x64x16 sub-cube max plane-relative error: tc f16 %.3e, fp32 %.3e"
+          % (errs[api.ENGINE_TC_F16], errs[api.ENGINE_FP32]))
+    assert errs[api.ENGINE_TC_F16] <= TOL[api.ENGINE_TC_F16]
+    assert errs[api.ENGINE_FP32] <= 1e-5
     f.close()
     t.close()
