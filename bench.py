@@ -72,6 +72,9 @@ def parse():
                          "(default: tc-bf16 for config3, tc-f16 otherwise)")
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="also time this many steps of the plain FP32 engine on the same field (0: skip)")
+    ap.add_argument("--tc-prefetch", type=int, default=-1, help="with --tc-config: prefetch distance (chunks)")
+    ap.add_argument("--tc-strip", type=int, default=-1, help="with --tc-config: persistent tile walk strip width")
+    ap.add_argument("--tune-reps", type=int, default=3, help="timed runs per autotuner setting")
     ap.add_argument("--tc-config", type=int, default=None,
                     help="tensor-core pipeline shape (0: 256 ch x 64-sample chunks x 2 stages, 1: 128 x 64 x 3, "
                          "2: 64 x 64 x 4, 3: 256 x 32 x 4, 4/5: 0/3 persistent); "
@@ -764,11 +767,14 @@ def main():
                             "direct": api.TC_WEIGHTS_DIRECT}[args.tc_weights])
         if args.tc_config is not None:
             ctx.tc_set_config(args.tc_config)
-            tune = {"config": args.tc_config, "how": "fixed by --tc-config"}
+            ctx.tc_set_pipeline(args.tc_prefetch, args.tc_strip)
+            tune = {"config": args.tc_config, "prefetch": args.tc_prefetch, "strip": args.tc_strip,
+                    "how": "fixed by --tc-config/--tc-prefetch/--tc-strip (-1: defaults)"}
         else:
-            best, ms = ctx.autotune(field, target, reps=2)
-            tune = {"config": best, "ms_per_config": [round(m, 3) for m in ms],
-                    "how": "hcg_autotune: best of 2 timed runs per pipeline shape"}
+            tune = ctx.autotune_ex(field, target, reps=args.tune_reps)
+            tune["how"] = ("hcg_autotune_ex: pipeline shape, then prefetch distance, then tile walk; each setting "
+                           "the best of %d timed runs after a warm-up; spread = (slowest - fastest) / fastest of "
+                           "the chosen setting's runs" % args.tune_reps)
     for _ in range(args.warmup):
         ctx.grid(field, target, cube, wts, engine=engine)
     ctx.synchronize()

@@ -42,6 +42,16 @@ class Info(C.Structure):
                 ("sphere_radius", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("shape", C.c_int), ("prefetch", C.c_int), ("strip", C.c_int), ("ms_shape", C.c_float * 6),
+                ("ms_prefetch", C.c_float * 5), ("ms_strip", C.c_float * 5), ("ms_best", C.c_float),
+                ("spread", C.c_float)]
+
+
+TUNE_PREFETCH = (2, 4, 6, 8, 12)
+TUNE_STRIP = (0, 4, 8, 16, 32)
+
+
 class Stats(C.Structure):
     _fields_ = [("pairs_candidate", C.c_uint64), ("pairs_within", C.c_uint64), ("ring_skips", C.c_uint64),
                 ("hard_roundings", C.c_uint64), ("ms_total", C.c_double), ("ms_phase", C.c_double * 4),
@@ -62,6 +72,8 @@ EXPORTS = {
     "hcg_tc_set_config": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_tc_set_weights": ([C.c_void_p, C.c_int], C.c_int),
     "hcg_autotune": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "hcg_autotune_ex": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p], C.c_int),
+    "hcg_tc_set_pipeline": ([C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_int),
     "hcg_field_sorted": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_field_band_samples": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p],
                                C.c_int),
@@ -78,6 +90,7 @@ EXPORTS = {
     "hcg_grid": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
     "hcg_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "hcg_synchronize": ([C.c_void_p], C.c_int),
+    "hcg_context_trim": ([C.c_void_p], C.c_int),
     "hcg_set_entry_budget": ([C.c_void_p, C.c_uint64], C.c_int),
     "hcg_set_coarsening_factor": ([C.c_void_p, C.c_uint32], C.c_int),
     "hcg_grid_batch": ([C.c_void_p, C.c_uint32, C.c_void_p], C.c_int),
@@ -272,6 +285,10 @@ class Context:
     def synchronize(self):
         self._check(self.L.hcg_synchronize(self.h))
 
+    def trim(self):
+        """Return the device memory the context's pool keeps for reuse."""
+        self._check(self.L.hcg_context_trim(self.h))
+
     def tc_set_config(self, config: int, channel_class: int = -1):
         self._check(self.L.hcg_tc_set_config(self.h, channel_class, config))
 
@@ -280,6 +297,21 @@ class Context:
         TC_WEIGHTS_ENTRIES (FP64 weight pass) or TC_WEIGHTS_DIRECT (evaluated in
         the kernel)."""
         self._check(self.L.hcg_tc_set_weights(self.h, mode))
+
+    def tc_set_pipeline(self, prefetch: int = -1, strip: int = -1, channel_class: int = -1):
+        """Prefetch distance (chunks) and persistent tile walk (strip width in
+        tiles, 0: rows) of the tensor-core engine; -1 restores the default."""
+        self._check(self.L.hcg_tc_set_pipeline(self.h, channel_class, prefetch, strip))
+
+    def autotune_ex(self, field: "Field", target: "Target", reps: int = 3) -> dict:
+        """The full search: shape, then prefetch distance, then tile walk."""
+        t = Tuning()
+        self._check(self.L.hcg_autotune_ex(self.h, field.h, target.h, reps, C.byref(t)))
+        return {"shape": t.shape, "prefetch": t.prefetch, "strip": t.strip,
+                "ms_shape": [round(x, 3) for x in t.ms_shape],
+                "ms_prefetch": dict(zip(TUNE_PREFETCH, [round(x, 3) for x in t.ms_prefetch])),
+                "ms_strip": dict(zip(TUNE_STRIP, [round(x, 3) for x in t.ms_strip])),
+                "ms_best": round(t.ms_best, 3), "spread": round(t.spread, 4), "reps": reps}
 
     def autotune(self, field: "Field", target: "Target", reps: int = 2):
         """Time each tensor-core pipeline shape on (field, target); keeps and

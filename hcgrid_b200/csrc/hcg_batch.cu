@@ -260,13 +260,14 @@ struct BatchState {
     unsigned long long *d_jusum = nullptr, *h_jusum = nullptr;  // per job: staged slots of its tiles (sum, largest)
     uint32_t map_cap = 0;
     unsigned long long entry_cap = 0;
+    cudaMemPool_t pool = nullptr;  // the context's memory pool
 };
 
 static cudaError_t grow(BatchState &B, int slot, size_t bytes, cudaStream_t s, void **out) {
     if (B.scratch_size[slot] < bytes) {
         if (B.scratch[slot]) cudaFreeAsync(B.scratch[slot], s);
         size_t want = bytes + bytes / 4 + 256;
-        cudaError_t e = cudaMallocAsync(&B.scratch[slot], want, s);
+        cudaError_t e = dalloc(&B.scratch[slot], want, s, B.pool);
         if (e != cudaSuccess) {
             B.scratch[slot] = nullptr;
             B.scratch_size[slot] = 0;
@@ -346,8 +347,9 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
     cudaError_t e = cudaSuccess;
     if (!ctx->batch) {
         BatchState *B = new BatchState();
+        B->pool = ctx->pool;
         cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
-        if ((e = cudaMallocAsync(&B->d_hdr, sizeof(BatchHdr), s)) != cudaSuccess ||
+        if ((e = dalloc(&B->d_hdr, sizeof(BatchHdr), s, ctx->pool)) != cudaSuccess ||
             (e = cudaMallocHost(&B->h_hdr, sizeof(BatchHdr))) != cudaSuccess) {
             if (B->d_hdr) cudaFreeAsync(B->d_hdr, s);
             if (B->h_hdr) cudaFreeHost(B->h_hdr);
@@ -367,20 +369,20 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if (B.d_jusum) cudaFreeAsync(B.d_jusum, s);
         if (B.h_jusum) cudaFreeHost(B.h_jusum);
         B.job_cap = std::max<uint32_t>(njobs, 64);
-        if ((e = cudaMallocAsync(&B.d_jobs, B.job_cap * sizeof(JobDesc), s)) != cudaSuccess) return e;
+        if ((e = dalloc(&B.d_jobs, B.job_cap * sizeof(JobDesc), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jobs, B.job_cap * sizeof(JobDesc))) != cudaSuccess) return e;
-        if ((e = cudaMallocAsync(&B.d_jovf, B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = dalloc(&B.d_jovf, B.job_cap * sizeof(unsigned long long), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jovf, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
-        if ((e = cudaMallocAsync(&B.d_jent, B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = dalloc(&B.d_jent, B.job_cap * sizeof(unsigned long long), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jent, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
-        if ((e = cudaMallocAsync(&B.d_jusum, 2 * B.job_cap * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = dalloc(&B.d_jusum, 2 * B.job_cap * sizeof(unsigned long long), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jusum, 2 * B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
     }
     if (2 * njobs > B.map_cap) {
         if (B.d_maps) cudaFreeAsync(B.d_maps, s);
         if (B.h_maps) cudaFreeHost(B.h_maps);
         B.map_cap = std::max<uint32_t>(2 * njobs, 128);
-        if ((e = cudaMallocAsync(&B.d_maps, B.map_cap * sizeof(CUtensorMap), s)) != cudaSuccess) return e;
+        if ((e = dalloc(&B.d_maps, B.map_cap * sizeof(CUtensorMap), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_maps, B.map_cap * sizeof(CUtensorMap))) != cudaSuccess) return e;
     }
     // item spaces and scratch sizes

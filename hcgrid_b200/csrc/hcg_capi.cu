@@ -76,7 +76,8 @@ void release_field(hcg_field *f, cudaStream_t s) {
     if (f->d_spec) cudaFreeAsync(f->d_spec, s);
     free_split(f, s);
     if (f->geom_refs && --*f->geom_refs > 0) return;
-    void *ps[] = {f->d_keys, f->d_perm, f->d_l2, f->d_b2, f->d_cb2, f->d_w, f->d_half, f->d_lut, f->d_rings, f->d_ptab};
+    void *ps[] = {f->d_keys, f->d_perm, f->d_inv, f->d_l2,    f->d_b2,
+                  f->d_cb2,  f->d_w,    f->d_half, f->d_lut, f->d_rings, f->d_ptab};
     for (void *p : ps)
         if (p) cudaFreeAsync(p, s);
     delete f->geom_refs;
@@ -94,7 +95,7 @@ void *hcg::Scratch::get(int slot, size_t bytes, cudaStream_t s, cudaError_t &err
         if (ptr[slot]) cudaFreeAsync(ptr[slot], s);
         size_t want = bytes + bytes / 4;
         void *p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, want, s);
+        cudaError_t e = dalloc(&p, want, s, pool);
         if (e != cudaSuccess) {
             ptr[slot] = nullptr;
             size[slot] = 0;
@@ -238,6 +239,26 @@ hcg_status hcg_context_create(int device, void *stream, hcg_context **out) {
         }
         c->own_stream = true;
     }
+    // the context's memory pool: freed buffers stay mapped for the next call
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    uint64_t keep = UINT64_MAX;
+    if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->pool) cudaMemPoolDestroy(c->pool);
+        c->pool = nullptr;  // the device's default pool then
+    }
+    c->scratch.pool = c->pool;
+    bool up = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) == cudaSuccess;
+    for (auto &ev : c->evu) up = up && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+    if (!up) {  // host spectra then go up in one copy
+        cudaGetLastError();
+        if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+        c->copy_stream = nullptr;
+    }
     if (cudaMalloc(&c->d_stats, sizeof(DevStats)) != cudaSuccess || cudaMemset(c->d_stats, 0, sizeof(DevStats)) ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
         cudaEventCreate(&c->evp[0]) != cudaSuccess || cudaEventCreate(&c->evp[1]) != cudaSuccess ||
@@ -262,7 +283,12 @@ static void ctx_teardown(hcg_context *ctx) {
     cudaEventDestroy(ctx->ev0);
     cudaEventDestroy(ctx->ev1);
     for (auto &ev : ctx->evp) cudaEventDestroy(ev);
+    for (auto &ev : ctx->evu)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    // every buffer of the pool was freed above or with its field or target
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }
 
@@ -360,7 +386,7 @@ hcg_status hcg_field_create(hcg_context *ctx, uint64_t n, const double *lon, con
     double *tmp = nullptr;
     if (mem == HCG_MEM_HOST) {
         size_t nb = n * sizeof(double);
-        cudaError_t e = cudaMallocAsync(&tmp, 3 * nb, s);
+        cudaError_t e = dalloc(&tmp, 3 * nb, s, ctx->pool);
         if (e != cudaSuccess) { delete f; return cuda_fail(ctx, e, "field upload"); }
         cudaMemcpyAsync(tmp, lon, nb, cudaMemcpyHostToDevice, s);
         cudaMemcpyAsync(tmp + n, lat, nb, cudaMemcpyHostToDevice, s);
@@ -402,9 +428,16 @@ hcg_status hcg_field_set_spectra(hcg_field *field, uint32_t nchan, const float *
     cudaStream_t s = ctx->stream;
     const float *dv = values;
     float *tmp = nullptr;
+    if (mem == HCG_MEM_HOST && ctx->copy_stream && field->n * (uint64_t)nchan * 4 > 2 * kUploadChunk) {
+        // large host spectra: chunked copies overlapped with the scatter into sorted order
+        free_split(field, s);
+        cudaError_t e = upload_spectra(ctx, field, values, nchan, layout);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "spectra upload");
+        return HCG_OK;
+    }
     if (mem == HCG_MEM_HOST) {
         size_t nb = field->n * (size_t)nchan * sizeof(float);
-        cudaError_t e = cudaMallocAsync(&tmp, nb, s);
+        cudaError_t e = dalloc(&tmp, nb, s, ctx->pool);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "spectra upload");
         CK(ctx, cudaMemcpyAsync(tmp, values, nb, cudaMemcpyHostToDevice, s), "spectra upload");
         dv = tmp;
@@ -485,8 +518,8 @@ static hcg_status make_target(hcg_context *ctx, uint32_t nx, uint32_t ny, const 
     t->nx = nx;
     t->ny = ny;
     size_t nb = (size_t)nx * ny * sizeof(double);
-    cudaError_t e = cudaMallocAsync(&t->d_x, nb, s);
-    if (e == cudaSuccess) e = cudaMallocAsync(&t->d_y, nb, s);
+    cudaError_t e = dalloc(&t->d_x, nb, s, ctx->pool);
+    if (e == cudaSuccess) e = dalloc(&t->d_y, nb, s, ctx->pool);
     if (e == cudaSuccess) e = cudaMemcpyAsync(t->d_x, x, nb, kind, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(t->d_y, y, nb, kind, s);
     if (e == cudaSuccess && kind == cudaMemcpyHostToDevice) e = cudaStreamSynchronize(s);
@@ -528,8 +561,8 @@ hcg_status hcg_target_from_header(hcg_context *ctx, const char *header, size_t l
     t->nx = nx;
     t->ny = ny;
     size_t nb = (size_t)nx * ny * sizeof(double);
-    cudaError_t e = cudaMallocAsync(&t->d_x, nb, s);
-    if (e == cudaSuccess) e = cudaMallocAsync(&t->d_y, nb, s);
+    cudaError_t e = dalloc(&t->d_x, nb, s, ctx->pool);
+    if (e == cudaSuccess) e = dalloc(&t->d_y, nb, s, ctx->pool);
     if (e == cudaSuccess) e = sin_coords_device(w, nx, ny, t->d_x, t->d_y, s);  // pixel centres on the device
     if (e != cudaSuccess) {
         if (t->d_x) cudaFreeAsync(t->d_x, s);
@@ -615,8 +648,43 @@ hcg_status hcg_tc_set_weights(hcg_context *ctx, int mode) {
     return HCG_OK;
 }
 
-hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, int *best,
-                        float *ms) {
+hcg_status hcg_tc_set_pipeline(hcg_context *ctx, int channel_class, int prefetch, int strip) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    if (channel_class < -1 || channel_class >= kTcClasses || prefetch < -1 || prefetch > 64 || strip < -1 ||
+        strip > 4096)
+        return fail(ctx, HCG_EINVAL, "prefetch must be -1..64 chunks and strip -1..4096 tiles");
+    for (int c = 0; c < kTcClasses; ++c)
+        if (channel_class < 0 || c == channel_class) {
+            ctx->tc_pf[c] = prefetch;
+            ctx->tc_strip[c] = strip;
+        }
+    return HCG_OK;
+}
+
+// Best and worst of `reps` timed gridding runs (after one warm-up) with the
+// context's current settings.
+static hcg_status tune_time(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, float *cube,
+                            float *wts, float &best, float &worst) {
+    best = 3.4e38f;
+    worst = 0.f;
+    for (int r = 0; r < reps + 1; ++r) {
+        hcg_status st = hcg_grid(ctx, field, target, cube, HCG_LAYOUT_SAMPLE_MAJOR, wts, HCG_MEM_DEVICE, field->xfmt);
+        if (st != HCG_OK) return st;
+        Guard g(ctx);
+        CK(ctx, cudaStreamSynchronize(ctx->stream), "autotune");
+        float m = 0.f;
+        if (cudaEventElapsedTime(&m, ctx->ev0, ctx->ev1) != cudaSuccess) cudaGetLastError();
+        if (r > 0) {
+            best = m < best ? m : best;
+            worst = m > worst ? m : worst;
+        }
+    }
+    return HCG_OK;
+}
+
+hcg_status hcg_autotune_ex(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps,
+                           hcg_tuning *out) {
     if (!ctx || !field || !target || reps < 1) return HCG_EINVAL;
     int cls;
     {
@@ -634,33 +702,63 @@ hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_targ
         wts = (float *)ctx->scratch.get(17, P * sizeof(float), ctx->stream, e);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "autotune buffers");
     }
-    float t[kTcConfigCount];
-    int pick = 0;
-    for (int c = 0; c < kTcConfigCount; ++c) {
-        {
-            Guard g(ctx);
-            ctx->tc_config[cls] = c;
-        }
-        t[c] = 3.4e38f;
-        for (int r = 0; r < reps + 1; ++r) {  // the first run is a warm-up
-            hcg_status st = hcg_grid(ctx, field, target, cube, HCG_LAYOUT_SAMPLE_MAJOR, wts, HCG_MEM_DEVICE,
-                                     field->xfmt);
-            if (st != HCG_OK) return st;
-            Guard g(ctx);
-            CK(ctx, cudaStreamSynchronize(ctx->stream), "autotune");
-            float m = 0.f;
-            if (cudaEventElapsedTime(&m, ctx->ev0, ctx->ev1) != cudaSuccess) cudaGetLastError();
-            if (r > 0 && m < t[c]) t[c] = m;
-        }
-        if (t[c] < t[pick]) pick = c;
-    }
-    {
+    hcg_tuning t = {};
+    const int pfs[5] = HCG_TUNE_PREFETCH, strips[5] = HCG_TUNE_STRIP;
+    auto set = [&](int shape, int pf, int strip) {
         Guard g(ctx);
-        ctx->tc_config[cls] = pick;
+        ctx->tc_config[cls] = shape;
+        ctx->tc_pf[cls] = pf;
+        ctx->tc_strip[cls] = strip;
+    };
+    float best, worst, spread = 0.f;
+    hcg_status st;
+    t.shape = 0;
+    for (int c = 0; c < kTcConfigCount; ++c) {  // shapes, with the default depth and walk
+        set(c, -1, -1);
+        if ((st = tune_time(ctx, field, target, reps, cube, wts, best, worst)) != HCG_OK) return st;
+        t.ms_shape[c] = best;
+        if (best < t.ms_shape[t.shape]) t.shape = c;
     }
-    if (best) *best = pick;
+    t.prefetch = -1;
+    float cur = t.ms_shape[t.shape];
+    for (int i = 0; i < 5; ++i) {  // prefetch distance with the best shape
+        set(t.shape, pfs[i], -1);
+        if ((st = tune_time(ctx, field, target, reps, cube, wts, best, worst)) != HCG_OK) return st;
+        t.ms_prefetch[i] = best;
+        if (best < cur) {
+            cur = best;
+            t.prefetch = pfs[i];
+        }
+    }
+    t.strip = -1;
+    for (int i = 0; i < 5; ++i) {  // tile walk with the best shape and prefetch
+        set(t.shape, t.prefetch, strips[i]);
+        if ((st = tune_time(ctx, field, target, reps, cube, wts, best, worst)) != HCG_OK) return st;
+        t.ms_strip[i] = best;
+        if (best < cur) {
+            cur = best;
+            t.strip = strips[i];
+        }
+    }
+    set(t.shape, t.prefetch, t.strip);
+    if ((st = tune_time(ctx, field, target, reps, cube, wts, best, worst)) != HCG_OK) return st;
+    spread = best > 0.f ? (worst - best) / best : 0.f;
+    t.ms_best = best;
+    t.spread = spread;
+    if (t.prefetch < 0) t.prefetch = kTcDefaultPrefetch;
+    if (t.strip < 0) t.strip = kTcDefaultStrip;
+    if (out) *out = t;
+    return HCG_OK;
+}
+
+hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, int *best,
+                        float *ms) {
+    hcg_tuning t;
+    hcg_status st = hcg_autotune_ex(ctx, field, target, reps, &t);
+    if (st != HCG_OK) return st;
+    if (best) *best = t.shape;
     if (ms)
-        for (int c = 0; c < kTcConfigCount; ++c) ms[c] = t[c];
+        for (int c = 0; c < kTcConfigCount; ++c) ms[c] = t.ms_shape[c];
     return HCG_OK;
 }
 
@@ -763,6 +861,14 @@ hcg_status hcg_set_coarsening_factor(hcg_context *ctx, uint32_t factor) {
     if (factor < 1 || factor > 3)
         return fail(ctx, HCG_EINVAL, "coarsening factor must be 1, 2 or 3 (the reference's kernel holds 3 pixels)");
     ctx->factor = factor;
+    return HCG_OK;
+}
+
+hcg_status hcg_context_trim(hcg_context *ctx) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream), "trim");
+    if (ctx->pool) CK(ctx, cudaMemPoolTrimTo(ctx->pool, 0), "trim");
     return HCG_OK;
 }
 

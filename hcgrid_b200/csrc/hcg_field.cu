@@ -367,6 +367,54 @@ __global__ void k_permute_cols(uint64_t n, uint32_t nchan, uint32_t cstride, con
     }
 }
 
+// inv[perm[j]] = j: the sorted position of each input sample.
+__global__ void k_inverse_perm(uint64_t n, const uint32_t *__restrict__ perm, uint32_t *__restrict__ inv) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (j < n) inv[perm[j]] = (uint32_t)j;
+}
+
+// One uploaded chunk of sample-major spectra (input rows [r0, r0 + rows))
+// scattered to its sorted rows: one warp per row, zero padding to cstride.
+__global__ void k_scatter_rows(uint64_t r0, uint64_t rows, uint32_t nchan, uint32_t cstride,
+                               const uint32_t *__restrict__ inv, const float *__restrict__ in,
+                               float *__restrict__ out) {
+    const uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    const float *src = in + r * nchan;
+    float *dst = out + (uint64_t)__ldg(inv + r0 + r) * cstride;
+    if ((nchan & 3) == 0 && ((uintptr_t)in & 15) == 0) {
+        for (uint32_t c = lane * 4; c < nchan; c += 128)
+            *reinterpret_cast<float4 *>(dst + c) = __ldg(reinterpret_cast<const float4 *>(src + c));
+    } else {
+        for (uint32_t c = lane; c < cstride; c += 32) dst[c] = c < nchan ? src[c] : 0.f;
+    }
+}
+
+// One uploaded chunk of channel-major spectra (planes [c0, c1) of n samples)
+// scattered to the sorted sample-major rows: 32 samples x 32 channels per
+// block through shared memory; the last chunk also writes the zero padding
+// channels up to cstride.
+__global__ void k_scatter_cols(uint64_t n, uint32_t c0, uint32_t c1, uint32_t cend, uint32_t cstride,
+                               const uint32_t *__restrict__ inv, const float *__restrict__ in,
+                               float *__restrict__ out) {
+    __shared__ float tile[32][33];
+    const uint64_t j0 = (uint64_t)blockIdx.x * 32;
+    const uint32_t cb = c0 + blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {
+        const uint64_t j = j0 + tx;
+        const uint32_t c = cb + r;
+        tile[r][tx] = (j < n && c < c1) ? in[(uint64_t)(c - c0) * n + j] : 0.f;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const uint64_t j = j0 + r;
+        const uint32_t c = cb + tx;
+        if (j < n && c < cend) out[(uint64_t)__ldg(inv + j) * cstride + c] = tile[tx][r];
+    }
+}
+
 }  // namespace
 
 cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, const double *d_lat,
@@ -385,12 +433,12 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
         e = (x);                       \
         if (e != cudaSuccess) goto fail; \
     } while (0)
-    TRY(cudaMallocAsync(&k0, (n + 1) * sizeof(uint64_t), s));
-    TRY(cudaMallocAsync(&k1, (n + 1) * sizeof(uint64_t), s));
-    TRY(cudaMallocAsync(&v0, n * sizeof(uint32_t), s));
-    TRY(cudaMallocAsync(&v1, n * sizeof(uint32_t), s));
-    TRY(cudaMallocAsync(&hist, (size_t)256 * nblocks * sizeof(uint32_t), s));
-    TRY(cudaMallocAsync(&range, sizeof(KeyRange) + sizeof(RingSpan), s));
+    TRY(dalloc(&k0, (n + 1) * sizeof(uint64_t), s, ctx->pool));
+    TRY(dalloc(&k1, (n + 1) * sizeof(uint64_t), s, ctx->pool));
+    TRY(dalloc(&v0, n * sizeof(uint32_t), s, ctx->pool));
+    TRY(dalloc(&v1, n * sizeof(uint32_t), s, ctx->pool));
+    TRY(dalloc(&hist, (size_t)256 * nblocks * sizeof(uint32_t), s, ctx->pool));
+    TRY(dalloc(&range, sizeof(KeyRange) + sizeof(RingSpan), s, ctx->pool));
     span = reinterpret_cast<RingSpan *>(range + 1);
     TRY(cudaMemsetAsync(&ctx->d_stats->invalid_input, 0, sizeof(unsigned long long), s));
     k_init_range<<<1, 1, 0, s>>>(range);
@@ -432,8 +480,8 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
     f->d_perm = v0;
     k0 = nullptr;
     v0 = nullptr;
-    TRY(cudaMallocAsync(&f->d_lut, (f->usedrings + 1) * sizeof(uint32_t), s));
-    TRY(cudaMallocAsync(&f->d_rings, f->usedrings * sizeof(RingRec), s));
+    TRY(dalloc(&f->d_lut, (f->usedrings + 1) * sizeof(uint32_t), s, ctx->pool));
+    TRY(dalloc(&f->d_rings, f->usedrings * sizeof(RingRec), s, ctx->pool));
     k_ring_lut<<<(unsigned)((f->usedrings + 1 + 255) / 256), 256, 0, s>>>(f->hpx, n, f->d_keys, f->firstring,
                                                                           f->usedrings, f->d_lut);
     k_ring_table<<<(unsigned)((f->usedrings + 255) / 256), 256, 0, s>>>(f->hpx, f->firstring, f->usedrings, f->d_lut,
@@ -453,7 +501,7 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
             R.tbl = total;
             total += R.span;
         }
-        if (total > 0 && total <= cap && cudaMallocAsync(&f->d_ptab, total * sizeof(uint32_t), s) == cudaSuccess) {
+        if (total > 0 && total <= cap && dalloc(&f->d_ptab, total * sizeof(uint32_t), s, ctx->pool) == cudaSuccess) {
             TRY(cudaMemcpyAsync(f->d_rings, hr.data(), hr.size() * sizeof(RingRec), cudaMemcpyHostToDevice, s));
             k_ring_ptab<<<(unsigned)f->usedrings, 256, 0, s>>>(f->d_rings, f->d_keys, f->d_ptab);
             TRY(cudaGetLastError());
@@ -466,12 +514,15 @@ cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, con
         }
         f->ptab_entries = f->d_ptab ? total : 0;
     }
-    TRY(cudaMallocAsync(&f->d_l2, n * sizeof(double), s));
-    TRY(cudaMallocAsync(&f->d_b2, n * sizeof(double), s));
-    TRY(cudaMallocAsync(&f->d_cb2, n * sizeof(double), s));
-    TRY(cudaMallocAsync(&f->d_half, n * sizeof(double4), s));
-    TRY(cudaMallocAsync(&f->d_w, n * sizeof(double), s));
-    TRY(cudaMallocAsync(&wbits, sizeof(unsigned long long), s));
+    TRY(dalloc(&f->d_l2, n * sizeof(double), s, ctx->pool));
+    TRY(dalloc(&f->d_b2, n * sizeof(double), s, ctx->pool));
+    TRY(dalloc(&f->d_cb2, n * sizeof(double), s, ctx->pool));
+    TRY(dalloc(&f->d_half, n * sizeof(double4), s, ctx->pool));
+    TRY(dalloc(&f->d_w, n * sizeof(double), s, ctx->pool));
+    TRY(dalloc(&wbits, sizeof(unsigned long long), s, ctx->pool));
+    TRY(dalloc(&f->d_inv, n * sizeof(uint32_t), s, ctx->pool));
+    k_inverse_perm<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, f->d_perm, f->d_inv);
+    TRY(cudaGetLastError());
     TRY(cudaMemsetAsync(wbits, 0, sizeof(unsigned long long), s));
     k_permute_geometry<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, f->d_perm, d_lon, d_lat, d_w, f->d_l2, f->d_b2,
                                                                    f->d_cb2, f->d_w, f->d_half, wbits);
@@ -497,6 +548,61 @@ fail:
     return e;
 }
 
+// Spectra from host memory, uploaded in chunks of kUploadChunk bytes through
+// two staging buffers: the copy of chunk k + 1 (copy stream) overlaps the
+// scatter of chunk k into sorted order (context stream). Copies wait for the
+// work queued on the context stream before the call, and every later use of
+// the spectra is ordered after the last scatter on the context stream.
+cudaError_t upload_spectra(hcg_context *ctx, hcg_field *f, const float *h_in, uint32_t nchan, int layout) {
+    cudaStream_t s = ctx->stream, cs = ctx->copy_stream;
+    const uint32_t cstride = (nchan + 3) & ~3u;
+    if (f->d_spec && f->cstride != cstride) {
+        cudaFreeAsync(f->d_spec, s);
+        f->d_spec = nullptr;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!f->d_spec) e = dalloc(&f->d_spec, f->n * cstride * sizeof(float), s, ctx->pool);
+    if (e != cudaSuccess) return e;
+    f->nchan = nchan;
+    f->cstride = cstride;
+    const uint64_t n = f->n;
+    // chunk geometry: whole input rows (sample-major) or whole planes (channel-major)
+    const uint64_t unit = layout == HCG_LAYOUT_SAMPLE_MAJOR ? (uint64_t)nchan * 4 : n * 4;
+    const uint64_t units = layout == HCG_LAYOUT_SAMPLE_MAJOR ? n : nchan;
+    const uint64_t per = std::max<uint64_t>(1, kUploadChunk / unit);
+    float *stage[2];
+    for (int b = 0; b < 2; ++b) {
+        stage[b] = (float *)ctx->scratch.get(19 + b, std::min(per, units) * unit, s, e);
+        if (e != cudaSuccess) return e;
+    }
+    if ((e = cudaEventRecord(ctx->evu[4], s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(cs, ctx->evu[4], 0)) != cudaSuccess) return e;
+    uint64_t k = 0;
+    for (uint64_t u0 = 0; u0 < units; u0 += per, ++k) {
+        const uint64_t cnt = std::min(per, units - u0);
+        const int b = (int)(k & 1);
+        if (k >= 2 && (e = cudaStreamWaitEvent(cs, ctx->evu[2 + b], 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(stage[b], h_in + u0 * (unit / 4), cnt * unit, cudaMemcpyHostToDevice, cs)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(ctx->evu[b], cs)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, ctx->evu[b], 0)) != cudaSuccess) return e;
+        if (layout == HCG_LAYOUT_SAMPLE_MAJOR) {
+            const uint64_t threads = cnt * 32;
+            k_scatter_rows<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(u0, cnt, nchan, cstride, f->d_inv,
+                                                                             stage[b], f->d_spec);
+        } else {
+            const uint32_t c0 = (uint32_t)u0, c1 = (uint32_t)(u0 + cnt);
+            const uint32_t cend = c1 == nchan ? cstride : c1;  // the last chunk writes the padding
+            dim3 grid((unsigned)((n + 31) / 32), (cend - c0 + 31) / 32);
+            k_scatter_cols<<<grid, dim3(32, 8), 0, s>>>(n, c0, c1, cend, cstride, f->d_inv, stage[b], f->d_spec);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ctx->evu[2 + b], s)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, uint32_t nchan, int layout) {
     cudaStream_t s = ctx->stream;
     uint32_t cstride = (nchan + 3) & ~3u;
@@ -505,7 +611,7 @@ cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, u
         f->d_spec = nullptr;
     }
     cudaError_t e = cudaSuccess;
-    if (!f->d_spec) e = cudaMallocAsync(&f->d_spec, f->n * cstride * sizeof(float), s);
+    if (!f->d_spec) e = dalloc(&f->d_spec, f->n * cstride * sizeof(float), s, ctx->pool);
     if (e != cudaSuccess) return e;
     f->nchan = nchan;
     f->cstride = cstride;

@@ -66,8 +66,21 @@ struct PixPrep {
     int pad;
 };
 
+// Stream-ordered allocation from a context's memory pool. The pool keeps
+// freed memory mapped (release threshold: never), so the multi-GB buffers of
+// one call are reused by the next instead of being unmapped at every
+// synchronize and mapped again; the pool is released with the context.
+inline cudaError_t dalloc(void **p, size_t bytes, cudaStream_t s, cudaMemPool_t pool) {
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
+}
+template <class T>
+inline cudaError_t dalloc(T **p, size_t bytes, cudaStream_t s, cudaMemPool_t pool) {
+    return dalloc(reinterpret_cast<void **>(p), bytes, s, pool);
+}
+
 // Grow-only device scratch buffers, stream-ordered.
 struct Scratch {
+    cudaMemPool_t pool = nullptr;
     std::vector<void *> ptr;
     std::vector<size_t> size;
     void *get(int slot, size_t bytes, cudaStream_t s, cudaError_t &err);
@@ -82,6 +95,8 @@ struct hcg_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaMemPool_t pool = nullptr;        // the context's device memory (dalloc)
+    cudaStream_t copy_stream = nullptr;  // host uploads overlapped with the context stream's kernels
     std::mutex mu;
     std::string err;
     // _prepare_grid_kernel state (gmap.cpp:64-99)
@@ -97,9 +112,12 @@ struct hcg_context {
     hcg::Scratch scratch;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evp[4] = {nullptr, nullptr, nullptr, nullptr};  // phase boundaries inside hcg_grid
+    cudaEvent_t evu[5] = {};  // chunked uploads: chunk copied (2), chunk scattered (2), call start
     float last_ms = 0.f;
     unsigned long long entry_budget = 4ULL << 30;  // bytes of (sample, weights) entries per launch run
     int tc_config[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // tensor-core pipeline shape per channel class (-1: default)
+    int tc_pf[8] = {-1, -1, -1, -1, -1, -1, -1, -1};      // prefetch distance (chunks) per class (-1: default)
+    int tc_strip[8] = {-1, -1, -1, -1, -1, -1, -1, -1};   // persistent tile walk per class (-1: default)
     int tc_weights = 0;  // tensor-core weight operands: 0 automatic, 1 from entries, 2 evaluated in the kernel
     uint32_t factor = 1;  // coarsening factor (hcg_set_coarsening_factor)
     void *batch = nullptr;                          // batch engine state (hcg_batch.cu)
@@ -118,6 +136,7 @@ struct hcg_field {
     uint64_t firstring = 0, usedrings = 0;
     uint64_t *d_keys = nullptr;   // n + 1, sorted, sentinel npix
     uint32_t *d_perm = nullptr;   // sorted position -> input index
+    uint32_t *d_inv = nullptr;    // input index -> sorted position
     double *d_l2 = nullptr;       // radians, sorted
     double *d_b2 = nullptr;
     double *d_cb2 = nullptr;      // cos(b2)
@@ -148,6 +167,8 @@ struct hcg_target {
 namespace hcg {
 constexpr int kTcClasses = 8;
 constexpr int kTcConfigCount = 6;  // tensor-core pipeline shapes (hcg_tc_set_config)
+constexpr int kTcDefaultPrefetch = 6;  // chunks the producer prefetches into L2 ahead of its loads
+constexpr int kTcDefaultStrip = 8;     // tile columns per strip of the persistent tile walk
 // channel class of a split field: 64-channel blocks 1, 2, 3-4, 5-8, ... -> 0, 1, 2, 3, ...
 inline int tc_class_of(uint32_t cpad) {
     const uint32_t b = cpad / 64;
@@ -185,6 +206,10 @@ inline bool tc_use_weights(const hcg_context *ctx, const hcg_field *f, unsigned 
 cudaError_t build_field(hcg_context *ctx, hcg_field *f, const double *d_lon, const double *d_lat,
                         const double *d_w, std::string &why);
 cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, uint32_t nchan, int layout);
+// Spectra from host memory in chunks, each scattered into sorted order while
+// the next is copied (needs ctx->copy_stream).
+constexpr uint64_t kUploadChunk = 256ull << 20;
+cudaError_t upload_spectra(hcg_context *ctx, hcg_field *f, const float *h_in, uint32_t nchan, int layout);
 // Coarsening (hcg_set_coarsening_factor): each pixel takes the window fields
 // of the first pixel of its run of `factor` along its row.
 cudaError_t coarsen_prep(PixPrep *prep, uint32_t nx, uint64_t npix, uint32_t factor, cudaStream_t s);

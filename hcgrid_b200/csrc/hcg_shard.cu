@@ -75,7 +75,7 @@ extern "C" hcg_status hcg_field_band_samples(hcg_context *ctx, const hcg_field *
     unsigned int got[2] = {UINT_MAX, 0};
     uint32_t lut[2] = {0, 0};
     const uint64_t p0 = (uint64_t)y0 * target->nx, p1 = (uint64_t)y1 * target->nx;
-    cudaError_t e = cudaMallocAsync(&rr, sizeof init, s);
+    cudaError_t e = dalloc(&rr, sizeof init, s, ctx->pool);
     if (e == cudaSuccess) e = cudaMemcpyAsync(rr, init, sizeof init, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && p1 > p0) {
         k_band_rings<<<(unsigned)((p1 - p0 + 255) / 256), 256, 0, s>>>(

@@ -178,10 +178,10 @@ cudaError_t split_spectra(hcg_context *ctx, hcg_field *f, int fmt_engine, std::s
     unsigned int *amax = nullptr;
     unsigned long long *bad = nullptr;
     const size_t nb = (size_t)n * cpad * sizeof(uint16_t);
-    if ((e = cudaMallocAsync(&hi, nb ? 2 * nb : 16, s)) != cudaSuccess ||
-        (e = cudaMallocAsync(&scale, cpad * sizeof(float), s)) != cudaSuccess ||
-        (e = cudaMallocAsync(&inv, cpad * sizeof(float), s)) != cudaSuccess ||
-        (e = cudaMallocAsync(&amax, cpad * sizeof(unsigned int) + sizeof(unsigned long long), s)) != cudaSuccess) {
+    if ((e = dalloc(&hi, nb ? 2 * nb : 16, s, ctx->pool)) != cudaSuccess ||
+        (e = dalloc(&scale, cpad * sizeof(float), s, ctx->pool)) != cudaSuccess ||
+        (e = dalloc(&inv, cpad * sizeof(float), s, ctx->pool)) != cudaSuccess ||
+        (e = dalloc(&amax, cpad * sizeof(unsigned int) + sizeof(unsigned long long), s, ctx->pool)) != cudaSuccess) {
         why = "split spectra of " + std::to_string(2 * nb) + " bytes";
         if (hi) cudaFreeAsync(hi, s);
         if (scale) cudaFreeAsync(scale, s);
@@ -269,6 +269,12 @@ cudaError_t tc_set_smem(const void *kernel, uint32_t bytes) {
 
 // Pipeline shape for a field: the autotuned choice of its channel class,
 // else the widest item its channels fill.
+void tc_pipeline(const hcg_context *ctx, const hcg_field *f, TcJob &J) {
+    const int c = tc_class_of(f->xcpad);
+    J.pf = (uint32_t)(ctx->tc_pf[c] >= 0 ? ctx->tc_pf[c] : kTcDefaultPrefetch);
+    J.strip = (uint32_t)(ctx->tc_strip[c] >= 0 ? ctx->tc_strip[c] : kTcDefaultStrip);
+}
+
 int tc_pick(const hcg_context *ctx, const hcg_field *f) {
     const int t = ctx->tc_config[tc_class_of(f->xcpad)];
     if (t >= 0 && t < kTcConfigCount) return t;
@@ -368,6 +374,7 @@ cudaError_t tc_weights(hcg_context *ctx, const hcg_field *f, const GridArgs &a, 
     J.out = out;
     J.ostride = ostride;
     J.wout = wout;
+    tc_pipeline(ctx, f, J);
     const uint32_t b = f->xcpad / 64;
     if (b >= 4) return launch_tc_weights<TcCfgN4S2>(ctx, f, J, T, ntiles, why);
     if (b >= 2) return launch_tc_weights<TcCfgN2S3>(ctx, f, J, T, ntiles, why);
@@ -388,6 +395,7 @@ cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, c
     J.out = out;
     J.ostride = ostride;
     J.wout = wout;
+    tc_pipeline(ctx, f, J);
     int cfg = tc_pick(ctx, f);
     // tiles longer than one accumulation segment take the persistent kernel,
     // which accumulates in segments (the one-item kernel does not)

@@ -115,7 +115,25 @@ struct TcJob {
     float *wout;
     const CUtensorMap *out_map;  // 3-D map of the cube (null: direct stores); box = one item
     GridArgs a;                  // geometry of the direct-weight builders (tc_build_weights)
+    uint32_t pf;                 // the producer prefetches chunk k + pf into L2 (pf <= stages: k + stages)
+    uint32_t strip;              // persistent kernels' tile walk: strips of `strip` tile columns (0: rows)
 };
+
+// Tile of the q-th item of a persistent launch over whole tile rows (ntiles =
+// rows x ntx): with strip > 0 the columns are taken in strips of `strip`
+// tiles, each strip row by row, so the tiles in flight at once form a compact
+// block whose neighbours share staged samples in L2; 0 walks whole rows.
+__host__ __device__ __forceinline__ uint64_t tc_walk(uint64_t q, uint64_t ntiles, uint32_t ntx, uint32_t strip) {
+    if (strip == 0 || strip >= ntx) return q;
+    const uint64_t rows = ntiles / ntx;
+    const uint64_t nfull = ntx / strip, full_items = nfull * rows * strip;
+    if (q < full_items) {
+        const uint64_t s = q / (rows * strip), r = q % (rows * strip);
+        return (r / strip) * ntx + s * strip + r % strip;
+    }
+    const uint64_t rem = ntx - nfull * strip, r = q - full_items;
+    return (r / rem) * ntx + nfull * strip + r % rem;
+}
 
 constexpr int kTcRing = 8;  // entries in flight per builder thread
 constexpr int kTcMaxStages = 4;
@@ -138,6 +156,8 @@ bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map, TcJob &J);
 bool tc_out_map(CUtensorMap *m, float *out, uint32_t ostride, uint32_t nx, uint32_t ny, uint32_t nchan, uint32_t nb);
 cudaError_t tc_set_smem(const void *kernel, uint32_t bytes);
 int tc_pick(const hcg_context *ctx, const hcg_field *f);
+// the channel class's prefetch distance and tile walk into J
+void tc_pipeline(const hcg_context *ctx, const hcg_field *f, TcJob &J);
 
 namespace {
 
@@ -265,6 +285,7 @@ __device__ __forceinline__ void tc_produce(SH &S, const TcJob &J, uint32_t cblk,
     const TcStage<Cfg> st{tc_smem_base()};
     const int lane = threadIdx.x & 31;
     const uint32_t bytes = NB8 * 2u * J.nb * 1024u;
+    const uint32_t pf = J.pf > ST ? J.pf : ST;  // chunks ahead of the loads that go to L2 first
     // TMA row of slot0: the ring run j with base[j] <= slot0 < base[j + 1]
     auto row_of = [&](uint32_t slot0) -> int {
         if (slot0 >= U) return (int)J.nrows;  // past the last sample: zero fill
@@ -275,6 +296,11 @@ __device__ __forceinline__ void tc_produce(SH &S, const TcJob &J, uint32_t cblk,
         }
         return (int)(S.ulo[lo] + (slot0 - S.base[lo]));
     };
+    // the item's chunks [ST, pf) are prefetched at its start; chunk k + pf with chunk k
+    for (uint32_t i = lane; i < (pf - ST) * (uint32_t)NB8; i += 32) {
+        const uint32_t c = ST + i / NB8;
+        if (c < nchunks) tma_prefetch_4d(J.map, 0, row_of(c * KC + 8 * (i % NB8)), (int)(cblk * J.nb), 0);
+    }
     for (uint32_t k = 0; k < nchunks; ++k) {
         const uint32_t g = gk + k, s = g % ST;
         int go = 1;
@@ -290,7 +316,7 @@ __device__ __forceinline__ void tc_produce(SH &S, const TcJob &J, uint32_t cblk,
         }
         if (!__shfl_sync(0xffffffffu, go, 0)) break;
         const int b = lane % NB8;
-        const uint32_t kk = lane < NB8 ? k : k + ST;
+        const uint32_t kk = lane < NB8 ? k : k + pf;
         if (lane < 2 * NB8 && kk < nchunks) {
             const int row = row_of(kk * KC + 8 * b);
             if (lane < NB8)
@@ -323,16 +349,18 @@ __device__ __forceinline__ bool tc_mma(SH &S, const TcJob &J, uint32_t nchunks, 
         tc_fence_after();
         const uint32_t ah = smem_u32(st.A_hi(s)), al = smem_u32(st.A_lo(s));
         const uint32_t bh = smem_u32(st.B(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
+        // K step 0's descriptors; step kk adds its byte offset / 16 (two 8-slot
+        // row groups per K step; 64-channel atoms 1 KB apart)
+        const uint64_t adh = smem_desc(ah, 16, Cfg::kAAtom, Cfg::kALayout);
+        const uint64_t adl = smem_desc(al, 16, Cfg::kAAtom, Cfg::kALayout);
+        const uint64_t bdh = smem_desc(bh, 1024, Cfg::kBGroup, 2);
+        const uint64_t bdl = smem_desc(bl, 1024, Cfg::kBGroup, 2);
 #pragma unroll
         for (int kk = 0; kk < (int)(KC / 16); ++kk) {
-            const uint64_t adh = smem_desc(ah + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
-            const uint64_t adl = smem_desc(al + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
-            // two 8-slot row groups per K step; 64-channel atoms 1 KB apart
-            const uint64_t bdh = smem_desc(bh + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
-            const uint64_t bdl = smem_desc(bl + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
-            mma_f16_ss(d_tmem, adh, bdh, idesc, acc);
-            mma_f16_ss(d_tmem, adh, bdl, idesc, 1);
-            mma_f16_ss(d_tmem, adl, bdh, idesc, 1);
+            const uint64_t ao = (uint64_t)(kk * 32 / 16), bo = (uint64_t)(kk * 2 * Cfg::kBGroup / 16);
+            mma_f16_ss(d_tmem, adh + ao, bdh + bo, idesc, acc);
+            mma_f16_ss(d_tmem, adh + ao, bdl + bo, idesc, 1);
+            mma_f16_ss(d_tmem, adl + ao, bdh + bo, idesc, 1);
             acc = 1;
         }
         mma_commit(&S.empty[s]);
@@ -389,17 +417,20 @@ __device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchun
                 break;
             }
             tc_fence_after();
+            // descriptors of K step 0; step kk adds its byte offset / 16 to the
+            // address field (shared-memory addresses stay below 2^18: no carry)
             const uint32_t ah = smem_u32(st.A_hi(s)), al = smem_u32(st.A_lo(s));
             const uint32_t bh = smem_u32(st.B(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
+            const uint64_t adh = smem_desc(ah, 16, Cfg::kAAtom, Cfg::kALayout);
+            const uint64_t adl = smem_desc(al, 16, Cfg::kAAtom, Cfg::kALayout);
+            const uint64_t bdh = smem_desc(bh, 1024, Cfg::kBGroup, 2);
+            const uint64_t bdl = smem_desc(bl, 1024, Cfg::kBGroup, 2);
 #pragma unroll
             for (int kk = 0; kk < (int)(KC / 16); ++kk) {
-                const uint64_t adh = smem_desc(ah + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
-                const uint64_t adl = smem_desc(al + kk * 32, 16, Cfg::kAAtom, Cfg::kALayout);
-                const uint64_t bdh = smem_desc(bh + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
-                const uint64_t bdl = smem_desc(bl + kk * 2 * Cfg::kBGroup, 1024, Cfg::kBGroup, 2);
-                mma_f16_ss(d_tmem, adh, bdh, idesc, acc);
-                mma_f16_ss(d_tmem, adh, bdl, idesc, 1);
-                mma_f16_ss(d_tmem, adl, bdh, idesc, 1);
+                const uint64_t ao = (uint64_t)(kk * 32 / 16), bo = (uint64_t)(kk * 2 * Cfg::kBGroup / 16);
+                mma_f16_ss(d_tmem, adh + ao, bdh + bo, idesc, acc);
+                mma_f16_ss(d_tmem, adh + ao, bdl + bo, idesc, 1);
+                mma_f16_ss(d_tmem, adl + ao, bdh + bo, idesc, 1);
                 acc = 1;
             }
             mma_commit(&S.empty[s]);
@@ -775,7 +806,7 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
     tc_fence_after();
     uint32_t gk = 0, il = 0, gs = 0, gse = 0;  // chunks, items, MMA and epilogue segments
     for (uint64_t it = blockIdx.x; it < nitems; it += gridDim.x, ++il) {
-        const uint64_t tile = J.T.t0 + it % ntiles;
+        const uint64_t tile = J.T.t0 + tc_walk(it % ntiles, ntiles, J.T.ntx, J.strip);
         const uint32_t cblk = (uint32_t)(it / ntiles);
         const uint32_t U = J.T.U[tile];
         const uint32_t nchunks = (U + KC - 1) / KC;
@@ -1071,7 +1102,7 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
     tc_fence_after();
     uint32_t gk = 0, il = 0, gs = 0, gse = 0;  // chunks, items, MMA and epilogue segments
     for (uint64_t it = blockIdx.x; it < nitems; it += gridDim.x, ++il) {
-        const uint64_t tile = J.T.t0 + it % ntiles;
+        const uint64_t tile = J.T.t0 + tc_walk(it % ntiles, ntiles, J.T.ntx, J.strip);
         const uint32_t cblk = (uint32_t)(it / ntiles);
         const uint32_t U = J.T.U[tile];
         const uint32_t nchunks = (U + KC - 1) / KC;

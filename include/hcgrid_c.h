@@ -175,6 +175,37 @@ hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config);
 hcg_status hcg_tc_set_weights(hcg_context *ctx, int mode);
 hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps, int *best,
                         float *ms);
+
+/* Pipeline depth and tile walk of the tensor-core engine, per channel class
+ * (-1: every class; a value of -1 restores the default):
+ *   prefetch  chunks of staged spectra the producer requests into L2 ahead of
+ *             its shared-memory loads (values up to the shape's stages mean
+ *             the stages themselves); default 6;
+ *   strip     the persistent kernels take the tiles of a launch in strips of
+ *             `strip` tile columns, row by row inside a strip, so that the
+ *             tiles in flight together form a compact block whose neighbours
+ *             share staged samples in L2 (0: whole tile rows); default 8.
+ * No reference counterpart. */
+hcg_status hcg_tc_set_pipeline(hcg_context *ctx, int channel_class, int prefetch, int strip);
+
+/* The autotuner's full search (hcg_autotune is its shape part): the
+ * pipeline shape (ms_shape, defaults elsewhere), then with that shape the
+ * prefetch distance over kTunePrefetch, then the strip width over
+ * kTuneStrip; each setting is timed `reps` times after a warm-up run and
+ * scored by its best run. The choices are kept for the field's channel class
+ * and returned; spread = (slowest - fastest) / fastest over the chosen
+ * setting's repeats. */
+#define HCG_TUNE_PREFETCH {2, 4, 6, 8, 12}
+#define HCG_TUNE_STRIP {0, 4, 8, 16, 32}
+typedef struct {
+    int shape, prefetch, strip;
+    float ms_shape[6];
+    float ms_prefetch[5];
+    float ms_strip[5];
+    float ms_best, spread;
+} hcg_tuning;
+hcg_status hcg_autotune_ex(hcg_context *ctx, const hcg_field *field, const hcg_target *target, int reps,
+                           hcg_tuning *out);
 /* Sorted keys (n+1 with the npix sentinel), permutation (n) and ring LUT
  * (usedrings+1); any pointer may be NULL. Host memory. */
 hcg_status hcg_field_sorted(const hcg_field *field, uint64_t *keys, uint32_t *perm, uint32_t *lut);
@@ -266,6 +297,13 @@ hcg_status hcg_set_entry_budget(hcg_context *ctx, uint64_t bytes);
  * this context; hcg_grid_batch on a context with factor > 1 grids each job
  * on its own. */
 hcg_status hcg_set_coarsening_factor(hcg_context *ctx, uint32_t factor);
+
+/* Device memory: every buffer of a context (fields, targets, scratch) comes
+ * from the context's own stream-ordered pool, which keeps freed memory
+ * mapped so that the next field or call reuses it without new mappings (no
+ * reference counterpart; the reference cudaMallocs and frees per run). This
+ * returns what the pool keeps beyond the buffers in use to the driver. */
+hcg_status hcg_context_trim(hcg_context *ctx);
 
 /* Wait for all work queued on the context's stream. */
 hcg_status hcg_synchronize(hcg_context *ctx);

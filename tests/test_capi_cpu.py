@@ -37,6 +37,32 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert set(names) <= set(api.EXPORTS), set(names) - set(api.EXPORTS)
 
 
+# The reference's C++ names (HCGrid/gmap.h, gridding.h, healpix.h) and
+# globals: a driver compiled against the reference's headers links to these.
+REFERENCE_CXX = ["_Healpix_init(unsigned long, unsigned int)",
+                 "_prepare_grid_kernel(unsigned int, double*, double, double)",
+                 "read_input_map(char const*)", "read_output_map(char const*)", "set_WCS()",
+                 "write_output_map(char const*)", "write_ordered_map(char const*, char const*)",
+                 "init_input_with_cpu(int const&)", "init_input_with_thrust(int const&)", "init_output()",
+                 "data_alloc()", "data_h2d()", "data_d2h()", "data_free()",
+                 "solve_gridding(char const*, char const*, char const*, char const*, int const&, int const&)"]
+REFERENCE_GLOBALS = ["h_GMaps", "h_Healpix", "h_lons", "h_lats", "h_data", "h_weights", "h_hpx_idx", "h_start_ring",
+                     "h_header", "h_zyx", "h_xwcs", "h_ywcs", "h_datacube", "h_weightscube", "h_kernel_params",
+                     "last_sphere_radius", "last_hpxmaxres"]
+
+
+def test_reference_cxx_names_and_globals_are_exported():
+    api.load(build_if_missing=True)
+    out = subprocess.run(["nm", "-DC", api.lib_path()], capture_output=True, text=True, check=True).stdout
+    defined = set()
+    for line in out.splitlines():
+        parts = line.split(None, 2)
+        if len(parts) == 3 and parts[1] in ("T", "B", "D"):
+            defined.add(parts[2])
+    missing = [n for n in REFERENCE_CXX + REFERENCE_GLOBALS if n not in defined]
+    assert not missing, missing
+
+
 def test_status_strings_and_no_device_errors():
     L = api.load()
     for s in range(8):

@@ -140,10 +140,12 @@ def test_coarsening_factor_matches_reference(case, factor):
         for ch in range(nchan):
             r = ref[ok, ch]
             assert np.abs(cube[ok, ch] - r).max() <= tol * np.abs(r).max(), (name, ch)
-    # a factor changes the result: the coarsened map is not the plain one
+    # away from the poles a factor changes the result (near them every pixel of
+    # a row takes whole rings over the same ring range, with or without it)
     ctx.set_coarsening_factor(1)
     plain, _ = ctx.grid(f, t, engine=api.ENGINE_FP32 if nchan > 1 else api.ENGINE_AUTO)
-    assert not np.allclose(plain[ok], outs["fp64"][ok], rtol=1e-9, equal_nan=True)
+    if case != "synth_polar":
+        assert not np.allclose(plain[ok], outs["fp64"][ok], rtol=1e-9, equal_nan=True)
     with pytest.raises(api.HcgError):
         ctx.set_coarsening_factor(4)
     f.close()
