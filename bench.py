@@ -54,8 +54,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config3", "config5"])
-    ap.add_argument("--jobs", type=int, default=200, help="config5: requests in the stream (the full form has 2000)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config3", "config4", "config5"])
+    ap.add_argument("--jobs", type=int, default=2000, help="config5: requests in the stream (the full form's 2000)")
+    ap.add_argument("--blocks", type=int, default=256, help="config4: scan blocks (the full form's 256)")
+    ap.add_argument("--stage-gb", type=float, default=48.0,
+                    help="config4/config5: device bytes of requests staged at once (a window)")
+    ap.add_argument("--oracle-checks", type=int, default=1,
+                    help="config5: check sampled requests against the FP64 oracle in the CPU leg (0: skip)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
     ap.add_argument("--detail", default=None, help="config5: write per-request times of the per-call arms here")
     ap.add_argument("--tc-weights", default="auto", choices=["auto", "entries", "direct"],
@@ -64,6 +69,9 @@ def parse():
                     help="config2 at N=1: also run the served form (config5) on this many requests and report it "
                          "under 'served_config5' (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--shard", default="bands", choices=["bands", "replicas"],
+                    help="N>1: split the one job into Dec bands of target rows, one per rank, gathered to rank 0 "
+                         "over NCCL (strong scaling), or grid a replica of the whole job on every rank (weak)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true",
                     help="skip the check of the timed cube against the FP64 oracle and the FP32 engine")
@@ -443,232 +451,318 @@ def reduce_max(torch, dist, v):
 
 
 # ---------------------------------------------------------------------------
-# served form (config 5): request stream through hcg_server vs plain per-call
-
-def device_block_spectra(lon_d, lat_d, shape, nchan, seed, torch, dev):
-    """[n][nchan] float32 spectra of one request on the device: 20 Gaussian
-    sources of the block's field with seeded line profiles, plus N(0, 0.05)."""
-    from hcgrid_b200 import synth
-    rng = np.random.default_rng(seed)
-    src = synth.make_sources(20, shape["ra"], shape["dec"], shape["size_deg"], rng)
-    ra = torch.tensor(src.ra, device=dev)
-    dec = torch.tensor(src.dec, device=dev)
-    amp = torch.tensor(src.amp, device=dev)
-    sig = torch.tensor(src.sigma_deg, device=dev)
-    c0 = rng.uniform(0.1, 0.9, len(src.amp)) * nchan
-    w = rng.uniform(0.01, 0.05, len(src.amp)) * nchan
-    ch = np.arange(nchan)
-    L = torch.tensor(np.exp(-((ch[None, :] - c0[:, None]) ** 2) / (2.0 * w[:, None] ** 2)), device=dev,
-                     dtype=torch.float32)
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(seed)
-    n = lon_d.shape[0]
-    S = torch.empty((n, nchan), dtype=torch.float32, device=dev)
-    step = max(1, (1 << 26) // max(nchan, 1))
-    for i in range(0, n, step):
-        lo, la = lon_d[i:i + step, None], lat_d[i:i + step, None]
-        dx = torch.remainder(lo - ra[None, :] + 180.0, 360.0) - 180.0
-        dx = dx * torch.cos(torch.deg2rad(dec))[None, :]
-        dy = la - dec[None, :]
-        G = (amp[None, :] * torch.exp(-(dx * dx + dy * dy) / (2.0 * sig[None, :] ** 2))).float()
-        torch.matmul(G, L, out=S[i:i + step])
-        S[i:i + step].add_(torch.randn((G.shape[0], nchan), generator=gen, device=dev), alpha=0.05)
-    return S
+# served form (config 5) and batched form (config 4): request streams staged
+# in windows (hcgrid_b200/streams.py), only the gridding timed
 
 
-def served_main(args):
-    print(json.dumps(served_run(args)))
+def check_sample(s, chans_max=3, side=16):
+    """Host copy of a staged request's cube at its central side x side pixels
+    and up to 3 channels spread over the band (for the per-result errors)."""
+    from hcgrid_b200 import streams
+    sh = s.r["shape"]
+    g, C = sh["grid"], sh["nchan"]
+    side = min(side, g)
+    x0 = (g - side) // 2
+    pix = ((np.arange(side)[:, None] + x0) * g + (np.arange(side)[None, :] + x0)).reshape(-1)
+    chans = streams.check_channels(C, chans_max)
+    cube = s.cube.view(-1, C)
+    import torch
+    return pix, chans, cube[torch.from_numpy(pix).to(cube.device)][:, torch.from_numpy(chans).to(cube.device)].cpu().numpy()
 
 
 def served_run(args):
-    """Config 5: a stream of gridding requests with config-4 shapes (seed 3),
-    30% of them re-gridding an earlier request's field with new spectra.
-    Fields (sorted samples, ring LUT) and targets stay resident; each request
-    brings its spectra (generated on the device, permuted into the request's
-    field share and, for the tensor-core engine, split into FP16 hi/lo) and
-    its output buffers. Requests are staged in windows that fit the HBM
-    admission budget; only the gridding is timed.
+    """Config 5: a stream of `args.jobs` gridding requests with config-4 shapes
+    (seed 3, no caps), 30% of them re-gridding an earlier request's field
+    with new spectra. Windows of requests are staged on the device within
+    the staging budget (fields and targets built on first use, resident
+    until their last request); on each window, every arm runs on the same
+    staged requests:
 
-    served: each window's requests go through hcg_server (continuous
-    batching over 2 lanes, persistent batch kernels replayed from a CUDA
-    graph, tensor-core channel sums, footprint admission). Capacity = work /
-    time from a window's first submit to its last completion (closed loop);
-    then Poisson arrivals at 80% of capacity give p50/p99 latency (submit ->
-    cube written). Arms beside it on the same requests: plain = one hcg_grid
-    call at a time on the FP32 engine; tc_per_call = one hcg_grid call at a
-    time on the tensor-core engine."""
+      plain        one hcg_grid call at a time, FP32 CUDA-core engine;
+      tc_per_call  one hcg_grid call at a time, tensor-core engine;
+      served       the window's requests submitted to hcg_server at once
+                   (continuous batching over 2 lanes, persistent batch
+                   kernels replayed from CUDA graphs, tensor cores,
+                   footprint admission against the HBM budget); capacity =
+                   work / time from a window's first submit to its last
+                   completion (closed loop).
+
+    A second pass stages the windows again and submits with Poisson arrivals
+    at 80% of the closed-loop capacity: p50/p99 latency (submit -> cube
+    written). Every 100th request and the 3 largest are checked: served
+    against the single call (bit for bit), the tensor cores against the FP32
+    engine and, in the CPU leg, both against the FP64 oracle."""
     import torch
-    from hcgrid_b200 import api, synth
+    from hcgrid_b200 import api, streams, synth
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     api.load(build_if_missing=True)
     budget = int(args.hbm_budget_gb * (1 << 30))
-    reqs = synth.config5_requests(njobs=args.jobs, seed=3, reuse=0.3, max_grid=2048, max_values=1 << 29,
-                                  max_cube=1 << 30)
+    reqs = synth.config5_requests(njobs=args.jobs, seed=3, reuse=0.3, max_grid=2048)
+    work = [streams.request_work(r) for r in reqs]
+    tot_work = sum(work)
+    big = set(np.argsort(work)[-3:].tolist())
+    checks = {r["request"] for r in reqs if r["request"] % 100 == 0 or r["request"] in big}
+    stage_budget = min(budget, int(args.stage_gb * (1 << 30)))
+    windows = streams.plan_windows(reqs, stage_budget)
     ctx = api.Context(0)
-    base = {}
-    for r in reqs:  # resident fields and targets, built once
-        fid = r["field"]
-        if fid in base:
-            continue
-        sh = r["shape"]
-        rng = np.random.default_rng(sh["seed"])
-        lon, lat = synth.raster_scan(sh["n"], sh["ra"], sh["dec"], sh["size_deg"], 2.0, rng)
-        sigma = sh["fwhm"] / 3600.0 * synth.FWHM_TO_SIGMA
-        ctx.prepare_grid_kernel(api.GAUSS1D, np.array([sigma, 0.0, 0.0]), 3.0 * sigma, sigma / 2.0)
-        f = ctx.field(lon, lat)
-        hdr = synth.sin_header(sh["grid"], sh["grid"], sh["ra"], sh["dec"], sh["size_deg"] / sh["grid"])
-        t = ctx.target_from_header(hdr)
-        base[fid] = (f, t, torch.from_numpy(lon).to(dev), torch.from_numpy(lat).to(dev))
-    ctx.synchronize()
-
-    def work(r):
-        return r["shape"]["n"] * r["shape"]["nchan"]
-
-    def footprint(r):
-        """device bytes of one request: spectra (FP32 during the upload, then
-        the hi/lo split), cube and weights, and the per-pixel scratch of the
-        batch engine (pixel setup, weight sums, tile tables, entries)."""
-        sh = r["shape"]
-        P = sh["grid"] ** 2
-        return 2 * sh["n"] * sh["nchan"] * 4 + P * (sh["nchan"] + 1) * 4 + P * 600
-
-    windows, cur, used = [], [], 0
-    stage_budget = min(budget, 64 << 30)  # staged requests; the rest of HBM is the lanes' working memory
-    for r in reqs:
-        fp = footprint(r)
-        if cur and used + fp > stage_budget:
-            windows.append(cur)
-            cur, used = [], 0
-        cur.append(r)
-        used += fp
-    if cur:
-        windows.append(cur)
-
-    def stage(win, tc):
-        out = []
-        for r in win:
-            sh = r["shape"]
-            f0, t, lon_d, lat_d = base[r["field"]]
-            S = device_block_spectra(lon_d, lat_d, sh, sh["nchan"], r["spectra_seed"], torch, dev)
-            torch.cuda.synchronize(dev)
-            f = f0.share()
-            f.set_spectra(S)
-            del S
-            if tc and sh["nchan"] > 1:
-                f.split_spectra(api.ENGINE_TC_F16, keep_fp32=False)
-            P = t.nx * t.ny
-            cube = torch.empty((P * sh["nchan"],), dtype=torch.float32, device=dev)
-            wts = torch.empty((P,), dtype=torch.float32, device=dev)
-            out.append((r, f, t, cube, wts))
-        ctx.synchronize()
-        return out
-
-    def release(staged):
-        for _, f, _, _, _ in staged:
-            f.close()
-        staged.clear()
-        ctx.synchronize()
-        torch.cuda.empty_cache()
-
-    detail = []  # per request: arm, shape, seconds, device phase times
-
-    def per_call(tc):
-        lat = []
+    ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
+    samples = {}  # request -> {arm: (pix, chans, values)}
+    plain_lat, tc_lat, lats_cl, busy, grids = [], [], [], 0.0, []
+    busy_part, work_part = {False: 0.0, True: 0.0}, {False: 0, True: 0}  # by "target has >= 2^20 pixels"
+    large_ids = set()  # requests whose targets have >= 2^20 pixels (the server runs them alone)
+    srv = api.Server(ctx, lanes=2, hbm_budget=budget, max_batch=64)
+    fields_built = 0
+    try:
+        run = streams.Runner(ctx, reqs, torch, dev)
+        warmed = False
         for win in windows:
-            staged = stage(win, tc)
-            for r, f, t, cube, wts in staged:
-                eng = api.ENGINE_TC_F16 if (tc and r["shape"]["nchan"] > 1) else api.ENGINE_FP32
+            staged = []
+            for r in win:  # FP32 spectra kept beside the split: every arm runs on this staging
+                st1 = run.stage([r], tc=False, keep=checks)[0]
+                if st1.cols is not None:
+                    samples.setdefault(r["request"], {})["cols"] = st1.cols
+                if r["shape"]["nchan"] > 1:
+                    st1.field.split_spectra(api.ENGINE_TC_F16, keep_fp32=True)
+                staged.append(st1)
+            ctx.synchronize()
+            for s in staged:  # plain FP32, one call at a time
                 t0 = time.perf_counter()
-                ctx.grid(f, t, cube, wts, engine=eng)
+                ctx.grid(s.field, s.target, s.cube, s.weights, engine=api.ENGINE_FP32)
                 ctx.synchronize()
-                lat.append(time.perf_counter() - t0)
-                st = ctx.stats()
-                detail.append({"arm": "tc" if tc else "plain", "request": r["request"], "shape": r["shape"],
-                               "s": lat[-1], "phase_ms": [round(x, 3) for x in st.ms_phase],
-                               "pairs_within": int(st.pairs_within)})
-            release(staged)
-        return lat
-
-    def served(rate):
-        srv = api.Server(ctx, lanes=2, hbm_budget=budget, max_batch=64)
-        lats, queues, busy = [], [], 0.0
-        rng = np.random.default_rng(3)
-        try:
-            for win in windows:
-                staged = stage(win, True)
-                arr = None
-                if rate:
-                    arr = np.cumsum(rng.exponential(1.0 / rate, len(staged)))
-                    arr -= arr[0]
-                tickets = []
+                plain_lat.append(time.perf_counter() - t0)
+                if s.r["request"] in checks:
+                    samples.setdefault(s.r["request"], {})["plain"] = check_sample(s)
+            for s in staged:  # tensor cores, one call at a time
+                eng = api.ENGINE_TC_F16 if s.r["shape"]["nchan"] > 1 else api.ENGINE_FP32
                 t0 = time.perf_counter()
-                for i, (r, f, t, cube, wts) in enumerate(staged):
-                    if arr is not None:
-                        d = t0 + arr[i] - time.perf_counter()
-                        if d > 0:
-                            time.sleep(d)
-                    tickets.append(srv.submit(f, t, cube, wts, api.SAMPLE_MAJOR, footprint=footprint(r)))
-                for (r, *_), tk in zip(staged, tickets):
-                    lt, q = srv.wait(tk)
-                    lats.append(lt)
-                    queues.append(q)
-                    detail.append({"arm": "served" if rate is None else "poisson", "request": r["request"],
-                                   "shape": r["shape"], "latency_s": lt, "queue_s": q})
-                busy += time.perf_counter() - t0
-                release(staged)
-            st = srv.stats()
-        finally:
-            srv.close()
-        return busy, lats, queues, st
-
-    tot_work = sum(work(r) for r in reqs)
-    plain_lat = per_call(False)
-    tc_lat = per_call(True)
-    served(None)  # warm-up: each lane captures its batch graph
-    busy, lats_cl, _, st_cl = served(None)
-    capacity = tot_work / busy
-    rate = 0.8 * len(reqs) / busy
-    busy_p, lats, queues, st = served(rate)
+                ctx.grid(s.field, s.target, s.cube, s.weights, engine=eng)
+                ctx.synchronize()
+                tc_lat.append(time.perf_counter() - t0)
+                grids.append(s.r["shape"]["grid"])
+                if s.r["shape"]["grid"] ** 2 >= 1 << 20:
+                    large_ids.add(len(tc_lat) - 1)
+                if s.r["request"] in checks:
+                    samples[s.r["request"]]["tc"] = check_sample(s)
+            if not warmed:  # each lane captures its batch graphs once, untimed
+                for s in staged[:8]:
+                    srv.wait(srv.submit(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR,
+                                        footprint=streams.footprint(s.r["shape"])))
+                warmed = True
+            # closed loop, timed in two parts: the window's small requests (the
+            # server batches them), then its large ones (each runs alone, as one
+            # hcg_grid); capacity = all work / both parts' time
+            for part in (False, True):
+                sub = [s for s in staged if (s.r["shape"]["grid"] ** 2 >= 1 << 20) == part]
+                if not sub:
+                    continue
+                t0 = time.perf_counter()
+                tickets = [srv.submit(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR,
+                                      footprint=streams.footprint(s.r["shape"])) for s in sub]
+                for tk in tickets:
+                    lats_cl.append(srv.wait(tk)[0])
+                dt = time.perf_counter() - t0
+                busy += dt
+                busy_part[part] += dt
+                work_part[part] += sum(streams.request_work(s.r) for s in sub)
+            for s in staged:
+                if s.r["request"] in checks:
+                    samples[s.r["request"]]["served"] = check_sample(s)
+            run.unstage(staged)
+        fields_built += run.built
+        run.close()
+        capacity = tot_work / busy
+        rate = 0.8 * len(reqs) / busy
+        # second pass: Poisson arrivals at 80% of the closed-loop capacity
+        rng = np.random.default_rng(3)
+        run = streams.Runner(ctx, reqs, torch, dev)
+        lats, queues, busy_p = [], [], 0.0
+        for win in windows:
+            staged = run.stage(win, tc=True)
+            arr = np.cumsum(rng.exponential(1.0 / rate, len(staged)))
+            arr -= arr[0]
+            t0 = time.perf_counter()
+            tickets = []
+            for i, s in enumerate(staged):
+                d = t0 + arr[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets.append(srv.submit(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR,
+                                          footprint=streams.footprint(s.r["shape"])))
+            for tk in tickets:
+                lt, q = srv.wait(tk)
+                lats.append(lt)
+                queues.append(q)
+            busy_p += time.perf_counter() - t0
+            run.unstage(staged)
+        fields_built += run.built
+        run.close()
+        st = srv.stats()
+    finally:
+        srv.close()
     pct = lambda v, q: float(np.percentile(np.asarray(v), q))
     plain = tot_work / sum(plain_lat)
+    tcv = tot_work / sum(tc_lat)
+    # served vs single call (bit for bit) and tensor cores vs FP32 engine, on the checked requests
+    served_same, tc_vs_fp32 = True, 0.0
+    for rid, d in samples.items():
+        if "served" in d and "tc" in d:
+            served_same &= bool(np.array_equal(d["served"][2], d["tc"][2], equal_nan=True))
+        if "plain" in d and "tc" in d:
+            tc_vs_fp32 = max(tc_vs_fp32, error_measures(d["tc"][2], d["plain"][2])["max_rel_err_plane"])
     out = {"metric": METRIC, "value": capacity, "unit": UNIT, "n_gpus": 1, "steps": len(reqs), "warmup": 1,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "fp16 hi/lo tensor-core channel sums (FP64 geometry)",
            "data": "synthetic (seeded config-5 request stream, hcgrid_b200/synth.py)",
-           "config": {"workload": "config5: %d requests, config-4 shapes (seed 3), 30%% field reuse, HBM budget "
-                                  "%.0f GB" % (len(reqs), args.hbm_budget_gb),
-                      "unique_fields": len(base), "windows": len(windows), "total_sample_channels": tot_work,
-                      "caps": "grid <= 2048, samples x channels <= 2^29, grid^2 x channels <= 2^30",
+           "config": {"workload": "config5: %d requests, config-4 shapes (seed 3, uncapped), 30%% field reuse, HBM "
+                                  "budget %.0f GB" % (len(reqs), args.hbm_budget_gb),
+                      "unique_fields": len({r["field"] for r in reqs}), "windows": len(windows),
+                      "staging_budget_gb": args.stage_gb, "total_sample_channels": tot_work,
+                      "fields_built": fields_built,
                       "engine": "served: hcg_server (2 lanes, batch graphs, tensor cores FP16 hi/lo); "
                                 "plain: hcg_grid FP32 engine per call"},
-           "served": {"capacity": capacity, "busy_s": round(busy, 4), "batches_closed_loop": st_cl["batches"],
+           "served": {"capacity": capacity, "busy_s": round(busy, 4), "batches": st["batches"],
                       "p50_s_closed_loop": pct(lats_cl, 50), "p99_s_closed_loop": pct(lats_cl, 99),
                       "poisson_rate_per_s": round(rate, 3), "throughput_at_80pct": tot_work / busy_p,
                       "p50_s": pct(lats, 50), "p99_s": pct(lats, 99), "queue_p99_s": pct(queues, 99)},
            "plain": {"value": plain, "p50_s": pct(plain_lat, 50), "p99_s": pct(plain_lat, 99),
                      "total_s": round(sum(plain_lat), 4)},
-           "tc_per_call": {"value": tot_work / sum(tc_lat), "p50_s": pct(tc_lat, 50), "p99_s": pct(tc_lat, 99),
+           "tc_per_call": {"value": tcv, "p50_s": pct(tc_lat, 50), "p99_s": pct(tc_lat, 99),
                            "total_s": round(sum(tc_lat), 4)},
-           "served_over_plain": round(capacity / plain, 3),
+           "served_over_plain": round(capacity / plain, 3), "served_over_tc_per_call": round(capacity / tcv, 3),
+           "by_size": {
+               "what": "closed-loop capacity of the server and per-call rates on the requests whose targets have "
+                       "< 2^20 pixels (batched by the server) and >= 2^20 pixels (run alone by both)",
+               "small": {"served": work_part[False] / max(busy_part[False], 1e-9),
+                         "tc_per_call": work_part[False] / max(sum(x for i, x in enumerate(tc_lat)
+                                                                    if i not in large_ids), 1e-9),
+                         "served_s": round(busy_part[False], 4)},
+               "large": {"served": work_part[True] / max(busy_part[True], 1e-9),
+                         "tc_per_call": work_part[True] / max(sum(tc_lat[i] for i in large_ids), 1e-9),
+                         "served_s": round(busy_part[True], 4)}},
+           "per_call_time_split": {
+               "what": "seconds of the per-call arms in requests whose targets have >= 2^20 pixels (the server "
+                       "runs those alone, as one hcg_grid each) and in the others (batched by the server)",
+               "large": {"requests": len(large_ids), "tc_s": round(sum(tc_lat[i] for i in large_ids), 3),
+                         "plain_s": round(sum(plain_lat[i] for i in large_ids), 3)},
+               "small": {"requests": len(tc_lat) - len(large_ids),
+                         "tc_s": round(sum(x for i, x in enumerate(tc_lat) if i not in large_ids), 3),
+                         "plain_s": round(sum(x for i, x in enumerate(plain_lat) if i not in large_ids), 3)},
+               "by_grid": {str(g): {"requests": grids.count(g),
+                                    "tc_s": round(sum(x for x, gg in zip(tc_lat, grids) if gg == g), 3),
+                                    "plain_s": round(sum(x for x, gg in zip(plain_lat, grids) if gg == g), 3)}
+                           for g in sorted(set(grids))}},
+           "checks": {"requests": sorted(samples), "served_equals_single_call": served_same,
+                      "tc_vs_fp32_engine_max_rel_err_plane": tc_vs_fp32},
            "gpu_launches": None, "e2e": None, "cpu_baseline": None}
-    if args.detail:
-        with open(args.detail, "w") as fh:
-            json.dump(detail, fh)
-    for f, t, _, _ in base.values():
-        f.close()
-        t.close()
+    if args.oracle_checks:
+        out["checks"]["vs_fp64_oracle"] = served_oracle_checks(reqs, samples)
+    ctx.close()
+    return out
+
+
+def served_oracle_checks(reqs, samples):
+    """The CPU leg's checker for the served stream: the FP64 oracle on each
+    checked request's sampled pixels and channels (the request's samples
+    regenerated on the host from their seed, its spectra columns as staged on
+    the device), against the tensor-core and served cubes. Requests above 2e8
+    candidate pair-channels are left to the comparison with the FP32 engine."""
+    from oracle import oracle as O
+    from hcgrid_b200 import api, synth
+    by_id = {r["request"]: r for r in reqs}
+    out = {}
+    for rid, d in sorted(samples.items()):
+        r = by_id[rid]
+        sh = r["shape"]
+        if synth.job_work(dict(sh, nchan=3)) > 2e8 or "tc" not in d or "cols" not in d:
+            continue
+        rng = np.random.default_rng(sh["seed"])
+        lon, lat = synth.raster_scan(sh["n"], sh["ra"], sh["dec"], sh["size_deg"], 2.0, rng)
+        pix, chans, got = d["tc"]
+        vals = d["cols"]
+        sigma = sh["fwhm"] / 3600.0 * synth.FWHM_TO_SIGMA
+        hdr = synth.sin_header(sh["grid"], sh["grid"], sh["ra"], sh["dec"], sh["size_deg"] / sh["grid"])
+        _, _, xw, yw = api.header_coords(hdr)
+        g = O.prepare_grid_kernel(sigma, 3.0 * sigma, sigma / 2.0)
+        ps = O.presort(g.hpx, lon, lat)
+        both = np.concatenate([vals, np.abs(vals)], axis=1)[ps.perm]
+        oc, ow, _ = O.grid(g, ps, lon[ps.perm], lat[ps.perm], both, xw[pix], yw[pix])
+        k = len(chans)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            ref, cond = oc[:, :k] / ow[:, None], oc[:, k:] / ow[:, None]
+        e = error_measures(got, ref, cond)
+        e["served"] = error_measures(d["served"][2], ref, cond)["max_rel_err_plane"] if "served" in d else None
+        e["shape"] = {k2: sh[k2] for k2 in ("n", "nchan", "grid", "fwhm")}
+        out[str(rid)] = e
+    return out
+
+
+def config4_run(args):
+    """Config 4, the batched form: 256 independent scan blocks (seed 2, the
+    config-4 shapes, each its own field), staged in windows that fit the
+    staging budget (all 256 hold 340 GB of spectra and 608 GB of cubes);
+    each window is gridded by one hcg_grid_batch call (persistent kernels fed
+    by device work queues, replayed from the context's captured graphs).
+    value = the blocks' sample-channels / the summed wall time of the batch
+    calls; the same blocks one hcg_grid call at a time (tensor cores) beside
+    it."""
+    import torch
+    from hcgrid_b200 import api, streams, synth
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    api.load(build_if_missing=True)
+    shapes = synth.config4_shapes(nblocks=args.blocks, seed=2)
+    reqs = [dict(request=i, field=i, shape=sh, spectra_seed=sh["seed"] + 1) for i, sh in enumerate(shapes)]
+    windows = streams.plan_windows(reqs, int(args.stage_gb * (1 << 30)))
+    ctx = api.Context(0)
+    run = streams.Runner(ctx, reqs, torch, dev)
+    t_batch, t_call, same = 0.0, 0.0, True
+    try:
+        first = True
+        for win in windows:
+            staged = run.stage(win, tc=True)
+            jobs = [(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR) for s in staged]
+            if first:  # captures the batch graphs, untimed
+                ctx.grid_batch(jobs[:4])
+                first = False
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            ctx.grid_batch(jobs)
+            t_batch += time.perf_counter() - t0
+            keep = [s.cube[:4096].clone() for s in staged]
+            for s, k in zip(staged, keep):
+                t0 = time.perf_counter()
+                ctx.grid(s.field, s.target, s.cube, s.weights)
+                ctx.synchronize()
+                t_call += time.perf_counter() - t0
+                same &= bool(torch.equal(torch.nan_to_num(s.cube[:4096], 7.0), torch.nan_to_num(k, 7.0)))
+            run.unstage(staged)
+    finally:
+        run.close()
+    work = sum(streams.request_work(r) for r in reqs)
+    out = {"metric": METRIC, "value": work / t_batch, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp16 hi/lo tensor-core channel sums (FP64 geometry); FP64 single-channel blocks",
+           "data": "synthetic (seeded config-4 scan blocks, hcgrid_b200/synth.py)",
+           "config": {"workload": "config4: %d scan blocks (seed 2), log-uniform 1e4-2e6 samples, 1-15 deg, "
+                                  "64^2-2048^2 SIN, {1,64,256,1024,2048} channels, FWHM {60,180,300}\""
+                                  % len(reqs), "windows": len(windows), "staging_budget_gb": args.stage_gb,
+                      "total_sample_channels": work},
+           "batch_s": round(t_batch, 4), "per_call_tc": {"value": work / t_call, "total_s": round(t_call, 4)},
+           "batch_over_per_call": round(t_call / t_batch, 3), "batch_equals_single_call": same,
+           "gpu_launches": None, "e2e": None, "cpu_baseline": None}
     ctx.close()
     return out
 
 
 def main():
     args = parse()
-    if args.workload == "config5":
+    if args.workload in ("config4", "config5"):
         if args.impl == "ours":
-            return served_main(args)
-        print(json.dumps({"impl": "reference", "unavailable": "the served form runs the B200 request loop; the "
-                          "reference's CPU path is timed on config2 and config1"}))
+            print(json.dumps(served_run(args) if args.workload == "config5" else config4_run(args)))
+            return
+        print(json.dumps({"impl": "reference", "unavailable": "the batched and served forms run the B200 batch "
+                          "engine and request loop; the reference's CPU path is timed on config2 and config1"}))
         return
     world, rank, local = dist_setup(args)
     job = job_for(args)
@@ -678,7 +772,7 @@ def main():
         # the served form (config 5) before the config-2 field takes its memory
         import torch
         sargs = argparse.Namespace(**vars(args))
-        sargs.jobs, sargs.detail = args.served_jobs, None
+        sargs.jobs, sargs.detail, sargs.oracle_checks = args.served_jobs, None, 0
         try:
             s = served_run(sargs)
             served = {"value": s["value"], "unit": UNIT, "requests": s["steps"],
@@ -729,7 +823,26 @@ def main():
         S = device_spectra(job, torch, dev)
     stream.synchronize()
     engine = ENGINES[args.engine]
-    field = ctx.field(lon_d, lat_d)
+    bands = None
+    if world > 1 and args.shard == "bands":
+        # Dec-band sharding of the one job: this rank grids target rows
+        # [y0, y1) from the contiguous range of ring-sorted samples they need
+        # (hcg_field_band_samples); only that range's spectra are attached
+        from hcgrid_b200 import shard
+        bands = shard.plan(job.ny, world)
+        y0, y1 = bands[rank]
+        geometry = ctx.field(lon_d, lat_d)  # sample positions only: the sort that gives the ranges
+        whole = ctx.target_from_header(job.header)
+        field, band_idx, band_target = shard.band_field(ctx, geometry, whole, job.lon, job.lat, y0, y1)
+        geometry.close()
+        whole.close()
+        if field is None:
+            raise RuntimeError("band [%d, %d) holds no samples" % (y0, y1))
+        S = S.index_select(0, torch.from_numpy(band_idx.astype(np.int64)).to(dev))
+        P = (y1 - y0) * job.nx
+    else:
+        field = ctx.field(lon_d, lat_d)
+    n_rank = S.shape[0]  # samples this rank grids from
     field.set_spectra(S)
     ctx.synchronize()
     # the checked sub-cube: central side x side pixels x k channels spread over
@@ -746,14 +859,14 @@ def main():
                  "sub_d": torch.from_numpy(subpix).to(dev), "chans_d": torch.from_numpy(chans).to(dev)}
     S_host = None
     if args.e2e_steps > 0:
-        S_host = torch.empty((job.n, job.nchan), dtype=torch.float32, pin_memory=True)
+        S_host = torch.empty(tuple(S.shape), dtype=torch.float32, pin_memory=True)
         S_host.copy_(S)
     del S  # the field holds its own (sorted) copy
     torch.cuda.empty_cache()
     plain_steps = args.plain_steps if (engine != api.ENGINE_FP32 and job.nchan > 1) else 0
     if engine != api.ENGINE_FP32 and job.nchan > 1:
         field.split_spectra(engine, keep_fp32=plain_steps > 0)
-    target = ctx.target_from_header(job.header)
+    target = band_target if bands else ctx.target_from_header(job.header)
     ctx.synchronize()
     torch.cuda.empty_cache()
     cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
@@ -803,6 +916,17 @@ def main():
         dist.barrier()
     ms_per_step = reduce_max(torch, dist, total_ms / args.steps)
     clocks = clk.summary()
+    assemble_ms = None
+    if bands:
+        # the band slabs to rank 0, device to device (NCCL gather), timed apart
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        ta = time.perf_counter()
+        whole_cube, whole_w = shard.assemble_tensors(dist, rank, world, bands, job.nx, cube, wts)
+        torch.cuda.synchronize(dev)
+        assemble_ms = reduce_max(torch, dist, (time.perf_counter() - ta) * 1e3)
+        del whole_cube, whole_w
+        torch.cuda.empty_cache()
     st = ctx.stats()  # counters of the last timed step (before the plain engine runs)
     timed_sub = None
     cube_timed = None
@@ -835,10 +959,11 @@ def main():
                 vs_fp32["what"] = "the whole timed cube against the FP32 engine's cube of the same field"
                 del cube_timed
                 torch.cuda.empty_cache()
-        plain = {"engine": ENGINE_TEXT["fp32"], "value": job.n * job.nchan * world / (pms * 1e-3),
+        plain = {"engine": ENGINE_TEXT["fp32"], "value": job.n * job.nchan * (1 if bands else world) / (pms * 1e-3),
                  "ms_per_step": round(pms, 3), "steps": plain_steps, "warmup": 2}
     work = job.n * job.nchan
-    value = work * world / (ms_per_step * 1e-3)
+    copies = 1 if bands else world  # bands: one job over all ranks; replicas: a job per rank
+    value = work * copies / (ms_per_step * 1e-3)
 
     # dominant kernel and its roofline
     tc = engine != api.ENGINE_FP32 and job.nchan > 1
@@ -851,11 +976,11 @@ def main():
     avg = [statistics.mean(x) for x in phase_ms]
     dom = int(np.argmax(avg))
     if dom == 3:
-        alg = job.n * 4 * job.nchan + P * (4 * job.nchan + 4)
+        alg = n_rank * 4 * job.nchan + P * (4 * job.nchan + 4)
         if job.nchan == 1:
-            alg = algorithmic_bytes(job.n, 1, P)
+            alg = algorithmic_bytes(n_rank, 1, P)
     else:
-        alg = algorithmic_bytes(job.n, 0, 0) if dom == 2 else P * 16
+        alg = algorithmic_bytes(n_rank, 0, 0) if dom == 2 else P * 16
     peak, peak_kind = peaks()
     achieved = alg / (avg[dom] * 1e-3) / 1e9
     traffic = None
@@ -870,7 +995,7 @@ def main():
                 if peak_kind == "measured" else "fallback 6650 GB/s", "traffic": traffic,
                 "algorithmic_bytes_per_launch": alg, "kernel_ms": round(avg[dom], 3),
                 "phase_ms": {n: round(a, 3) for n, a in zip(phase_names, avg)},
-                "whole_step_hbm_frac": round(algorithmic_bytes(job.n, job.nchan, P) / (ms_per_step * 1e-3) / 1e9 / peak, 4),
+                "whole_step_hbm_frac": round(algorithmic_bytes(n_rank, job.nchan, P) / (ms_per_step * 1e-3) / 1e9 / peak, 4),
                 "pairs_within": int(st.pairs_within), "pairs_candidate": int(st.pairs_candidate)}
     if tc and dom == 3:
         tpk, tkind = tensor_peak()
@@ -893,7 +1018,19 @@ def main():
     # end to end through the C ABI from host buffers
     e2e = None
     if args.e2e_steps > 0:
-        lon_h, lat_h = np.ascontiguousarray(job.lon), np.ascontiguousarray(job.lat)
+        if bands:
+            lon_h, lat_h = np.ascontiguousarray(job.lon[band_idx]), np.ascontiguousarray(job.lat[band_idx])
+            _, _, hx, hy = api.header_coords(job.header)
+            bx = np.ascontiguousarray(hx[bands[rank][0] * job.nx:bands[rank][1] * job.nx])
+            by = np.ascontiguousarray(hy[bands[rank][0] * job.nx:bands[rank][1] * job.nx])
+
+            def make_target():
+                return ctx.target(job.nx, bands[rank][1] - bands[rank][0], bx, by)
+        else:
+            lon_h, lat_h = np.ascontiguousarray(job.lon), np.ascontiguousarray(job.lat)
+
+            def make_target():
+                return ctx.target_from_header(job.header)
         cube_h = torch.empty((P, job.nchan), dtype=torch.float32, pin_memory=True)
         w_h = torch.empty(P, dtype=torch.float32, pin_memory=True)
         times = []
@@ -902,16 +1039,23 @@ def main():
                 dist.barrier()
             t0 = time.perf_counter()
             f2 = ctx.field(lon_h, lat_h)
+            ta = time.perf_counter()
             f2.set_spectra(S_host)
+            tb = time.perf_counter()
             if tc:
                 f2.split_spectra(engine, keep_fp32=False)
-            t2 = ctx.target_from_header(job.header)
+            tc_ = time.perf_counter()
+            t2 = make_target()
             ctx.grid(f2, t2, cube_h, w_h, engine=engine)
             dt = time.perf_counter() - t0
             f2.close()
             t2.close()
             if i > 0:
                 times.append(dt)
+                # host time of each call in the timed step (no synchronize between them)
+                timed_calls = {"hcg_field_create": round(ta - t0, 4), "hcg_field_set_spectra": round(tb - ta, 4),
+                               "hcg_field_split_spectra": round(tc_ - tb, 4),
+                               "hcg_target_from_header + hcg_grid": round(t0 + dt - tc_, 4)}
         # one more pass, untimed, with a synchronize after each call: where
         # the end-to-end time goes
         calls = {}
@@ -931,7 +1075,7 @@ def main():
         if tc:
             f2.split_spectra(engine, keep_fp32=False)
             mark("hcg_field_split_spectra")
-        t2 = ctx.target_from_header(job.header)
+        t2 = make_target()
         mark("hcg_target_from_header")
         ctx.grid(f2, t2, cube_h, w_h, engine=engine)
         mark("hcg_grid")
@@ -939,10 +1083,10 @@ def main():
         t2.close()
         mark("destroy")
         t_e2e = reduce_max(torch, dist, statistics.mean(times))
-        h2d = 16 * job.n + 4 * job.n * job.nchan
+        h2d = 16 * n_rank + 4 * n_rank * job.nchan  # this rank's inputs
         d2h = 4 * P * job.nchan + 4 * P
-        e2e = {"value": work * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "s_per_step": round(t_e2e, 4), "calls_s_untimed_pass": calls,
+        e2e = {"value": work * copies / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "s_per_step": round(t_e2e, 4), "calls_s_untimed_pass": calls, "calls_s_last_timed_step": timed_calls,
                "path": "hcg_field_create + hcg_field_set_spectra%s + hcg_target_from_header + hcg_grid, host pinned"
                        % (" + hcg_field_split_spectra" if tc else "")}
 
@@ -973,12 +1117,14 @@ def main():
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None,
+               "scaling": "strong" if bands else "weak", "vs_baseline": None,
                "dtype": DTYPE_TEXT[args.engine] if job.nchan > 1 else DTYPE_TEXT["fp32"],
                "data": "synthetic (seeded %s generator, hcgrid_b200/synth.py)" % job.name,
                "config": {"workload": workload_text(job),
                           "samples": job.n, "channels": job.nchan, "pixels": P, "nside": ctx.info(field).nside,
-                          "parallelism": "replica per GPU" if world > 1 else "single GPU",
+                          "parallelism": ("dec bands of target rows, one per rank, NCCL gather to rank 0"
+                                          if bands else "replica per GPU" if world > 1 else "single GPU"),
+                          "bands": bands, "assemble_ms": assemble_ms,
                           "l2": "inputs larger than L2 (spectra %.1f GB), no flush" % (4 * job.n * job.nchan / 1e9),
                           "engine": ENGINE_TEXT[args.engine] if job.nchan > 1 else ENGINE_TEXT["fp32"],
                           "tc_pipeline": tune, "tc_weights": args.tc_weights},

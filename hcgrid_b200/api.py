@@ -48,7 +48,7 @@ class Tuning(C.Structure):
                 ("spread", C.c_float)]
 
 
-TUNE_PREFETCH = (2, 4, 6, 8, 12)
+TUNE_PREFETCH = (0, 2, 4, 6, 8)
 TUNE_STRIP = (0, 4, 8, 16, 32)
 
 

@@ -784,12 +784,18 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
     }
     CK(ctx, cudaMemsetAsync(ctx->d_stats, 0, offsetof(DevStats, invalid_input), ctx->stream), "stats reset");
     // The batch kernels evaluate GAUSS1D; jobs with the other kernels run on
-    // their own after the batch, as do the jobs the batch routes out.
+    // their own after the batch, as do the jobs the batch routes out. Jobs of
+    // at least kBatchMaxPixels target pixels fill the GPU by themselves and go
+    // straight to the single-job path (its persistent kernels), without a
+    // pass through the batch's geometry graph.
+    auto alone_now = [&](const hcg_job &j) {
+        return j.field->kernel_type != HCG_GAUSS1D || ctx->factor > 1 || job_pixels(j) >= kBatchMaxPixels;
+    };
     std::vector<hcg_job> shared;
     std::vector<uint32_t> index;  // shared job -> caller's job
     for (uint32_t i = 0; i < njobs; ++i) {
         // coarsened runs grid on the single-job path
-        if (jobs[i].field->kernel_type != HCG_GAUSS1D || ctx->factor > 1) continue;
+        if (alone_now(jobs[i])) continue;
         shared.push_back(jobs[i]);
         index.push_back(i);
     }
@@ -801,7 +807,7 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
     if (e != cudaSuccess) return cuda_fail(ctx, e, "grid batch", why);
     std::vector<char> alone(njobs, 0);
     for (uint32_t k = 0; k < shared.size(); ++k) alone[index[k]] = fallback[k];
-    for (uint32_t i = 0; i < njobs; ++i) alone[i] |= jobs[i].field->kernel_type != HCG_GAUSS1D || ctx->factor > 1;
+    for (uint32_t i = 0; i < njobs; ++i) alone[i] |= alone_now(jobs[i]);
     for (uint32_t i = 0; i < njobs; ++i) {
         if (!alone[i]) continue;
         e = grid_field(ctx, jobs[i].field, jobs[i].target, jobs[i].cube, jobs[i].layout, jobs[i].weights,

@@ -167,8 +167,9 @@ struct hcg_target {
 namespace hcg {
 constexpr int kTcClasses = 8;
 constexpr int kTcConfigCount = 6;  // tensor-core pipeline shapes (hcg_tc_set_config)
-constexpr int kTcDefaultPrefetch = 6;  // chunks the producer prefetches into L2 ahead of its loads
+constexpr int kTcDefaultPrefetch = 0;  // chunks the producer prefetches into L2 ahead of its loads (0: none)
 constexpr int kTcDefaultStrip = 8;     // tile columns per strip of the persistent tile walk
+constexpr uint64_t kBatchMaxPixels = 1ull << 20;  // larger targets skip hcg_grid_batch's batch pass
 // channel class of a split field: 64-channel blocks 1, 2, 3-4, 5-8, ... -> 0, 1, 2, 3, ...
 inline int tc_class_of(uint32_t cpad) {
     const uint32_t b = cpad / 64;

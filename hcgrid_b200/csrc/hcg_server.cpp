@@ -1,13 +1,17 @@
 // Request loop for serving gridding jobs (continuous batching).
 //
 // Clients submit jobs (a resident field, a target and device output
-// buffers) as they arrive. A dispatcher thread admits pending jobs in
-// arrival order while their HBM footprint fits the budget and hands them to
-// one of `lanes` worker lanes: a job whose target has at least
-// kSingleJobPixels pixels alone, with the GPU to itself (its kernels fill the
-// GPU by themselves; it runs through hcg_grid), else a batch of consecutive
-// smaller jobs (at most `max_batch`, through hcg_grid_batch's persistent
-// kernels). Each lane owns its own context (stream + captured batch graphs)
+// buffers) as they arrive. A dispatcher thread hands pending jobs to one of
+// `lanes` worker lanes while their HBM footprint fits the budget: a job whose
+// target has at least kSingleJobPixels pixels alone, with the GPU to itself
+// (its kernels fill the GPU by themselves; it runs through hcg_grid), else a
+// batch of smaller jobs (at most `max_batch`, through hcg_grid_batch's
+// persistent kernels). The oldest pending job decides what runs next. If it
+// is small, every pending small job joins its batch in arrival order, large
+// ones skipped, so large jobs between them do not split the batch. If it is
+// large, it waits for the GPU to be idle; meanwhile the small jobs queued
+// behind it may pass it on a free lane, at most kMaxPasses batches, so a
+// large job is not starved. Each lane owns its own context (stream + captured batch graphs)
 // on the same device, so a batch that arrives while another batch is on the
 // GPU is launched right away and the two overlap on the device. When a lane finishes, its footprint is
 // released and the dispatcher admits more jobs. Every job records submit,
@@ -37,12 +41,15 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr uint64_t kSingleJobPixels = 1ull << 20;
+constexpr uint32_t kMaxPasses = 2;  // batches that may pass a waiting large job
 
 struct Pending {
     uint64_t ticket;
     hcg_job job;
     uint64_t bytes;
     double t_submit;
+    bool large;
+    uint32_t passed = 0;  // batches dispatched while this job waited at the queue's head
 };
 
 struct Done {
@@ -117,20 +124,26 @@ struct hcg_server {
     void dispatch() {
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
-            // A large job runs with the GPU to itself (its persistent kernels
-            // assign work statically: CTAs that start late behind another
-            // lane's kernels stretch the whole launch); batches of small jobs
-            // overlap each other.
+            size_t busy = 0;
+            bool busy_single = false;
+            auto any_small = [&] {
+                for (const Pending &p : queue)
+                    if (!p.large) return true;
+                return false;
+            };
             cv_work.wait(lk, [&] {
                 if (stop && queue.empty()) return true;
                 if (queue.empty()) return false;
-                size_t busy = 0;
+                busy = 0;
+                busy_single = false;
                 for (size_t i = 0; i < lanes.size(); ++i) {
-                    if (lane_busy[i] && lane_single[i]) return false;
                     busy += lane_busy[i] ? 1 : 0;
+                    busy_single |= lane_busy[i] && lane_single[i];
                 }
-                if (hcg::job_pixels(queue.front().job) >= kSingleJobPixels) return busy == 0;
-                return busy < lanes.size();
+                if (busy_single || busy == lanes.size()) return false;
+                const Pending &f = queue.front();
+                if (!f.large || busy == 0) return true;
+                return f.passed < kMaxPasses && any_small();
             });
             if (stop && queue.empty()) {
                 cv_work.notify_all();
@@ -139,17 +152,34 @@ struct hcg_server {
             size_t li = 0;
             while (li < lanes.size() && lane_busy[li]) ++li;
             if (li == lanes.size()) continue;
-            // admit in arrival order while the footprint fits (a job larger
-            // than the whole budget runs alone once nothing else is resident)
             std::vector<Pending> b;
-            const bool single = hcg::job_pixels(queue.front().job) >= kSingleJobPixels;
-            while (!queue.empty() && b.size() < (single ? 1u : max_batch)) {
-                const Pending &p = queue.front();
-                if (!b.empty() && hcg::job_pixels(p.job) >= kSingleJobPixels) break;  // large jobs run alone
-                if (in_use + p.bytes > budget && !(in_use == 0 && b.empty())) break;
-                in_use += p.bytes;
-                b.push_back(p);
+            const bool single = queue.front().large && busy == 0;
+            if (single) {  // nothing else is resident: the budget holds it
+                b.push_back(queue.front());
+                in_use += b[0].bytes;
                 queue.pop_front();
+            } else {
+                // the pending small jobs in arrival order, while the footprint
+                // fits (one larger than the whole budget runs once nothing
+                // else is resident)
+                const bool passing = queue.front().large;
+                std::deque<Pending> rest;
+                bool full = false;
+                for (Pending &p : queue) {
+                    if (full || p.large || b.size() >= max_batch) {
+                        rest.push_back(p);
+                        continue;
+                    }
+                    if (in_use + p.bytes > budget && !(in_use == 0 && b.empty())) {
+                        full = true;
+                        rest.push_back(p);
+                        continue;
+                    }
+                    in_use += p.bytes;
+                    b.push_back(p);
+                }
+                queue.swap(rest);
+                if (passing && !b.empty()) ++queue.front().passed;
             }
             if (b.empty()) {  // wait for memory to be released
                 cv_done.wait(lk);
@@ -196,7 +226,7 @@ hcg_status hcg_server_submit(hcg_server *s, const hcg_job *job, uint64_t footpri
     if (!s || !job || !ticket) return HCG_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return HCG_ESTATE;
-    Pending p{s->next_ticket++, *job, footprint_bytes, s->now()};
+    Pending p{s->next_ticket++, *job, footprint_bytes, s->now(), hcg::job_pixels(*job) >= kSingleJobPixels};
     s->done[p.ticket].t_submit = p.t_submit;
     *ticket = p.ticket;
     s->queue.push_back(p);

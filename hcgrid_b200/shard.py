@@ -92,3 +92,51 @@ def assemble(dist, rank: int, world: int, bands, nx: int, cube_rows, w_rows):
         cube[y0 * nx:y1 * nx] = c
         w[y0 * nx:y1 * nx] = ww
     return cube, w
+
+
+def assemble_tensors(dist, rank: int, world: int, bands, nx: int, cube_rows, w_rows):
+    """assemble() for torch tensors: rank 0 receives every band slab through
+    one torch.distributed gather (NCCL keeps CUDA tensors on the device; any
+    backend works for CPU tensors). Slabs are padded to the largest band so
+    the gather moves equal sizes. Returns the whole cube [ny * nx, C] and
+    weight map on rank 0, (None, None) elsewhere."""
+    import torch
+    if dist is None or world == 1:
+        return cube_rows, w_rows
+    nchan = cube_rows.shape[1]
+    rows = max(y1 - y0 for y0, y1 in bands) * nx
+    slab = torch.zeros((rows, nchan + 1), dtype=cube_rows.dtype, device=cube_rows.device)
+    n = cube_rows.shape[0]
+    slab[:n, :nchan] = cube_rows
+    slab[:n, nchan] = w_rows
+    got = [torch.empty_like(slab) for _ in range(world)] if rank == 0 else None
+    dist.gather(slab, got, dst=0)
+    if rank != 0:
+        return None, None
+    ny = bands[-1][1]
+    cube = torch.empty((ny * nx, nchan), dtype=cube_rows.dtype, device=cube_rows.device)
+    w = torch.empty(ny * nx, dtype=cube_rows.dtype, device=cube_rows.device)
+    for (y0, y1), g in zip(bands, got):
+        k = (y1 - y0) * nx
+        cube[y0 * nx:y1 * nx] = g[:k, :nchan]
+        w[y0 * nx:y1 * nx] = g[:k, nchan]
+    return cube, w
+
+
+def band_field(ctx: api.Context, geometry: api.Field, target: api.Target, lon, lat, y0: int, y1: int, perm=None):
+    """The samples rows [y0, y1) of `target` need: (field of those samples in
+    sorted order, their input indices, the band's target). The field is
+    created from host coordinates of that range only; spectra are attached
+    by the caller (values[idx])."""
+    s0, s1 = geometry.band_samples(target, y0, y1)
+    if perm is None:
+        perm = geometry.sorted()[1]
+    idx = perm[s0:s1]
+    nx = target.nx
+    xw, yw = target.coords()
+    p0, p1 = y0 * nx, y1 * nx
+    bt = ctx.target(nx, y1 - y0, np.ascontiguousarray(xw[p0:p1]), np.ascontiguousarray(yw[p0:p1]))
+    if s1 == s0:
+        return None, idx, bt
+    f = ctx.field(np.ascontiguousarray(lon[idx]), np.ascontiguousarray(lat[idx]))
+    return f, idx, bt

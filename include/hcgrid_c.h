@@ -178,9 +178,11 @@ hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_targ
 
 /* Pipeline depth and tile walk of the tensor-core engine, per channel class
  * (-1: every class; a value of -1 restores the default):
- *   prefetch  chunks of staged spectra the producer requests into L2 ahead of
- *             its shared-memory loads (values up to the shape's stages mean
- *             the stages themselves); default 6;
+ *   prefetch  chunks of staged spectra the producer also requests into L2
+ *             ahead of its shared-memory loads (0: none; values up to the
+ *             shape's stages mean the stages themselves); a prefetch
+ *             instruction holds the producer warp as long as a load, so it
+ *             pays only where the loads' latency is exposed; default 0;
  *   strip     the persistent kernels take the tiles of a launch in strips of
  *             `strip` tile columns, row by row inside a strip, so that the
  *             tiles in flight together form a compact block whose neighbours
@@ -195,7 +197,7 @@ hcg_status hcg_tc_set_pipeline(hcg_context *ctx, int channel_class, int prefetch
  * scored by its best run. The choices are kept for the field's channel class
  * and returned; spread = (slowest - fastest) / fastest over the chosen
  * setting's repeats. */
-#define HCG_TUNE_PREFETCH {2, 4, 6, 8, 12}
+#define HCG_TUNE_PREFETCH {0, 2, 4, 6, 8}
 #define HCG_TUNE_STRIP {0, 4, 8, 16, 32}
 typedef struct {
     int shape, prefetch, strip;
@@ -262,8 +264,10 @@ typedef struct {
  * is a CUDA graph replayed per batch. Jobs may differ in sample count, map
  * size, channel count and kernel (each field grids with the kernel setup it
  * was created under; the batch pass takes GAUSS1D jobs, GAUSS2D and
- * TAPERED_SINC jobs run after it one at a time). Returns when all cubes are
- * written; each cube equals what hcg_grid writes for that job. */
+ * TAPERED_SINC jobs run after it one at a time, as do jobs whose targets
+ * have 2^20 pixels or more: those fill the GPU by themselves). Returns when
+ * all cubes are written; each cube equals what hcg_grid writes for that
+ * job. */
 hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs);
 
 /* Serving loop with continuous batching. `lanes` contexts on `device` (the

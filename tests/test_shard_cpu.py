@@ -92,6 +92,64 @@ def test_assemble_over_two_gloo_ranks():
     assert outs[1]["none"]
 
 
+TENSOR_SCRIPT = r"""
+import datetime, json, sys
+sys.path.insert(0, %r)
+import numpy as np
+import torch
+import torch.distributed as dist
+from hcgrid_b200 import shard
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+rank, world = dist.get_rank(), dist.get_world_size()
+nx, ny, nchan = 5, 40, 3
+bands = shard.plan(ny, world)
+y0, y1 = bands[rank]
+rows = torch.arange(y0 * nx, y1 * nx, dtype=torch.float32)
+cube = rows[:, None] * 10 + torch.arange(nchan, dtype=torch.float32)[None, :]
+c, ww = shard.assemble_tensors(dist, rank, world, bands, nx, cube, rows + 0.5)
+if rank == 0:
+    want = torch.arange(ny * nx, dtype=torch.float32)
+    ok = torch.equal(c, want[:, None] * 10 + torch.arange(nchan, dtype=torch.float32)[None, :]) and \
+        torch.equal(ww, want + 0.5)
+    print(json.dumps({"rank": 0, "ok": bool(ok)}))
+else:
+    print(json.dumps({"rank": rank, "none": c is None and ww is None}))
+dist.destroy_process_group()
+"""
+
+
+def _run_ranks(script, world=2):
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    procs = []
+    for rank in range(world):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, "-c", script % ROOT], cwd=ROOT, env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        try:
+            out, err = p.communicate(timeout=120)
+        except subprocess.TimeoutExpired:
+            for q in procs:
+                q.kill()
+            raise
+        assert p.returncode == 0, err[-2000:]
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    return outs
+
+
+def test_assemble_tensors_gathers_unequal_bands_over_gloo():
+    """The tensor gather behind the band-sharded bench (NCCL on CUDA tensors
+    there): unequal bands (16 and 24 rows) padded to equal sizes, unpadded
+    into the whole cube on rank 0."""
+    outs = _run_ranks(TENSOR_SCRIPT)
+    assert outs[0]["ok"] and outs[1]["none"]
+
+
 # The band sample range, argued in hcgrid_b200/csrc/hcg_shard.cu, checked with
 # the FP64 oracle on the CPU: complete rings of the band, one sample in front.
 
