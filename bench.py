@@ -2,7 +2,8 @@
 """Benchmark of the B200 gridder on the reference's headline workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload config2|config1|config5] [--served-jobs J]
+                    [--workload config2|config1|config3|config4|config5] [--served-jobs J]
+                    [--shard bands|replicas]
 
 A step is one gridding pass (hcg_grid: pixel setup, candidate selection,
 FP64 weights, channel sums, normalisation) over the resident field of the
@@ -18,8 +19,12 @@ At N=1 the config-2 line also carries `served_config5`: the served form
 the plain FP32 engine and the tensor-core engine per call on the same
 requests; `--workload config5` prints its full record).
 
-Multi-GPU (torchrun): every rank grids its own copy of the job (weak
-scaling, no collective on the data path); timings are the max over ranks.
+Multi-GPU (torchrun): with --shard bands (the default) the one job is split
+into Dec bands of target rows, one per rank; each rank grids its band from
+the contiguous range of ring-sorted samples the band needs (strong scaling,
+no collective in the timed steps) and rank 0 then gathers the band slabs
+(NCCL, timed apart as `assemble_ms`). With --shard replicas every rank grids
+its own copy of the job (weak scaling). Timings are the max over ranks.
 
 --impl reference times the reference's own CPU path (oracle/_ref: HCGrid's
 host pre-sort plus its kernel body built for the host cores) on a bounded
@@ -62,7 +67,8 @@ def parse():
     ap.add_argument("--oracle-checks", type=int, default=1,
                     help="config5: check sampled requests against the FP64 oracle in the CPU leg (0: skip)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
-    ap.add_argument("--detail", default=None, help="config5: write per-request times of the per-call arms here")
+    ap.add_argument("--lanes", type=int, default=2, help="config5: server lanes")
+    ap.add_argument("--detail", default=None, help="config5: write per-window times of the served and per-call arms here")
     ap.add_argument("--tc-weights", default="auto", choices=["auto", "entries", "direct"],
                     help="tensor-core weight operands (hcg_tc_set_weights)")
     ap.add_argument("--served-jobs", type=int, default=200,
@@ -481,7 +487,7 @@ def served_run(args):
       plain        one hcg_grid call at a time, FP32 CUDA-core engine;
       tc_per_call  one hcg_grid call at a time, tensor-core engine;
       served       the window's requests submitted to hcg_server at once
-                   (continuous batching over 2 lanes, persistent batch
+                   (continuous batching over --lanes lanes, persistent batch
                    kernels replayed from CUDA graphs, tensor cores,
                    footprint admission against the HBM budget); capacity =
                    work / time from a window's first submit to its last
@@ -509,15 +515,17 @@ def served_run(args):
     ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
     samples = {}  # request -> {arm: (pix, chans, values)}
     plain_lat, tc_lat, lats_cl, busy, grids = [], [], [], 0.0, []
-    busy_part, work_part = {False: 0.0, True: 0.0}, {False: 0, True: 0}  # by "target has >= 2^20 pixels"
-    large_ids = set()  # requests whose targets have >= 2^20 pixels (the server runs them alone)
-    srv = api.Server(ctx, lanes=2, hbm_budget=budget, max_batch=64)
+    busy_part, work_part = {False: 0.0, True: 0.0}, {False: 0, True: 0}  # by "fills the GPU alone"
+    large_ids = set()  # requests whose channel sums fill the GPU (the server runs them alone)
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    srv = api.Server(ctx, lanes=args.lanes, hbm_budget=budget, max_batch=64)
     fields_built = 0
     try:
         run = streams.Runner(ctx, reqs, torch, dev)
-        warmed = False
-        for win in windows:
+        detail = open(args.detail, "w") if args.detail else None
+        for wi, win in enumerate(windows):
             staged = []
+            lat0 = len(tc_lat)
             for r in win:  # FP32 spectra kept beside the split: every arm runs on this staging
                 st1 = run.stage([r], tc=False, keep=checks)[0]
                 if st1.cols is not None:
@@ -540,20 +548,21 @@ def served_run(args):
                 ctx.synchronize()
                 tc_lat.append(time.perf_counter() - t0)
                 grids.append(s.r["shape"]["grid"])
-                if s.r["shape"]["grid"] ** 2 >= 1 << 20:
+                if streams.fills_gpu(s.r["shape"], nsm):
                     large_ids.add(len(tc_lat) - 1)
                 if s.r["request"] in checks:
                     samples[s.r["request"]]["tc"] = check_sample(s)
-            if not warmed:  # each lane captures its batch graphs once, untimed
-                for s in staged[:8]:
-                    srv.wait(srv.submit(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR,
-                                        footprint=streams.footprint(s.r["shape"])))
-                warmed = True
+            # the window once through the server, untimed: lanes capture their
+            # batch graphs and grow their scratch to the window's sizes, as the
+            # per-call arms' context already has from the passes above
+            for tk in [srv.submit(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR,
+                                  footprint=streams.footprint(s.r["shape"])) for s in staged]:
+                srv.wait(tk)
             # closed loop, timed in two parts: the window's small requests (the
-            # server batches them), then its large ones (each runs alone, as one
-            # hcg_grid); capacity = all work / both parts' time
+            # server batches them), then the ones that fill the GPU alone (each
+            # runs as one hcg_grid); capacity = all work / both parts' time
             for part in (False, True):
-                sub = [s for s in staged if (s.r["shape"]["grid"] ** 2 >= 1 << 20) == part]
+                sub = [s for s in staged if streams.fills_gpu(s.r["shape"], nsm) == part]
                 if not sub:
                     continue
                 t0 = time.perf_counter()
@@ -565,12 +574,19 @@ def served_run(args):
                 busy += dt
                 busy_part[part] += dt
                 work_part[part] += sum(streams.request_work(s.r) for s in sub)
+                if detail:
+                    tcs = sum(tc_lat[lat0 + i] for i, s in enumerate(staged)
+                              if streams.fills_gpu(s.r["shape"], nsm) == part)
+                    detail.write(json.dumps({"window": wi, "large": part, "requests": len(sub), "served_s": dt,
+                                             "tc_per_call_s": tcs}) + "\n")
             for s in staged:
                 if s.r["request"] in checks:
                     samples[s.r["request"]]["served"] = check_sample(s)
             run.unstage(staged)
         fields_built += run.built
         run.close()
+        if detail:
+            detail.close()
         capacity = tot_work / busy
         rate = 0.8 * len(reqs) / busy
         # second pass: Poisson arrivals at 80% of the closed-loop capacity
@@ -619,7 +635,7 @@ def served_run(args):
                       "unique_fields": len({r["field"] for r in reqs}), "windows": len(windows),
                       "staging_budget_gb": args.stage_gb, "total_sample_channels": tot_work,
                       "fields_built": fields_built,
-                      "engine": "served: hcg_server (2 lanes, batch graphs, tensor cores FP16 hi/lo); "
+                      "engine": "served: hcg_server (%d lanes, batch graphs, tensor cores FP16 hi/lo); " % args.lanes +
                                 "plain: hcg_grid FP32 engine per call"},
            "served": {"capacity": capacity, "busy_s": round(busy, 4), "batches": st["batches"],
                       "p50_s_closed_loop": pct(lats_cl, 50), "p99_s_closed_loop": pct(lats_cl, 99),
@@ -631,8 +647,8 @@ def served_run(args):
                            "total_s": round(sum(tc_lat), 4)},
            "served_over_plain": round(capacity / plain, 3), "served_over_tc_per_call": round(capacity / tcv, 3),
            "by_size": {
-               "what": "closed-loop capacity of the server and per-call rates on the requests whose targets have "
-                       "< 2^20 pixels (batched by the server) and >= 2^20 pixels (run alone by both)",
+               "what": "closed-loop capacity of the server and per-call rates on the requests batched by the "
+                       "server (small) and on those whose channel sums fill the GPU (large: run alone by both)",
                "small": {"served": work_part[False] / max(busy_part[False], 1e-9),
                          "tc_per_call": work_part[False] / max(sum(x for i, x in enumerate(tc_lat)
                                                                     if i not in large_ids), 1e-9),
@@ -641,8 +657,9 @@ def served_run(args):
                          "tc_per_call": work_part[True] / max(sum(tc_lat[i] for i in large_ids), 1e-9),
                          "served_s": round(busy_part[True], 4)}},
            "per_call_time_split": {
-               "what": "seconds of the per-call arms in requests whose targets have >= 2^20 pixels (the server "
-                       "runs those alone, as one hcg_grid each) and in the others (batched by the server)",
+               "what": "seconds of the per-call arms in requests whose channel sums fill the GPU (2^20 pixels or "
+                       "more, or one 16x8-pixel x 256-channel item per SM; the server runs those alone, as one "
+                       "hcg_grid each) and in the others (batched by the server)",
                "large": {"requests": len(large_ids), "tc_s": round(sum(tc_lat[i] for i in large_ids), 3),
                          "plain_s": round(sum(plain_lat[i] for i in large_ids), 3)},
                "small": {"requests": len(tc_lat) - len(large_ids),
@@ -717,14 +734,14 @@ def config4_run(args):
     ctx = api.Context(0)
     run = streams.Runner(ctx, reqs, torch, dev)
     t_batch, t_call, same = 0.0, 0.0, True
+    tuning = None
     try:
-        first = True
         for win in windows:
             staged = run.stage(win, tc=True)
             jobs = [(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR) for s in staged]
-            if first:  # captures the batch graphs, untimed
-                ctx.grid_batch(jobs[:4])
-                first = False
+            if tuning is None:  # untimed: the batch graphs are captured and the batch autotuner picks
+                # a tensor-core shape per channel class on the first window's blocks
+                tuning = ctx.autotune_batch(jobs, reps=args.tune_reps)
             ctx.synchronize()
             t0 = time.perf_counter()
             ctx.grid_batch(jobs)
@@ -750,6 +767,10 @@ def config4_run(args):
                       "total_sample_channels": work},
            "batch_s": round(t_batch, 4), "per_call_tc": {"value": work / t_call, "total_s": round(t_call, 4)},
            "batch_over_per_call": round(t_call / t_batch, 3), "batch_equals_single_call": same,
+           "batch_tuning": {"classes": tuning, "how": "hcg_autotune_batch on the first window: per channel class, "
+                            "each of the 4 shapes (0: 256 ch x 32 slots x 4 stages, 1: 256 x 64 x 2, "
+                            "2: 128 x 64 x 3, 3: 64 x 64 x 4) timed as one hcg_grid_batch of the class's "
+                            "blocks, best of %d runs after a warm-up" % args.tune_reps},
            "gpu_launches": None, "e2e": None, "cpu_baseline": None}
     ctx.close()
     return out

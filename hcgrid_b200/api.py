@@ -48,6 +48,13 @@ class Tuning(C.Structure):
                 ("spread", C.c_float)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("channel_class", C.c_int), ("shape", C.c_int), ("jobs", C.c_uint32), ("ms", C.c_float * 4),
+                ("spread", C.c_float)]
+
+
+BATCH_SHAPES = 4  # hcg_batch_set_shape: 0: 256 ch x 32 slots x 4 stages, 1: 256 x 64 x 2, 2: 128 x 64 x 3, 3: 64 x 64 x 4
+
 TUNE_PREFETCH = (0, 2, 4, 6, 8)
 TUNE_STRIP = (0, 4, 8, 16, 32)
 
@@ -94,6 +101,9 @@ EXPORTS = {
     "hcg_set_entry_budget": ([C.c_void_p, C.c_uint64], C.c_int),
     "hcg_set_coarsening_factor": ([C.c_void_p, C.c_uint32], C.c_int),
     "hcg_grid_batch": ([C.c_void_p, C.c_uint32, C.c_void_p], C.c_int),
+    "hcg_batch_set_shape": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_autotune_batch": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p,
+                            C.POINTER(C.c_uint32)], C.c_int),
     "hcg_grid_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "hcg_server_create": ([C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)], C.c_int),
     "hcg_server_submit": ([C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
@@ -329,6 +339,23 @@ class Context:
                 raise ValueError("batch outputs must be CUDA tensors")
             arr[i] = Job(f.h.value, t.h.value, cube.data_ptr(), w.data_ptr() if w is not None else None, layout)
         self._check(self.L.hcg_grid_batch(self.h, len(jobs), arr))
+
+    def batch_set_shape(self, shape: int, channel_class: int = -1):
+        """Pipeline shape of the batch pass's tensor-core kernel (0-3) for a
+        channel class (-1: every class); shape -1 restores the default."""
+        self._check(self.L.hcg_batch_set_shape(self.h, channel_class, shape))
+
+    def autotune_batch(self, jobs, reps: int = 3) -> list:
+        """hcg_autotune_batch over `jobs` (as for grid_batch): per channel class
+        present, the shape chosen, its ms per shape and spread."""
+        arr = (Job * len(jobs))()
+        for i, (f, t, cube, w, layout) in enumerate(jobs):
+            arr[i] = Job(f.h.value, t.h.value, cube.data_ptr(), w.data_ptr() if w is not None else None, layout)
+        out = (BatchTuning * 8)()
+        n = C.c_uint32()
+        self._check(self.L.hcg_autotune_batch(self.h, len(jobs), arr, reps, 8, out, C.byref(n)))
+        return [{"channel_class": out[i].channel_class, "shape": out[i].shape, "jobs": out[i].jobs,
+                 "ms": [round(x, 4) for x in out[i].ms], "spread": round(out[i].spread, 4)} for i in range(n.value)]
 
     def set_entry_budget(self, nbytes: int):
         self._check(self.L.hcg_set_entry_budget(self.h, nbytes))

@@ -48,16 +48,21 @@ struct JobDesc {
     double *wsum;
     PixPrep *prep;
     // first item of this job in each phase's item space
-    unsigned long long pix_base, grp_base, tile_base, acc_base, c1_base, tc_base;
+    unsigned long long pix_base, grp_base, tile_base, acc_base, c1_base;
+    unsigned long long tc_base;  // in the item space of the job's tensor-core shape
+    uint32_t tc_shape;           // kb_tc pipeline shape (kKbNb)
     TcJob tc;  // tensor-core engine arguments (jobs whose field holds split spectra)
     uint32_t skip;  // routed to the single-job path: no entries, no sums here
 };
 
-enum { Q_TILE = 0, Q_COUNT, Q_GEOM, Q_ACC, Q_C1, Q_TC, Q_N };
+enum { Q_TILE = 0, Q_COUNT, Q_GEOM, Q_ACC, Q_C1, Q_TC, Q_N = Q_TC + kKbShapes };
 
 struct BatchHdr {
     uint32_t njobs;
-    unsigned long long tot_pix, tot_grp, tot_tile, tot_acc, tot_c1, tot_tc;
+    unsigned long long tot_pix, tot_grp, tot_tile, tot_acc, tot_c1;
+    unsigned long long tot_tc[kKbShapes];  // items of each tensor-core shape
+    const uint32_t *tc_list;               // jobs of shape k: tc_list[tc_off[k] .. tc_off[k + 1])
+    uint32_t tc_off[kKbShapes + 1];
     unsigned long long head[Q_N];
     unsigned long long entry_cap;      // entries the pool holds
     unsigned long long entries_needed; // total entries of the batch (set by the scan)
@@ -185,22 +190,42 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
 }
 
 // Tensor-core channel sums: one CTA per SM takes (job, channel block, tile)
-// items from the queue; barrier phases and TMEM persist across items.
-using KbTcCfg = TcCfgN4K32;  // the batch kernel's pipeline shape
+// items from the queue of its pipeline shape SH (the jobs whose channel
+// class the context assigns that shape); barrier phases and TMEM persist
+// across items. One launch per shape, in sequence; a shape without items
+// returns at once.
+template <int SH>
+struct KbShape;
+template <> struct KbShape<0> { using Cfg = TcCfgN4K32; };
+template <> struct KbShape<1> { using Cfg = TcCfgN4S2; };
+template <> struct KbShape<2> { using Cfg = TcCfgN2S3; };
+template <> struct KbShape<3> { using Cfg = TcCfgN1S4; };
+static_assert(kKbShapes == 4, "one KbShape per batch tensor-core shape");
 
+template <int SH>
 __global__ void __launch_bounds__(kTcThreads, 1)
     kb_tc(BatchHdr *H, const JobDesc *__restrict__ jobs, unsigned long long *timeouts,
           unsigned long long *macs) {
+    using KbTcCfg = typename KbShape<SH>::Cfg;
+    static_assert(KbTcCfg::kNb == kKbNb[SH], "shape table and configurations agree");
     __shared__ TcShared S;
-    if (H->pool_overflow) return;  // entries incomplete: this pass is replayed after the pool grows
+    // entries incomplete (this pass is replayed after the pool grows), or no items of this shape
+    if (H->pool_overflow || H->tot_tc[SH] == 0) return;
     tc_setup<KbTcCfg>(S);
     uint32_t gk = 0, itn = 0;
+    const uint32_t *list = H->tc_list + H->tc_off[SH];
+    const int nlist = (int)(H->tc_off[SH + 1] - H->tc_off[SH]);
     for (;;) {
-        if (threadIdx.x == 0) S.item = S.abort ? ~0ULL : atomicAdd(&H->head[Q_TC], 1ULL);
+        if (threadIdx.x == 0) S.item = S.abort ? ~0ULL : atomicAdd(&H->head[Q_TC + SH], 1ULL);
         __syncthreads();
         const unsigned long long it = S.item;
-        if (it >= H->tot_tc) break;
-        const int j = find_job(jobs, H->njobs, it, [](const JobDesc &d) { return d.tc_base; });
+        if (it >= H->tot_tc[SH]) break;
+        int lo = 0, hi = nlist;  // the shape's last job whose base is <= it
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (jobs[list[mid]].tc_base <= it) lo = mid; else hi = mid;
+        }
+        const int j = (int)list[lo];
         if (jobs[j].skip) {
             __syncthreads();  // every thread has read S.item
             continue;
@@ -258,6 +283,7 @@ struct BatchState {
     unsigned long long *d_jovf = nullptr, *h_jovf = nullptr;  // per job: tiles beyond the ring table
     unsigned long long *d_jent = nullptr, *h_jent = nullptr;  // per job: entries
     unsigned long long *d_jusum = nullptr, *h_jusum = nullptr;  // per job: staged slots of its tiles (sum, largest)
+    uint32_t *d_tclist = nullptr, *h_tclist = nullptr;          // tensor-core jobs grouped by shape
     uint32_t map_cap = 0;
     unsigned long long entry_cap = 0;
     cudaMemPool_t pool = nullptr;  // the context's memory pool
@@ -284,7 +310,11 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     const int smem = kStageSlots * kSlice * (int)sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(kb_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    if ((e = tc_set_smem((const void *)kb_tc, KbTcCfg::kSmem)) != cudaSuccess) return e;
+    if ((e = tc_set_smem((const void *)kb_tc<0>, KbShape<0>::Cfg::kSmem)) != cudaSuccess ||
+        (e = tc_set_smem((const void *)kb_tc<1>, KbShape<1>::Cfg::kSmem)) != cudaSuccess ||
+        (e = tc_set_smem((const void *)kb_tc<2>, KbShape<2>::Cfg::kSmem)) != cudaSuccess ||
+        (e = tc_set_smem((const void *)kb_tc<3>, KbShape<3>::Cfg::kSmem)) != cudaSuccess)
+        return e;
     const int n = B.nsm;
     for (int part = 0; part < 2; ++part) {
         cudaGraph_t graph;
@@ -302,8 +332,11 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
         } else {
             kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
             kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs);
-            kb_tc<<<n, kTcThreads, KbTcCfg::kSmem, s>>>(B.d_hdr, B.d_jobs, &ctx->d_stats->timeouts,
-                                                  &ctx->d_stats->tc_macs);
+            unsigned long long *to = &ctx->d_stats->timeouts, *macs = &ctx->d_stats->tc_macs;
+            kb_tc<0><<<n, kTcThreads, KbShape<0>::Cfg::kSmem, s>>>(B.d_hdr, B.d_jobs, to, macs);
+            kb_tc<1><<<n, kTcThreads, KbShape<1>::Cfg::kSmem, s>>>(B.d_hdr, B.d_jobs, to, macs);
+            kb_tc<2><<<n, kTcThreads, KbShape<2>::Cfg::kSmem, s>>>(B.d_hdr, B.d_jobs, to, macs);
+            kb_tc<3><<<n, kTcThreads, KbShape<3>::Cfg::kSmem, s>>>(B.d_hdr, B.d_jobs, to, macs);
             kb_1chan<<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
         }
         cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -332,6 +365,8 @@ cudaError_t batch_release(hcg_context *ctx) {
     if (B->h_jent) cudaFreeHost(B->h_jent);
     if (B->d_jusum) cudaFreeAsync(B->d_jusum, ctx->stream);
     if (B->h_jusum) cudaFreeHost(B->h_jusum);
+    if (B->d_tclist) cudaFreeAsync(B->d_tclist, ctx->stream);
+    if (B->h_tclist) cudaFreeHost(B->h_tclist);
     if (B->h_hdr) cudaFreeHost(B->h_hdr);
     if (B->h_jobs) cudaFreeHost(B->h_jobs);
     delete B;
@@ -368,6 +403,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if (B.h_jent) cudaFreeHost(B.h_jent);
         if (B.d_jusum) cudaFreeAsync(B.d_jusum, s);
         if (B.h_jusum) cudaFreeHost(B.h_jusum);
+        if (B.d_tclist) cudaFreeAsync(B.d_tclist, s);
+        if (B.h_tclist) cudaFreeHost(B.h_tclist);
         B.job_cap = std::max<uint32_t>(njobs, 64);
         if ((e = dalloc(&B.d_jobs, B.job_cap * sizeof(JobDesc), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jobs, B.job_cap * sizeof(JobDesc))) != cudaSuccess) return e;
@@ -377,6 +414,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if ((e = cudaMallocHost(&B.h_jent, B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
         if ((e = dalloc(&B.d_jusum, 2 * B.job_cap * sizeof(unsigned long long), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jusum, 2 * B.job_cap * sizeof(unsigned long long))) != cudaSuccess) return e;
+        if ((e = dalloc(&B.d_tclist, B.job_cap * sizeof(uint32_t), s, ctx->pool)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&B.h_tclist, B.job_cap * sizeof(uint32_t))) != cudaSuccess) return e;
     }
     if (2 * njobs > B.map_cap) {
         if (B.d_maps) cudaFreeAsync(B.d_maps, s);
@@ -387,6 +426,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
     }
     // item spaces and scratch sizes
     unsigned long long pix = 0, grp = 0, tile = 0, acc = 0, c1 = 0, tcn = 0;
+    unsigned long long tcs[kKbShapes] = {};  // tensor-core items per shape
     std::vector<JobDesc> J(njobs);
     for (uint32_t i = 0; i < njobs; ++i) {
         const hcg_field *f = jobs[i].field;
@@ -408,7 +448,8 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         d.nslices = tc ? 0 : (f->cstride + kSlice - 1) / kSlice;
         if (tc) {
             d.T.pad = 8;  // ring runs as boxes of 8 samples
-            if (!tc_prepare_job(f, KbTcCfg::kNb, &B.h_maps[2 * i], d.tc)) {
+            d.tc_shape = (uint32_t)kb_shape_of(ctx, f);
+            if (!tc_prepare_job(f, (int)kKbNb[d.tc_shape], &B.h_maps[2 * i], d.tc)) {
                 why = "cuTensorMapEncodeTiled";
                 return cudaErrorInvalidValue;
             }
@@ -418,13 +459,28 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         d.tile_base = tile;
         d.acc_base = acc;
         d.c1_base = c1;
-        d.tc_base = tcn;
+        d.tc_base = tcs[d.tc_shape];
         pix += P;
         grp += d.g.ngroups;
         tile += ntiles;
         acc += ntiles * d.nslices;
-        if (tc) tcn += ntiles * d.tc.ncb;
+        if (tc) {
+            tcs[d.tc_shape] += ntiles * d.tc.ncb;
+            tcn += ntiles * d.tc.ncb;
+        }
         if (f->nchan == 1) c1 += P;
+    }
+    // tensor-core jobs grouped by shape, in job order within a shape (their
+    // bases rise along the list)
+    uint32_t tc_off[kKbShapes + 1] = {};
+    {
+        uint32_t k = 0;
+        for (int sh = 0; sh < kKbShapes; ++sh) {
+            tc_off[sh] = k;
+            for (uint32_t i = 0; i < njobs; ++i)
+                if (J[i].tc.nb && J[i].tc_shape == (uint32_t)sh) B.h_tclist[k++] = i;
+        }
+        tc_off[kKbShapes] = k;
     }
     void *p_prep, *p_wsum, *p_cap, *p_cnt, *p_off, *p_tiles, *p_ridx, *p_scan;
     const size_t tile_words = 3 + kTileMaxRings + kTileMaxRings + 1;  // r0, nr, U, ulo[], base[]
@@ -529,7 +585,9 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         h.tot_tile = tile;
         h.tot_acc = acc;
         h.tot_c1 = c1;
-        h.tot_tc = tcn;
+        for (int sh = 0; sh < kKbShapes; ++sh) h.tot_tc[sh] = tcs[sh];
+        h.tc_list = B.d_tclist;
+        for (int sh = 0; sh <= kKbShapes; ++sh) h.tc_off[sh] = tc_off[sh];
         h.entry_cap = B.entry_cap;
         h.e_idx = (uint32_t *)p_eidx;
         h.e_w = (float4 *)p_ew;
@@ -545,8 +603,10 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         (e = cudaMemsetAsync(B.d_jovf, 0, njobs * sizeof(unsigned long long), s)) != cudaSuccess ||
         (e = cudaMemsetAsync(B.d_jusum, 0, 2 * njobs * sizeof(unsigned long long), s)) != cudaSuccess)
         return e;
-    if (tcn && (e = cudaMemcpyAsync(B.d_maps, B.h_maps, 2 * njobs * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
-                                    s)) != cudaSuccess)
+    if (tcn && ((e = cudaMemcpyAsync(B.d_maps, B.h_maps, 2 * njobs * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                                     s)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(B.d_tclist, B.h_tclist, tc_off[kKbShapes] * sizeof(uint32_t),
+                                     cudaMemcpyHostToDevice, s)) != cudaSuccess))
         return e;
     if (!B.exec_geom && (e = capture(ctx, B)) != cudaSuccess) return e;
     // geometry graph, then the entry totals of every job

@@ -9,6 +9,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <chrono>
 #include <new>
 #include <string>
 #include <vector>
@@ -132,6 +133,22 @@ static bool writable_on(const void *p, int device) {
 
 uint64_t hcg::job_pixels(const hcg_job &job) {
     return job.target ? (uint64_t)job.target->nx * job.target->ny : 0;
+}
+
+int hcg::device_sms(int device) {
+    int n = 0;
+    return cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) == cudaSuccess ? n : 0;
+}
+
+// A job whose channel sums fill the GPU by themselves: at least 2^20 target
+// pixels, or a multi-channel job with at least one (tile, 256-channel block)
+// item per SM.
+bool hcg::job_fills_gpu(const hcg_job &job, int nsm) {
+    if (!job.target || !job.field) return false;
+    if (job_pixels(job) >= kBatchMaxPixels) return true;
+    if (job.field->nchan <= 1) return false;
+    const uint64_t tiles = (uint64_t)((job.target->nx + 15) / 16) * ((job.target->ny + 7) / 8);  // 16 x 8-pixel tiles
+    return tiles * ((job.field->nchan + 255) / 256) >= (uint64_t)(nsm > 0 ? nsm : 148);
 }
 
 // hcg_grid after its argument checks; the caller holds the context lock.
@@ -762,6 +779,72 @@ hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_targ
     return HCG_OK;
 }
 
+hcg_status hcg_batch_set_shape(hcg_context *ctx, int channel_class, int shape) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    if (channel_class < -1 || channel_class >= kTcClasses || shape < -1 || shape >= kKbShapes)
+        return fail(ctx, HCG_EINVAL, "channel class must be -1..7 and shape -1..3");
+    for (int c = 0; c < kTcClasses; ++c)
+        if (channel_class < 0 || c == channel_class) ctx->kb_shape[c] = shape;
+    return HCG_OK;
+}
+
+hcg_status hcg_autotune_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, int reps, uint32_t max_out,
+                              hcg_batch_tuning *out, uint32_t *nout) {
+    if (!ctx || !jobs || njobs == 0 || reps < 1 || (max_out && !out)) return HCG_EINVAL;
+    // the jobs the batch pass takes on the tensor cores, by channel class
+    std::vector<std::vector<hcg_job>> by(kTcClasses);
+    {
+        Guard g(ctx);
+        for (uint32_t i = 0; i < njobs; ++i) {
+            const hcg_job &j = jobs[i];
+            if (!j.field || !j.target || !j.cube) return fail(ctx, HCG_EINVAL, "job " + std::to_string(i) + " incomplete");
+            if (auto_engine(j.field) == HCG_ENGINE_FP32 || j.field->kernel_type != HCG_GAUSS1D ||
+                job_pixels(j) >= kBatchMaxPixels)
+                continue;
+            by[tc_class_of(j.field->xcpad)].push_back(j);
+        }
+    }
+    uint32_t n = 0;
+    for (int cls = 0; cls < kTcClasses; ++cls) {
+        if (by[cls].empty()) continue;
+        hcg_batch_tuning t = {};
+        t.channel_class = cls;
+        t.jobs = (uint32_t)by[cls].size();
+        t.shape = kKbDefaultShape;
+        for (int sh = 0; sh < kKbShapes; ++sh) {
+            {
+                Guard g(ctx);
+                ctx->kb_shape[cls] = sh;
+            }
+            float best = 3.4e38f, worst = 0.f;
+            for (int r = 0; r < reps + 1; ++r) {  // run 0 warms up
+                const auto t0 = std::chrono::steady_clock::now();
+                hcg_status st = hcg_grid_batch(ctx, t.jobs, by[cls].data());
+                if (st != HCG_OK) return st;
+                const float ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                if (r > 0) {
+                    best = ms < best ? ms : best;
+                    worst = ms > worst ? ms : worst;
+                }
+            }
+            t.ms[sh] = best;
+            if (sh == 0 || best < t.ms[t.shape]) {
+                t.shape = sh;
+                t.spread = best > 0.f ? (worst - best) / best : 0.f;
+            }
+        }
+        {
+            Guard g(ctx);
+            ctx->kb_shape[cls] = t.shape;
+        }
+        if (n < max_out) out[n] = t;
+        ++n;
+    }
+    if (nout) *nout = n < max_out ? n : max_out;
+    return HCG_OK;
+}
+
 hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs) {
     if (!ctx || (njobs && !jobs)) return HCG_EINVAL;
     Guard g(ctx);
@@ -817,7 +900,9 @@ hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs)
             float ms = 0.f;
             cudaStreamSynchronize(ctx->stream);
             cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-            fprintf(stderr, "[hcg batch] job %u on its own: %.3f ms\n", i, ms);
+            fprintf(stderr, "[hcg batch] job %u on its own (%llu samples, %u channels, %ux%u pixels): %.3f ms\n", i,
+                    (unsigned long long)jobs[i].field->n, jobs[i].field->nchan, jobs[i].target->nx, jobs[i].target->ny,
+                    ms);
         }
     }
     CK(ctx, cudaStreamSynchronize(ctx->stream), "grid batch");

@@ -84,7 +84,12 @@ __global__ void __launch_bounds__(256) k_tile_rings(GridArgs a, GroupArgs g, Til
     tile_rings_item(a, g, T, T.t0 + blockIdx.x);
 }
 
-__global__ void __launch_bounds__(kTileThreads) k_tile_accum(GroupArgs g, TileArgs T,
+// Rows per staging buffer of k_tile_accum: two buffers of 192 rows x 64
+// channels (96 KB) let two CTAs share an SM, so one CTA's chunk barrier is
+// covered by the other's work.
+constexpr int kAccumChunk = 192;
+
+__global__ void __launch_bounds__(kTileThreads, 2) k_tile_accum(GroupArgs g, TileArgs T,
                                                             const unsigned long long *__restrict__ off,
                                                             const uint32_t *__restrict__ cnt,
                                                             const uint32_t *__restrict__ e_slot,
@@ -95,8 +100,8 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_accum(GroupArgs g, TileAr
                                                             uint32_t ostride, float *__restrict__ wout) {
     // slices of a tile are adjacent blocks: they run together and share the
     // tile's entries through L2
-    tile_accum_item(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan, cstride, out, ostride, wout, T.t0 + blockIdx.y,
-                    blockIdx.x * kSlice);
+    tile_accum_item<kAccumChunk>(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan, cstride, out, ostride, wout,
+                                 T.t0 + blockIdx.y, blockIdx.x * kSlice);
 }
 
 // Exclusive scan of n uint32 counts into uint64 offsets (out[n] = total),
@@ -298,7 +303,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             return e;
         }
         float *dst = d_cube;
-        const int smem = kStageSlots * kSlice * (int)sizeof(float);
+        const int smem = 2 * kAccumChunk * kSlice * (int)sizeof(float);
         static bool attr_set = false;
         if (tiled && !attr_set) {
             if ((e = cudaFuncSetAttribute(k_tile_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=

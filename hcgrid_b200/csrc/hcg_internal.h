@@ -119,6 +119,7 @@ struct hcg_context {
     int tc_pf[8] = {-1, -1, -1, -1, -1, -1, -1, -1};      // prefetch distance (chunks) per class (-1: default)
     int tc_strip[8] = {-1, -1, -1, -1, -1, -1, -1, -1};   // persistent tile walk per class (-1: default)
     int tc_weights = 0;  // tensor-core weight operands: 0 automatic, 1 from entries, 2 evaluated in the kernel
+    int kb_shape[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // batch tensor-core shape per channel class (-1: default)
     uint32_t factor = 1;  // coarsening factor (hcg_set_coarsening_factor)
     void *batch = nullptr;                          // batch engine state (hcg_batch.cu)
 };
@@ -170,6 +171,14 @@ constexpr int kTcConfigCount = 6;  // tensor-core pipeline shapes (hcg_tc_set_co
 constexpr int kTcDefaultPrefetch = 0;  // chunks the producer prefetches into L2 ahead of its loads (0: none)
 constexpr int kTcDefaultStrip = 8;     // tile columns per strip of the persistent tile walk
 constexpr uint64_t kBatchMaxPixels = 1ull << 20;  // larger targets skip hcg_grid_batch's batch pass
+// Pipeline shapes of the batch engine's tensor-core kernel (kb_tc), chosen
+// per channel class (hcg_batch_set_shape, hcg_autotune_batch): 64-channel
+// blocks per item (the MMA's N / 64), K slots per chunk and stages.
+//   0: 256 channels x 32 slots x 4 stages   1: 256 x 64 x 2
+//   2: 128 x 64 x 3                         3: 64 x 64 x 4
+constexpr int kKbShapes = 4;
+constexpr uint32_t kKbNb[kKbShapes] = {4, 4, 2, 1};
+constexpr int kKbDefaultShape = 0;
 // channel class of a split field: 64-channel blocks 1, 2, 3-4, 5-8, ... -> 0, 1, 2, 3, ...
 inline int tc_class_of(uint32_t cpad) {
     const uint32_t b = cpad / 64;
@@ -187,6 +196,11 @@ inline bool tc_weights_fit(const hcg_field *f) { return f->wbound <= 0x1p100; }
 // with a narrow taper width) is refused, which leaves 2^28 for the sample
 // count times |x| below FP32's range; single-channel fields sum in FP64.
 inline bool fp32_weights_fit(const hcg_field *f) { return f->nchan <= 1 || !(f->wbound > 0x1p100); }
+// the batch engine's tensor-core shape for a split field's channel class
+inline int kb_shape_of(const hcg_context *ctx, const hcg_field *f) {
+    const int c = ctx->kb_shape[tc_class_of(f->xcpad)];
+    return c >= 0 && c < kKbShapes ? c : kKbDefaultShape;
+}
 inline int auto_engine(const hcg_field *f) {
     return (f->xfmt && f->nchan > 1 && f->xnonfinite == 0 && tc_weights_fit(f)) ? f->xfmt : HCG_ENGINE_FP32;
 }
@@ -225,7 +239,9 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
                        std::string &why);
 cudaError_t batch_release(hcg_context *ctx);
 bool batch_trace();
-uint64_t job_pixels(const hcg_job &job);  // the target's pixel count (the server's job classes)
+uint64_t job_pixels(const hcg_job &job);         // the target's pixel count
+bool job_fills_gpu(const hcg_job &job, int nsm);  // the server's large jobs (run alone)
+int device_sms(int device);                       // streaming multiprocessors of a device (0: unknown)
 hcg_status grid_job(hcg_context *ctx, const hcg_job &job);  // one server job, device buffers, automatic engine
 struct SinWcs;
 int parse_sin_header(const char *header, size_t len, uint32_t &nx, uint32_t &ny, SinWcs &w, std::string &why);

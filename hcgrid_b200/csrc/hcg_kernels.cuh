@@ -998,8 +998,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // chunks of kChunk rows, double-buffered: while the entries of one chunk are
 // summed, the next chunk streams in through cp.async. 16 threads per 2x2
 // group each own 4 channels of the slice, so a staged value feeds 4 pixels.
-// Block-collective (every thread of a kTileThreads block; kStageSlots *
-// kSlice floats of dynamic shared memory).
+// Block-collective (every thread of a kTileThreads block; 2 * CH * kSlice
+// floats of dynamic shared memory).
+template <int CH = kChunk>
 __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileArgs &T,
                                                 const unsigned long long *__restrict__ off,
                                                 const uint32_t *__restrict__ cnt,
@@ -1008,7 +1009,7 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
                                                 const float *__restrict__ spec, uint32_t nchan, uint32_t cstride,
                                                 float *__restrict__ out, uint32_t ostride,
                                                 float *__restrict__ wout, uint64_t tile, uint32_t c0) {
-    extern __shared__ float4 s_spec[];  // [2][kChunk][kSlice / 4]
+    extern __shared__ float4 s_spec[];  // [2][CH][kSlice / 4]
     __shared__ uint32_t s_ulo[kTileMaxRings], s_base[kTileMaxRings + 1];
     __syncthreads();  // shared state of a previous item is no longer read
     const int tid = threadIdx.x, q = tid & (kSlice / 4 - 1), gl = tid / (kSlice / 4);
@@ -1029,10 +1030,10 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
-    // stage rows [cs, min(U, cs + kChunk)) into buffer b: 16 threads per row
+    // stage rows [cs, min(U, cs + CH)) into buffer b: 16 threads per row
     auto stage = [&](uint32_t cs, int b) {
-        const uint32_t ce = min(U, cs + kChunk);
-        float4 *dst = s_spec + (size_t)b * kChunk * (kSlice / 4);
+        const uint32_t ce = min(U, cs + CH);
+        float4 *dst = s_spec + (size_t)b * CH * (kSlice / 4);
         for (uint32_t i = tid; i < (ce - cs) * (kSlice / 4); i += kTileThreads) {
             uint32_t row = i / (kSlice / 4), part = i % (kSlice / 4);
             uint32_t slot = cs + row;
@@ -1049,47 +1050,31 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
         }
         cp_async_commit();
     };
-    const uint32_t nchunks = (U + kChunk - 1) / kChunk;
+    const uint32_t nchunks = (U + CH - 1) / CH;
     if (nchunks > 0) stage(0, 0);
     for (uint32_t k = 0; k < nchunks; ++k) {
-        const uint32_t cs = k * kChunk, ce = min(U, cs + kChunk);
+        const uint32_t cs = k * CH, ce = min(U, cs + CH);
         if (k + 1 < nchunks) {
-            stage(cs + kChunk, (k + 1) & 1);
+            stage(cs + CH, (k + 1) & 1);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const float4 *buf = s_spec + (size_t)(k & 1) * kChunk * (kSlice / 4);
-        // entries four at a time, the next four loaded while these are summed
-        uint32_t sl[4], nsl[4];
-        float4 w[4], nw[4];
-        bool have = e + 4 <= e_end;
-        if (have) {
+        const float4 *buf = s_spec + (size_t)(k & 1) * CH * (kSlice / 4);
+        // entries kSet at a time from two register sets in turn: the next set
+        // is loaded while one is summed, and no set is copied
+        constexpr int kSet = 3;
+        auto load = [&](uint32_t *sl, float4 *w, uint64_t at) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                nsl[u] = __ldg(e_slot + e + u);
-                nw[u] = __ldg(e_w + e + u);
+            for (int u = 0; u < kSet; ++u) {
+                sl[u] = __ldg(e_slot + at + u);
+                w[u] = __ldg(e_w + at + u);
             }
-        }
-        while (have) {
+        };
+        auto sum = [&](const uint32_t *sl, const float4 *w) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                sl[u] = nsl[u];
-                w[u] = nw[u];
-            }
-            if (sl[3] >= ce) break;
-            e += 4;
-            have = e + 4 <= e_end;
-            if (have) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    nsl[u] = __ldg(e_slot + e + u);
-                    nw[u] = __ldg(e_w + e + u);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kSet; ++u) {
                 const float4 sv = buf[(sl[u] - cs) * (kSlice / 4) + q];
                 const float wv[4] = {w[u].x, w[u].y, w[u].z, w[u].w};
 #pragma unroll
@@ -1099,6 +1084,25 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
                     acc[kk].z = fmaf(wv[kk], sv.z, acc[kk].z);
                     acc[kk].w = fmaf(wv[kk], sv.w, acc[kk].w);
                 }
+            }
+        };
+        if (e + kSet <= e_end) {
+            uint32_t sa[kSet], sb[kSet];
+            float4 wa[kSet], wb[kSet];
+            load(sa, wa, e);
+            for (;;) {  // sa holds entries [e, e + kSet)
+                const bool nb = e + 2 * kSet <= e_end;
+                if (nb) load(sb, wb, e + kSet);
+                if (sa[kSet - 1] >= ce) break;
+                sum(sa, wa);
+                e += kSet;
+                if (!nb) break;
+                const bool na = e + 2 * kSet <= e_end;  // sb holds entries [e, e + kSet)
+                if (na) load(sa, wa, e + kSet);
+                if (sb[kSet - 1] >= ce) break;
+                sum(sb, wb);
+                e += kSet;
+                if (!na) break;
             }
         }
         for (; e < e_end; ++e) {

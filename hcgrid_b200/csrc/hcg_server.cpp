@@ -2,21 +2,22 @@
 //
 // Clients submit jobs (a resident field, a target and device output
 // buffers) as they arrive. A dispatcher thread hands pending jobs to one of
-// `lanes` worker lanes while their HBM footprint fits the budget: a job whose
-// target has at least kSingleJobPixels pixels alone, with the GPU to itself
-// (its kernels fill the GPU by themselves; it runs through hcg_grid), else a
-// batch of smaller jobs (at most `max_batch`, through hcg_grid_batch's
-// persistent kernels). The oldest pending job decides what runs next. If it
-// is small, every pending small job joins its batch in arrival order, large
-// ones skipped, so large jobs between them do not split the batch. If it is
-// large, it waits for the GPU to be idle; meanwhile the small jobs queued
-// behind it may pass it on a free lane, at most kMaxPasses batches, so a
-// large job is not starved. Each lane owns its own context (stream + captured batch graphs)
-// on the same device, so a batch that arrives while another batch is on the
-// GPU is launched right away and the two overlap on the device. When a lane finishes, its footprint is
-// released and the dispatcher admits more jobs. Every job records submit,
-// start and finish times (host steady clock), from which the latency
-// percentiles are taken.
+// `lanes` worker lanes while their HBM footprint fits the budget. A job whose
+// channel sums fill the GPU by themselves (2^20 target pixels or more, or at
+// least one channel-sum item per SM) runs alone, with the GPU to itself,
+// through hcg_grid; smaller jobs run in batches (at most `max_batch`, through
+// hcg_grid_batch's persistent kernels). The oldest pending job decides what
+// runs next. If it is small, every pending small job joins its batch in
+// arrival order, large ones skipped, so large jobs between them do not split
+// the batch. If it is large, it waits for the GPU to be idle; meanwhile the
+// small jobs queued behind it may pass it on a free lane, at most kMaxPasses
+// batches, so a large job is not starved. Each lane owns its own context
+// (stream + captured batch graphs) on the same device, so a batch that
+// arrives while another batch is on the GPU is launched right away and the
+// two overlap on the device. When a lane finishes, its footprint is released
+// and the dispatcher admits more jobs. Every job records submit, start and
+// finish times (host steady clock), from which the latency percentiles are
+// taken.
 #include <stdint.h>
 #include <string.h>
 
@@ -33,14 +34,14 @@
 #include "hcgrid_c.h"
 
 namespace hcg {  // hcg_capi.cu
-uint64_t job_pixels(const hcg_job &job);                    // the target's pixel count
+bool job_fills_gpu(const hcg_job &job, int nsm);            // the job's channel sums fill the GPU alone
 hcg_status grid_job(hcg_context *ctx, const hcg_job &job);  // hcg_grid of one job on a lane's context
+int device_sms(int device);                                 // streaming multiprocessors of a device
 }
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
-constexpr uint64_t kSingleJobPixels = 1ull << 20;
 constexpr uint32_t kMaxPasses = 2;  // batches that may pass a waiting large job
 
 struct Pending {
@@ -66,6 +67,7 @@ struct hcg_server {
     std::vector<hcg_context *> lanes;
     uint64_t budget = 0, in_use = 0;
     uint32_t max_batch = 64;
+    int nsm = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Pending> queue;
@@ -202,6 +204,7 @@ hcg_status hcg_server_create(hcg_context *ctx, int device, uint32_t lanes, uint6
     s->primary = ctx;
     s->budget = hbm_budget_bytes;
     s->max_batch = max_batch;
+    s->nsm = hcg::device_sms(device);
     s->lanes.push_back(ctx);
     for (uint32_t i = 1; i < lanes; ++i) {
         hcg_context *c = nullptr;
@@ -226,7 +229,7 @@ hcg_status hcg_server_submit(hcg_server *s, const hcg_job *job, uint64_t footpri
     if (!s || !job || !ticket) return HCG_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return HCG_ESTATE;
-    Pending p{s->next_ticket++, *job, footprint_bytes, s->now(), hcg::job_pixels(*job) >= kSingleJobPixels};
+    Pending p{s->next_ticket++, *job, footprint_bytes, s->now(), hcg::job_fills_gpu(*job, s->nsm)};
     s->done[p.ticket].t_submit = p.t_submit;
     *ticket = p.ticket;
     s->queue.push_back(p);

@@ -272,18 +272,14 @@ struct TcStage {
     __device__ __forceinline__ uint8_t *B(uint32_t s) const { return smem + s * Cfg::kStageBytes + 2 * Cfg::kAHalf; }
 };
 
-// Producer (whole warps), one item: per chunk one 4-D TMA box per run of 8
-// slots. With `npw` producer warps, warp `pw` issues boxes pw, pw + npw, ...
-// (one lane each, in parallel: a box-load instruction holds its warp for
-// hundreds of cycles, and separate warps issue concurrently); warp 0 also
-// arms the stage's barrier with the chunk's bytes and, with J.pf > 0, its
-// lanes after the loads prefetch the boxes of chunk k + pf into L2. `ulo` /
-// `base` hold the item's ring table (nrt rings; shared or global memory);
-// `gk` is the CTA's chunk count before the item.
+// Producer (the whole warp 0), one item: per chunk one 4-D TMA box per run of
+// 8 slots, issued by lanes 0..KC/8-1 in parallel; with J.pf > 0 lanes
+// KC/8..2KC/8-1 also prefetch the boxes of chunk k + pf into L2. S.ulo /
+// S.base hold the item's ring table (nrt rings); `gk` is the CTA's chunk count
+// before the item.
 template <class Cfg, class SH>
 __device__ __forceinline__ void tc_produce(SH &S, const TcJob &J, uint32_t cblk, uint32_t U, uint32_t nchunks,
-                                           uint32_t gk, int nrt, unsigned long long *timeouts, const uint32_t *ulo,
-                                           const uint32_t *base, int pw = 0, int npw = 1) {
+                                           uint32_t gk, int nrt, unsigned long long *timeouts) {
     using namespace sm100;
     constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
     constexpr int NB8 = (int)(KC / 8);
@@ -291,20 +287,19 @@ __device__ __forceinline__ void tc_produce(SH &S, const TcJob &J, uint32_t cblk,
     const int lane = threadIdx.x & 31;
     const uint32_t bytes = NB8 * 2u * J.nb * 1024u;
     const uint32_t pf = J.pf > ST ? J.pf : ST;  // chunks ahead of the loads that go to L2 first
-    const int nbw = (NB8 - pw + npw - 1) / npw;  // boxes of this warp per chunk
-    const bool pref = J.pf && pw == 0;           // pf 0: no prefetches
+    const int nlanes = J.pf ? 2 * NB8 : NB8;     // pf 0: no prefetches
     // TMA row of slot0: the ring run j with base[j] <= slot0 < base[j + 1]
     auto row_of = [&](uint32_t slot0) -> int {
         if (slot0 >= U) return (int)J.nrows;  // past the last sample: zero fill
         int lo = 0, hi = nrt;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (base[mid] <= slot0) lo = mid; else hi = mid;
+            if (S.base[mid] <= slot0) lo = mid; else hi = mid;
         }
-        return (int)(ulo[lo] + (slot0 - base[lo]));
+        return (int)(S.ulo[lo] + (slot0 - S.base[lo]));
     };
     // the item's chunks [ST, pf) are prefetched at its start; chunk k + pf with chunk k
-    for (uint32_t i = lane; pref && i < (pf - ST) * (uint32_t)NB8; i += 32) {
+    for (uint32_t i = lane; J.pf && i < (pf - ST) * (uint32_t)NB8; i += 32) {
         const uint32_t c = ST + i / NB8;
         if (c < nchunks) tma_prefetch_4d(J.map, 0, row_of(c * KC + 8 * (i % NB8)), (int)(cblk * J.nb), 0);
     }
@@ -317,18 +312,19 @@ __device__ __forceinline__ void tc_produce(SH &S, const TcJob &J, uint32_t cblk,
             } else if (g >= ST && !mbar_wait(&S.empty[s], ((g / ST) - 1) & 1, kTcWaitNs)) {
                 tc_give_up(S, timeouts);
                 go = 0;
-            } else if (pw == 0) {
+            } else {
                 mbar_arrive_expect_tx(&S.full_b[s], bytes);
             }
         }
         if (!__shfl_sync(0xffffffffu, go, 0)) break;
-        if (lane < nbw) {
-            const int b = pw + npw * lane;
-            tma_load_4d(st.B(s) + b * Cfg::kBGroup, J.map, &S.full_b[s], 0, row_of(k * KC + 8 * b),
-                        (int)(cblk * J.nb), 0);
-        } else if (pref && lane < nbw + NB8 && k + pf < nchunks) {
-            const int b = lane - nbw;
-            tma_prefetch_4d(J.map, 0, row_of((k + pf) * KC + 8 * b), (int)(cblk * J.nb), 0);
+        const int b = lane % NB8;
+        const uint32_t kk = lane < NB8 ? k : k + pf;
+        if (lane < nlanes && kk < nchunks) {
+            const int row = row_of(kk * KC + 8 * b);
+            if (lane < NB8)
+                tma_load_4d(st.B(s) + b * Cfg::kBGroup, J.map, &S.full_b[s], 0, row, (int)(cblk * J.nb), 0);
+            else
+                tma_prefetch_4d(J.map, 0, row, (int)(cblk * J.nb), 0);
         }
     }
 }
@@ -560,7 +556,7 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
     const uint32_t nchunks = (U + Cfg::kK - 1) / Cfg::kK;
     const uint32_t taddr = S.tmem;
     if (warp == 0) {
-        tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, T.nr[tile], timeouts, S.ulo, S.base);
+        tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, T.nr[tile], timeouts);
     } else if (warp == 1) {
         if (lane == 0) {
             tc_mma<Cfg>(S, J, nchunks, gk, taddr, timeouts, macs);
@@ -661,17 +657,14 @@ __device__ __forceinline__ void tc_item(TcShared &S, const TcJob &J, uint64_t ti
 
 // ---------------------------------------------------------------- persistent
 // One CTA per SM over a static sequence of items (item it = blockIdx.x +
-// i * gridDim.x; channel blocks outer, tiles inner). Each role walks the
-// sequence on its own, coupled to the others only through mbarriers: the
-// producer runs ahead into the next item while the MMAs of the current one
-// run, and four epilogue warps (6-9) drain item i's accumulator while the MMAs
-// of item i+1 fill the other one (two TMEM accumulators of 256 columns).
-// Warps 10.. are more producer warps: each issues its share of every chunk's
-// boxes, from its own copy of the item's ring table (the table in global
-// memory when the item has more than kTcPRings rings).
-constexpr int kTcProducers = 2;
-constexpr int kTcPRings = 128;
-constexpr int kTcPersistThreads = 320 + 32 * (kTcProducers - 1);
+// i * gridDim.x; a tile's channel blocks are consecutive items, so they run on
+// neighbouring SMs together and read the tile's entries from HBM once). Each
+// role walks the sequence on its own, coupled to the others only through
+// mbarriers: the producer runs ahead into the next item while the MMAs of the
+// current one run, and four epilogue warps (6-9) drain item i's accumulator
+// while the MMAs of item i+1 fill the other one (two TMEM accumulators of 256
+// columns).
+constexpr int kTcPersistThreads = 320;
 
 struct TcPShared {
     uint64_t full_a[kTcMaxStages], full_b[kTcMaxStages], empty[kTcMaxStages];
@@ -679,8 +672,6 @@ struct TcPShared {
     uint32_t tmem;
     volatile int abort;
     uint32_t ulo[kTileMaxRings], base[kTileMaxRings + 1];  // the producer's current item
-    uint32_t pulo[kTcProducers - 1][kTcPRings];            // the other producer warps' items
-    uint32_t pbase[kTcProducers - 1][kTcPRings + 1];
     float inv_scale[2][kTcMaxN];                           // the epilogue's items (by parity)
     float4 ring_w[kTcRing * kTcBuilders];
     uint32_t ring_slot[kTcRing * kTcBuilders];
@@ -830,26 +821,13 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
             for (int j = lane; j < nrt; j += 32) S.ulo[j] = J.T.ulo[tile * kTileMaxRings + j];
             for (int j = lane; j <= nrt; j += 32) S.base[j] = J.T.base[tile * (kTileMaxRings + 1) + j];
             __syncwarp();
-            tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts, S.ulo, S.base, 0, kTcProducers);
+            tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
         } else if (warp == 1) {
             if (lane == 0) tc_mma_seg<Cfg>(S, J, nchunks, gk, gs, timeouts, macs);
         } else if (warp < 6) {
             tc_build<Cfg>(S, J, tile, nchunks, gk, tid - 64, timeouts);
-        } else if (warp < 10) {
-            tc_epilogue_direct(S, J, tile, cblk, nchunks, il, gse, tid - 192, timeouts);
         } else {
-            const int pw = warp - 9;
-            const int nrt = J.T.nr[tile];
-            const uint32_t *ulo = J.T.ulo + tile * kTileMaxRings, *base = J.T.base + tile * (kTileMaxRings + 1);
-            if (nrt <= kTcPRings) {
-                __syncwarp();
-                for (int j = lane; j < nrt; j += 32) S.pulo[pw - 1][j] = ulo[j];
-                for (int j = lane; j <= nrt; j += 32) S.pbase[pw - 1][j] = base[j];
-                __syncwarp();
-                ulo = S.pulo[pw - 1];
-                base = S.pbase[pw - 1];
-            }
-            tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts, ulo, base, pw, kTcProducers);
+            tc_epilogue_direct(S, J, tile, cblk, nchunks, il, gse, tid - 192, timeouts);
         }
         gk += nchunks;
     }
@@ -1138,7 +1116,7 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
             for (int j = lane; j < nrt; j += 32) S.ulo[j] = J.T.ulo[tile * kTileMaxRings + j];
             for (int j = lane; j <= nrt; j += 32) S.base[j] = J.T.base[tile * (kTileMaxRings + 1) + j];
             __syncwarp();
-            tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts, S.ulo, S.base);
+            tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
         } else if (warp == 1) {
             if (lane == 0) tc_mma_seg<Cfg>(S, J, nchunks, gk, gs, timeouts, macs);
         } else if (tid < 64 + kTcDBuilders) {

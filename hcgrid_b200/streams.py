@@ -27,6 +27,18 @@ def request_work(r: dict) -> int:
     return r["shape"]["n"] * r["shape"]["nchan"]
 
 
+def fills_gpu(shape: dict, nsm: int = 148) -> bool:
+    """The server's large jobs (run alone, as one hcg_grid each): 2^20 target
+    pixels or more, or a multi-channel job with at least one channel-sum item
+    (16 x 8-pixel tile, 256-channel block) per SM."""
+    g = shape["grid"]
+    if g * g >= 1 << 20:
+        return True
+    if shape["nchan"] <= 1:
+        return False
+    return ((g + 15) // 16) * ((g + 7) // 8) * ((shape["nchan"] + 255) // 256) >= nsm
+
+
 def footprint(shape: dict) -> int:
     """Device bytes of one staged request: FP32 spectra while they are
     attached, the 16-bit hi/lo split, cube, weight map and the per-pixel

@@ -270,6 +270,35 @@ typedef struct {
  * job. */
 hcg_status hcg_grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs);
 
+/* Pipeline shape of the batch pass's tensor-core kernel, per channel class
+ * (the tensor-core classes of hcg_tc_set_pipeline; -1: every class; shape -1
+ * restores the default 0). Every shape takes 16 x 8-pixel tiles (128 pixels
+ * per item, the MMA's M); they differ in channels per item (the MMA's N),
+ * sample slots per pipeline chunk and pipeline depth:
+ *   0: 256 channels x 32 slots x 4 stages   1: 256 x 64 x 2
+ *   2: 128 x 64 x 3                         3: 64 x 64 x 4
+ * The cubes do not depend on the shape. No reference counterpart (HCGrid
+ * grids one job per call). */
+#define HCG_BATCH_SHAPES 4
+hcg_status hcg_batch_set_shape(hcg_context *ctx, int channel_class, int shape);
+
+/* Autotuner of the batch pass: the jobs the batch pass would take on the
+ * tensor cores are grouped by channel class; for each class present, every
+ * shape runs the class's jobs as one hcg_grid_batch (one warm-up, then
+ * `reps` timed runs, host clock around the call), the fastest best-of-reps
+ * is kept for the class (hcg_batch_set_shape) and reported in out[0..*nout)
+ * (at most max_out entries); spread = (slowest - fastest) / fastest of the
+ * chosen shape's runs. The jobs' cubes are written along the way. */
+typedef struct {
+    int channel_class;
+    int shape;
+    uint32_t jobs;
+    float ms[HCG_BATCH_SHAPES];
+    float spread;
+} hcg_batch_tuning;
+hcg_status hcg_autotune_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, int reps, uint32_t max_out,
+                              hcg_batch_tuning *out, uint32_t *nout);
+
 /* Serving loop with continuous batching. `lanes` contexts on `device` (the
  * first is ctx) each replay their own batch graph on their own stream, so a
  * batch admitted while another runs overlaps with it on the GPU. Jobs are

@@ -141,6 +141,46 @@ def test_tensor_core_batch_equals_single_calls(ctx, tc_jobs, jobs):
             assert np.abs(cube[~nan] - c32[~nan]).max() <= 5e-5 * scale
 
 
+@pytest.mark.parametrize("shape", range(api.BATCH_SHAPES))
+def test_tensor_core_batch_shapes_equal_single_calls(ctx, tc_jobs, shape):
+    """Every pipeline shape of the batch pass's tensor-core kernel (channels
+    per item, slots per chunk, stages) gives the single call's cube bit for
+    bit."""
+    ctx.batch_set_shape(shape)
+    try:
+        got = run_batch(ctx, tc_jobs, [api.SAMPLE_MAJOR] * len(tc_jobs))
+    finally:
+        ctx.batch_set_shape(-1)
+    for (job, f, t), (cube, w) in zip(tc_jobs, got):
+        ref_cube, ref_w = single(ctx, job, f, t, api.SAMPLE_MAJOR)
+        np.testing.assert_array_equal(cube, ref_cube)
+        np.testing.assert_array_equal(w, ref_w)
+
+
+def test_batch_autotuner_picks_a_shape_per_channel_class(ctx, tc_jobs):
+    """hcg_autotune_batch times every shape per channel class of the batch's
+    tensor-core jobs (64 channels: class 0, 96: class 1, 256: class 2), keeps
+    the fastest, and the tuned batch still equals the single calls."""
+    spec = []
+    for job, f, t in tc_jobs:
+        P = t.nx * t.ny
+        spec.append((f, t, torch.empty((P * job.nchan,), device="cuda"), torch.empty((P,), device="cuda"),
+                     api.SAMPLE_MAJOR))
+    try:
+        res = ctx.autotune_batch(spec, reps=2)
+        assert sorted(r["channel_class"] for r in res) == [0, 1, 2]
+        for r in res:
+            assert r["jobs"] == 1 and 0 <= r["shape"] < api.BATCH_SHAPES
+            assert all(m > 0 for m in r["ms"]) and r["ms"][r["shape"]] == min(r["ms"]) and r["spread"] >= 0
+        got = run_batch(ctx, tc_jobs, [api.SAMPLE_MAJOR] * len(tc_jobs))
+    finally:
+        ctx.batch_set_shape(-1)
+    for (job, f, t), (cube, w) in zip(tc_jobs, got):
+        ref_cube, ref_w = single(ctx, job, f, t, api.SAMPLE_MAJOR)
+        np.testing.assert_array_equal(cube, ref_cube)
+        np.testing.assert_array_equal(w, ref_w)
+
+
 def test_tensor_core_job_alone_equals_job_in_mix(ctx, tc_jobs):
     mix = run_batch(ctx, tc_jobs, [api.SAMPLE_MAJOR] * len(tc_jobs))
     for i in (1, 2, 3):

@@ -28,3 +28,16 @@ def test_config5_stream_is_uncapped():
     assert len(reqs) == 2000
     assert max(r["shape"]["n"] * r["shape"]["nchan"] for r in reqs) > 1 << 31
     assert max(r["shape"]["grid"] for r in reqs) == 2048
+
+
+def test_fills_gpu_matches_the_server_rule():
+    """Large jobs: 2^20 pixels, or one 16x8-pixel x 256-channel item per SM."""
+    sh = lambda g, c: {"grid": g, "nchan": c}
+    assert streams.fills_gpu(sh(1024, 1)) and streams.fills_gpu(sh(2048, 64))
+    assert not streams.fills_gpu(sh(512, 1))           # single channel below 2^20 pixels
+    assert streams.fills_gpu(sh(256, 64))              # 512 tiles
+    assert not streams.fills_gpu(sh(128, 256))         # 128 items
+    assert streams.fills_gpu(sh(128, 257))             # 256 items
+    assert not streams.fills_gpu(sh(64, 1024))         # 32 x 4 = 128 items
+    assert streams.fills_gpu(sh(64, 2048))             # 32 x 8 = 256 items
+    assert not streams.fills_gpu(sh(64, 2048), nsm=300)
