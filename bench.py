@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--oracle-checks", type=int, default=1,
                     help="config5: check sampled requests against the FP64 oracle in the CPU leg (0: skip)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
-    ap.add_argument("--lanes", type=int, default=2, help="config5: server lanes")
+    ap.add_argument("--lanes", type=int, default=1, help="config5: server lanes")
     ap.add_argument("--detail", default=None, help="config5: write per-window times of the served and per-call arms here")
     ap.add_argument("--tc-weights", default="auto", choices=["auto", "entries", "direct"],
                     help="tensor-core weight operands (hcg_tc_set_weights)")
@@ -635,7 +635,8 @@ def served_run(args):
                       "unique_fields": len({r["field"] for r in reqs}), "windows": len(windows),
                       "staging_budget_gb": args.stage_gb, "total_sample_channels": tot_work,
                       "fields_built": fields_built,
-                      "engine": "served: hcg_server (%d lanes, batch graphs, tensor cores FP16 hi/lo); " % args.lanes +
+                      "engine": "served: hcg_server (%d lane%s, batch graphs, tensor cores FP16 hi/lo); "
+                                % (args.lanes, "" if args.lanes == 1 else "s") +
                                 "plain: hcg_grid FP32 engine per call"},
            "served": {"capacity": capacity, "busy_s": round(busy, 4), "batches": st["batches"],
                       "p50_s_closed_loop": pct(lats_cl, 50), "p99_s_closed_loop": pct(lats_cl, 99),

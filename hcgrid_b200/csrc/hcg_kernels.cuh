@@ -883,40 +883,43 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
     }
     for (int j = tid; j < nrt; j += blockDim.x) { s_lo[j] = 0xffffffffu; s_hi[j] = 0; }
     __syncthreads();
-    // one (group, ring) pair per thread: the union of the group's four
-    // windows (group_item's count) and the tile union (min / max over groups)
-    for (int i = tid; i < kTileGroups * nrt; i += blockDim.x) {
-        const int gq = i % kTileGroups, j = i / kTileGroups;
+    // one (group, ring, pixel) triple per thread, the four pixels of a group in
+    // consecutive lanes: each thread forms one window (its dependent loads run
+    // beside the other lanes'), the quad's shuffles give the group's union
+    // (group_item's count) and the tile union takes min / max over groups. The
+    // loop runs whole warps (inactive lanes hold empty windows).
+    const int total = 4 * kTileGroups * nrt;
+    for (int ib = 0; ib < total; ib += blockDim.x) {
+        const int i = ib + tid;
+        const bool act = i < total;
+        const int q = i & 3, quad = i >> 2;
+        const int gq = quad % kTileGroups, j = quad / kTileGroups;
         const int k = r0 + j;
-        uint32_t glo = 0xffffffffu, ghi = 0;
-        const RingRec R = a.rings[k];
-        uint32_t wlo[4] = {0, 0, 0, 0}, whi[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        uint32_t lo = 0, hi = 0;
+        if (act) {
             const int p = (2 * (gq / (kTileX / 2)) + (q >> 1)) * kTileX + 2 * (gq % (kTileX / 2)) + (q & 1);
             const PixPrep &P = s_prep[p];
             if (P.nr > 0 && k >= P.ur && k < P.ur + P.nr) {
-                uint32_t lo, hi, rl;
-                if (!ring_window_mc(a, R, P, lo, hi, rl)) {
-                    wlo[q] = 1;  // lo > hi: the reference would spin on this ring
+                uint32_t rl;
+                if (!ring_window_mc(a, a.rings[k], P, lo, hi, rl)) {
+                    lo = 1;  // lo > hi: the reference would spin on this ring
+                    hi = 0;
                     ++skips;
                 } else {
                     cand += rl;
-                    wlo[q] = lo;
-                    whi[q] = hi;
-                    if (hi > lo) {
-                        glo = min(glo, lo);
-                        ghi = max(ghi, hi);
-                    }
                 }
             }
         }
-        if (T.win && j < kWinSpan) {
-            uint4 *w = T.win + ((tile * kWinSpan + j) * kTileGroups + gq) * 2;
-            w[0] = make_uint4(wlo[0], whi[0], wlo[1], whi[1]);
-            w[1] = make_uint4(wlo[2], whi[2], wlo[3], whi[3]);
+        uint32_t glo = hi > lo ? lo : 0xffffffffu, ghi = hi > lo ? hi : 0;
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            glo = min(glo, __shfl_xor_sync(0xffffffffu, glo, o));
+            ghi = max(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
         }
-        if (glo < ghi) {
+        if (!act) continue;
+        if (T.win && j < kWinSpan)
+            reinterpret_cast<uint2 *>(T.win + ((tile * kWinSpan + j) * kTileGroups + gq) * 2)[q] = make_uint2(lo, hi);
+        if (q == 0 && glo < ghi) {
             atomicAdd(&s_cnt[gq], ghi - glo);
             atomicMin(&s_lo[j], glo);
             atomicMax(&s_hi[j], ghi);
