@@ -757,6 +757,35 @@ def config4_run(args):
             run.unstage(staged)
     finally:
         run.close()
+    # where batching pays: the same blocks at the small end of each range
+    # (10,000 samples, 64^2 pixels, 1 or 64 channels), launch-bound one by one
+    tiny = [dict(request=i, field=i, shape=dict(r["shape"], n=10000, grid=64,
+                                                nchan=1 if r["shape"]["nchan"] == 1 else 64),
+                 spectra_seed=r["spectra_seed"]) for i, r in enumerate(reqs)]
+    run = streams.Runner(ctx, tiny, torch, dev)
+    try:
+        staged = run.stage(tiny, tc=True)
+        jobs = [(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR) for s in staged]
+        tb, tc1 = [], []
+        for rep in range(4):  # the first of each is a warm-up
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            ctx.grid_batch(jobs)
+            tb.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            for s in staged:
+                ctx.grid(s.field, s.target, s.cube, s.weights)
+            ctx.synchronize()
+            tc1.append(time.perf_counter() - t0)
+        run.unstage(staged)
+    finally:
+        run.close()
+    tiny_work = sum(streams.request_work(r) for r in tiny)
+    tiny_out = {"what": "the 256 blocks at 10,000 samples, 64^2 pixels and 1 or 64 channels: one hcg_grid_batch "
+                        "against one hcg_grid call at a time (best of 3 after a warm-up)",
+                "batch_s": round(min(tb[1:]), 5), "per_call_s": round(min(tc1[1:]), 5),
+                "batch": tiny_work / min(tb[1:]), "per_call": tiny_work / min(tc1[1:]),
+                "batch_over_per_call": round(min(tc1[1:]) / min(tb[1:]), 3)}
     work = sum(streams.request_work(r) for r in reqs)
     out = {"metric": METRIC, "value": work / t_batch, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -768,6 +797,7 @@ def config4_run(args):
                       "total_sample_channels": work},
            "batch_s": round(t_batch, 4), "per_call_tc": {"value": work / t_call, "total_s": round(t_call, 4)},
            "batch_over_per_call": round(t_call / t_batch, 3), "batch_equals_single_call": same,
+           "launch_bound_blocks": tiny_out,
            "batch_tuning": {"classes": tuning, "how": "hcg_autotune_batch on the first window: per channel class, "
                             "each of the 4 shapes (0: 256 ch x 32 slots x 4 stages, 1: 256 x 64 x 2, "
                             "2: 128 x 64 x 3, 3: 64 x 64 x 4) timed as one hcg_grid_batch of the class's "

@@ -191,11 +191,13 @@ static hcg_status grid_checked(hcg_context *ctx, const hcg_field *field, const h
     std::string why;
     cudaError_t e = grid_field(ctx, field, target, dc, layout, dw, engine, why);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "grid", why);
-    if (tc) {
+    if (tc || field->nchan > 1) {
         unsigned long long to = 0;
         CK(ctx, cudaMemcpyAsync(&to, &ctx->d_stats->timeouts, sizeof(to), cudaMemcpyDeviceToHost, s), "timeouts");
         CK(ctx, cudaStreamSynchronize(s), "grid");
-        if (to) return fail(ctx, HCG_ETIMEOUT, std::to_string(to) + " tensor-core pipeline waits ran out");
+        if (to)
+            return fail(ctx, HCG_ETIMEOUT, std::to_string(to) + (tc ? " tensor-core" : " FP32 staging") +
+                                                " pipeline waits ran out");
     }
     if (mem == HCG_MEM_HOST) {
         CK(ctx, cudaMemcpyAsync(cube, dc, cube_bytes, cudaMemcpyDeviceToHost, s), "cube download");

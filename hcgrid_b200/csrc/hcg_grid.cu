@@ -84,11 +84,6 @@ __global__ void __launch_bounds__(256) k_tile_rings(GridArgs a, GroupArgs g, Til
     tile_rings_item(a, g, T, T.t0 + blockIdx.x);
 }
 
-// Rows per staging buffer of k_tile_accum: two buffers of 192 rows x 64
-// channels (96 KB) let two CTAs share an SM, so one CTA's chunk barrier is
-// covered by the other's work.
-constexpr int kAccumChunk = 192;
-
 __global__ void __launch_bounds__(kTileThreads, 2) k_tile_accum(GroupArgs g, TileArgs T,
                                                             const unsigned long long *__restrict__ off,
                                                             const uint32_t *__restrict__ cnt,
@@ -97,11 +92,12 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_tile_accum(GroupArgs g, Til
                                                             const double *__restrict__ wsum,
                                                             const float *__restrict__ spec, uint32_t nchan,
                                                             uint32_t cstride, float *__restrict__ out,
-                                                            uint32_t ostride, float *__restrict__ wout) {
+                                                            uint32_t ostride, float *__restrict__ wout,
+                                                            unsigned long long *timeouts) {
     // slices of a tile are adjacent blocks: they run together and share the
     // tile's entries through L2
-    tile_accum_item<kAccumChunk>(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan, cstride, out, ostride, wout,
-                                 T.t0 + blockIdx.y, blockIdx.x * kSlice);
+    tile_accum_item<kAccumBufs, kAccumRows>(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan, cstride, out, ostride,
+                                            wout, T.t0 + blockIdx.y, blockIdx.x * kSlice, timeouts);
 }
 
 // Exclusive scan of n uint32 counts into uint64 offsets (out[n] = total),
@@ -303,7 +299,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             return e;
         }
         float *dst = d_cube;
-        const int smem = 2 * kAccumChunk * kSlice * (int)sizeof(float);
+        const int smem = kAccumBufs * kAccumRows * kSlice * (int)sizeof(float);
         static bool attr_set = false;
         if (tiled && !attr_set) {
             if ((e = cudaFuncSetAttribute(k_tile_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
@@ -336,7 +332,8 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
                 Tc.t0 = (uint64_t)ch.first * T.ntx;
                 dim3 grid((f->cstride + kSlice - 1) / kSlice, (unsigned)((uint64_t)(ch.second - ch.first) * T.ntx));
                 k_tile_accum<<<grid, kTileThreads, smem, s>>>(gc, Tc, off, cnt, e_idx, e_w, wsum, f->d_spec,
-                                                               f->nchan, f->cstride, dst, ostride, d_wts);
+                                                               f->nchan, f->cstride, dst, ostride, d_wts,
+                                                               &ctx->d_stats->timeouts);
             } else {
                 k_group_accum<<<cb, 256, 0, s>>>(gc, off, cnt, e_idx, e_w, wsum, f->d_spec, f->nchan, f->cstride,
                                                  dst, ostride, d_wts);

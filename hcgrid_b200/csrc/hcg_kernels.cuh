@@ -8,6 +8,7 @@
 #include <cmath>
 
 #include "hcg_internal.h"
+#include "hcg_sm100.cuh"
 
 namespace hcg {
 namespace {
@@ -975,8 +976,10 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
 // chunk; 16 threads per 2x2 group each own 4 channels of the slice, so a
 // staged value is used for 4 pixels. Output [pixel][channel].
 constexpr int kSlice = 64, kTileThreads = (kTileX / 2) * (kTileY / 2) * (kSlice / 4);
-constexpr int kStageSlots = 768;              // rows of staged spectra (two buffers of kStageSlots / 2)
-constexpr int kChunk = kStageSlots / 2;
+// FP32 staging rings (buffers x rows of kSlice channels): k_tile_accum's
+// 96 KB lets two CTAs share an SM; kb_accum runs one CTA per SM.
+constexpr int kAccumBufs = 4, kAccumRows = 96;
+constexpr int kBatchAccumBufs = 4, kBatchAccumRows = 192;
 
 // 16-byte asynchronous global -> shared copy (zero-filled when !valid).
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
@@ -993,17 +996,30 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// One arrival on `bar` once all of this thread's earlier cp.async copies have
+// landed (the barrier's count includes it).
+__device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(sm100::smem_u32(bar)) : "memory");
+}
+constexpr uint64_t kTileWaitNs = 1000000000ull;  // bound of the FP32 staging ring's barrier waits
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Channel sums of one tile for one slice of kSlice channels. The tile's
 // union of candidate spectra (its slots) is staged in shared memory in
-// chunks of kChunk rows, double-buffered: while the entries of one chunk are
-// summed, the next chunk streams in through cp.async. 16 threads per 2x2
-// group each own 4 channels of the slice, so a staged value feeds 4 pixels.
-// Block-collective (every thread of a kTileThreads block; 2 * CH * kSlice
-// floats of dynamic shared memory).
-template <int CH = kChunk>
+// chunks of CH rows through a ring of NB buffers: every thread copies its
+// share of a chunk with cp.async and arrives on the chunk's `full` barrier
+// when its copies land; each warp arrives on the buffer's `empty` barrier
+// when it has summed the chunk, and the chunk NB - 2 ahead is staged into a
+// buffer only once every warp is done with that buffer's previous chunk. So a
+// warp whose groups have many entries in one chunk holds the others back only
+// two chunks later, not at every chunk. 16 threads per 2x2 group each own 4
+// channels of the slice, so a staged value feeds 4 pixels. Block-collective
+// (every thread of a kTileThreads block; NB * CH * kSlice floats of dynamic
+// shared memory). A barrier wait that runs out (1 s) is counted in
+// `timeouts` and the item winds down.
+template <int NB, int CH>
 __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileArgs &T,
                                                 const unsigned long long *__restrict__ off,
                                                 const uint32_t *__restrict__ cnt,
@@ -1011,15 +1027,28 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
                                                 const float4 *__restrict__ e_w, const double *__restrict__ wsum,
                                                 const float *__restrict__ spec, uint32_t nchan, uint32_t cstride,
                                                 float *__restrict__ out, uint32_t ostride,
-                                                float *__restrict__ wout, uint64_t tile, uint32_t c0) {
-    extern __shared__ float4 s_spec[];  // [2][CH][kSlice / 4]
+                                                float *__restrict__ wout, uint64_t tile, uint32_t c0,
+                                                unsigned long long *timeouts) {
+    static_assert(NB >= 3, "the chunk NB - 2 ahead is staged while one is summed");
+    constexpr int kWarps = kTileThreads / 32;
+    extern __shared__ float4 s_spec[];  // [NB][CH][kSlice / 4]
     __shared__ uint32_t s_ulo[kTileMaxRings], s_base[kTileMaxRings + 1];
+    __shared__ uint64_t s_full[NB], s_empty[NB];
+    __shared__ volatile int s_abort;
     __syncthreads();  // shared state of a previous item is no longer read
     const int tid = threadIdx.x, q = tid & (kSlice / 4 - 1), gl = tid / (kSlice / 4);
     const int nrt = T.nr[tile];
     const uint32_t U = T.U[tile];
     for (int j = tid; j < nrt; j += kTileThreads) s_ulo[j] = T.ulo[tile * kTileMaxRings + j];
     for (int j = tid; j <= nrt; j += kTileThreads) s_base[j] = T.base[tile * (kTileMaxRings + 1) + j];
+    if (tid == 0) {
+        for (int b = 0; b < NB; ++b) {
+            sm100::mbar_init(&s_full[b], kTileThreads);
+            sm100::mbar_init(&s_empty[b], kWarps);
+        }
+        s_abort = 0;
+        sm100::mbar_fence_init();
+    }
     const uint32_t gxi = (uint32_t)(tile % T.ntx) * (kTileX / 2) + gl % (kTileX / 2);
     const uint32_t gyi = (uint32_t)(tile / T.ntx) * (kTileY / 2) + gl / (kTileX / 2);
     const bool gvalid = gxi < g.gx && (uint64_t)gyi * g.gx + gxi < g.ngroups;
@@ -1033,7 +1062,8 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
-    // stage rows [cs, min(U, cs + CH)) into buffer b: 16 threads per row
+    // stage rows [cs, min(U, cs + CH)) into buffer b (16 threads per row); the
+    // thread's arrival on full[b] completes when its copies have landed
     auto stage = [&](uint32_t cs, int b) {
         const uint32_t ce = min(U, cs + CH);
         float4 *dst = s_spec + (size_t)b * CH * (kSlice / 4);
@@ -1051,20 +1081,30 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
             const float *src = spec + (uint64_t)idx * cstride + (ok ? c : 0);
             cp_async16(dst + row * (kSlice / 4) + part, src, ok);
         }
-        cp_async_commit();
+        cp_async_arrive(&s_full[b]);
     };
     const uint32_t nchunks = (U + CH - 1) / CH;
-    if (nchunks > 0) stage(0, 0);
+    for (uint32_t k = 0; k < NB - 2 && k < nchunks; ++k) stage(k * CH, (int)k);
     for (uint32_t k = 0; k < nchunks; ++k) {
         const uint32_t cs = k * CH, ce = min(U, cs + CH);
-        if (k + 1 < nchunks) {
-            stage(cs + CH, (k + 1) & 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
+        const int b = (int)(k % NB);
+        // the chunk NB - 2 ahead, into the buffer of chunk k - 2 once every warp is done with it
+        const uint32_t kn = k + NB - 2;
+        if (kn < nchunks) {
+            const int bn = (int)(kn % NB);
+            if (kn >= (uint32_t)NB && !s_abort &&
+                !sm100::mbar_wait(&s_empty[bn], ((kn / NB) - 1) & 1, kTileWaitNs)) {
+                atomicAdd(timeouts, 1ULL);
+                s_abort = 1;
+            }
+            stage(kn * CH, bn);
         }
-        __syncthreads();
-        const float4 *buf = s_spec + (size_t)(k & 1) * CH * (kSlice / 4);
+        if (!s_abort && !sm100::mbar_wait(&s_full[b], (k / NB) & 1, kTileWaitNs)) {
+            atomicAdd(timeouts, 1ULL);
+            s_abort = 1;
+        }
+        if (s_abort) break;
+        const float4 *buf = s_spec + (size_t)b * CH * (kSlice / 4);
         // entries kSet at a time from two register sets in turn: the next set
         // is loaded while one is summed, and no set is copied
         constexpr int kSet = 3;
@@ -1122,8 +1162,10 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
                 acc[kk].w = fmaf(wv[kk], sv.w, acc[kk].w);
             }
         }
-        __syncthreads();  // buffer k & 1 is restaged at iteration k + 1
+        __syncwarp();
+        if ((tid & 31) == 0) sm100::mbar_arrive(&s_empty[b]);  // this warp is done with buffer b
     }
+    cp_async_wait_all();  // no copy into the ring outlives the item
     if (!gvalid) return;
     const uint32_t c = c0 + 4 * q;
 #pragma unroll
