@@ -68,6 +68,9 @@ def parse():
                     help="config5: check sampled requests against the FP64 oracle in the CPU leg (0: skip)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0, help="config5: admission budget")
     ap.add_argument("--lanes", type=int, default=1, help="config5: server lanes")
+    ap.add_argument("--layout", default="channel", choices=["channel", "sample"],
+                    help="cube layout of the config-1/2/3 steps: channel = [channel][pixel], the reference's "
+                         "h_datacube planes; sample = [pixel][channel]")
     ap.add_argument("--detail", default=None, help="config5: write per-window times of the served and per-call arms here")
     ap.add_argument("--tc-weights", default="auto", choices=["auto", "entries", "direct"],
                     help="tensor-core weight operands (hcg_tc_set_weights)")
@@ -921,7 +924,10 @@ def main():
     target = band_target if bands else ctx.target_from_header(job.header)
     ctx.synchronize()
     torch.cuda.empty_cache()
-    cube = torch.empty((P, job.nchan), dtype=torch.float32, device=dev)
+    LAY = api.CHANNEL_MAJOR if args.layout == "channel" else api.SAMPLE_MAJOR
+    pm = (lambda c: c.t()) if LAY == api.CHANNEL_MAJOR else (lambda c: c)  # a [pixel][channel] view
+    cube = torch.empty((job.nchan, P) if LAY == api.CHANNEL_MAJOR else (P, job.nchan), dtype=torch.float32,
+                       device=dev)
     wts = torch.empty(P, dtype=torch.float32, device=dev)
     # prep, tile rings, count of overflowed tiles, 3-pass scan, row offsets, weights, sums
     launches_per_step = 2 if job.nchan == 1 else 9
@@ -941,7 +947,7 @@ def main():
                            "the best of %d timed runs after a warm-up; spread = (slowest - fastest) / fastest of "
                            "the chosen setting's runs" % args.tune_reps)
     for _ in range(args.warmup):
-        ctx.grid(field, target, cube, wts, engine=engine)
+        ctx.grid(field, target, cube, wts, layout=LAY, engine=engine)
     ctx.synchronize()
     stats = ctx.stats()
 
@@ -956,7 +962,7 @@ def main():
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         for _ in range(args.steps):
-            ctx.grid(field, target, cube, wts, engine=engine)
+            ctx.grid(field, target, cube, wts, layout=LAY, engine=engine)
             st = ctx.stats()  # phase times of this step (device events on the launching stream)
             for i in range(4):
                 phase_ms[i].append(st.ms_phase[i])
@@ -974,7 +980,7 @@ def main():
         dist.barrier()
         torch.cuda.synchronize(dev)
         ta = time.perf_counter()
-        whole_cube, whole_w = shard.assemble_tensors(dist, rank, world, bands, job.nx, cube, wts)
+        whole_cube, whole_w = shard.assemble_tensors(dist, rank, world, bands, job.nx, pm(cube), wts)
         torch.cuda.synchronize(dev)
         assemble_ms = reduce_max(torch, dist, (time.perf_counter() - ta) * 1e3)
         del whole_cube, whole_w
@@ -983,7 +989,7 @@ def main():
     timed_sub = None
     cube_timed = None
     if check is not None:
-        timed_sub = cube[check["sub_d"]][:, check["chans_d"]].double().cpu().numpy()
+        timed_sub = pm(cube)[check["sub_d"]][:, check["chans_d"]].double().cpu().numpy()
         if plain_steps > 0 and torch.cuda.mem_get_info(dev)[0] > cube.numel() * 4 + (8 << 30):
             cube_timed = cube.clone()  # the last timed step's cube, against the FP32 engine's below
     plain = None
@@ -992,7 +998,7 @@ def main():
     if plain_steps > 0:
         # the plain FP32 CUDA-core engine on the same resident field, same timing rules
         for _ in range(2):
-            ctx.grid(field, target, cube, wts, engine=api.ENGINE_FP32)
+            ctx.grid(field, target, cube, wts, layout=LAY, engine=api.ENGINE_FP32)
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize(dev)
@@ -1000,14 +1006,14 @@ def main():
         pe1 = torch.cuda.Event(enable_timing=True)
         pe0.record(stream)
         for _ in range(plain_steps):
-            ctx.grid(field, target, cube, wts, engine=api.ENGINE_FP32)
+            ctx.grid(field, target, cube, wts, layout=LAY, engine=api.ENGINE_FP32)
         pe1.record(stream)
         torch.cuda.synchronize(dev)
         pms = reduce_max(torch, dist, pe0.elapsed_time(pe1) / plain_steps)
         if check is not None:
-            plain_sub = cube[check["sub_d"]][:, check["chans_d"]].double().cpu().numpy()
+            plain_sub = pm(cube)[check["sub_d"]][:, check["chans_d"]].double().cpu().numpy()
             if cube_timed is not None:
-                vs_fp32 = device_cube_errors(torch, cube_timed, cube)
+                vs_fp32 = device_cube_errors(torch, pm(cube_timed), pm(cube))
                 vs_fp32["what"] = "the whole timed cube against the FP32 engine's cube of the same field"
                 del cube_timed
                 torch.cuda.empty_cache()
@@ -1083,7 +1089,8 @@ def main():
 
             def make_target():
                 return ctx.target_from_header(job.header)
-        cube_h = torch.empty((P, job.nchan), dtype=torch.float32, pin_memory=True)
+        cube_h = torch.empty((job.nchan, P) if LAY == api.CHANNEL_MAJOR else (P, job.nchan), dtype=torch.float32,
+                             pin_memory=True)
         w_h = torch.empty(P, dtype=torch.float32, pin_memory=True)
         times = []
         for i in range(args.e2e_steps + 1):
@@ -1098,7 +1105,7 @@ def main():
                 f2.split_spectra(engine, keep_fp32=False)
             tc_ = time.perf_counter()
             t2 = make_target()
-            ctx.grid(f2, t2, cube_h, w_h, engine=engine)
+            ctx.grid(f2, t2, cube_h, w_h, layout=LAY, engine=engine)
             dt = time.perf_counter() - t0
             f2.close()
             t2.close()
@@ -1129,7 +1136,7 @@ def main():
             mark("hcg_field_split_spectra")
         t2 = make_target()
         mark("hcg_target_from_header")
-        ctx.grid(f2, t2, cube_h, w_h, engine=engine)
+        ctx.grid(f2, t2, cube_h, w_h, layout=LAY, engine=engine)
         mark("hcg_grid")
         f2.close()
         t2.close()
@@ -1178,6 +1185,8 @@ def main():
                                           if bands else "replica per GPU" if world > 1 else "single GPU"),
                           "bands": bands, "assemble_ms": assemble_ms,
                           "l2": "inputs larger than L2 (spectra %.1f GB), no flush" % (4 * job.n * job.nchan / 1e9),
+                          "cube_layout": ("[channel][pixel] (the reference's h_datacube planes)"
+                                          if LAY == api.CHANNEL_MAJOR else "[pixel][channel]"),
                           "engine": ENGINE_TEXT[args.engine] if job.nchan > 1 else ENGINE_TEXT["fp32"],
                           "tc_pipeline": tune, "tc_weights": args.tc_weights},
                "gpu_launches": launches_per_step * args.steps, "clocks": clocks, "roofline": roofline,

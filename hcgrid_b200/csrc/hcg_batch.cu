@@ -407,6 +407,12 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         if (B.h_jusum) cudaFreeHost(B.h_jusum);
         if (B.d_tclist) cudaFreeAsync(B.d_tclist, s);
         if (B.h_tclist) cudaFreeHost(B.h_tclist);
+        // the captured graphs hold the job table's and the entry totals'
+        // addresses as launch arguments: capture again with the new ones (no
+        // replay is in flight: every batch ends with a stream synchronize)
+        if (B.exec_geom) cudaGraphExecDestroy(B.exec_geom);
+        if (B.exec_sums) cudaGraphExecDestroy(B.exec_sums);
+        B.exec_geom = B.exec_sums = nullptr;
         B.job_cap = std::max<uint32_t>(njobs, 64);
         if ((e = dalloc(&B.d_jobs, B.job_cap * sizeof(JobDesc), s, ctx->pool)) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&B.h_jobs, B.job_cap * sizeof(JobDesc))) != cudaSuccess) return e;

@@ -66,6 +66,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64
     return true;
 }
 
+// ---------------------------------------------------------------- 256-bit global access
+// Eight floats at a 32-byte aligned global address in one access (sm_100).
+__device__ __forceinline__ void st_global_v8(float *p, const float (&o)[8]) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(o[0]), "f"(o[1]),
+                 "f"(o[2]), "f"(o[3]), "f"(o[4]), "f"(o[5]), "f"(o[6]), "f"(o[7])
+                 : "memory");
+}
+__device__ __forceinline__ void ld_global_v8(const float *p, float (&o)[8]) {
+    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]), "=f"(o[4]), "=f"(o[5]), "=f"(o[6]), "=f"(o[7])
+                 : "l"(p)
+                 : "memory");
+}
+
 // ---------------------------------------------------------------- TMA
 // 2-D tiled load of one box into shared memory, completing on `bar` by bytes.
 // c0 is the innermost coordinate (elements), c1 the row.

@@ -751,7 +751,24 @@ __device__ __forceinline__ void tc_epilogue_direct(SH &S, const TcJob &J, uint64
                     }
             } else {
                 float *dst = J.out + p * J.ostride + c0;
-                if ((J.ostride & 3) == 0 && c0 + 32 <= J.nchan && (((uintptr_t)J.out) & 15) == 0) {
+                if ((J.ostride & 7) == 0 && c0 + 32 <= J.nchan && (((uintptr_t)J.out) & 31) == 0) {
+                    // 32-byte accesses: each store fills whole sectors of the pixel's row
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        float o[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) o[u] = v[8 * i + u];
+                        if (q) {
+                            float b[8];
+                            ld_global_v8(dst + 8 * i, b);
+#pragma unroll
+                            for (int u = 0; u < 8; ++u) o[u] += b[u];
+                        }
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) o[u] *= f;
+                        st_global_v8(dst + 8 * i, o);
+                    }
+                } else if ((J.ostride & 3) == 0 && c0 + 32 <= J.nchan && (((uintptr_t)J.out) & 15) == 0) {
                     float4 *d4 = reinterpret_cast<float4 *>(dst);
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {

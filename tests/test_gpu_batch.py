@@ -91,6 +91,21 @@ def test_batch_replay_after_growth(ctx, jobs):
         np.testing.assert_array_equal(big[i][0], big[i + len(jobs)][0])
 
 
+def test_batch_past_the_job_table_capacity(ctx, jobs):
+    """A batch of more jobs than the job table holds (64 at first) after a
+    small one: the table is reallocated and the captured graphs, which take
+    its address, are captured again; every cube equals the single call's."""
+    run_batch(ctx, jobs[:2], [api.SAMPLE_MAJOR] * 2)
+    many = (jobs * 15)[:70]
+    got = run_batch(ctx, many, [api.SAMPLE_MAJOR] * len(many))
+    ref = [single(ctx, job, f, t, api.SAMPLE_MAJOR) for job, f, t in jobs]
+    for i, (cube, w) in enumerate(got):
+        np.testing.assert_array_equal(cube, ref[i % len(jobs)][0])
+        np.testing.assert_array_equal(w, ref[i % len(jobs)][1])
+    again = run_batch(ctx, jobs[:2], [api.SAMPLE_MAJOR] * 2)  # and a small batch after it
+    np.testing.assert_array_equal(again[1][0], ref[1][0])
+
+
 def test_batch_jobs_match_oracle(ctx, jobs):
     got = run_batch(ctx, jobs, [api.SAMPLE_MAJOR] * len(jobs))
     for (job, f, t), (cube, w) in zip(jobs, got):
