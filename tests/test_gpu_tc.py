@@ -195,6 +195,38 @@ def test_tc_weight_modes_match_oracle(ctx, dense, mode, engine, layout):
     assert err <= TOL[engine]
 
 
+@pytest.mark.parametrize("engine", ENGINES)
+def test_tc_segments_in_both_cube_layouts(ctx, engine):
+    """Tiles longer than one accumulation segment (the dense beam of the
+    fixture above) with 256 channels, so pixel-major rows take the 32-byte
+    stores and later segments are added to the stored partial sums: the
+    pixel-major cube equals the channel-plane cube bit for bit and is within
+    the split's tolerance of the FP32 engine."""
+    shape = dict(block=0, n=20_000, size_deg=0.3, ra=150.0, dec=20.0, grid=64, nchan=256, fwhm=180.0, seed=5)
+    job = synth.block_job(shape)
+    prepare(ctx, job)
+    f = ctx.field(job.lon, job.lat)
+    f.set_spectra(job.values)
+    t = ctx.target_from_header(job.header)
+    try:
+        c32, w32 = ctx.grid(f, t, engine=api.ENGINE_FP32)
+        f.split_spectra(engine, keep_fp32=False)
+        ctx.tc_set_weights(api.TC_WEIGHTS_ENTRIES)
+        cs, ws = ctx.grid(f, t, layout=api.SAMPLE_MAJOR, engine=engine)
+        cc, wc = ctx.grid(f, t, layout=api.CHANNEL_MAJOR, engine=engine)
+        st = ctx.stats()
+    finally:
+        ctx.tc_set_weights(api.TC_WEIGHTS_AUTO)
+        f.close()
+        t.close()
+    assert st.tc_macs > 0
+    np.testing.assert_array_equal(cs, cc.T)
+    np.testing.assert_array_equal(ws, wc)
+    np.testing.assert_array_equal(ws, w32)
+    np.testing.assert_array_equal(np.isnan(cs), np.isnan(c32))
+    assert plane_errors(cs, c32.astype(np.float64)) <= TOL[engine]
+
+
 def test_tc_weight_modes_deterministic_and_checked(ctx, dense):
     """Each mode gives the same bits on every call; the automatic mode is one
     of the two; unknown modes are refused."""
