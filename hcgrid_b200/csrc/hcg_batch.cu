@@ -461,6 +461,9 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
                 why = "cuTensorMapEncodeTiled";
                 return cudaErrorInvalidValue;
             }
+            d.g.pack = 1;  // the tensor-core builders take packed hi/lo weights
+            d.g.fmt = d.tc.fmt;
+            d.g.wscale = d.tc.wscale;
         }
         d.pix_base = pix;
         d.grp_base = grp;

@@ -310,6 +310,10 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
         bool first = true;
         for (auto &ch : chunks) {
             GroupArgs gc = g;
+            if (tiled && tc) {  // the tensor-core builders take packed hi/lo weights
+                gc.pack = 1;
+                tc_entry_format(f, gc.fmt, gc.wscale);
+            }
             gc.g0 = std::min<uint64_t>((uint64_t)ch.first * groups_per_row, g.ngroups);
             gc.g1 = std::min<uint64_t>((uint64_t)ch.second * groups_per_row, g.ngroups);
             gc.ebase = ro[ch.first];

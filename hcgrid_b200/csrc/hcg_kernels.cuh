@@ -3,6 +3,8 @@
 // both execute the same arithmetic. The method is described in hcg_grid.cu.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -436,11 +438,48 @@ __device__ __forceinline__ void grid1_item(const GridArgs &a, const float *__res
 }  // namespace
 
 // Launch arguments shared by the kernels of several translation units.
+namespace {
+
+// FP16 / BF16 halves of the tensor-core weight operand (fmt 0: FP16, 1: BF16).
+__device__ __forceinline__ uint16_t tc_to16(float v, uint32_t fmt) {
+    return fmt ? __bfloat16_as_ushort(__float2bfloat16_rn(v)) : __half_as_ushort(__float2half_rn(v));
+}
+
+__device__ __forceinline__ float tc_from16(uint16_t b, uint32_t fmt) {
+    return fmt ? __bfloat162float(__ushort_as_bfloat16(b)) : __half2float(__ushort_as_half(b));
+}
+
+// hi/lo split of two weights at once (paired conversions): `hi` and `lo` hold
+// the 16-bit values of a (low half) and b (high half), the same values as
+// tc_to16 of each and of its remainder.
+__device__ __forceinline__ void tc_split2(float a, float b, uint32_t fmt, uint32_t &hi, uint32_t &lo) {
+    if (fmt) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        const float2 f = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(a - f.x, b - f.y);
+        hi = *reinterpret_cast<const uint32_t *>(&h);
+        lo = *reinterpret_cast<const uint32_t *>(&l);
+    } else {
+        const __half2 h = __floats2half2_rn(a, b);
+        const float2 f = __half22float2(h);
+        const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
+        hi = *reinterpret_cast<const uint32_t *>(&h);
+        lo = *reinterpret_cast<const uint32_t *>(&l);
+    }
+}
+
+}  // namespace
+
 struct GroupArgs {
     uint32_t nx, ny, gx;
     uint64_t ngroups;
     uint64_t g0, g1;             // groups handled by this launch
     unsigned long long ebase;    // entry offset of group g0 in the entry buffer
+    // entries for the tensor-core builders: the four weights times wscale as
+    // 16-bit hi/lo pairs {hi(w0, w1), lo(w0, w1), hi(w2, w3), lo(w2, w3)}
+    // (fmt 0: FP16, 1: BF16) instead of four FP32 weights
+    uint32_t pack = 0, fmt = 0;
+    float wscale = 1.f;
 };
 
 // Tiles of kTileX x kTileY pixels (kTileX/2 x kTileY/2 groups) whose union of
@@ -470,8 +509,12 @@ struct TileArgs {
     unsigned long long *ustat;  // [0]: sum, [1]: largest of the tiles' staged slots U (or null)
 };
 
+// hcg_tc.cu: the tensor-core builders' entry format of a field with split
+// spectra (GroupArgs::fmt and ::wscale).
+void tc_entry_format(const hcg_field *f, uint32_t &fmt, float &wscale);
 // hcg_tc.cu: tensor-core accumulation of `ntiles` tiles from T.t0, after
-// k_group emitted the entries (slot mode) and the weight sums.
+// k_group emitted the entries (slot mode, packed hi/lo weights) and the
+// weight sums.
 cudaError_t tc_accum(hcg_context *ctx, const hcg_field *f, const GroupArgs &g, const TileArgs &T, uint64_t ntiles,
                      const unsigned long long *off, const uint32_t *cnt, const uint32_t *e_slot, const float4 *e_w,
                      const double *wsum, float *out, uint32_t ostride, float *wout, unsigned long long umax,
@@ -625,7 +668,14 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
             if (any) {
                 unsigned long long pos = eoff + base + __popc(ball & lt);
                 e_idx[pos] = slots ? (uint32_t)((long long)idx + s_shift) : idx;
-                e_w[pos] = make_float4(wq[0], wq[1], wq[2], wq[3]);
+                if (g.pack) {
+                    uint32_t h01, l01, h23, l23;
+                    tc_split2(wq[0] * g.wscale, wq[1] * g.wscale, g.fmt, h01, l01);
+                    tc_split2(wq[2] * g.wscale, wq[3] * g.wscale, g.fmt, h23, l23);
+                    reinterpret_cast<uint4 *>(e_w)[pos] = make_uint4(h01, l01, h23, l23);
+                } else {
+                    e_w[pos] = make_float4(wq[0], wq[1], wq[2], wq[3]);
+                }
             }
             base += __popc(ball);
         }

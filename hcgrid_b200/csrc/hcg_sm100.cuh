@@ -263,5 +263,11 @@ __host__ __device__ constexpr uint32_t idesc_f16_kmaj_a_mnmaj_b(uint32_t fmt, ui
            | ((M >> 4) << 24);    // M / 16
 }
 
+// The same with A MN-major too (both operands stored pixel / channel
+// contiguous, 128-byte swizzled atoms of 64 elements x 8 K rows).
+__host__ __device__ constexpr uint32_t idesc_f16_mnmaj_a_mnmaj_b(uint32_t fmt, uint32_t M, uint32_t N) {
+    return idesc_f16_kmaj_a_mnmaj_b(fmt, M, N) | (1u << 15);  // A MN-major
+}
+
 }  // namespace sm100
 }  // namespace hcg

@@ -250,6 +250,11 @@ bool tc_out_map(CUtensorMap *m, float *out, uint32_t ostride, uint32_t nx, uint3
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+void tc_entry_format(const hcg_field *f, uint32_t &fmt, float &wscale) {
+    fmt = f->xfmt == HCG_ENGINE_TC_BF16 ? 1u : 0u;
+    wscale = tc_weight_scale(f, fmt != 0);
+}
+
 bool tc_prepare_job(const hcg_field *f, int nb_max, CUtensorMap *map, TcJob &J) {
     const uint32_t nblk64 = f->xcpad / 64;
     J.nb = nblk64 < (uint32_t)nb_max ? nblk64 : (uint32_t)nb_max;

@@ -77,6 +77,9 @@ struct TcCfg {
     static constexpr uint32_t kARow = KC * 2;                  // bytes per operand row
     static constexpr uint32_t kAAtom = 8 * kARow;              // 8-row swizzle atom
     static constexpr uint32_t kALayout = KC == 64 ? 2u : 4u;   // descriptor layout: SWIZZLE_128B / _64B
+    // the entries builders' MN-major weight operand: per 8-slot K group two
+    // 1 KB atoms of 64 pixels x 8 slots (128-byte swizzle)
+    static constexpr uint32_t kAMnGroup = 2048;
     static constexpr uint32_t kBGroup = 2 * NB * 1024;         // one 8-slot row group: hi blocks, lo blocks
     static constexpr uint32_t kBBytes = (KC / 8) * kBGroup;
     static constexpr uint32_t kStageBytes = 2 * kAHalf + kBBytes;
@@ -160,33 +163,6 @@ int tc_pick(const hcg_context *ctx, const hcg_field *f);
 void tc_pipeline(const hcg_context *ctx, const hcg_field *f, TcJob &J);
 
 namespace {
-
-__device__ __forceinline__ uint16_t tc_to16(float v, uint32_t fmt) {
-    return fmt ? __bfloat16_as_ushort(__float2bfloat16_rn(v)) : __half_as_ushort(__float2half_rn(v));
-}
-
-__device__ __forceinline__ float tc_from16(uint16_t b, uint32_t fmt) {
-    return fmt ? __bfloat162float(__ushort_as_bfloat16(b)) : __half2float(__ushort_as_half(b));
-}
-
-// hi/lo split of two weights at once (paired conversions): `hi` and `lo` hold
-// the 16-bit values of a (low half) and b (high half), the same values as
-// tc_to16 of each and of its remainder.
-__device__ __forceinline__ void tc_split2(float a, float b, uint32_t fmt, uint32_t &hi, uint32_t &lo) {
-    if (fmt) {
-        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-        const float2 f = __bfloat1622float2(h);
-        const __nv_bfloat162 l = __floats2bfloat162_rn(a - f.x, b - f.y);
-        hi = *reinterpret_cast<const uint32_t *>(&h);
-        lo = *reinterpret_cast<const uint32_t *>(&l);
-    } else {
-        const __half2 h = __floats2half2_rn(a, b);
-        const float2 f = __half22float2(h);
-        const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
-        hi = *reinterpret_cast<const uint32_t *>(&h);
-        lo = *reinterpret_cast<const uint32_t *>(&l);
-    }
-}
 
 // byte offset of element (row m, column k) of a K-major 128-row x KC-column
 // 16-bit operand in swizzled 8-row atoms (the 16-byte chunk index is XORed
@@ -338,7 +314,7 @@ __device__ __forceinline__ bool tc_mma(SH &S, const TcJob &J, uint32_t nchunks, 
     using namespace sm100;
     constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
     const TcStage<Cfg> st{tc_smem_base()};
-    const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
+    const uint32_t idesc = idesc_f16_mnmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
     uint32_t acc = 0;
     bool ok = true;
     for (uint32_t k = 0; k < nchunks && !S.abort; ++k) {
@@ -353,13 +329,13 @@ __device__ __forceinline__ bool tc_mma(SH &S, const TcJob &J, uint32_t nchunks, 
         const uint32_t bh = smem_u32(st.B(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
         // K step 0's descriptors; step kk adds its byte offset / 16 (two 8-slot
         // row groups per K step; 64-channel atoms 1 KB apart)
-        const uint64_t adh = smem_desc(ah, 16, Cfg::kAAtom, Cfg::kALayout);
-        const uint64_t adl = smem_desc(al, 16, Cfg::kAAtom, Cfg::kALayout);
+        const uint64_t adh = smem_desc(ah, 1024, Cfg::kAMnGroup, 2);  // MN-major A (tc_build)
+        const uint64_t adl = smem_desc(al, 1024, Cfg::kAMnGroup, 2);
         const uint64_t bdh = smem_desc(bh, 1024, Cfg::kBGroup, 2);
         const uint64_t bdl = smem_desc(bl, 1024, Cfg::kBGroup, 2);
 #pragma unroll
         for (int kk = 0; kk < (int)(KC / 16); ++kk) {
-            const uint64_t ao = (uint64_t)(kk * 32 / 16), bo = (uint64_t)(kk * 2 * Cfg::kBGroup / 16);
+            const uint64_t ao = (uint64_t)(kk * 2 * Cfg::kAMnGroup / 16), bo = (uint64_t)(kk * 2 * Cfg::kBGroup / 16);
             mma_f16_ss(d_tmem, adh + ao, bdh + bo, idesc, acc);
             mma_f16_ss(d_tmem, adh + ao, bdl + bo, idesc, 1);
             mma_f16_ss(d_tmem, adl + ao, bdh + bo, idesc, 1);
@@ -391,13 +367,16 @@ __host__ __device__ constexpr uint32_t tc_segments(uint32_t nchunks) {
 
 // MMA issue (one thread) of one item in segments; `gs` counts the CTA's
 // segments (accumulator gs & 1, barriers acc_full / acc_empty by parity).
-template <class Cfg, class SH>
+// AMN: the weight operand is MN-major (the entries builders, tc_build), else
+// K-major (the direct builders, tc_build_weights).
+template <class Cfg, bool AMN, class SH>
 __device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchunks, uint32_t gk, uint32_t &gs,
                                            unsigned long long *timeouts, unsigned long long *macs) {
     using namespace sm100;
     constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
     const TcStage<Cfg> st{tc_smem_base()};
-    const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
+    const uint32_t idesc =
+        AMN ? idesc_f16_mnmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb) : idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
     const uint32_t nseg = tc_segments(nchunks);
     bool ok = true;
     uint32_t k = 0, issued = 0;
@@ -423,13 +402,14 @@ __device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchun
             // address field (shared-memory addresses stay below 2^18: no carry)
             const uint32_t ah = smem_u32(st.A_hi(s)), al = smem_u32(st.A_lo(s));
             const uint32_t bh = smem_u32(st.B(s)), bl = bh + J.nb * 1024;  // lo blocks follow the hi blocks
-            const uint64_t adh = smem_desc(ah, 16, Cfg::kAAtom, Cfg::kALayout);
-            const uint64_t adl = smem_desc(al, 16, Cfg::kAAtom, Cfg::kALayout);
+            const uint64_t adh = AMN ? smem_desc(ah, 1024, Cfg::kAMnGroup, 2) : smem_desc(ah, 16, Cfg::kAAtom, Cfg::kALayout);
+            const uint64_t adl = AMN ? smem_desc(al, 1024, Cfg::kAMnGroup, 2) : smem_desc(al, 16, Cfg::kAAtom, Cfg::kALayout);
             const uint64_t bdh = smem_desc(bh, 1024, Cfg::kBGroup, 2);
             const uint64_t bdl = smem_desc(bl, 1024, Cfg::kBGroup, 2);
 #pragma unroll
             for (int kk = 0; kk < (int)(KC / 16); ++kk) {
-                const uint64_t ao = (uint64_t)(kk * 32 / 16), bo = (uint64_t)(kk * 2 * Cfg::kBGroup / 16);
+                const uint64_t ao = (uint64_t)(AMN ? kk * 2 * Cfg::kAMnGroup / 16 : kk * 32 / 16);
+                const uint64_t bo = (uint64_t)(kk * 2 * Cfg::kBGroup / 16);
                 mma_f16_ss(d_tmem, adh + ao, bdh + bo, idesc, acc);
                 mma_f16_ss(d_tmem, adh + ao, bdl + bo, idesc, 1);
                 mma_f16_ss(d_tmem, adl + ao, bdh + bo, idesc, 1);
@@ -446,20 +426,24 @@ __device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchun
     if (issued) atomicAdd(macs, 3ull * kTcM * (64ull * J.nb) * (uint64_t)KC * issued);
 }
 
-// Builders (kTcBuilders threads, index bt), one item: the weights of the
-// chunk's entries into the zeroed K-major operand.
+// Builders (kTcBuilders threads, index bt), one item: the chunk's entries
+// into the MN-major weight operand (pixels contiguous in 128-byte swizzled
+// atoms of 64 pixels x 8 slots). The weight pass stores each entry's weights
+// already split into 16-bit hi/lo pairs (GroupArgs::pack), so a 2 x 2 group's
+// entry is four 32-bit stores: hi and lo of its two horizontal pixel pairs.
+// Warp w's eight groups are the tile's pixels 32w .. 32w + 31 (rows 2w and
+// 2w + 1), so each warp zeroes exactly its own cells of the chunk before it
+// scatters into them and no warp waits for another.
 template <class Cfg, class SH>
 __device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, uint32_t nchunks, uint32_t gk, int bt,
                                          unsigned long long *timeouts) {
-    const float wscale = J.wscale;  // kernel-parameter scalars held in registers for the loops below
-    const uint32_t fmt = J.fmt;
     using namespace sm100;
     constexpr uint32_t ST = Cfg::kStages, KC = Cfg::kK;
     const TcStage<Cfg> st{tc_smem_base()};
     const TileArgs &T = J.T;
     const GroupArgs &G = J.g;
-    const int gq = bt >> 2, sub = bt & 3;
-    const uint32_t gxl = gq & 7, gyl = gq >> 3;
+    const int gq = bt >> 2, sub = bt & 3, lane = bt & 31, w = bt >> 5;
+    const uint32_t gxl = gq & 7, gyl = gq >> 3;  // gyl == w
     const uint32_t gxi = (uint32_t)(tile % T.ntx) * (kTileX / 2) + gxl;
     const uint32_t gyi = (uint32_t)(tile / T.ntx) * (kTileY / 2) + gyl;
     const uint64_t grp = (uint64_t)gyi * G.gx + gxi;
@@ -489,9 +473,13 @@ __device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, u
 #pragma unroll
     for (int i = 0; i < kTcRing; ++i) issue(i);
     int head = 0;
-    uint32_t mrow[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) mrow[q] = (2 * gyl + (q >> 1)) * kTileX + 2 * gxl + (q & 1);
+    // byte offset of (pixel m, chunk slot col): atom (col / 8, m / 64) of 1 KB,
+    // row col % 8 of 128 bytes, 16-byte chunk (m % 64) / 8 XORed with that row
+    auto a_off = [](uint32_t m, uint32_t col) -> uint32_t {
+        const uint32_t r = col & 7u;
+        return ((col >> 3) * 2u + (m >> 6)) * 1024u + r * 128u + ((((m & 63u) >> 3) ^ r) << 4) + ((m & 7u) << 1);
+    };
+    const uint32_t m0 = 2 * gyl * kTileX + 2 * gxl, m1 = m0 + kTileX;  // the group's pixel pairs (x, x + 1)
     for (uint32_t k = 0; k < nchunks; ++k) {
         const uint32_t g = gk + k, s = g % ST;
         // warp-uniform exits: the zeroing below ends with __syncwarp
@@ -503,17 +491,14 @@ __device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, u
         }
         uint8_t *ah = st.A_hi(s), *al = st.A_lo(s);
         {
-            // the group's four threads zero the group's four operand rows (hi and
-            // lo); the scatter below writes only into these rows
-            constexpr int kPieces = Cfg::kARow / 16;
-            const uint32_t m = mrow[sub];
-            uint4 *rh = (uint4 *)(ah + (m >> 3) * Cfg::kAAtom + (m & 7) * Cfg::kARow);
-            uint4 *rl = (uint4 *)(al + (m >> 3) * Cfg::kAAtom + (m & 7) * Cfg::kARow);
-#pragma unroll
-            for (int i = 0; i < kPieces; ++i) {
-                const int c = (i + bt) & (kPieces - 1);  // rotated: fewer bank conflicts
-                rh[c] = make_uint4(0, 0, 0, 0);
-                rl[c] = make_uint4(0, 0, 0, 0);
+            // this warp's cells: pixels 32w .. 32w + 31 of every slot row, four
+            // 16-byte chunks of an atom row (hi and lo)
+            constexpr uint32_t kPieces = 4 * KC;
+            for (uint32_t p = (uint32_t)lane; p < kPieces; p += 32) {
+                const uint32_t r = p >> 2, c = 4u * (uint32_t)(w & 1) + (p & 3u);
+                const uint32_t o = ((r >> 3) * 2u + (uint32_t)(w >> 1)) * 1024u + (r & 7u) * 128u + ((c ^ (r & 7u)) << 4);
+                *reinterpret_cast<uint4 *>(ah + o) = make_uint4(0, 0, 0, 0);
+                *reinterpret_cast<uint4 *>(al + o) = make_uint4(0, 0, 0, 0);
             }
             __syncwarp();
         }
@@ -522,18 +507,13 @@ __device__ __forceinline__ void tc_build(SH &S, const TcJob &J, uint64_t tile, u
             cp_async_wait<kTcRing - 1>();  // the ring's oldest copy has landed
             const uint32_t slot = rs[head * kTcBuilders];
             if (slot >= ce) break;
-            const float4 wq = rw[head * kTcBuilders];
+            const float4 wq = rw[head * kTcBuilders];  // {hi(p0, p1), lo(p0, p1), hi(p2, p3), lo(p2, p3)}
             const uint32_t col = slot - cs;
-            const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float w = wv[q] * wscale;
-                const uint16_t h = tc_to16(w, fmt);
-                const uint16_t l = tc_to16(w - tc_from16(h, fmt), fmt);
-                const uint32_t o = tc_a_offset<KC>(mrow[q], col);
-                *(uint16_t *)(ah + o) = h;
-                *(uint16_t *)(al + o) = l;
-            }
+            const uint32_t o0 = a_off(m0, col), o1 = a_off(m1, col);
+            *reinterpret_cast<uint32_t *>(ah + o0) = __float_as_uint(wq.x);
+            *reinterpret_cast<uint32_t *>(al + o0) = __float_as_uint(wq.y);
+            *reinterpret_cast<uint32_t *>(ah + o1) = __float_as_uint(wq.z);
+            *reinterpret_cast<uint32_t *>(al + o1) = __float_as_uint(wq.w);
             issue(head);
             head = (head + 1) & (kTcRing - 1);
         }
@@ -840,7 +820,7 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
             __syncwarp();
             tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
         } else if (warp == 1) {
-            if (lane == 0) tc_mma_seg<Cfg>(S, J, nchunks, gk, gs, timeouts, macs);
+            if (lane == 0) tc_mma_seg<Cfg, true>(S, J, nchunks, gk, gs, timeouts, macs);
         } else if (warp < 6) {
             tc_build<Cfg>(S, J, tile, nchunks, gk, tid - 64, timeouts);
         } else {
@@ -1135,7 +1115,7 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
             __syncwarp();
             tc_produce<Cfg>(S, J, cblk, U, nchunks, gk, nrt, timeouts);
         } else if (warp == 1) {
-            if (lane == 0) tc_mma_seg<Cfg>(S, J, nchunks, gk, gs, timeouts, macs);
+            if (lane == 0) tc_mma_seg<Cfg, false>(S, J, nchunks, gk, gs, timeouts, macs);
         } else if (tid < 64 + kTcDBuilders) {
             tc_build_weights<Cfg>(S, J, tile, cblk, U, nchunks, gk, il, tid - 64, timeouts);
         } else {
