@@ -54,7 +54,9 @@ __global__ void __launch_bounds__(256) k_grid_1chan(GridArgs a, uint64_t npixmap
     if (p < npixmap) grid1_item<GEN>(a, data, cstride, out, wout, p);
 }
 
-template <bool COUNT, bool GEN = false>  // GEN: fields whose kernel is not GAUSS1D
+// GEN: fields whose kernel is not GAUSS1D; PACK: entries as 16-bit hi/lo
+// pairs for the tensor-core builders (1) or as FP32 weights (0)
+template <bool COUNT, bool GEN = false, int PACK = 0>
 __global__ void __launch_bounds__(256, 3) k_group(GridArgs a, GroupArgs g, uint32_t *__restrict__ cap,
                                                const unsigned long long *__restrict__ off,
                                                uint32_t *__restrict__ e_idx, float4 *__restrict__ e_w,
@@ -65,7 +67,7 @@ __global__ void __launch_bounds__(256, 3) k_group(GridArgs a, GroupArgs g, uint3
     int warp = threadIdx.x >> 5;
     uint64_t grp = g.g0 + blockIdx.x * 8ull + warp;
     if (grp < g.g1)
-        group_item<COUNT, GEN>(a, g, cap, off, e_idx, e_w, cnt, wsum, tiles, grp, s_prep[warp], s_half[warp]);
+        group_item<COUNT, GEN, PACK>(a, g, cap, off, e_idx, e_w, cnt, wsum, tiles, grp, s_prep[warp], s_half[warp]);
 }
 
 __global__ void __launch_bounds__(256) k_group_accum(GroupArgs g, const unsigned long long *__restrict__ off,
@@ -319,10 +321,18 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             gc.ebase = ro[ch.first];
             if (gc.g1 <= gc.g0) continue;
             unsigned cb = (unsigned)((gc.g1 - gc.g0 + 7) / 8);
-            if (f->kernel_type == HCG_GAUSS1D)
-                k_group<false><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tiled ? T : none);
-            else
-                k_group<false, true><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tiled ? T : none);
+            const TileArgs &tt = tiled ? T : none;
+            if (f->kernel_type == HCG_GAUSS1D) {
+                if (gc.pack)
+                    k_group<false, false, 1><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tt);
+                else
+                    k_group<false, false, 0><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tt);
+            } else {
+                if (gc.pack)
+                    k_group<false, true, 1><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tt);
+                else
+                    k_group<false, true, 0><<<cb, 256, 0, s>>>(a, gc, nullptr, off, e_idx, e_w, cnt, wsum, tt);
+            }
             if (first) cudaEventRecord(ctx->evp[2], s);  // phase marks are exact for a single chunk
             first = false;
             if (tiled && tc) {

@@ -534,7 +534,8 @@ namespace {
 // its tile's staged list instead of the sample index.
 // Warp-collective: every lane passes the same group; s_prep is this warp's
 // 4-entry shared-memory slot.
-template <bool COUNT, bool GEN = false>  // GEN as pair_weight_s
+// PACK: 0 FP32 weights, 1 packed hi/lo pairs (GroupArgs::pack), 2 as g.pack says.
+template <bool COUNT, bool GEN = false, int PACK = 2>  // GEN as pair_weight_s
 __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g, uint32_t *__restrict__ cap,
                                            const unsigned long long *__restrict__ off,
                                            uint32_t *__restrict__ e_idx, float4 *__restrict__ e_w,
@@ -663,19 +664,22 @@ __device__ __forceinline__ void group_item(const GridArgs &a, const GroupArgs &g
                         }
                     }
                 }
+                if (PACK == 1 || (PACK == 2 && g.pack)) {
+                    // the four slots carry {hi(w0, w1), lo(w0, w1), hi(w2, w3), lo(w2, w3)}
+                    uint32_t h01, l01, h23, l23;
+                    tc_split2(wq[0] * g.wscale, wq[1] * g.wscale, g.fmt, h01, l01);
+                    tc_split2(wq[2] * g.wscale, wq[3] * g.wscale, g.fmt, h23, l23);
+                    wq[0] = __uint_as_float(h01);
+                    wq[1] = __uint_as_float(l01);
+                    wq[2] = __uint_as_float(h23);
+                    wq[3] = __uint_as_float(l23);
+                }
             }
             unsigned ball = __ballot_sync(0xffffffffu, any);
             if (any) {
                 unsigned long long pos = eoff + base + __popc(ball & lt);
                 e_idx[pos] = slots ? (uint32_t)((long long)idx + s_shift) : idx;
-                if (g.pack) {
-                    uint32_t h01, l01, h23, l23;
-                    tc_split2(wq[0] * g.wscale, wq[1] * g.wscale, g.fmt, h01, l01);
-                    tc_split2(wq[2] * g.wscale, wq[3] * g.wscale, g.fmt, h23, l23);
-                    reinterpret_cast<uint4 *>(e_w)[pos] = make_uint4(h01, l01, h23, l23);
-                } else {
-                    e_w[pos] = make_float4(wq[0], wq[1], wq[2], wq[3]);
-                }
+                e_w[pos] = make_float4(wq[0], wq[1], wq[2], wq[3]);
             }
             base += __popc(ball);
         }

@@ -350,19 +350,22 @@ __device__ __forceinline__ bool tc_mma(SH &S, const TcJob &J, uint32_t nchunks, 
 // Accumulation segments of the persistent kernels: the tensor cores' FP32
 // accumulation drops low bits of the products it adds (the sums come out low
 // by up to ~2^-24 of the running sum per MMA), so long K loops drift. An
-// item's chunks are accumulated in segments of kTcSegChunks chunks (the last
-// one also takes a remainder of up to kTcSegChunks / 2 chunks), each in a
-// fresh accumulator (the two TMEM halves in turn), and the epilogue adds the
+// item's chunks are accumulated in segments of kTcSegSlots staged slots (the
+// last one also takes a remainder of up to half a segment), each in a fresh
+// accumulator (the two TMEM halves in turn), and the epilogue adds the
 // segments with round-to-nearest FP32 adds (in the cube buffer) before it
 // normalises them.
-constexpr uint32_t kTcSegChunks = 16;
+constexpr uint32_t kTcSegSlots = 1024;
 // The one-item kernels (k_tile_tc, the batch kernel) accumulate an item in one
 // segment: they take tiles of at most this many staged slots (longer ones go to
 // the persistent kernels).
 constexpr uint32_t kTcOneSegmentSlots = 1536;
 
+// segments of an item of `nchunks` chunks of KC slots
+template <uint32_t KC>
 __host__ __device__ constexpr uint32_t tc_segments(uint32_t nchunks) {
-    return nchunks > kTcSegChunks + kTcSegChunks / 2 ? (nchunks + kTcSegChunks / 2 - 1) / kTcSegChunks : 1;
+    constexpr uint32_t seg = kTcSegSlots / KC;  // chunks per segment
+    return nchunks > seg + seg / 2 ? (nchunks + seg / 2 - 1) / seg : 1;
 }
 
 // MMA issue (one thread) of one item in segments; `gs` counts the CTA's
@@ -377,7 +380,7 @@ __device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchun
     const TcStage<Cfg> st{tc_smem_base()};
     const uint32_t idesc =
         AMN ? idesc_f16_mnmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb) : idesc_f16_kmaj_a_mnmaj_b(J.fmt, kTcM, 64 * J.nb);
-    const uint32_t nseg = tc_segments(nchunks);
+    const uint32_t nseg = tc_segments<KC>(nchunks);
     bool ok = true;
     uint32_t k = 0, issued = 0;
     for (uint32_t q = 0; q < nseg; ++q, ++gs) {
@@ -388,7 +391,7 @@ __device__ __forceinline__ void tc_mma_seg(SH &S, const TcJob &J, uint32_t nchun
         }
         tc_fence_after();
         const uint32_t d_tmem = S.tmem + a * 256u;
-        const uint32_t kend = q + 1 == nseg ? nchunks : (q + 1) * kTcSegChunks;
+        const uint32_t kend = q + 1 == nseg ? nchunks : (q + 1) * (kTcSegSlots / KC);
         uint32_t acc = 0;
         for (; k < kend && ok && !S.abort; ++k) {
             const uint32_t g = gk + k, s = g % ST, ph = (g / ST) & 1;
@@ -660,7 +663,7 @@ struct TcPShared {
 // Epilogue warps (128 threads, index eb), one item from accumulator `a`:
 // normalise and store straight from registers (16-byte stores along channels
 // for [pixel][channel] cubes; along pixels for [channel][pixel] cubes).
-template <class SH, bool WSMEM = false>
+template <uint32_t KC, class SH, bool WSMEM = false>
 __device__ __forceinline__ void tc_epilogue_direct(SH &S, const TcJob &J, uint64_t tile, uint32_t cblk,
                                                    uint32_t nchunks, uint32_t il, uint32_t &gse, int eb,
                                                    unsigned long long *timeouts) {
@@ -681,7 +684,7 @@ __device__ __forceinline__ void tc_epilogue_direct(SH &S, const TcJob &J, uint64
     const uint64_t P = (uint64_t)G.nx * G.ny;
     const uint64_t p = (uint64_t)yy * G.nx + xx;
     const float *sc = S.inv_scale[ia];
-    const uint32_t nseg = tc_segments(nchunks);
+    const uint32_t nseg = tc_segments<KC>(nchunks);
     bool store = false;
     float inv = 0.f;
     for (uint32_t q = 0; q < nseg; ++q, ++gse) {
@@ -824,7 +827,7 @@ __device__ __forceinline__ void tc_persist(TcPShared &S, const TcJob &J, uint64_
         } else if (warp < 6) {
             tc_build<Cfg>(S, J, tile, nchunks, gk, tid - 64, timeouts);
         } else {
-            tc_epilogue_direct(S, J, tile, cblk, nchunks, il, gse, tid - 192, timeouts);
+            tc_epilogue_direct<KC>(S, J, tile, cblk, nchunks, il, gse, tid - 192, timeouts);
         }
         gk += nchunks;
     }
@@ -1119,7 +1122,7 @@ __device__ __forceinline__ void tc_persist_weights(TcDShared &S, const TcJob &J,
         } else if (tid < 64 + kTcDBuilders) {
             tc_build_weights<Cfg>(S, J, tile, cblk, U, nchunks, gk, il, tid - 64, timeouts);
         } else {
-            tc_epilogue_direct<TcDShared, true>(S, J, tile, cblk, nchunks, il, gse, tid - (64 + kTcDBuilders),
+            tc_epilogue_direct<KC, TcDShared, true>(S, J, tile, cblk, nchunks, il, gse, tid - (64 + kTcDBuilders),
                                                 timeouts);
         }
         gk += nchunks;
