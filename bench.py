@@ -942,10 +942,11 @@ def main():
             tune = {"config": args.tc_config, "prefetch": args.tc_prefetch, "strip": args.tc_strip,
                     "how": "fixed by --tc-config/--tc-prefetch/--tc-strip (-1: defaults)"}
         else:
+            ctx.autotune_layout(LAY)
             tune = ctx.autotune_ex(field, target, reps=args.tune_reps)
             tune["how"] = ("hcg_autotune_ex: pipeline shape, then prefetch distance, then tile walk; each setting "
-                           "the best of %d timed runs after a warm-up; spread = (slowest - fastest) / fastest of "
-                           "the chosen setting's runs" % args.tune_reps)
+                           "the best of %d timed runs after a warm-up, gridding in the bench's cube layout; "
+                           "spread = (slowest - fastest) / fastest of the chosen setting's runs" % args.tune_reps)
     for _ in range(args.warmup):
         ctx.grid(field, target, cube, wts, layout=LAY, engine=engine)
     ctx.synchronize()
@@ -1145,7 +1146,8 @@ def main():
         h2d = 16 * n_rank + 4 * n_rank * job.nchan  # this rank's inputs
         d2h = 4 * P * job.nchan + 4 * P
         e2e = {"value": work * copies / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "s_per_step": round(t_e2e, 4), "calls_s_untimed_pass": calls, "calls_s_last_timed_step": timed_calls,
+               "s_per_step": round(t_e2e, 4), "s_steps": [round(x, 4) for x in times],
+               "calls_s_untimed_pass": calls, "calls_s_last_timed_step": timed_calls,
                "path": "hcg_field_create + hcg_field_set_spectra%s + hcg_target_from_header + hcg_grid, host pinned"
                        % (" + hcg_field_split_spectra" if tc else "")}
 

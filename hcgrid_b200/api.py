@@ -102,6 +102,7 @@ EXPORTS = {
     "hcg_set_coarsening_factor": ([C.c_void_p, C.c_uint32], C.c_int),
     "hcg_grid_batch": ([C.c_void_p, C.c_uint32, C.c_void_p], C.c_int),
     "hcg_batch_set_shape": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_autotune_layout": ([C.c_void_p, C.c_int], C.c_int),
     "hcg_autotune_batch": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p,
                             C.POINTER(C.c_uint32)], C.c_int),
     "hcg_grid_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
@@ -312,6 +313,10 @@ class Context:
         """Prefetch distance (chunks) and persistent tile walk (strip width in
         tiles, 0: rows) of the tensor-core engine; -1 restores the default."""
         self._check(self.L.hcg_tc_set_pipeline(self.h, channel_class, prefetch, strip))
+
+    def autotune_layout(self, layout: int):
+        """Cube layout the single-job autotuners time (SAMPLE_MAJOR by default)."""
+        self._check(self.L.hcg_autotune_layout(self.h, layout))
 
     def autotune_ex(self, field: "Field", target: "Target", reps: int = 3) -> dict:
         """The full search: shape, then prefetch distance, then tile walk."""

@@ -688,7 +688,7 @@ static hcg_status tune_time(hcg_context *ctx, const hcg_field *field, const hcg_
     best = 3.4e38f;
     worst = 0.f;
     for (int r = 0; r < reps + 1; ++r) {
-        hcg_status st = hcg_grid(ctx, field, target, cube, HCG_LAYOUT_SAMPLE_MAJOR, wts, HCG_MEM_DEVICE, field->xfmt);
+        hcg_status st = hcg_grid(ctx, field, target, cube, ctx->tune_layout, wts, HCG_MEM_DEVICE, field->xfmt);
         if (st != HCG_OK) return st;
         Guard g(ctx);
         CK(ctx, cudaStreamSynchronize(ctx->stream), "autotune");
@@ -699,6 +699,15 @@ static hcg_status tune_time(hcg_context *ctx, const hcg_field *field, const hcg_
             worst = m > worst ? m : worst;
         }
     }
+    return HCG_OK;
+}
+
+hcg_status hcg_autotune_layout(hcg_context *ctx, int layout) {
+    if (!ctx) return HCG_EINVAL;
+    Guard g(ctx);
+    if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
+        return fail(ctx, HCG_EINVAL, "unknown layout");
+    ctx->tune_layout = layout;
     return HCG_OK;
 }
 

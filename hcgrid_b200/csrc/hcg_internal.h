@@ -119,6 +119,7 @@ struct hcg_context {
     int tc_pf[8] = {-1, -1, -1, -1, -1, -1, -1, -1};      // prefetch distance (chunks) per class (-1: default)
     int tc_strip[8] = {-1, -1, -1, -1, -1, -1, -1, -1};   // persistent tile walk per class (-1: default)
     int tc_weights = 0;  // tensor-core weight operands: 0 automatic, 1 from entries, 2 evaluated in the kernel
+    int tune_layout = HCG_LAYOUT_SAMPLE_MAJOR;  // cube layout the single-job autotuner times
     int kb_shape[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // batch tensor-core shape per channel class (-1: default)
     uint32_t factor = 1;  // coarsening factor (hcg_set_coarsening_factor)
     void *batch = nullptr;                          // batch engine state (hcg_batch.cu)

@@ -190,6 +190,12 @@ hcg_status hcg_autotune(hcg_context *ctx, const hcg_field *field, const hcg_targ
  * No reference counterpart. */
 hcg_status hcg_tc_set_pipeline(hcg_context *ctx, int channel_class, int prefetch, int strip);
 
+/* Cube layout the single-job autotuners (hcg_autotune, hcg_autotune_ex) grid
+ * in while they time the pipeline choices (default HCG_LAYOUT_SAMPLE_MAJOR):
+ * the epilogue's stores differ between layouts, so tune in the layout the
+ * application grids in. No reference counterpart. */
+hcg_status hcg_autotune_layout(hcg_context *ctx, int layout);
+
 /* The autotuner's full search (hcg_autotune is its shape part): the
  * pipeline shape (ms_shape, defaults elsewhere), then with that shape the
  * prefetch distance over kTunePrefetch, then the strip width over

@@ -336,10 +336,21 @@ def test_pipeline_shapes_and_autotune(ctx, small):
         best, ms = ctx.autotune(f, t, reps=1)
         print("autotune", best, ms)
         assert best in range(6) and all(m > 0 for m in ms)
+        # timed in channel-plane cubes: the choice is still a valid shape and grids within tolerance
+        ctx.autotune_layout(api.CHANNEL_MAJOR)
+        best, ms = ctx.autotune(f, t, reps=1)
+        print("autotune (channel planes)", best, ms)
+        assert best in range(6) and all(m > 0 for m in ms)
+        c, w = ctx.grid(f, t, engine=api.ENGINE_TC_F16, layout=api.CHANNEL_MAJOR)
+        np.testing.assert_array_equal(w, w32)
+        assert plane_errors(np.ascontiguousarray(c.T), ref) <= TOL[api.ENGINE_TC_F16]
         with pytest.raises(RuntimeError, match="HCG_EINVAL"):
             ctx.tc_set_config(6)
+        with pytest.raises(RuntimeError, match="HCG_EINVAL"):
+            ctx.autotune_layout(7)
     finally:
         ctx.tc_set_config(-1)
+        ctx.autotune_layout(api.SAMPLE_MAJOR)
 
 
 def test_coarse_pixels_many_rings(ctx):
