@@ -33,6 +33,7 @@ sample of the same workload and extrapolates to the whole job.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -837,6 +838,7 @@ def main():
                       "workload": s["config"]["workload"]}
         except Exception as ex:  # reported, not fatal
             served = {"value": None, "error": repr(ex)}
+        gc.collect()  # the served leg's server, fields and buffers are released here, not inside a later timed step
         torch.cuda.empty_cache()
     if args.impl == "reference":
         if rank == 0:
@@ -1093,7 +1095,10 @@ def main():
         cube_h = torch.empty((job.nchan, P) if LAY == api.CHANNEL_MAJOR else (P, job.nchan), dtype=torch.float32,
                              pin_memory=True)
         w_h = torch.empty(P, dtype=torch.float32, pin_memory=True)
+        gc.collect()  # garbage of the earlier legs is not collected inside a timed step
         times = []
+        steps_calls = []  # host time of each call, every timed step
+        free_gb = []  # device memory free after each step (the context's pool keeps what it maps)
         for i in range(args.e2e_steps + 1):
             if dist is not None:
                 dist.barrier()
@@ -1110,12 +1115,14 @@ def main():
             dt = time.perf_counter() - t0
             f2.close()
             t2.close()
+            free_gb.append(round(torch.cuda.mem_get_info(dev)[0] / 1e9, 2))
             if i > 0:
                 times.append(dt)
                 # host time of each call in the timed step (no synchronize between them)
                 timed_calls = {"hcg_field_create": round(ta - t0, 4), "hcg_field_set_spectra": round(tb - ta, 4),
                                "hcg_field_split_spectra": round(tc_ - tb, 4),
                                "hcg_target_from_header + hcg_grid": round(t0 + dt - tc_, 4)}
+                steps_calls.append(list(timed_calls.values()))
         # one more pass, untimed, with a synchronize after each call: where
         # the end-to-end time goes
         calls = {}
@@ -1147,6 +1154,7 @@ def main():
         d2h = 4 * P * job.nchan + 4 * P
         e2e = {"value": work * copies / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "s_per_step": round(t_e2e, 4), "s_steps": [round(x, 4) for x in times],
+               "calls_s_timed_steps": steps_calls, "device_free_gb_after_step": free_gb,
                "calls_s_untimed_pass": calls, "calls_s_last_timed_step": timed_calls,
                "path": "hcg_field_create + hcg_field_set_spectra%s + hcg_target_from_header + hcg_grid, host pinned"
                        % (" + hcg_field_split_spectra" if tc else "")}

@@ -173,8 +173,8 @@ __global__ void __launch_bounds__(256) kb_job_entries(const BatchHdr *__restrict
         jent[j] = H->off_all[jobs[j].grp_base + jobs[j].g.ngroups] - H->off_all[jobs[j].grp_base];
 }
 
-__global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobDesc *__restrict__ jobs,
-                                                        unsigned long long *timeouts) {
+__global__ void __launch_bounds__(kBatchTileThreads) kb_accum(BatchHdr *H, const JobDesc *__restrict__ jobs,
+                                                             unsigned long long *timeouts) {
     if (H->pool_overflow) return;  // entries incomplete: this pass is replayed after the pool grows
     for (;;) {
         unsigned long long it = block_fetch(H, Q_ACC);
@@ -185,9 +185,9 @@ __global__ void __launch_bounds__(kTileThreads) kb_accum(BatchHdr *H, const JobD
         unsigned long long local = it - J.acc_base;
         uint64_t tile = local / J.nslices;
         uint32_t c0 = (uint32_t)(local % J.nslices) * kSlice;
-        tile_accum_item<kBatchAccumBufs, kBatchAccumRows>(J.g, J.T, J.off, J.cnt, H->e_idx, H->e_w, J.wsum, J.spec,
-                                                          J.nchan, J.cstride, J.out, J.ostride, J.wout, tile, c0,
-                                                          timeouts);
+        tile_accum_item<kBatchAccumBufs, kBatchAccumRows, kBatchAccumCpt, kSlice>(
+            J.g, J.T, J.off, J.cnt, H->e_idx, H->e_w, J.wsum, J.spec, J.nchan, J.cstride, J.out, J.ostride, J.wout,
+            tile, c0, timeouts);
     }
 }
 
@@ -333,7 +333,7 @@ static cudaError_t capture(hcg_context *ctx, BatchState &B) {
             kb_job_entries<<<1, 256, 0, s>>>(B.d_hdr, B.d_jobs, B.d_jent);
         } else {
             kb_group<false><<<n * kPersistPerSM, 256, 0, s>>>(B.d_hdr, B.d_jobs);
-            kb_accum<<<n, kTileThreads, smem, s>>>(B.d_hdr, B.d_jobs, &ctx->d_stats->timeouts);
+            kb_accum<<<n, kBatchTileThreads, smem, s>>>(B.d_hdr, B.d_jobs, &ctx->d_stats->timeouts);
             unsigned long long *to = &ctx->d_stats->timeouts, *macs = &ctx->d_stats->tc_macs;
             kb_tc<0><<<n, kTcThreads, KbShape<0>::Cfg::kSmem, s>>>(B.d_hdr, B.d_jobs, to, macs);
             kb_tc<1><<<n, kTcThreads, KbShape<1>::Cfg::kSmem, s>>>(B.d_hdr, B.d_jobs, to, macs);

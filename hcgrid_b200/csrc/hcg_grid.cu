@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(256) k_tile_rings(GridArgs a, GroupArgs g, Til
     tile_rings_item(a, g, T, T.t0 + blockIdx.x);
 }
 
-__global__ void __launch_bounds__(kTileThreads, 2) k_tile_accum(GroupArgs g, TileArgs T,
+__global__ void __launch_bounds__(kTileThreads, kAccumCtas) k_tile_accum(GroupArgs g, TileArgs T,
                                                             const unsigned long long *__restrict__ off,
                                                             const uint32_t *__restrict__ cnt,
                                                             const uint32_t *__restrict__ e_slot,
@@ -98,8 +98,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_tile_accum(GroupArgs g, Til
                                                             unsigned long long *timeouts) {
     // slices of a tile are adjacent blocks: they run together and share the
     // tile's entries through L2
-    tile_accum_item<kAccumBufs, kAccumRows>(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan, cstride, out, ostride,
-                                            wout, T.t0 + blockIdx.y, blockIdx.x * kSlice, timeouts);
+    tile_accum_item<kAccumBufs, kAccumRows, kAccumCpt, kAccumSlice>(g, T, off, cnt, e_slot, e_w, wsum, spec, nchan,
+                                                                    cstride, out, ostride, wout, T.t0 + blockIdx.y,
+                                                                    blockIdx.x * kAccumSlice, timeouts);
 }
 
 // Exclusive scan of n uint32 counts into uint64 offsets (out[n] = total),
@@ -301,7 +302,7 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             return e;
         }
         float *dst = d_cube;
-        const int smem = kAccumBufs * kAccumRows * kSlice * (int)sizeof(float);
+        const int smem = kAccumBufs * kAccumRows * kAccumSlice * (int)sizeof(float);
         static bool attr_set = false;
         if (tiled && !attr_set) {
             if ((e = cudaFuncSetAttribute(k_tile_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
@@ -344,7 +345,8 @@ cudaError_t grid_field(hcg_context *ctx, const hcg_field *f, const hcg_target *t
             } else if (tiled) {
                 TileArgs Tc = T;
                 Tc.t0 = (uint64_t)ch.first * T.ntx;
-                dim3 grid((f->cstride + kSlice - 1) / kSlice, (unsigned)((uint64_t)(ch.second - ch.first) * T.ntx));
+                dim3 grid((f->cstride + kAccumSlice - 1) / kAccumSlice,
+                          (unsigned)((uint64_t)(ch.second - ch.first) * T.ntx));
                 k_tile_accum<<<grid, kTileThreads, smem, s>>>(gc, Tc, off, cnt, e_idx, e_w, wsum, f->d_spec,
                                                                f->nchan, f->cstride, dst, ostride, d_wts,
                                                                &ctx->d_stats->timeouts);

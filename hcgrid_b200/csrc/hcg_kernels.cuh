@@ -1025,15 +1025,22 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
     }
 }
 
-// Channel sums of one tile for one slice of kSlice channels: the tile's
-// union of candidate spectra (slots) is staged in shared memory chunk by
-// chunk; 16 threads per 2x2 group each own 4 channels of the slice, so a
-// staged value is used for 4 pixels. Output [pixel][channel].
-constexpr int kSlice = 64, kTileThreads = (kTileX / 2) * (kTileY / 2) * (kSlice / 4);
-// FP32 staging rings (buffers x rows of kSlice channels): k_tile_accum's
-// 96 KB lets two CTAs share an SM; kb_accum runs one CTA per SM.
-constexpr int kAccumBufs = 4, kAccumRows = 96;
-constexpr int kBatchAccumBufs = 4, kBatchAccumRows = 192;
+// Channel sums of one tile for one slice of SL channels: the tile's union
+// of candidate spectra (slots) is staged in shared memory chunk by chunk;
+// SL / CPT threads per 2x2 group each own CPT channels of the slice, so a
+// staged value is used for 4 pixels. A CTA has one thread per (group,
+// channel part): tile_threads(CPT, SL).
+constexpr int kSlice = 64;  // the batch engine's slice
+constexpr int tile_threads(int cpt, int sl) { return (kTileX / 2) * (kTileY / 2) * (sl / cpt); }
+// FP32 staging rings (buffers x rows of a slice), channels per thread and
+// slice width. k_tile_accum: 16 threads per 2x2 group, 8 channels each, over
+// 128 channels (one 512-thread CTA per SM, a 192 KB ring), so a group's
+// entries are loaded once per 128 channels; kb_accum: 16 threads per group,
+// 4 channels each, over 64 channels.
+constexpr int kAccumBufs = 4, kAccumRows = 96, kAccumCpt = 8, kAccumSlice = 128, kAccumCtas = 1;
+constexpr int kBatchAccumBufs = 4, kBatchAccumRows = 192, kBatchAccumCpt = 4;
+constexpr int kTileThreads = tile_threads(kAccumCpt, kAccumSlice);
+constexpr int kBatchTileThreads = tile_threads(kBatchAccumCpt, kSlice);
 
 // 16-byte asynchronous global -> shared copy (zero-filled when !valid).
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
@@ -1060,7 +1067,7 @@ constexpr uint64_t kTileWaitNs = 1000000000ull;  // bound of the FP32 staging ri
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Channel sums of one tile for one slice of kSlice channels. The tile's
+// Channel sums of one tile for one slice of SL channels. The tile's
 // union of candidate spectra (its slots) is staged in shared memory in
 // chunks of CH rows through a ring of NB buffers: every thread copies its
 // share of a chunk with cp.async and arrives on the chunk's `full` barrier
@@ -1068,12 +1075,13 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // when it has summed the chunk, and the chunk NB - 2 ahead is staged into a
 // buffer only once every warp is done with that buffer's previous chunk. So a
 // warp whose groups have many entries in one chunk holds the others back only
-// two chunks later, not at every chunk. 16 threads per 2x2 group each own 4
-// channels of the slice, so a staged value feeds 4 pixels. Block-collective
-// (every thread of a kTileThreads block; NB * CH * kSlice floats of dynamic
-// shared memory). A barrier wait that runs out (1 s) is counted in
-// `timeouts` and the item winds down.
-template <int NB, int CH>
+// two chunks later, not at every chunk. SL / CPT threads per 2x2 group
+// each own CPT channels of the slice (float4 q, q + SL / CPT, ... of a
+// row, so the group's loads of one row are contiguous), and a staged value
+// feeds 4 pixels. Block-collective (every thread of a tile_threads(CPT, SL)
+// block; NB * CH * SL floats of dynamic shared memory). A barrier wait
+// that runs out (1 s) is counted in `timeouts` and the item winds down.
+template <int NB, int CH, int CPT, int SL>
 __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileArgs &T,
                                                 const unsigned long long *__restrict__ off,
                                                 const uint32_t *__restrict__ cnt,
@@ -1084,20 +1092,21 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
                                                 float *__restrict__ wout, uint64_t tile, uint32_t c0,
                                                 unsigned long long *timeouts) {
     static_assert(NB >= 3, "the chunk NB - 2 ahead is staged while one is summed");
-    constexpr int kWarps = kTileThreads / 32;
-    extern __shared__ float4 s_spec[];  // [NB][CH][kSlice / 4]
+    static_assert(CPT % 4 == 0 && SL % CPT == 0, "whole float4 channel quads per thread");
+    constexpr int kThreads = tile_threads(CPT, SL), kWarps = kThreads / 32, kTpg = SL / CPT, kQ = CPT / 4;
+    extern __shared__ float4 s_spec[];  // [NB][CH][SL / 4]
     __shared__ uint32_t s_ulo[kTileMaxRings], s_base[kTileMaxRings + 1];
     __shared__ uint64_t s_full[NB], s_empty[NB];
     __shared__ volatile int s_abort;
     __syncthreads();  // shared state of a previous item is no longer read
-    const int tid = threadIdx.x, q = tid & (kSlice / 4 - 1), gl = tid / (kSlice / 4);
+    const int tid = threadIdx.x, q = tid % kTpg, gl = tid / kTpg;
     const int nrt = T.nr[tile];
     const uint32_t U = T.U[tile];
-    for (int j = tid; j < nrt; j += kTileThreads) s_ulo[j] = T.ulo[tile * kTileMaxRings + j];
-    for (int j = tid; j <= nrt; j += kTileThreads) s_base[j] = T.base[tile * (kTileMaxRings + 1) + j];
+    for (int j = tid; j < nrt; j += kThreads) s_ulo[j] = T.ulo[tile * kTileMaxRings + j];
+    for (int j = tid; j <= nrt; j += kThreads) s_base[j] = T.base[tile * (kTileMaxRings + 1) + j];
     if (tid == 0) {
         for (int b = 0; b < NB; ++b) {
-            sm100::mbar_init(&s_full[b], kTileThreads);
+            sm100::mbar_init(&s_full[b], kThreads);
             sm100::mbar_init(&s_empty[b], kWarps);
         }
         s_abort = 0;
@@ -1112,28 +1121,41 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
         e = off[grp] - g.ebase;
         e_end = e + cnt[grp];
     }
-    float4 acc[4];
+    float4 acc[4][kQ];  // [pixel of the group][channel quad of the thread]
 #pragma unroll
-    for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int j = 0; j < kQ; ++j) acc[k][j] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
-    // stage rows [cs, min(U, cs + CH)) into buffer b (16 threads per row); the
-    // thread's arrival on full[b] completes when its copies have landed
+    // stage rows [cs, min(U, cs + CH)) into buffer b: each warp takes kRows
+    // consecutive rows, its lane r finds row r's sample (the ring j with
+    // base[j] <= slot < base[j+1]) once, and the warp's 16-byte copies take
+    // their row's sample from that lane; the thread's arrival on full[b]
+    // completes when its copies have landed
+    constexpr uint32_t kRows = (CH + kWarps - 1) / kWarps, kParts = SL / 4;
+    static_assert(kRows <= 32 && 32 % kParts == 0, "one lane per staged row of a warp, whole rows per pass");
+    const uint32_t lane = tid & 31, warp = tid >> 5;
+    const uint32_t pc = c0 + 4 * (lane % kParts);  // the channels of this lane's copies (32 % kParts == 0)
+    const bool pok = pc < cstride;
     auto stage = [&](uint32_t cs, int b) {
-        const uint32_t ce = min(U, cs + CH);
-        float4 *dst = s_spec + (size_t)b * CH * (kSlice / 4);
-        for (uint32_t i = tid; i < (ce - cs) * (kSlice / 4); i += kTileThreads) {
-            uint32_t row = i / (kSlice / 4), part = i % (kSlice / 4);
-            uint32_t slot = cs + row;
-            int lo = 0, hi = nrt;  // ring j with base[j] <= slot < base[j+1]
+        const uint32_t ce = min(U, cs + CH), r0 = cs + warp * kRows;
+        const uint32_t nr = r0 < ce ? min(kRows, ce - r0) : 0;
+        uint32_t idx = 0;
+        if (lane < nr) {
+            const uint32_t slot = r0 + lane;
+            int lo = 0, hi = nrt;
             while (hi - lo > 1) {
                 int mid = (lo + hi) >> 1;
                 if (s_base[mid] <= slot) lo = mid; else hi = mid;
             }
-            uint32_t idx = s_ulo[lo] + (slot - s_base[lo]);
-            uint32_t c = c0 + 4 * part;
-            bool ok = c < cstride;
-            const float *src = spec + (uint64_t)idx * cstride + (ok ? c : 0);
-            cp_async16(dst + row * (kSlice / 4) + part, src, ok);
+            idx = s_ulo[lo] + (slot - s_base[lo]);
+        }
+        float4 *dst = s_spec + ((size_t)b * CH + (r0 - cs)) * kParts + lane % kParts;
+        const float *src0 = spec + (pok ? pc : 0);
+        for (uint32_t i0 = 0; i0 < nr * kParts; i0 += 32) {  // warp-uniform trip count
+            const uint32_t row = (i0 + lane) / kParts;
+            const uint32_t ri = __shfl_sync(0xffffffffu, idx, row & 31);
+            if (i0 + lane < nr * kParts) cp_async16(dst + row * kParts, src0 + (uint64_t)ri * cstride, pok);
         }
         cp_async_arrive(&s_full[b]);
     };
@@ -1158,7 +1180,21 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
             s_abort = 1;
         }
         if (s_abort) break;
-        const float4 *buf = s_spec + (size_t)b * CH * (kSlice / 4);
+        const float4 *buf = s_spec + (size_t)b * CH * (SL / 4) + q;
+        auto fma_entry = [&](uint32_t sl, const float4 &w) {
+            const float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int j = 0; j < kQ; ++j) {
+                const float4 sv = buf[(sl - cs) * (SL / 4) + j * kTpg];
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    acc[kk][j].x = fmaf(wv[kk], sv.x, acc[kk][j].x);
+                    acc[kk][j].y = fmaf(wv[kk], sv.y, acc[kk][j].y);
+                    acc[kk][j].z = fmaf(wv[kk], sv.z, acc[kk][j].z);
+                    acc[kk][j].w = fmaf(wv[kk], sv.w, acc[kk][j].w);
+                }
+            }
+        };
         // entries kSet at a time from two register sets in turn: the next set
         // is loaded while one is summed, and no set is copied
         constexpr int kSet = 3;
@@ -1171,17 +1207,7 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
         };
         auto sum = [&](const uint32_t *sl, const float4 *w) {
 #pragma unroll
-            for (int u = 0; u < kSet; ++u) {
-                const float4 sv = buf[(sl[u] - cs) * (kSlice / 4) + q];
-                const float wv[4] = {w[u].x, w[u].y, w[u].z, w[u].w};
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    acc[kk].x = fmaf(wv[kk], sv.x, acc[kk].x);
-                    acc[kk].y = fmaf(wv[kk], sv.y, acc[kk].y);
-                    acc[kk].z = fmaf(wv[kk], sv.z, acc[kk].z);
-                    acc[kk].w = fmaf(wv[kk], sv.w, acc[kk].w);
-                }
-            }
+            for (int u = 0; u < kSet; ++u) fma_entry(sl[u], w[u]);
         };
         if (e + kSet <= e_end) {
             uint32_t sa[kSet], sb[kSet];
@@ -1205,23 +1231,13 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
         for (; e < e_end; ++e) {
             uint32_t sl = __ldg(e_slot + e);
             if (sl >= ce) break;
-            const float4 w = __ldg(e_w + e);
-            const float4 sv = buf[(sl - cs) * (kSlice / 4) + q];
-            const float wv[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                acc[kk].x = fmaf(wv[kk], sv.x, acc[kk].x);
-                acc[kk].y = fmaf(wv[kk], sv.y, acc[kk].y);
-                acc[kk].z = fmaf(wv[kk], sv.z, acc[kk].z);
-                acc[kk].w = fmaf(wv[kk], sv.w, acc[kk].w);
-            }
+            fma_entry(sl, __ldg(e_w + e));
         }
         __syncwarp();
         if ((tid & 31) == 0) sm100::mbar_arrive(&s_empty[b]);  // this warp is done with buffer b
     }
     cp_async_wait_all();  // no copy into the ring outlives the item
     if (!gvalid) return;
-    const uint32_t c = c0 + 4 * q;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         uint32_t xx = 2 * gxi + (k & 1), yy = 2 * gyi + (k >> 1);
@@ -1230,8 +1246,11 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
         double ws = wsum[p];
         float inv = (float)(1.0 / ws);
         if (wout && c0 == 0 && q == 0) wout[p] = (float)ws;
-        const float v[4] = {acc[k].x * inv, acc[k].y * inv, acc[k].z * inv, acc[k].w * inv};
-        store_cube4(out, ostride, (uint64_t)g.nx * g.ny, p, c, nchan, v);
+#pragma unroll
+        for (int j = 0; j < kQ; ++j) {
+            const float v[4] = {acc[k][j].x * inv, acc[k][j].y * inv, acc[k][j].z * inv, acc[k][j].w * inv};
+            store_cube4(out, ostride, (uint64_t)g.nx * g.ny, p, c0 + 4 * (q + j * kTpg), nchan, v);
+        }
     }
 }
 
