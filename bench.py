@@ -1095,7 +1095,11 @@ def main():
         cube_h = torch.empty((job.nchan, P) if LAY == api.CHANNEL_MAJOR else (P, job.nchan), dtype=torch.float32,
                              pin_memory=True)
         w_h = torch.empty(P, dtype=torch.float32, pin_memory=True)
-        gc.collect()  # garbage of the earlier legs is not collected inside a timed step
+        # garbage of the earlier legs is collected now, and the objects that
+        # survive are left out of later collections, so that no collection
+        # of the harness's own objects runs inside a timed step
+        gc.collect()
+        gc.freeze()
         times = []
         steps_calls = []  # host time of each call, every timed step
         free_gb = []  # device memory free after each step (the context's pool keeps what it maps)

@@ -1034,10 +1034,13 @@ constexpr int kSlice = 64;  // the batch engine's slice
 constexpr int tile_threads(int cpt, int sl) { return (kTileX / 2) * (kTileY / 2) * (sl / cpt); }
 // FP32 staging rings (buffers x rows of a slice), channels per thread and
 // slice width. k_tile_accum: 16 threads per 2x2 group, 8 channels each, over
-// 128 channels (one 512-thread CTA per SM, a 192 KB ring), so a group's
-// entries are loaded once per 128 channels; kb_accum: 16 threads per group,
-// 4 channels each, over 64 channels.
-constexpr int kAccumBufs = 4, kAccumRows = 96, kAccumCpt = 8, kAccumSlice = 128, kAccumCtas = 1;
+// 128 channels (one 512-thread CTA per SM), so a group's entries are loaded
+// once per 128 channels; its ring is three 144-row buffers (216 KB): long
+// chunks leave the warps a chunk of slack between barrier waits (measured on
+// 4M x 1,024 -> 1200^2: 96-row chunks x 4 buffers 34.3 ms, 128 x 3 31.8 ms,
+// 144 x 3 30.5 ms). kb_accum: 16 threads per group, 4 channels each, over
+// 64 channels.
+constexpr int kAccumBufs = 3, kAccumRows = 144, kAccumCpt = 8, kAccumSlice = 128, kAccumCtas = 1;
 constexpr int kBatchAccumBufs = 4, kBatchAccumRows = 192, kBatchAccumCpt = 4;
 constexpr int kTileThreads = tile_threads(kAccumCpt, kAccumSlice);
 constexpr int kBatchTileThreads = tile_threads(kBatchAccumCpt, kSlice);
