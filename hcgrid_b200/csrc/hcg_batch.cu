@@ -184,8 +184,8 @@ __global__ void __launch_bounds__(kBatchTileThreads) kb_accum(BatchHdr *H, const
         if (J.skip) continue;
         unsigned long long local = it - J.acc_base;
         uint64_t tile = local / J.nslices;
-        uint32_t c0 = (uint32_t)(local % J.nslices) * kSlice;
-        tile_accum_item<kBatchAccumBufs, kBatchAccumRows, kBatchAccumCpt, kSlice>(
+        uint32_t c0 = (uint32_t)(local % J.nslices) * kBatchSlice;
+        tile_accum_item<kBatchAccumBufs, kBatchAccumRows, kBatchAccumCpt, kBatchSlice>(
             J.g, J.T, J.off, J.cnt, H->e_idx, H->e_w, J.wsum, J.spec, J.nchan, J.cstride, J.out, J.ostride, J.wout,
             tile, c0, timeouts);
     }
@@ -309,7 +309,7 @@ static cudaError_t grow(BatchState &B, int slot, size_t bytes, cudaStream_t s, v
 
 static cudaError_t capture(hcg_context *ctx, BatchState &B) {
     cudaStream_t s = ctx->stream;
-    const int smem = kBatchAccumBufs * kBatchAccumRows * kSlice * (int)sizeof(float);
+    const int smem = kBatchAccumBufs * kBatchAccumRows * kBatchSlice * (int)sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(kb_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     if ((e = tc_set_smem((const void *)kb_tc<0>, KbShape<0>::Cfg::kSmem)) != cudaSuccess ||
@@ -453,7 +453,7 @@ cudaError_t grid_batch(hcg_context *ctx, uint32_t njobs, const hcg_job *jobs, st
         d.T.nty = (t->ny + kTileY - 1) / kTileY;
         uint64_t ntiles = (f->nchan > 1) ? (uint64_t)d.T.ntx * d.T.nty : 0;
         const bool tc = batch_uses_tc(f);
-        d.nslices = tc ? 0 : (f->cstride + kSlice - 1) / kSlice;
+        d.nslices = tc ? 0 : (f->cstride + kBatchSlice - 1) / kBatchSlice;
         if (tc) {
             d.T.pad = 8;  // ring runs as boxes of 8 samples
             d.tc_shape = (uint32_t)kb_shape_of(ctx, f);

@@ -1030,20 +1030,20 @@ __device__ __forceinline__ void tile_rings_item(const GridArgs &a, const GroupAr
 // SL / CPT threads per 2x2 group each own CPT channels of the slice, so a
 // staged value is used for 4 pixels. A CTA has one thread per (group,
 // channel part): tile_threads(CPT, SL).
-constexpr int kSlice = 64;  // the batch engine's slice
 constexpr int tile_threads(int cpt, int sl) { return (kTileX / 2) * (kTileY / 2) * (sl / cpt); }
 // FP32 staging rings (buffers x rows of a slice), channels per thread and
-// slice width. k_tile_accum: 16 threads per 2x2 group, 8 channels each, over
-// 128 channels (one 512-thread CTA per SM), so a group's entries are loaded
-// once per 128 channels; its ring is three 144-row buffers (216 KB): long
-// chunks leave the warps a chunk of slack between barrier waits (measured on
-// 4M x 1,024 -> 1200^2: 96-row chunks x 4 buffers 34.3 ms, 128 x 3 31.8 ms,
-// 144 x 3 30.5 ms). kb_accum: 16 threads per group, 4 channels each, over
-// 64 channels.
+// slice width, the same for k_tile_accum and the batch engine's kb_accum:
+// 16 threads per 2x2 group, 8 channels each, over 128 channels (one
+// 512-thread CTA per SM), so a group's entries are loaded once per 128
+// channels; the ring is three 144-row buffers (216 KB): long chunks leave
+// the warps a chunk of slack between barrier waits (measured on 4M x 1,024
+// -> 1200^2: 96-row chunks x 4 buffers 34.3 ms, 128 x 3 31.8 ms, 144 x 3
+// 30.5 ms).
 constexpr int kAccumBufs = 3, kAccumRows = 144, kAccumCpt = 8, kAccumSlice = 128, kAccumCtas = 1;
-constexpr int kBatchAccumBufs = 4, kBatchAccumRows = 192, kBatchAccumCpt = 4;
+constexpr int kBatchAccumBufs = kAccumBufs, kBatchAccumRows = kAccumRows, kBatchAccumCpt = kAccumCpt,
+              kBatchSlice = kAccumSlice;
 constexpr int kTileThreads = tile_threads(kAccumCpt, kAccumSlice);
-constexpr int kBatchTileThreads = tile_threads(kBatchAccumCpt, kSlice);
+constexpr int kBatchTileThreads = tile_threads(kBatchAccumCpt, kBatchSlice);
 
 // 16-byte asynchronous global -> shared copy (zero-filled when !valid).
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
@@ -1200,12 +1200,20 @@ __device__ __forceinline__ void tile_accum_item(const GroupArgs &g, const TileAr
         };
         // entries kSet at a time from two register sets in turn: the next set
         // is loaded while one is summed, and no set is copied
-        constexpr int kSet = 3;
+        // (one lane of the group also asks L1 for the entries kPrefetch ahead,
+        // which the registers cannot hold: measured 29.1 against 30.5 ms of
+        // channel sums on 4M x 1,024 -> 1200^2)
+        constexpr int kSet = 3, kPrefetch = 24;
         auto load = [&](uint32_t *sl, float4 *w, uint64_t at) {
 #pragma unroll
             for (int u = 0; u < kSet; ++u) {
                 sl[u] = __ldg(e_slot + at + u);
                 w[u] = __ldg(e_w + at + u);
+            }
+            if (q == 0) {  // the group's last entry at most
+                const uint64_t pa = min(at + kPrefetch, e_end - 1);
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(e_w + pa));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(e_slot + pa));
             }
         };
         auto sum = [&](const uint32_t *sl, const float4 *w) {
