@@ -10,9 +10,11 @@ FP64 weights, channel sums, normalisation) over the resident field of the
 workload: config 2 = 4,000,000 raster-scan samples x 1,024 float32 channels
 onto a 1200x1200 SIN grid, GAUSS1D FWHM 180" (seeded synthetic data, see
 hcgrid_b200/synth.py). `value` is gridded sample-channels/s with inputs
-resident in HBM; `e2e` repeats the metric through the C ABI from host
-buffers (field creation with the on-device sort, spectra upload, gridding,
-cube download). Inputs are larger than L2 (16 GB of spectra), so no flush.
+resident in HBM; `e2e` repeats the metric through the C ABI from pinned
+host buffers (field creation with the on-device sort, then hcg_grid_planes:
+the spectra as channel planes uploaded, split and gridded block by block with
+the cube downloaded as blocks finish). Inputs are larger than L2 (16 GB of
+spectra), so no flush.
 
 At N=1 the config-2 line also carries `served_config5`: the served form
 (config 5, a stream of J gridding requests through hcg_server, timed against
@@ -79,6 +81,9 @@ def parse():
                     help="config2 at N=1: also run the served form (config5) on this many requests and report it "
                          "under 'served_config5' (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--plane-block", type=int, default=0,
+                    help="end to end: channels per block of hcg_grid_planes (a multiple of 64; 0: the "
+                         "library's 128)")
     ap.add_argument("--shard", default="bands", choices=["bands", "replicas"],
                     help="N>1: split the one job into Dec bands of target rows, one per rank, gathered to rank 0 "
                          "over NCCL (strong scaling), or grid a replica of the whole job on every rank (weak)")
@@ -914,8 +919,13 @@ def main():
         vals = S[:, torch.from_numpy(chans).to(dev)].double().cpu().numpy()
         check = {"side": side, "chans": chans, "sub": subpix, "vals": vals,
                  "sub_d": torch.from_numpy(subpix).to(dev), "chans_d": torch.from_numpy(chans).to(dev)}
-    S_host = None
+    S_host = planes_host = None
     if args.e2e_steps > 0:
+        # the host spectra of the end-to-end leg: channel planes [nchan][n] in
+        # input sample order (the reference's h_data[channel][sample]) for
+        # hcg_grid_planes, and sample rows [n][nchan] for the per-call path
+        planes_host = torch.empty((S.shape[1], S.shape[0]), dtype=torch.float32, pin_memory=True)
+        planes_host.copy_(S.t())
         S_host = torch.empty(tuple(S.shape), dtype=torch.float32, pin_memory=True)
         S_host.copy_(S)
     del S  # the field holds its own (sorted) copy
@@ -1109,28 +1119,19 @@ def main():
             t0 = time.perf_counter()
             f2 = ctx.field(lon_h, lat_h)
             ta = time.perf_counter()
-            f2.set_spectra(S_host)
-            tb = time.perf_counter()
-            if tc:
-                f2.split_spectra(engine, keep_fp32=False)
-            tc_ = time.perf_counter()
             t2 = make_target()
-            ctx.grid(f2, t2, cube_h, w_h, layout=LAY, engine=engine)
+            ctx.grid_planes(f2, t2, planes_host, cube_h, w_h, layout=LAY, engine=engine, block=args.plane_block)
             dt = time.perf_counter() - t0
             f2.close()
             t2.close()
             free_gb.append(round(torch.cuda.mem_get_info(dev)[0] / 1e9, 2))
             if i > 0:
                 times.append(dt)
-                # host time of each call in the timed step (no synchronize between them)
-                timed_calls = {"hcg_field_create": round(ta - t0, 4), "hcg_field_set_spectra": round(tb - ta, 4),
-                               "hcg_field_split_spectra": round(tc_ - tb, 4),
-                               "hcg_target_from_header + hcg_grid": round(t0 + dt - tc_, 4)}
-                steps_calls.append(list(timed_calls.values()))
-        # one more pass, untimed, with a synchronize after each call: where
-        # the end-to-end time goes
+                steps_calls.append([round(ta - t0, 4), round(t0 + dt - ta, 4)])
+        # the per-call path once, untimed, with a synchronize after each call
         calls = {}
         t0 = time.perf_counter()
+        t_start = t0
 
         def mark(name):
             nonlocal t0
@@ -1150,18 +1151,23 @@ def main():
         mark("hcg_target_from_header")
         ctx.grid(f2, t2, cube_h, w_h, layout=LAY, engine=engine)
         mark("hcg_grid")
+        per_call_s = round(time.perf_counter() - t_start, 4)
         f2.close()
         t2.close()
-        mark("destroy")
         t_e2e = reduce_max(torch, dist, statistics.mean(times))
         h2d = 16 * n_rank + 4 * n_rank * job.nchan  # this rank's inputs
         d2h = 4 * P * job.nchan + 4 * P
         e2e = {"value": work * copies / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "s_per_step": round(t_e2e, 4), "s_steps": [round(x, 4) for x in times],
                "calls_s_timed_steps": steps_calls, "device_free_gb_after_step": free_gb,
-               "calls_s_untimed_pass": calls, "calls_s_last_timed_step": timed_calls,
-               "path": "hcg_field_create + hcg_field_set_spectra%s + hcg_target_from_header + hcg_grid, host pinned"
-                       % (" + hcg_field_split_spectra" if tc else "")}
+               "path": "hcg_field_create (sort) + hcg_target_from_header + hcg_grid_planes (channel planes in "
+                       "pinned host memory, %d-channel blocks: upload, split, gridding and cube download "
+                       "overlapped)" % (args.plane_block or 128),
+               "calls_s_timed_steps_what": "[hcg_field_create, hcg_target_from_header + hcg_grid_planes]",
+               "per_call_path": {"s": per_call_s, "calls_s": calls,
+                                 "path": "hcg_field_create + hcg_field_set_spectra (sample rows)%s + "
+                                         "hcg_target_from_header + hcg_grid, one untimed pass with a synchronize "
+                                         "after each call" % (" + hcg_field_split_spectra" if tc else "")}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -95,6 +95,8 @@ EXPORTS = {
     "hcg_header_coords": ([C.c_char_p, C.c_size_t, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p,
                            C.c_void_p], C.c_int),
     "hcg_grid": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "hcg_grid_planes": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int,
+                         C.c_void_p, C.c_int, C.c_uint32], C.c_int),
     "hcg_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "hcg_synchronize": ([C.c_void_p], C.c_int),
     "hcg_context_trim": ([C.c_void_p], C.c_int),
@@ -286,6 +288,27 @@ class Context:
         cp, mem = _ptr(cube)
         wp, _ = _ptr(weights)
         self._check(self.L.hcg_grid(self.h, field.h, target.h, cp, layout, wp, mem, engine))
+        return cube, weights
+
+    def grid_planes(self, geometry: "Field", target: "Target", planes, cube=None, weights=None,
+                    layout: int = CHANNEL_MAJOR, engine: int = ENGINE_AUTO, block: int = 0):
+        """Host channel planes [nchan, n] in, host cube out, pipelined in
+        blocks of channels (hcg_grid_planes). Without `cube`, returns numpy
+        arrays (cube [nchan, npix] or [npix, nchan], weights [npix])."""
+        if hasattr(planes, "is_cuda") and planes.is_cuda:
+            raise ValueError("planes must be host memory")
+        nchan = planes.shape[0]
+        npix = target.nx * target.ny
+        shape = (npix, nchan) if layout == SAMPLE_MAJOR else (nchan, npix)
+        if cube is None:
+            cube = np.empty(shape, np.float32)
+            weights = np.empty(npix, np.float32)
+        pp, _ = _ptr(planes)
+        cp, cmem = _ptr(cube)
+        wp, wmem = _ptr(weights)
+        if cmem != MEM_HOST or (weights is not None and wmem != MEM_HOST):
+            raise ValueError("cube and weights must be host memory")
+        self._check(self.L.hcg_grid_planes(self.h, geometry.h, target.h, pp, nchan, cp, layout, wp, engine, block))
         return cube, weights
 
     def stats(self) -> Stats:

@@ -648,6 +648,129 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
     return grid_checked(ctx, field, target, cube, layout, weights_out, mem, engine);
 }
 
+hcg_status hcg_grid_planes(hcg_context *ctx, const hcg_field *geometry, const hcg_target *target,
+                           const float *planes, uint32_t nchan, float *cube, int layout, float *weights_out,
+                           int engine, uint32_t block) {
+    if (!ctx || !geometry || !target || !planes || !cube || nchan == 0) return HCG_EINVAL;
+    Guard g(ctx);
+    if (!ctx->prepared) return fail(ctx, HCG_ESTATE, "hcg_prepare_grid_kernel must come first");
+    if (geometry->ctx->device != ctx->device || target->ctx->device != ctx->device)
+        return fail(ctx, HCG_EINVAL, "field or target lives on another device than the context");
+    if (layout != HCG_LAYOUT_SAMPLE_MAJOR && layout != HCG_LAYOUT_CHANNEL_MAJOR)
+        return fail(ctx, HCG_EINVAL, "unknown layout");
+    if (block == 0) block = kPlaneBlock;
+    if (block % 64) return fail(ctx, HCG_EINVAL, "block must be a multiple of 64 channels");
+    if (engine == HCG_ENGINE_AUTO) engine = nchan > 1 ? HCG_ENGINE_TC_F16 : HCG_ENGINE_FP32;
+    if (engine < HCG_ENGINE_FP32 || engine > HCG_ENGINE_TC_F16) return fail(ctx, HCG_EINVAL, "unknown engine");
+    cudaStream_t s = ctx->stream, cs = ctx->copy_stream, us = nullptr, dl = nullptr;
+    if (!cs) return fail(ctx, HCG_EDEVICE, "the context has no copy stream");
+    const uint64_t n = geometry->n;
+    const size_t P = (size_t)target->nx * target->ny;
+    const uint32_t nblk = (nchan + block - 1) / block;
+    // events: chunk copied (2), staging buffer free (2), block uploaded (2),
+    // block cube downloaded (2), block gridded, buffers ready
+    cudaEvent_t ev[10] = {};
+    cudaEvent_t *ev_copied = ev, *ev_free = ev + 2, *ev_up = ev + 4, *ev_dl = ev + 6;
+    cudaEvent_t &ev_grid = ev[8], &ev_ready = ev[9];
+    hcg_field *fb[2] = {nullptr, nullptr};
+    uint64_t chunks = 0;
+    const char *where = "plane pipeline";
+    cudaError_t e = cudaSuccess;
+    auto run = [&]() -> hcg_status {
+        // earlier uploads on the copy stream have ended before its staging buffers are reused
+        if ((e = cudaStreamSynchronize(cs)) != cudaSuccess) return cuda_fail(ctx, e, where);
+        if ((e = cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&dl, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(ctx, e, where);
+        for (auto &x : ev)
+            if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(ctx, e, where);
+        // staging (two chunks of whole planes), two block cubes, the weights
+        const uint64_t per = std::max<uint64_t>(1, kUploadChunk / std::max<uint64_t>(1, n * 4));
+        const uint64_t stage_bytes = std::min<uint64_t>(per, block) * n * 4;
+        float *stage[2], *dcube[2], *dw = nullptr;
+        for (int b = 0; b < 2; ++b) {
+            stage[b] = (float *)ctx->scratch.get(19 + b, stage_bytes, s, e);
+            dcube[b] = (float *)ctx->scratch.get(22 + b, (size_t)std::min(block, nchan) * P * sizeof(float), s, e);
+        }
+        if (weights_out) dw = (float *)ctx->scratch.get(24, P * sizeof(float), s, e);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "plane pipeline buffers");
+        if ((e = cudaEventRecord(ev_ready, s)) != cudaSuccess || (e = cudaStreamWaitEvent(cs, ev_ready, 0)) ||
+            (e = cudaStreamWaitEvent(us, ev_ready, 0)) || (e = cudaStreamWaitEvent(dl, ev_ready, 0)))
+            return cuda_fail(ctx, e, where);
+        for (int b = 0; b < 2 && b < (int)nblk; ++b) {
+            fb[b] = new (std::nothrow) hcg_field(*geometry);
+            if (!fb[b]) return fail(ctx, HCG_ENOMEM, "host allocation");
+            fb[b]->d_spec = nullptr;
+            fb[b]->nchan = fb[b]->cstride = 0;
+            fb[b]->d_xhi = fb[b]->d_xlo = nullptr;
+            fb[b]->d_xinv = nullptr;
+            fb[b]->xcpad = 0;
+            fb[b]->xfmt = 0;
+            fb[b]->xnonfinite = 0;
+            ++*fb[b]->geom_refs;
+        }
+        auto upload = [&](uint32_t b) -> cudaError_t {
+            const uint32_t c0 = b * block, nb = std::min(block, nchan - c0);
+            cudaError_t u = upload_plane_block(ctx, fb[b & 1], planes + (size_t)c0 * n, nb, cs, us, stage, stage_bytes,
+                                               ev_copied, ev_free, chunks);
+            return u != cudaSuccess ? u : cudaEventRecord(ev_up[b & 1], us);
+        };
+        if ((e = upload(0)) != cudaSuccess) return cuda_fail(ctx, e, "spectra upload");
+        for (uint32_t b = 0; b < nblk; ++b) {
+            // the next block's copies go out before this block's gridding holds the host
+            if (b + 1 < nblk && (e = upload(b + 1)) != cudaSuccess) return cuda_fail(ctx, e, "spectra upload");
+            const uint32_t c0 = b * block, nb = std::min(block, nchan - c0);
+            hcg_field *f = fb[b & 1];
+            const bool tc = engine != HCG_ENGINE_FP32 && nb > 1;
+            if ((e = cudaStreamWaitEvent(s, ev_up[b & 1], 0)) != cudaSuccess) return cuda_fail(ctx, e, where);
+            if (tc) {
+                std::string why;
+                if ((e = split_spectra(ctx, f, engine, why)) != cudaSuccess) return cuda_fail(ctx, e, "spectra split", why);
+                cudaFreeAsync(f->d_spec, s);
+                f->d_spec = nullptr;
+            }
+            if (b >= 2 && (e = cudaStreamWaitEvent(s, ev_dl[b & 1], 0)) != cudaSuccess) return cuda_fail(ctx, e, where);
+            hcg_status st = grid_checked(ctx, f, target, dcube[b & 1], layout, b == 0 ? dw : nullptr, HCG_MEM_DEVICE,
+                                         tc ? engine : HCG_ENGINE_FP32);
+            if (st != HCG_OK) return st;
+            free_split(f, s);
+            if (f->d_spec) cudaFreeAsync(f->d_spec, s);
+            f->d_spec = nullptr;
+            if ((e = cudaEventRecord(ev_grid, s)) != cudaSuccess || (e = cudaStreamWaitEvent(dl, ev_grid, 0)))
+                return cuda_fail(ctx, e, where);
+            if (layout == HCG_LAYOUT_CHANNEL_MAJOR)
+                e = cudaMemcpyAsync(cube + (size_t)c0 * P, dcube[b & 1], (size_t)nb * P * sizeof(float),
+                                    cudaMemcpyDeviceToHost, dl);
+            else
+                e = cudaMemcpy2DAsync(cube + c0, (size_t)nchan * sizeof(float), dcube[b & 1], (size_t)nb * sizeof(float),
+                                      (size_t)nb * sizeof(float), P, cudaMemcpyDeviceToHost, dl);
+            if (e == cudaSuccess && b == 0 && weights_out)
+                e = cudaMemcpyAsync(weights_out, dw, P * sizeof(float), cudaMemcpyDeviceToHost, dl);
+            if (e != cudaSuccess || (e = cudaEventRecord(ev_dl[b & 1], dl)) != cudaSuccess)
+                return cuda_fail(ctx, e, "cube download");
+        }
+        if ((e = cudaStreamSynchronize(dl)) != cudaSuccess) return cuda_fail(ctx, e, "cube download");
+        return HCG_OK;
+    };
+    hcg_status st = run();
+    // wind down: nothing queued outlives the buffers and fields below
+    cudaStreamSynchronize(cs);
+    if (us) cudaStreamSynchronize(us);
+    if (dl) cudaStreamSynchronize(dl);
+    cudaStreamSynchronize(s);
+    for (auto &f : fb)
+        if (f) {
+            release_field(f, s);
+            delete f;
+        }
+    for (auto &x : ev)
+        if (x) cudaEventDestroy(x);
+    if (us) cudaStreamDestroy(us);
+    if (dl) cudaStreamDestroy(dl);
+    return st;
+}
+
 hcg_status hcg_tc_set_config(hcg_context *ctx, int channel_class, int config) {
     if (!ctx) return HCG_EINVAL;
     Guard g(ctx);

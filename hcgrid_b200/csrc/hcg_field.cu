@@ -603,6 +603,44 @@ cudaError_t upload_spectra(hcg_context *ctx, hcg_field *f, const float *h_in, ui
     return cudaSuccess;
 }
 
+// `nb` channel planes (host floats [nb][n] at h_planes) into f's sorted
+// spectra, in chunks of whole planes through the two staging buffers: copies
+// on cs, scatters on us. A chunk's copy waits until the scatter that last read
+// its staging buffer is done (ev_free), the scatter for its copy (ev_copied);
+// `chunks` counts the chunks of every call that shares the staging buffers.
+cudaError_t upload_plane_block(hcg_context *ctx, hcg_field *f, const float *h_planes, uint32_t nb, cudaStream_t cs,
+                               cudaStream_t us, float *const stage[2], uint64_t stage_bytes,
+                               cudaEvent_t ev_copied[2], cudaEvent_t ev_free[2], uint64_t &chunks) {
+    const uint32_t cstride = (nb + 3) & ~3u;
+    const uint64_t n = f->n;
+    cudaError_t e = cudaSuccess;
+    if (f->d_spec && f->cstride != cstride) {
+        cudaFreeAsync(f->d_spec, us);
+        f->d_spec = nullptr;
+    }
+    if (!f->d_spec && (e = dalloc(&f->d_spec, n * cstride * sizeof(float), us, ctx->pool)) != cudaSuccess) return e;
+    f->nchan = nb;
+    f->cstride = cstride;
+    if (n == 0) return cudaSuccess;
+    const uint64_t per = std::max<uint64_t>(1, stage_bytes / (n * 4));
+    for (uint64_t u0 = 0; u0 < nb; u0 += per, ++chunks) {
+        const uint64_t cnt = std::min<uint64_t>(per, nb - u0);
+        const int b = (int)(chunks & 1);
+        if (chunks >= 2 && (e = cudaStreamWaitEvent(cs, ev_free[b], 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(stage[b], h_planes + u0 * n, cnt * n * 4, cudaMemcpyHostToDevice, cs)) != cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(ev_copied[b], cs)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(us, ev_copied[b], 0)) != cudaSuccess) return e;
+        const uint32_t c0 = (uint32_t)u0, c1 = (uint32_t)(u0 + cnt);
+        const uint32_t cend = c1 == nb ? cstride : c1;  // the last chunk writes the padding
+        dim3 grid((unsigned)((n + 31) / 32), (cend - c0 + 31) / 32);
+        k_scatter_cols<<<grid, dim3(32, 8), 0, us>>>(n, c0, c1, cend, cstride, f->d_inv, stage[b], f->d_spec);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ev_free[b], us)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, uint32_t nchan, int layout) {
     cudaStream_t s = ctx->stream;
     uint32_t cstride = (nchan + 3) & ~3u;

@@ -225,7 +225,14 @@ cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, u
 // Spectra from host memory in chunks, each scattered into sorted order while
 // the next is copied (needs ctx->copy_stream).
 constexpr uint64_t kUploadChunk = 256ull << 20;
+constexpr uint32_t kPlaneBlock = 128;  // hcg_grid_planes' default block of channels
 cudaError_t upload_spectra(hcg_context *ctx, hcg_field *f, const float *h_in, uint32_t nchan, int layout);
+// Channel planes [nb][n] from host memory into a field's sorted spectra
+// (hcg_grid_planes): copies on cs, scatters on us, staging buffers shared
+// across calls through ev_copied / ev_free and the running chunk count.
+cudaError_t upload_plane_block(hcg_context *ctx, hcg_field *f, const float *h_planes, uint32_t nb, cudaStream_t cs,
+                               cudaStream_t us, float *const stage[2], uint64_t stage_bytes,
+                               cudaEvent_t ev_copied[2], cudaEvent_t ev_free[2], uint64_t &chunks);
 // Coarsening (hcg_set_coarsening_factor): each pixel takes the window fields
 // of the first pixel of its run of `factor` along its row.
 cudaError_t coarsen_prep(PixPrep *prep, uint32_t nx, uint64_t npix, uint32_t factor, cudaStream_t s);

@@ -253,6 +253,24 @@ hcg_status hcg_target_destroy(hcg_target *t);
  * weights_out live. */
 hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *target, float *cube, int layout,
                     float *weights_out, int mem, int engine);
+/* Host spectra in, host cube out, as one pipelined call: `planes` holds the
+ * spectra as channel planes in input sample order, [nchan][n] floats (the
+ * reference's h_data[channel][sample]); `geometry` is a field of the same n
+ * samples from hcg_field_create (its own spectra, if any, are not used).
+ * The channels go through in blocks of `block` (a multiple of 64; 0: 128):
+ * while block b is split and gridded, block b + 1 is uploaded and block b - 1
+ * downloaded, the two copies on their own streams in the two directions of
+ * the bus. cube: [nchan][npix] (HCG_LAYOUT_CHANNEL_MAJOR) or [npix][nchan];
+ * weights_out optional, [npix]. planes, cube and weights_out are host memory,
+ * page-locked for the copies to overlap. engine: HCG_ENGINE_FP32 or a
+ * tensor-core engine (each block is split for it; AUTO: FP16 hi/lo); the
+ * results equal hcg_grid's on the same spectra channel for channel. The
+ * statistics (hcg_get_stats) are the last block's. Counterpart: the
+ * reference's per-channel streams, each uploading its channel, gridding it
+ * and downloading its plane (HCGrid+/gridding-omp.cu:616-626). */
+hcg_status hcg_grid_planes(hcg_context *ctx, const hcg_field *geometry, const hcg_target *target,
+                           const float *planes, uint32_t nchan, float *cube, int layout, float *weights_out,
+                           int engine, uint32_t block);
 hcg_status hcg_get_stats(hcg_context *ctx, hcg_stats *out);
 
 /* One job of a batch: a field (with spectra), a target and DEVICE output
