@@ -83,7 +83,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--plane-block", type=int, default=0,
                     help="end to end: channels per block of hcg_grid_planes (a multiple of 64; 0: the "
-                         "library's 128)")
+                         "library's 64)")
     ap.add_argument("--shard", default="bands", choices=["bands", "replicas"],
                     help="N>1: split the one job into Dec bands of target rows, one per rank, gathered to rank 0 "
                          "over NCCL (strong scaling), or grid a replica of the whole job on every rank (weak)")
@@ -1090,7 +1090,7 @@ def main():
     e2e = None
     if args.e2e_steps > 0:
         if bands:
-            lon_h, lat_h = np.ascontiguousarray(job.lon[band_idx]), np.ascontiguousarray(job.lat[band_idx])
+            lon_h, lat_h = job.lon[band_idx], job.lat[band_idx]
             _, _, hx, hy = api.header_coords(job.header)
             bx = np.ascontiguousarray(hx[bands[rank][0] * job.nx:bands[rank][1] * job.nx])
             by = np.ascontiguousarray(hy[bands[rank][0] * job.nx:bands[rank][1] * job.nx])
@@ -1098,10 +1098,13 @@ def main():
             def make_target():
                 return ctx.target(job.nx, bands[rank][1] - bands[rank][0], bx, by)
         else:
-            lon_h, lat_h = np.ascontiguousarray(job.lon), np.ascontiguousarray(job.lat)
+            lon_h, lat_h = job.lon, job.lat
 
             def make_target():
                 return ctx.target_from_header(job.header)
+        # sample positions in pinned host memory too
+        lon_h = torch.from_numpy(np.ascontiguousarray(lon_h)).pin_memory()
+        lat_h = torch.from_numpy(np.ascontiguousarray(lat_h)).pin_memory()
         cube_h = torch.empty((job.nchan, P) if LAY == api.CHANNEL_MAJOR else (P, job.nchan), dtype=torch.float32,
                              pin_memory=True)
         w_h = torch.empty(P, dtype=torch.float32, pin_memory=True)
@@ -1162,7 +1165,7 @@ def main():
                "calls_s_timed_steps": steps_calls, "device_free_gb_after_step": free_gb,
                "path": "hcg_field_create (sort) + hcg_target_from_header + hcg_grid_planes (channel planes in "
                        "pinned host memory, %d-channel blocks: upload, split, gridding and cube download "
-                       "overlapped)" % (args.plane_block or 128),
+                       "overlapped)" % (args.plane_block or 64),
                "calls_s_timed_steps_what": "[hcg_field_create, hcg_target_from_header + hcg_grid_planes]",
                "per_call_path": {"s": per_call_s, "calls_s": calls,
                                  "path": "hcg_field_create + hcg_field_set_spectra (sample rows)%s + "

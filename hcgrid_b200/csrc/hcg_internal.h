@@ -225,7 +225,7 @@ cudaError_t permute_spectra(hcg_context *ctx, hcg_field *f, const float *d_in, u
 // Spectra from host memory in chunks, each scattered into sorted order while
 // the next is copied (needs ctx->copy_stream).
 constexpr uint64_t kUploadChunk = 256ull << 20;
-constexpr uint32_t kPlaneBlock = 128;  // hcg_grid_planes' default block of channels
+constexpr uint32_t kPlaneBlock = 64;  // hcg_grid_planes' default block of channels
 cudaError_t upload_spectra(hcg_context *ctx, hcg_field *f, const float *h_in, uint32_t nchan, int layout);
 // Channel planes [nb][n] from host memory into a field's sorted spectra
 // (hcg_grid_planes): copies on cs, scatters on us, staging buffers shared

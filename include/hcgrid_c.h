@@ -257,7 +257,7 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
  * spectra as channel planes in input sample order, [nchan][n] floats (the
  * reference's h_data[channel][sample]); `geometry` is a field of the same n
  * samples from hcg_field_create (its own spectra, if any, are not used).
- * The channels go through in blocks of `block` (a multiple of 64; 0: 128):
+ * The channels go through in blocks of `block` (a multiple of 64; 0: 64):
  * while block b is split and gridded, block b + 1 is uploaded and block b - 1
  * downloaded, the two copies on their own streams in the two directions of
  * the bus. cube: [nchan][npix] (HCG_LAYOUT_CHANNEL_MAJOR) or [npix][nchan];
