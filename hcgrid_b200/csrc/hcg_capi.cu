@@ -695,8 +695,10 @@ hcg_status hcg_grid_planes(hcg_context *ctx, const hcg_field *geometry, const hc
         }
         if (weights_out) dw = (float *)ctx->scratch.get(24, P * sizeof(float), s, e);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "plane pipeline buffers");
-        if ((e = cudaEventRecord(ev_ready, s)) != cudaSuccess || (e = cudaStreamWaitEvent(cs, ev_ready, 0)) ||
-            (e = cudaStreamWaitEvent(us, ev_ready, 0)) || (e = cudaStreamWaitEvent(dl, ev_ready, 0)))
+        if ((e = cudaEventRecord(ev_ready, s)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(cs, ev_ready, 0)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(us, ev_ready, 0)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(dl, ev_ready, 0)) != cudaSuccess)
             return cuda_fail(ctx, e, where);
         for (int b = 0; b < 2 && b < (int)nblk; ++b) {
             fb[b] = new (std::nothrow) hcg_field(*geometry);
@@ -737,7 +739,8 @@ hcg_status hcg_grid_planes(hcg_context *ctx, const hcg_field *geometry, const hc
             free_split(f, s);
             if (f->d_spec) cudaFreeAsync(f->d_spec, s);
             f->d_spec = nullptr;
-            if ((e = cudaEventRecord(ev_grid, s)) != cudaSuccess || (e = cudaStreamWaitEvent(dl, ev_grid, 0)))
+            if ((e = cudaEventRecord(ev_grid, s)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(dl, ev_grid, 0)) != cudaSuccess)
                 return cuda_fail(ctx, e, where);
             if (layout == HCG_LAYOUT_CHANNEL_MAJOR)
                 e = cudaMemcpyAsync(cube + (size_t)c0 * P, dcube[b & 1], (size_t)nb * P * sizeof(float),
