@@ -98,6 +98,9 @@ def parse():
     ap.add_argument("--tc-prefetch", type=int, default=-1, help="with --tc-config: prefetch distance (chunks)")
     ap.add_argument("--tc-strip", type=int, default=-1, help="with --tc-config: persistent tile walk strip width")
     ap.add_argument("--tune-reps", type=int, default=3, help="timed runs per autotuner setting")
+    ap.add_argument("--batch-shape", type=int, default=None, choices=[0, 1, 2, 3],
+                    help="config4: the batch pass's tensor-core shape for every channel class (default: "
+                         "hcg_autotune_batch on the first window)")
     ap.add_argument("--tc-config", type=int, default=None,
                     help="tensor-core pipeline shape (0: 256 ch x 64-sample chunks x 2 stages, 1: 128 x 64 x 3, "
                          "2: 64 x 64 x 4, 3: 256 x 32 x 4, 4/5: 0/3 persistent); "
@@ -749,6 +752,10 @@ def config4_run(args):
         for win in windows:
             staged = run.stage(win, tc=True)
             jobs = [(s.field, s.target, s.cube, s.weights, api.SAMPLE_MAJOR) for s in staged]
+            if tuning is None and args.batch_shape is not None:
+                ctx.batch_set_shape(args.batch_shape)
+                ctx.grid_batch(jobs)  # untimed: the batch graphs are captured
+                tuning = [{"shape": args.batch_shape, "how": "fixed by --batch-shape for every class"}]
             if tuning is None:  # untimed: the batch graphs are captured and the batch autotuner picks
                 # a tensor-core shape per channel class on the first window's blocks
                 tuning = ctx.autotune_batch(jobs, reps=args.tune_reps)
