@@ -263,8 +263,11 @@ hcg_status hcg_grid(hcg_context *ctx, const hcg_field *field, const hcg_target *
  * the bus. cube: [nchan][npix] (HCG_LAYOUT_CHANNEL_MAJOR) or [npix][nchan];
  * weights_out optional, [npix]. planes, cube and weights_out are host memory,
  * page-locked for the copies to overlap. engine: HCG_ENGINE_FP32 or a
- * tensor-core engine (each block is split for it; AUTO: FP16 hi/lo); the
- * results equal hcg_grid's on the same spectra channel for channel. The
+ * tensor-core engine (each block is split for it; AUTO: FP16 hi/lo). The
+ * FP32 engine's cube equals hcg_grid's bit for bit; the tensor cores run
+ * the pipeline shape of each block's channel count, which agrees with
+ * hcg_grid's to the FP32 accumulation's rounding; a block of one channel
+ * takes the single-channel FP64 path, as a one-channel field does. The
  * statistics (hcg_get_stats) are the last block's. Counterpart: the
  * reference's per-channel streams, each uploading its channel, gridding it
  * and downloading its plane (HCGrid+/gridding-omp.cu:616-626). */
