@@ -72,6 +72,8 @@ def test_status_strings_and_no_device_errors():
     assert st == 4  # HCG_EDEVICE: no such device, no exit()
     assert L.hcg_grid(None, None, None, None, 0, None, 0, 0) == 1  # HCG_EINVAL
     assert L.hcg_field_band_samples(None, None, None, 0, 0, None, None) == 1
+    assert L.hcg_grid_planes(None, None, None, None, 0, None, 1, None, 0, 0) == 1
+    assert L.hcg_autotune_layout(None, 0) == 1
 
 
 def _reference_header(path):
